@@ -1,0 +1,165 @@
+/*
+ * oracle_b200.h — C ABI of the B200 (sm_100a) LH82 anelastic dynamical-core step.
+ *
+ * The reference (justingwatford-dev/Oraclev8) is a Python/NumPy code whose
+ * array seam is oracle_v8/backend.py; this library is the compiled engine a
+ * backend shim binds with ctypes.  Every entry point below names the reference
+ * function whose semantics it implements (path:line inside the reference).
+ *
+ * Conventions
+ *  - State fields are C-order (nx, ny, nz) with z contiguous; w is
+ *    (nx, ny, nz+1) with index 0 the surface and nz the lid
+ *    (oracle_v8/solver/tendency.py:119-172).
+ *  - Field pointers are DEVICE pointers owned by the caller (e.g. torch
+ *    tensors); the library borrows them for the duration of a call and never
+ *    frees them.  Their element type is double for OB_PREC_F64 plans and
+ *    float for OB_PREC_F32 plans.
+ *  - Plan-owned scratch (spectral buffers, stage buffers, constants) is
+ *    allocated once in oracle_b200_plan_create and released by
+ *    oracle_b200_plan_destroy.
+ *  - All work is enqueued on the caller's stream; nothing synchronises except
+ *    oracle_b200_read_diag.
+ *  - Every function returns an OB_* status; oracle_b200_last_error() gives the
+ *    message of the last failure on the calling thread.  The Python layer maps
+ *    OB_ERR_ARG to ValueError and the others to RuntimeError, matching the
+ *    reference's exception types (tendency.py:539-545, operator_config.py:126-138).
+ */
+#ifndef ORACLE_B200_H
+#define ORACLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OB_OK 0
+#define OB_ERR_ARG 1       /* bad argument / shape contract */
+#define OB_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define OB_ERR_NONFINITE 3 /* non-finite value detected by a device check */
+#define OB_ERR_UNSUPPORTED 4
+
+#define OB_PREC_F64 0
+#define OB_PREC_F32 1
+
+#define OB_ADV_NONE 0
+#define OB_ADV_CENTERED2 1
+#define OB_ADV_UPWIND5H 2
+
+#define OB_COR_NONE 0
+#define OB_COR_FPLANE 1
+#define OB_COR_BETA 2
+
+/* Slow-component selection masks for oracle_b200_tendency. */
+#define OB_TEND_ADVECTION 1
+#define OB_TEND_CORIOLIS 2
+#define OB_TEND_DAMPING 4
+#define OB_TEND_HEATING 8
+
+/* Layout of the diagnostics block read by oracle_b200_read_diag
+ * (StepDiagnostics, oracle_v8/solver/integrator.py:83-132). */
+#define OB_DIAG_MAX_U 0
+#define OB_DIAG_MAX_V 1
+#define OB_DIAG_MAX_W 2
+#define OB_DIAG_MAX_TH 3
+#define OB_DIAG_PHI_MIN 4      /* min of (phi_fast - mean(phi_fast)) at k=0 */
+#define OB_DIAG_PHI_MAX 5
+#define OB_DIAG_COMPAT0 6      /* compat residual of the 3 fast-stage solves */
+#define OB_DIAG_DISC0 9        /* discrete-operator residual of the 3 stages */
+#define OB_DIAG_LAST_COMPAT 12 /* last solve's compat residual */
+#define OB_DIAG_LAST_DISC 13   /* last solve's discrete residual */
+#define OB_DIAG_COUNT 16
+
+typedef struct OracleGridDesc {
+    int nx, ny, nz;      /* even nx, ny; nz >= 3 */
+    double Lx, Ly, Lz;   /* metres */
+    int precision;       /* OB_PREC_* */
+} OracleGridDesc;
+
+/* Active components, mirroring the OperatorConfig slots
+ * (oracle_v8/solver/operator_config.py:91-105).  Host arrays are copied into
+ * plan-owned device memory at creation; the caller may free them afterwards. */
+typedef struct OracleComponentDesc {
+    int buoyancy;               /* BuoyancyComponent (tendency.py:508-552) */
+    int projection;             /* AnelasticProjection (tendency.py:677-832) */
+    int advection;              /* OB_ADV_*; AdvectionComponent (tendency.py:835-1068) */
+    int coriolis;               /* OB_COR_*; CoriolisComponent (tendency.py:1071-1256) */
+    double f0, u_env, v_env;    /* Coriolis f0 and geostrophic background */
+    const double *f_y;          /* (ny) f(y) for OB_COR_BETA (tendency.py:1168-1200) */
+    int damping;                /* HelmholtzDivergenceDampingComponent (tendency.py:1741-1845) */
+    double epsilon;
+    int heating;                /* DiabaticHeatingComponent (tendency.py:1671-1738) */
+    const double *heat_r;       /* (nx*ny) Q_max * f_r(x, y) */
+    const double *heat_z;       /* (nz) f_z(z) */
+    const double *rho0;         /* (nz) base-state density, full levels */
+    const double *theta0;       /* (nz) base-state potential temperature */
+    int poisson_diag_every;     /* ORACLE_POISSON_DIAG_EVERY (tendency.py:769-774) */
+} OracleComponentDesc;
+
+typedef struct OracleStatePtrs {
+    void *u, *v, *w, *theta_prime, *phi;
+} OracleStatePtrs;
+
+typedef struct OraclePlan OraclePlan;
+
+/* Build a plan: validates the grid, uploads constants, builds FFT and Thomas
+ * tables and allocates scratch.  Replaces the constructors of
+ * VariableCoefficientPoissonSolver (poisson.py:112-137), AnelasticProjection
+ * (tendency.py:700-715) and RK3Integrator (integrator.py:179-183). */
+int oracle_b200_plan_create(const OracleGridDesc *grid, const OracleComponentDesc *comp,
+                            OraclePlan **out);
+int oracle_b200_plan_destroy(OraclePlan *plan);
+
+/* Bytes of device scratch the plan holds. */
+size_t oracle_b200_plan_scratch_bytes(const OraclePlan *plan);
+
+/* One full WS-RK3 step with Strang-split slow terms: RK3Integrator.step
+ * (integrator.py:189-311).  `in` and `out` may alias (in-place step).
+ * want_diag != 0 computes the six StepDiagnostics reductions on the device
+ * (integrator.py:287-295); read them with oracle_b200_read_diag. */
+int oracle_b200_step(OraclePlan *plan, const OracleStatePtrs *in, const OracleStatePtrs *out,
+                     double dt, int want_diag, void *stream);
+
+/* AnelasticProjection.apply_projection (tendency.py:717-790), in place on
+ * u, v, w; phi receives the projection potential.  log_diag != 0 records the
+ * compatibility and discrete residuals of this solve. */
+int oracle_b200_project(OraclePlan *plan, void *u, void *v, void *w, void *phi,
+                        int log_diag, void *stream);
+
+/* anelastic_divergence (tendency.py:393-437): d = div(rho u). */
+int oracle_b200_divergence(OraclePlan *plan, const void *u, const void *v, const void *w,
+                           void *d, void *stream);
+
+/* _phi_gradient (tendency.py:440-500). gz has nz+1 levels, zero at the ends. */
+int oracle_b200_phi_gradient(OraclePlan *plan, const void *phi, void *gx, void *gy, void *gz,
+                             void *stream);
+
+/* VariableCoefficientPoissonSolver.solve (poisson.py:202-277). */
+int oracle_b200_poisson_solve(OraclePlan *plan, const void *d, void *phi, int log_diag,
+                              void *stream);
+
+/* VariableCoefficientPoissonSolver.apply_operator (poisson.py:139-200). */
+int oracle_b200_apply_operator(OraclePlan *plan, const void *phi, void *out, void *stream);
+
+/* BuoyancyComponent.compute_tendency (tendency.py:513-546): dw_dt, nz+1 levels. */
+int oracle_b200_buoyancy(OraclePlan *plan, const void *theta_prime, void *dw_dt, void *stream);
+
+/* Sum of the selected SLOW tendencies (OB_TEND_* mask) in OperatorConfig slot
+ * order, as _apply_slow accumulates them (integrator.py:346-357).  dt_slow is
+ * the dt the components receive (the damper divides by it).  Outputs that no
+ * selected component writes are set to zero. */
+int oracle_b200_tendency(OraclePlan *plan, int mask, const OracleStatePtrs *state,
+                         void *du, void *dv, void *dw, void *dth, double dt_slow,
+                         void *stream);
+
+/* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
+int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);
+
+const char *oracle_b200_last_error(void);
+int oracle_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORACLE_B200_H */

@@ -1,0 +1,104 @@
+"""ctypes binding of liboracle_b200.so (the C ABI in include/oracle_b200.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing, every
+entry point raises RuntimeError.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_int, c_size_t, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+OB_OK, OB_ERR_ARG, OB_ERR_CUDA, OB_ERR_NONFINITE, OB_ERR_UNSUPPORTED = 0, 1, 2, 3, 4
+OB_PREC_F64, OB_PREC_F32 = 0, 1
+OB_ADV_NONE, OB_ADV_CENTERED2, OB_ADV_UPWIND5H = 0, 1, 2
+OB_COR_NONE, OB_COR_FPLANE, OB_COR_BETA = 0, 1, 2
+OB_TEND_ADVECTION, OB_TEND_CORIOLIS, OB_TEND_DAMPING, OB_TEND_HEATING = 1, 2, 4, 8
+DIAG = dict(max_u=0, max_v=1, max_w=2, max_th=3, phi_min=4, phi_max=5, compat0=6, disc0=9,
+            last_compat=12, last_disc=13)
+DIAG_COUNT = 16
+
+LIB_PATH = Path(__file__).resolve().parent / "liboracle_b200.so"
+
+EXPORTS = (
+    "oracle_b200_plan_create", "oracle_b200_plan_destroy", "oracle_b200_plan_scratch_bytes",
+    "oracle_b200_step", "oracle_b200_project", "oracle_b200_divergence",
+    "oracle_b200_phi_gradient", "oracle_b200_poisson_solve", "oracle_b200_apply_operator",
+    "oracle_b200_buoyancy", "oracle_b200_tendency", "oracle_b200_read_diag",
+    "oracle_b200_last_error", "oracle_b200_version",
+)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int), ("Lx", c_double),
+                ("Ly", c_double), ("Lz", c_double), ("precision", c_int)]
+
+
+class ComponentDesc(ctypes.Structure):
+    _fields_ = [("buoyancy", c_int), ("projection", c_int), ("advection", c_int),
+                ("coriolis", c_int), ("f0", c_double), ("u_env", c_double),
+                ("v_env", c_double), ("f_y", POINTER(c_double)), ("damping", c_int),
+                ("epsilon", c_double), ("heating", c_int), ("heat_r", POINTER(c_double)),
+                ("heat_z", POINTER(c_double)), ("rho0", POINTER(c_double)),
+                ("theta0", POINTER(c_double)), ("poisson_diag_every", c_int)]
+
+
+class StatePtrs(ctypes.Structure):
+    _fields_ = [("u", c_void_p), ("v", c_void_p), ("w", c_void_p),
+                ("theta_prime", c_void_p), ("phi", c_void_p)]
+
+
+_lib = None
+
+
+def load(path: Path | None = None):
+    """Load the library (once).  Raises RuntimeError when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"{p.name} not found: build it with `python -m oraclev8_b200.build` "
+            "(the B200 backend has no CPU fallback)")
+    lib = ctypes.CDLL(str(p))
+    vp = c_void_p
+    sig = {
+        "oracle_b200_plan_create": ([POINTER(GridDesc), POINTER(ComponentDesc), POINTER(vp)], c_int),
+        "oracle_b200_plan_destroy": ([vp], c_int),
+        "oracle_b200_plan_scratch_bytes": ([vp], c_size_t),
+        "oracle_b200_step": ([vp, POINTER(StatePtrs), POINTER(StatePtrs), c_double, c_int, vp], c_int),
+        "oracle_b200_project": ([vp, vp, vp, vp, vp, c_int, vp], c_int),
+        "oracle_b200_divergence": ([vp, vp, vp, vp, vp, vp], c_int),
+        "oracle_b200_phi_gradient": ([vp, vp, vp, vp, vp, vp], c_int),
+        "oracle_b200_poisson_solve": ([vp, vp, vp, c_int, vp], c_int),
+        "oracle_b200_apply_operator": ([vp, vp, vp, vp], c_int),
+        "oracle_b200_buoyancy": ([vp, vp, vp, vp], c_int),
+        "oracle_b200_tendency": ([vp, c_int, POINTER(StatePtrs), vp, vp, vp, vp, c_double, vp], c_int),
+        "oracle_b200_read_diag": ([vp, POINTER(c_double), c_int, vp], c_int),
+        "oracle_b200_last_error": ([], ctypes.c_char_p),
+        "oracle_b200_version": ([], c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc == OB_OK:
+        return
+    msg = _lib.oracle_b200_last_error().decode(errors="replace") if _lib else "?"
+    if rc == OB_ERR_ARG:
+        raise ValueError(msg)
+    raise RuntimeError(f"oracle_b200 error {rc}: {msg}")
+
+
+def dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(POINTER(c_double))

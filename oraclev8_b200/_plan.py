@@ -1,0 +1,217 @@
+"""Device plan: one compiled configuration of the LH82 step on one grid.
+
+Wraps an ``OraclePlan*`` of the C ABI.  Tensors passed in must be contiguous
+CUDA tensors of the plan's dtype (float64 for "fp64", float32 for "fp32").
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+PRECISIONS = {"fp64": (L.OB_PREC_F64, torch.float64), "fp32": (L.OB_PREC_F32, torch.float32)}
+
+
+def require_cuda() -> None:
+    if not torch.cuda.is_available():
+        raise RuntimeError("the oraclev8_b200 backend needs a CUDA device (no CPU fallback)")
+
+
+@dataclass
+class PlanSpec:
+    nx: int
+    ny: int
+    nz: int
+    Lx: float
+    Ly: float
+    Lz: float
+    rho0: np.ndarray
+    theta0: np.ndarray
+    precision: str = "fp64"
+    buoyancy: bool = False
+    projection: bool = False
+    advection: int = L.OB_ADV_NONE
+    coriolis: int = L.OB_COR_NONE
+    f0: float = 0.0
+    u_env: float = 0.0
+    v_env: float = 0.0
+    f_y: Optional[np.ndarray] = None
+    damping: bool = False
+    epsilon: float = 0.0
+    heating: bool = False
+    heat_r: Optional[np.ndarray] = None
+    heat_z: Optional[np.ndarray] = None
+    poisson_diag_every: int = 60
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+class Plan:
+    def __init__(self, spec: PlanSpec):
+        require_cuda()
+        self.lib = L.load()
+        if spec.precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {spec.precision!r}")
+        self.spec = spec
+        self.prec, self.dtype = PRECISIONS[spec.precision]
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        g = L.GridDesc(spec.nx, spec.ny, spec.nz, spec.Lx, spec.Ly, spec.Lz, self.prec)
+        keep = [_f64(spec.rho0), _f64(spec.theta0), _f64(spec.f_y), _f64(spec.heat_r),
+                _f64(spec.heat_z)]
+        rho0, theta0, f_y, heat_r, heat_z = keep
+        if rho0.shape != (spec.nz,) or theta0.shape != (spec.nz,):
+            raise ValueError(f"rho0/theta0 must have shape ({spec.nz},)")
+        c = L.ComponentDesc(int(spec.buoyancy), int(spec.projection), int(spec.advection),
+                            int(spec.coriolis), float(spec.f0), float(spec.u_env),
+                            float(spec.v_env), L.dptr(f_y), int(spec.damping),
+                            float(spec.epsilon), int(spec.heating), L.dptr(heat_r),
+                            L.dptr(heat_z), L.dptr(rho0), L.dptr(theta0),
+                            int(spec.poisson_diag_every))
+        h = ctypes.c_void_p()
+        L.check(self.lib.oracle_b200_plan_create(ctypes.byref(g), ctypes.byref(c), ctypes.byref(h)))
+        self.handle = h
+        self.shape = (spec.nx, spec.ny, spec.nz)
+        self.wshape = (spec.nx, spec.ny, spec.nz + 1)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.oracle_b200_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    # -- helpers -------------------------------------------------------------
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self.lib.oracle_b200_plan_scratch_bytes(self.handle))
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _ptr(self, t: torch.Tensor, shape) -> ctypes.c_void_p:
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"expected a CUDA torch.Tensor, got {type(t).__name__}")
+        if t.device.type != "cuda" or t.dtype != self.dtype or not t.is_contiguous():
+            raise ValueError(f"expected a contiguous {self.dtype} CUDA tensor, got "
+                             f"{t.dtype} on {t.device} (contiguous={t.is_contiguous()})")
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"shape {tuple(t.shape)} does not match expected {tuple(shape)}")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def state_ptrs(self, u, v, w, th, phi) -> L.StatePtrs:
+        s, ws = self.shape, self.wshape
+        return L.StatePtrs(self._ptr(u, s), self._ptr(v, s), self._ptr(w, ws),
+                           self._ptr(th, s), self._ptr(phi, s))
+
+    def empty(self, wlevels=False):
+        return torch.empty(self.wshape if wlevels else self.shape, dtype=self.dtype,
+                           device=self.device)
+
+    # -- entry points ----------------------------------------------------------
+    def step(self, ins: L.StatePtrs, outs: L.StatePtrs, dt: float, want_diag: bool):
+        L.check(self.lib.oracle_b200_step(self.handle, ctypes.byref(ins), ctypes.byref(outs),
+                                          float(dt), int(want_diag), self._stream()))
+
+    def read_diag(self) -> np.ndarray:
+        buf = (ctypes.c_double * L.DIAG_COUNT)()
+        L.check(self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream()))
+        return np.frombuffer(buf, dtype=np.float64).copy()
+
+    def project(self, u, v, w, phi, log_diag=False):
+        s = self.shape
+        L.check(self.lib.oracle_b200_project(self.handle, self._ptr(u, s), self._ptr(v, s),
+                                             self._ptr(w, self.wshape), self._ptr(phi, s),
+                                             int(log_diag), self._stream()))
+
+    def divergence(self, u, v, w, out=None):
+        out = self.empty() if out is None else out
+        s = self.shape
+        L.check(self.lib.oracle_b200_divergence(self.handle, self._ptr(u, s), self._ptr(v, s),
+                                                self._ptr(w, self.wshape), self._ptr(out, s),
+                                                self._stream()))
+        return out
+
+    def phi_gradient(self, phi):
+        gx, gy, gz = self.empty(), self.empty(), self.empty(True)
+        s = self.shape
+        L.check(self.lib.oracle_b200_phi_gradient(self.handle, self._ptr(phi, s),
+                                                  self._ptr(gx, s), self._ptr(gy, s),
+                                                  self._ptr(gz, self.wshape), self._stream()))
+        return gx, gy, gz
+
+    def poisson_solve(self, d, log_diag=False):
+        phi = self.empty()
+        s = self.shape
+        L.check(self.lib.oracle_b200_poisson_solve(self.handle, self._ptr(d, s),
+                                                   self._ptr(phi, s), int(log_diag),
+                                                   self._stream()))
+        return phi
+
+    def apply_operator(self, phi):
+        out = self.empty()
+        s = self.shape
+        L.check(self.lib.oracle_b200_apply_operator(self.handle, self._ptr(phi, s),
+                                                    self._ptr(out, s), self._stream()))
+        return out
+
+    def buoyancy(self, th):
+        dw = self.empty(True)
+        L.check(self.lib.oracle_b200_buoyancy(self.handle, self._ptr(th, self.shape),
+                                              self._ptr(dw, self.wshape), self._stream()))
+        return dw
+
+    def tendency(self, mask, u, v, w, th, dt_slow):
+        du, dv, dw, dth = self.empty(), self.empty(), self.empty(True), self.empty()
+        phi_dummy = th  # the tendency entry point does not read phi
+        sp = self.state_ptrs(u, v, w, th, phi_dummy)
+        s = self.shape
+        L.check(self.lib.oracle_b200_tendency(self.handle, int(mask), ctypes.byref(sp),
+                                              self._ptr(du, s), self._ptr(dv, s),
+                                              self._ptr(dw, self.wshape), self._ptr(dth, s),
+                                              float(dt_slow), self._stream()))
+        return du, dv, dw, dth
+
+
+# ---------------------------------------------------------------------------
+# Small cache of operator plans (component-level calls and module functions)
+# ---------------------------------------------------------------------------
+_CACHE: "dict[tuple, Plan]" = {}
+_CACHE_MAX = 8
+
+
+def _key(spec: PlanSpec) -> tuple:
+    def b(a):
+        return None if a is None else np.asarray(a, dtype=np.float64).tobytes()
+    return (spec.nx, spec.ny, spec.nz, float(spec.Lx), float(spec.Ly), float(spec.Lz),
+            spec.precision, b(spec.rho0), b(spec.theta0), spec.buoyancy, spec.projection,
+            spec.advection, spec.coriolis, float(spec.f0), float(spec.u_env),
+            float(spec.v_env), b(spec.f_y), spec.damping, float(spec.epsilon), spec.heating,
+            b(spec.heat_r), b(spec.heat_z), spec.poisson_diag_every)
+
+
+def cached_plan(spec: PlanSpec) -> Plan:
+    k = _key(spec)
+    p = _CACHE.get(k)
+    if p is None:
+        if len(_CACHE) >= _CACHE_MAX:
+            _CACHE.pop(next(iter(_CACHE)))
+        p = Plan(spec)
+        _CACHE[k] = p
+    return p
+
+
+def precision_of(t: torch.Tensor) -> str:
+    if t.dtype == torch.float64:
+        return "fp64"
+    if t.dtype == torch.float32:
+        return "fp32"
+    raise ValueError(f"unsupported dtype {t.dtype}; use float64 or float32")

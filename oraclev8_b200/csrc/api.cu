@@ -1,0 +1,863 @@
+// C ABI of the B200 LH82 step library.  See include/oracle_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/oracle_b200.h"
+#include "kernels.cuh"
+
+using namespace ob;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define OB_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(OB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                  __FILE__, __LINE__);                                                   \
+  } while (0)
+
+#define OB_LAUNCHED()                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = cudaGetLastError();                                                 \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(OB_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                   \
+  } while (0)
+
+constexpr int kThomasCols = 32;
+constexpr int kFftThreads = 256;
+constexpr size_t kSmemBudget = 112 * 1024;  // two CTAs per SM
+constexpr size_t kSmemMax = 227 * 1024;
+
+bool factorize(int M, FftPlan& p) {
+  p.M = M;
+  p.np = 0;
+  int m = M;
+  while (m > 1 && m % 4 == 0) {
+    p.r[p.np++] = 4;
+    m /= 4;
+  }
+  const int rs[3] = {2, 3, 5};
+  for (int r : rs)
+    while (m % r == 0 && m > 1) {
+      if (p.np >= 20) return false;
+      p.r[p.np++] = r;
+      m /= r;
+    }
+  return m == 1;
+}
+
+// 2 pi fftfreq(n, d=L/n), with NumPy's operation order (numpy/fft/_helper.py).
+std::vector<double> wavenumbers(int n, double L) {
+  const double d = L / n;
+  const double val = 1.0 / ((double)n * d);
+  const int N = (n - 1) / 2 + 1;
+  std::vector<double> k(n);
+  for (int i = 0; i < n; ++i) {
+    const long si = (i < N) ? i : (long)i - n;
+    k[i] = (2.0 * M_PI) * ((double)si * val);
+  }
+  return k;
+}
+
+template <class T>
+std::vector<cplx<T>> twiddles(int N) {
+  std::vector<cplx<T>> tw(N);
+  for (int t = 0; t < N; ++t) {
+    const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)t /
+                          (long double)N;
+    tw[t].x = (T)cosl(a);
+    tw[t].y = (T)sinl(a);
+  }
+  return tw;
+}
+
+}  // namespace
+
+struct OraclePlan {
+  int prec = 0;
+  GridK g{};
+  int buoyancy = 0, projection = 0, advection = 0, coriolis = 0, damping = 0, heating = 0;
+  double f0 = 0, u_env = 0, v_env = 0, epsilon = 0;
+  int diag_every = 60;
+  long solve_count = 0;
+  FftPlan px{}, py{};
+  int zc_fx = 1, zc_fy = 1, zc_iy = 1, zc_ix = 1;
+  size_t esz = 8;  // element size of T
+  // device constants
+  double *kx = nullptr, *ky = nullptr, *rho = nullptr, *rhoh = nullptr, *theta0 = nullptr;
+  double *dth0 = nullptr, *fy = nullptr, *heat_r = nullptr, *heat_z = nullptr;
+  double *ta = nullptr, *tc = nullptr, *tnegs = nullptr, *ta0 = nullptr, *tcp0 = nullptr,
+         *tinv0 = nullptr;
+  void *twx = nullptr, *twy = nullptr;
+  // scratch
+  void *S1 = nullptr, *S2 = nullptr, *S3 = nullptr;           // spectral
+  void *Au = nullptr, *Av = nullptr, *Aw = nullptr, *Ath = nullptr, *Aphi = nullptr;
+  void *Su = nullptr, *Sv = nullptr, *Sw = nullptr, *Sphi = nullptr;
+  void *Du = nullptr, *Dv = nullptr;                         // damper / temp
+  double* diag = nullptr;
+  DiagPart* parts = nullptr;
+  int nparts = 0;
+  std::vector<void*> allocs;
+  size_t scratch_bytes = 0;
+};
+
+namespace {
+
+template <class P>
+int dalloc(OraclePlan* p, P** out, size_t bytes) {
+  void* q = nullptr;
+  OB_CUDA(cudaMalloc(&q, bytes));
+  p->allocs.push_back(q);
+  p->scratch_bytes += bytes;
+  *out = reinterpret_cast<P*>(q);
+  return OB_OK;
+}
+
+int upload(OraclePlan* p, double** out, const double* host, size_t n) {
+  int rc = dalloc(p, out, n * sizeof(double));
+  if (rc) return rc;
+  OB_CUDA(cudaMemcpy(*out, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  return OB_OK;
+}
+
+int pick_zc(int nz, size_t per_zc, size_t fixed) {
+  int best = 1;
+  for (int zc : {16, 8, 4, 2, 1}) {
+    if (zc > nz && zc > 1) continue;
+    if (fixed + per_zc * (size_t)zc <= kSmemBudget) {
+      best = zc;
+      break;
+    }
+  }
+  return best;
+}
+
+size_t smem_fx(const OraclePlan* p, int nf) {
+  return 2ull * (p->g.M + 1) * nf * p->zc_fx * 2 * p->esz;
+}
+size_t smem_fy(const OraclePlan* p, int nf, int zc) { return 2ull * p->g.ny * nf * zc * 2 * p->esz; }
+size_t smem_ix(const OraclePlan* p, int B) { return (size_t)(2 * p->g.M + 1) * B * 2 * p->esz; }
+size_t smem_thomas(const OraclePlan* p) { return 3ull * kThomasCols * (p->g.nz + 1) * 8; }
+
+template <class T>
+int set_smem_attrs() {
+  const int mx = (int)kSmemMax;
+  OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_DIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_DIV_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fy<T, FY_DIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fy<T, FY_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fy<T, FY_HELM>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_iy<T, IY_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_iy<T, IY_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_CORRECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_thomas<T, kThomasCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  return OB_OK;
+}
+
+ThomasK thomas_args(const OraclePlan* p) {
+  ThomasK t;
+  t.a = p->ta;
+  t.c = p->tc;
+  t.negs = p->tnegs;
+  t.rho = p->rho;
+  t.rhoh = p->rhoh;
+  t.kx = p->kx;
+  t.ky = p->ky;
+  t.a0 = p->ta0;
+  t.cp0 = p->tcp0;
+  t.inv0 = p->tinv0;
+  t.dz = p->g.dz;
+  t.scale = 1.0 / ((double)p->g.nx * (double)p->g.ny);
+  return t;
+}
+
+dim3 grid_x(const OraclePlan* p, int zc) { return dim3(p->g.ny, (p->g.nz + zc - 1) / zc); }
+dim3 grid_y(const OraclePlan* p, int zc) { return dim3(p->g.nxh, (p->g.nz + zc - 1) / zc); }
+
+// ---- projection pipeline -------------------------------------------------
+// stage_sdt < 0: in-place projection of (u, v, w) with phi output.
+// stage_sdt >= 0: inputs are the anchor state (u, v, w, th); the provisional
+// stage state w + sdt * b_half is formed on the fly and the projected result
+// goes to (uo, vo, wo, phio).
+template <class T>
+int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
+                 double stage_sdt, T* uo, T* vo, T* wo, T* phio, int slot_c, int slot_d,
+                 cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  C* S3 = (C*)p->S3;
+  p->solve_count += 1;
+  const int de = p->diag_every < 1 ? 1 : p->diag_every;
+  const bool log = (de == 1) || (p->solve_count % de == 1);
+  double* diag = nullptr;
+  if (log) {
+    diag = p->diag;
+    OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
+  } else {
+    OB_CUDA(cudaMemsetAsync(p->diag + slot_c, 0, sizeof(double), st));
+    OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
+  }
+  const bool stage = stage_sdt >= 0.0;
+  if (stage)
+    k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+        g, p->px, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2, nullptr);
+  else
+    k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+        g, p->px, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2, nullptr);
+  OB_LAUNCHED();
+  k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr);
+  OB_LAUNCHED();
+  const long ncols = (long)g.nxh * g.ny;
+  k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
+                                                   slot_d);
+  OB_LAUNCHED();
+  k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2);
+  OB_LAUNCHED();
+  const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
+  if (stage)
+    k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th,
+        stage_sdt, p->theta0, uo, vo, wo, phio);
+  else
+    k_ix<T, IX_CORRECT><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th, 0.0,
+        p->theta0, uo, vo, wo, phio);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// Helmholtz divergence damping tendency (tendency.py:1800-1839) into Du, Dv.
+template <class T>
+int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
+      g, p->px, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+      (const C*)p->twx, S1, S2, nullptr);
+  OB_LAUNCHED();
+  const double scale = -(p->epsilon / dt_slow) / ((double)g.nx * (double)g.ny);
+  k_fy<T, FY_HELM><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2);
+  OB_LAUNCHED();
+  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2);
+  OB_LAUNCHED();
+  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+      g, p->px, p->zc_ix, 2, S1, S2, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
+      nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+SlowK slow_args(const OraclePlan* p) {
+  SlowK s;
+  s.adv = p->advection;
+  s.cor = p->coriolis;
+  s.heat = p->heating;
+  s.damp = p->damping;
+  s.f0 = p->f0;
+  s.u_env = p->u_env;
+  s.v_env = p->v_env;
+  s.fy = p->fy;
+  s.dth0 = p->dth0;
+  s.heat_r = p->heat_r;
+  s.heat_z = p->heat_z;
+  s.inv2dx = 1.0 / (2.0 * p->g.dx);
+  s.inv2dy = 1.0 / (2.0 * p->g.dy);
+  s.inv60dx = 1.0 / (60.0 * p->g.dx);
+  s.inv60dy = 1.0 / (60.0 * p->g.dy);
+  s.inv2dz = 1.0 / (2.0 * p->g.dz);
+  s.invdz = 1.0 / p->g.dz;
+  return s;
+}
+
+template <class T, int OUT>
+int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const T* w,
+              const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
+  dim3 blk(32, 8);
+  dim3 grd((p->g.ny + 7) / 8, p->g.nx);
+  k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                      (const T*)p->Dv, uo, vo, wo, tho);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+template <class T>
+int copy_field(void* dst, const void* src, size_t n, cudaStream_t st) {
+  if (dst == src) return OB_OK;
+  OB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  return OB_OK;
+}
+
+template <class T>
+int diag_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th, const T* phi,
+              cudaStream_t st) {
+  k_diag_partial<T><<<p->nparts, 256, 0, st>>>(p->g, u, v, w, th, phi, p->parts);
+  OB_LAUNCHED();
+  k_diag_final<<<1, 32, 0, st>>>(p->parts, p->nparts,
+                                 (double)p->g.nx * p->g.ny * p->g.nz, p->diag);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+#define RC(x)            \
+  do {                   \
+    int rc_ = (x);       \
+    if (rc_) return rc_; \
+  } while (0)
+
+template <class T>
+int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* out, double dt,
+              int want_diag, cudaStream_t st) {
+  const size_t n = (size_t)p->g.nx * p->g.ny * p->g.nz;
+  const size_t nw = (size_t)p->g.nx * p->g.ny * (p->g.nz + 1);
+  const double dts = dt * 0.5;
+  const bool slow = p->advection || p->coriolis || p->damping || p->heating;
+  const bool mom = p->advection || p->coriolis || p->damping;
+  const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_DAMPING | OB_TEND_HEATING;
+  // anchor state y^n after the first slow half step
+  const T *au = (const T*)in->u, *av = (const T*)in->v, *aw = (const T*)in->w,
+          *ath = (const T*)in->theta_prime, *aphi = (const T*)in->phi;
+  if (slow) {
+    if (p->damping) RC(damper_impl<T>(p, (const T*)in->u, (const T*)in->v, dts, st));
+    RC((slow_impl<T, 0>(p, all, dts, (const T*)in->u, (const T*)in->v, (const T*)in->w,
+                        (const T*)in->theta_prime, (T*)p->Au, (T*)p->Av, (T*)p->Aw,
+                        (T*)p->Ath, st)));
+    if (mom && p->projection)
+      RC(project_impl<T>(p, (T*)p->Au, (T*)p->Av, (T*)p->Aw, nullptr, -1.0, (T*)p->Au,
+                         (T*)p->Av, (T*)p->Aw, (T*)p->Aphi, OB_DIAG_LAST_COMPAT,
+                         OB_DIAG_LAST_DISC, st));
+    else
+      RC(copy_field<T>(p->Aphi, in->phi, n, st));
+    au = (const T*)p->Au;
+    av = (const T*)p->Av;
+    aw = (const T*)p->Aw;
+    ath = (const T*)p->Ath;
+    aphi = (const T*)p->Aphi;
+  }
+  // fast stages (integrator.py:232-258)
+  const T *su = au, *sv = av, *sw = aw, *sphi = aphi;
+  if (p->buoyancy && p->projection) {
+    const double alphas[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
+    for (int s = 0; s < 3; ++s) {
+      const double sdt = alphas[s] * dt;
+      RC(project_impl<T>(p, au, av, aw, ath, sdt, (T*)p->Su, (T*)p->Sv, (T*)p->Sw,
+                         (T*)p->Sphi, OB_DIAG_COMPAT0 + s, OB_DIAG_DISC0 + s, st));
+    }
+    su = (const T*)p->Su;
+    sv = (const T*)p->Sv;
+    sw = (const T*)p->Sw;
+    sphi = (const T*)p->Sphi;
+  } else if (p->buoyancy) {
+    return fail(OB_ERR_UNSUPPORTED, "buoyancy without a projection is not supported");
+  } else if (p->projection) {
+    // no fast physics: one projection of y^n (integrator.py:242-258)
+    T* tu = slow ? (T*)p->Au : (T*)p->Su;
+    T* tv = slow ? (T*)p->Av : (T*)p->Sv;
+    T* tw = slow ? (T*)p->Aw : (T*)p->Sw;
+    T* tp = slow ? (T*)p->Aphi : (T*)p->Sphi;
+    if (!slow) {
+      RC(copy_field<T>(tu, in->u, n, st));
+      RC(copy_field<T>(tv, in->v, n, st));
+      RC(copy_field<T>(tw, in->w, nw, st));
+    }
+    RC(project_impl<T>(p, tu, tv, tw, nullptr, -1.0, tu, tv, tw, tp, OB_DIAG_LAST_COMPAT,
+                       OB_DIAG_LAST_DISC, st));
+    su = tu;
+    sv = tv;
+    sw = tw;
+    sphi = tp;
+  }
+  // second slow half step (integrator.py:261-276)
+  if (slow) {
+    if (p->damping) RC(damper_impl<T>(p, su, sv, dts, st));
+    RC((slow_impl<T, 0>(p, all, dts, su, sv, sw, ath, (T*)out->u, (T*)out->v, (T*)out->w,
+                        (T*)out->theta_prime, st)));
+    if (mom && p->projection)
+      RC(project_impl<T>(p, (T*)out->u, (T*)out->v, (T*)out->w, nullptr, -1.0, (T*)out->u,
+                         (T*)out->v, (T*)out->w, (T*)out->phi, OB_DIAG_LAST_COMPAT,
+                         OB_DIAG_LAST_DISC, st));
+    else
+      RC(copy_field<T>(out->phi, sphi, n, st));
+  } else {
+    RC(copy_field<T>(out->u, su, n, st));
+    RC(copy_field<T>(out->v, sv, n, st));
+    RC(copy_field<T>(out->w, sw, nw, st));
+    RC(copy_field<T>(out->theta_prime, ath, n, st));
+    RC(copy_field<T>(out->phi, sphi, n, st));
+  }
+  if (want_diag)
+    RC(diag_impl<T>(p, (const T*)out->u, (const T*)out->v, (const T*)out->w,
+                    (const T*)out->theta_prime, sphi, st));
+  return OB_OK;
+}
+
+template <class T>
+int divergence_impl(OraclePlan* p, const T* u, const T* v, const T* w, T* d, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  C* S3 = (C*)p->S3;
+  k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+      g, p->px, p->zc_fx, 3, u, v, w, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+      (const C*)p->twx, S1, S2, nullptr);
+  OB_LAUNCHED();
+  k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr);
+  OB_LAUNCHED();
+  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 1, S3, nullptr, p->ky, (const C*)p->twy,
+      1.0 / ((double)g.nx * (double)g.ny), S1, nullptr);
+  OB_LAUNCHED();
+  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+      g, p->px, p->zc_ix, 1, S1, nullptr, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
+      nullptr, nullptr, 0.0, p->theta0, d, nullptr, nullptr, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// forward 2-D real FFT of one field into S3 (unnormalised)
+template <class T>
+int fwd_scalar(OraclePlan* p, const T* f, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
+      g, p->px, p->zc_fx, 1, f, nullptr, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0,
+      p->kx, (const C*)p->twx, (C*)p->S1, nullptr, nullptr);
+  OB_LAUNCHED();
+  k_fy<T, FY_FIELDS><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 1, (C*)p->S1, nullptr, p->kx, p->ky, (const C*)p->twy, 1.0,
+      (C*)p->S3, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// inverse 2-D real FFT of S3 (scaled) into out
+template <class T>
+int inv_scalar(OraclePlan* p, double scale, T* out, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 1, (C*)p->S3, nullptr, p->ky, (const C*)p->twy, scale, (C*)p->S1,
+      nullptr);
+  OB_LAUNCHED();
+  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+      g, p->px, p->zc_ix, 1, (C*)p->S1, nullptr, nullptr, p->kx, (const C*)p->twx, nullptr,
+      nullptr, nullptr, nullptr, 0.0, p->theta0, out, nullptr, nullptr, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+template <class T>
+int gradient_impl(OraclePlan* p, const T* phi, T* gx, T* gy, T* gz, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  RC(fwd_scalar<T>(p, phi, st));
+  k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, (C*)p->S3, nullptr, p->ky, (const C*)p->twy,
+      1.0 / ((double)g.nx * (double)g.ny), (C*)p->S1, (C*)p->S2);
+  OB_LAUNCHED();
+  k_ix<T, IX_GRAD><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
+      g, p->px, p->zc_ix, 0, (C*)p->S1, (C*)p->S2, nullptr, p->kx, (const C*)p->twx, nullptr,
+      nullptr, nullptr, nullptr, 0.0, p->theta0, gx, gy, gz, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+template <class T>
+int solve_impl(OraclePlan* p, const T* d, T* phi, int log_diag, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  RC(fwd_scalar<T>(p, d, st));
+  double* diag = nullptr;
+  if (log_diag) {
+    diag = p->diag;
+    OB_CUDA(cudaMemsetAsync(p->diag + OB_DIAG_LAST_DISC, 0, sizeof(double), st));
+  }
+  const long ncols = (long)g.nxh * g.ny;
+  k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+                             smem_thomas(p), st>>>(g, thomas_args(p), (C*)p->S3, (C*)p->S3,
+                                                   diag, OB_DIAG_LAST_COMPAT, OB_DIAG_LAST_DISC);
+  OB_LAUNCHED();
+  return inv_scalar<T>(p, 1.0, phi, st);
+}
+
+template <class T>
+int apply_op_impl(OraclePlan* p, const T* phi, T* out, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  RC(fwd_scalar<T>(p, phi, st));
+  const size_t ns = (size_t)g.nxh * g.ny * g.nz;
+  k_neg_ksq<T><<<(unsigned)std::min<size_t>((ns + 255) / 256, 65535), 256, 0, st>>>(
+      g, (C*)p->S3, p->kx, p->ky, (C*)p->S3);
+  OB_LAUNCHED();
+  RC(inv_scalar<T>(p, 1.0 / ((double)g.nx * (double)g.ny), (T*)p->Du, st));
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  k_apply_vert<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
+      g, phi, (const T*)p->Du, p->rho, p->rhoh, out);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+template <class T>
+int buoyancy_impl(OraclePlan* p, const T* th, T* dw, cudaStream_t st) {
+  const size_t n = (size_t)p->g.nx * p->g.ny * (p->g.nz + 1);
+  k_buoyancy<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
+      p->g, th, p->theta0, dw);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+template <class T>
+int tendency_impl(OraclePlan* p, int mask, const OracleStatePtrs* s, T* du, T* dv, T* dw,
+                  T* dth, double dt_slow, cudaStream_t st) {
+  if ((mask & OB_TEND_DAMPING) && p->damping)
+    RC(damper_impl<T>(p, (const T*)s->u, (const T*)s->v, dt_slow, st));
+  return slow_impl<T, 1>(p, mask, 0.0, (const T*)s->u, (const T*)s->v, (const T*)s->w,
+                         (const T*)s->theta_prime, du, dv, dw, dth, st);
+}
+
+int check_plan(const OraclePlan* p) {
+  if (!p) return fail(OB_ERR_ARG, "plan is NULL");
+  return OB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+
+extern "C" {
+
+const char* oracle_b200_last_error(void) { return g_err.c_str(); }
+
+int oracle_b200_version(void) { return 1; }
+
+size_t oracle_b200_plan_scratch_bytes(const OraclePlan* p) { return p ? p->scratch_bytes : 0; }
+
+int oracle_b200_plan_destroy(OraclePlan* p) {
+  if (!p) return OB_OK;
+  for (void* q : p->allocs) cudaFree(q);
+  delete p;
+  return OB_OK;
+}
+
+int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDesc* comp,
+                            OraclePlan** out) {
+  if (!grid || !comp || !out) return fail(OB_ERR_ARG, "NULL argument to plan_create");
+  *out = nullptr;
+  const int nx = grid->nx, ny = grid->ny, nz = grid->nz;
+  if (nx < 4 || ny < 4 || (nx & 1) || (ny & 1))
+    return fail(OB_ERR_ARG, "nx and ny must be even and >= 4 (got %d, %d)", nx, ny);
+  if (nz < 3) return fail(OB_ERR_ARG, "nz must be >= 3 (got %d)", nz);
+  if (!(grid->Lx > 0 && grid->Ly > 0 && grid->Lz > 0))
+    return fail(OB_ERR_ARG, "domain lengths must be positive");
+  if (grid->precision != OB_PREC_F64 && grid->precision != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "unknown precision %d", grid->precision);
+  if (!comp->rho0 || !comp->theta0) return fail(OB_ERR_ARG, "rho0 and theta0 are required");
+  if (comp->advection < 0 || comp->advection > 2)
+    return fail(OB_ERR_ARG, "unknown advection scheme %d", comp->advection);
+  if (comp->coriolis < 0 || comp->coriolis > 2)
+    return fail(OB_ERR_ARG, "unknown coriolis mode %d", comp->coriolis);
+  if (comp->coriolis == OB_COR_BETA && !comp->f_y)
+    return fail(OB_ERR_ARG, "beta-plane Coriolis needs f_y");
+  if (comp->heating && (!comp->heat_r || !comp->heat_z))
+    return fail(OB_ERR_ARG, "heating needs heat_r and heat_z");
+  if ((long)nx * ny * (nz + 1) > (1L << 31))
+    return fail(OB_ERR_ARG, "grid too large for 32-bit launch geometry");
+
+  OraclePlan* p = new OraclePlan();
+  auto bail = [&](int rc) {
+    oracle_b200_plan_destroy(p);
+    return rc;
+  };
+  p->prec = grid->precision;
+  p->esz = p->prec == OB_PREC_F64 ? 8 : 4;
+  p->g.nx = nx;
+  p->g.ny = ny;
+  p->g.nz = nz;
+  p->g.M = nx / 2;
+  p->g.nxh = nx / 2 + 1;
+  p->g.dx = grid->Lx / nx;
+  p->g.dy = grid->Ly / ny;
+  p->g.dz = grid->Lz / nz;
+  p->buoyancy = comp->buoyancy != 0;
+  p->projection = comp->projection != 0;
+  p->advection = comp->advection;
+  p->coriolis = comp->coriolis;
+  p->damping = comp->damping != 0;
+  p->heating = comp->heating != 0;
+  p->f0 = comp->f0;
+  p->u_env = comp->u_env;
+  p->v_env = comp->v_env;
+  p->epsilon = comp->epsilon;
+  p->diag_every = comp->poisson_diag_every;
+  if (!factorize(nx / 2, p->px) || !factorize(ny, p->py))
+    return bail(fail(OB_ERR_ARG, "nx/2=%d and ny=%d must factor into 2, 3, 5", nx / 2, ny));
+
+  const double dz = p->g.dz;
+  const double* rf = comp->rho0;
+  // rho on half levels (tendency.py:748-754)
+  std::vector<double> rh(nz + 1);
+  for (int k = 1; k < nz; ++k) rh[k] = 0.5 * (rf[k - 1] + rf[k]);
+  rh[0] = rf[0];
+  rh[nz] = rf[nz - 1];
+  // Thomas tables (poisson.py:286-325)
+  const double dz2 = dz * dz;
+  std::vector<double> rl(nz), ru(nz), a(nz), c(nz), negs(nz);
+  for (int k = 0; k < nz; ++k) {
+    rl[k] = rh[k] / dz2;
+    ru[k] = rh[k + 1] / dz2;
+  }
+  for (int k = 0; k < nz; ++k) {
+    a[k] = rl[k];
+    c[k] = ru[k];
+    negs[k] = -(rl[k] + ru[k]);
+  }
+  a[0] = 0.0;
+  c[nz - 1] = 0.0;
+  negs[0] = -ru[0];
+  negs[nz - 1] = -rl[nz - 1];
+  const int n0 = nz - 1;
+  std::vector<double> a0(n0), b0(n0), c0(n0), inv0(n0), cp0(n0);
+  for (int j = 0; j < n0; ++j) {
+    a0[j] = rl[j + 1];
+    b0[j] = -(rl[j + 1] + ru[j + 1]);
+    c0[j] = ru[j + 1];
+  }
+  a0[0] = 0.0;
+  a0[n0 - 1] = rl[nz - 1];
+  c0[n0 - 1] = 0.0;
+  b0[n0 - 1] = -rl[nz - 1];
+  inv0[0] = 1.0 / b0[0];
+  cp0[0] = c0[0] * inv0[0];
+  for (int j = 1; j < n0; ++j) {
+    const double den = b0[j] - a0[j] * cp0[j - 1];
+    inv0[j] = 1.0 / den;
+    cp0[j] = (j < n0 - 1) ? c0[j] * inv0[j] : 0.0;
+  }
+  // d theta0 / dz (tendency.py:1013-1016)
+  const double* t0 = comp->theta0;
+  std::vector<double> dth0(nz);
+  for (int k = 1; k < nz - 1; ++k) dth0[k] = (t0[k + 1] - t0[k - 1]) / (2.0 * dz);
+  dth0[0] = (t0[1] - t0[0]) / dz;
+  dth0[nz - 1] = (t0[nz - 1] - t0[nz - 2]) / dz;
+
+  std::vector<double> kx = wavenumbers(nx, grid->Lx), ky = wavenumbers(ny, grid->Ly);
+  int rc;
+  if ((rc = upload(p, &p->kx, kx.data(), nx))) return bail(rc);
+  if ((rc = upload(p, &p->ky, ky.data(), ny))) return bail(rc);
+  if ((rc = upload(p, &p->rho, rf, nz))) return bail(rc);
+  if ((rc = upload(p, &p->rhoh, rh.data(), nz + 1))) return bail(rc);
+  if ((rc = upload(p, &p->theta0, t0, nz))) return bail(rc);
+  if ((rc = upload(p, &p->dth0, dth0.data(), nz))) return bail(rc);
+  if ((rc = upload(p, &p->ta, a.data(), nz))) return bail(rc);
+  if ((rc = upload(p, &p->tc, c.data(), nz))) return bail(rc);
+  if ((rc = upload(p, &p->tnegs, negs.data(), nz))) return bail(rc);
+  if ((rc = upload(p, &p->ta0, a0.data(), n0))) return bail(rc);
+  if ((rc = upload(p, &p->tcp0, cp0.data(), n0))) return bail(rc);
+  if ((rc = upload(p, &p->tinv0, inv0.data(), n0))) return bail(rc);
+  if (p->coriolis == OB_COR_BETA)
+    if ((rc = upload(p, &p->fy, comp->f_y, ny))) return bail(rc);
+  if (p->heating) {
+    if ((rc = upload(p, &p->heat_r, comp->heat_r, (size_t)nx * ny))) return bail(rc);
+    if ((rc = upload(p, &p->heat_z, comp->heat_z, nz))) return bail(rc);
+  }
+  if (p->prec == OB_PREC_F64) {
+    auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
+    if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<double>)))) return bail(rc);
+    if ((rc = dalloc(p, &p->twy, ny * sizeof(cplx<double>)))) return bail(rc);
+    if (cudaMemcpy(p->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice))
+      return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
+    if ((rc = set_smem_attrs<double>())) return bail(rc);
+  } else {
+    auto tx = twiddles<float>(nx), ty = twiddles<float>(ny);
+    if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<float>)))) return bail(rc);
+    if ((rc = dalloc(p, &p->twy, ny * sizeof(cplx<float>)))) return bail(rc);
+    if (cudaMemcpy(p->twx, tx.data(), nx * sizeof(cplx<float>), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<float>), cudaMemcpyHostToDevice))
+      return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
+    if ((rc = set_smem_attrs<float>())) return bail(rc);
+  }
+
+  // chunk sizes: largest z-chunk whose shared-memory footprint allows two CTAs/SM
+  const size_t ce = 2 * p->esz;  // complex element
+  p->zc_fx = pick_zc(nz, 2ull * (p->g.M + 1) * 3 * ce, 0);
+  p->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, 0);
+  p->zc_iy = p->zc_fy;
+  p->zc_ix = pick_zc(nz, (size_t)(2 * p->g.M + 1) * 3 * ce, (size_t)(2 * p->g.M + 1) * ce);
+  if (smem_fx(p, 3) > kSmemMax || smem_fy(p, 2, p->zc_fy) > kSmemMax ||
+      smem_ix(p, 3 * p->zc_ix + 1) > kSmemMax || smem_thomas(p) > kSmemMax)
+    return bail(fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx,
+                     ny, nz));
+
+  const size_t n = (size_t)nx * ny * nz, nw = (size_t)nx * ny * (nz + 1);
+  const size_t ns = (size_t)p->g.nxh * ny * nz;
+  const size_t e = p->esz;
+  if ((rc = dalloc(p, &p->S1, ns * 2 * e)) || (rc = dalloc(p, &p->S2, ns * 2 * e)) ||
+      (rc = dalloc(p, &p->S3, ns * 2 * e)) || (rc = dalloc(p, &p->Au, n * e)) ||
+      (rc = dalloc(p, &p->Av, n * e)) || (rc = dalloc(p, &p->Aw, nw * e)) ||
+      (rc = dalloc(p, &p->Ath, n * e)) || (rc = dalloc(p, &p->Aphi, n * e)) ||
+      (rc = dalloc(p, &p->Su, n * e)) || (rc = dalloc(p, &p->Sv, n * e)) ||
+      (rc = dalloc(p, &p->Sw, nw * e)) || (rc = dalloc(p, &p->Sphi, n * e)) ||
+      (rc = dalloc(p, &p->Du, n * e)) || (rc = dalloc(p, &p->Dv, n * e)))
+    return bail(rc);
+  if ((rc = dalloc(p, &p->diag, 64 * sizeof(double)))) return bail(rc);
+  OB_CUDA(cudaMemset(p->diag, 0, 64 * sizeof(double)));
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  p->nparts = nsm * 4;
+  if ((rc = dalloc(p, &p->parts, p->nparts * sizeof(DiagPart)))) return bail(rc);
+  *out = p;
+  return OB_OK;
+}
+
+#define DISPATCH(P, CALL_F64, CALL_F32) ((P)->prec == OB_PREC_F64 ? (CALL_F64) : (CALL_F32))
+
+int oracle_b200_step(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* out,
+                     double dt, int want_diag, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!in || !out || !in->u || !in->v || !in->w || !in->theta_prime || !in->phi || !out->u ||
+      !out->v || !out->w || !out->theta_prime || !out->phi)
+    return fail(OB_ERR_ARG, "step: NULL state pointer");
+  if (!std::isfinite(dt)) return fail(OB_ERR_ARG, "step: dt must be finite");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p, step_impl<double>(p, in, out, dt, want_diag, st),
+                  step_impl<float>(p, in, out, dt, want_diag, st));
+}
+
+int oracle_b200_project(OraclePlan* p, void* u, void* v, void* w, void* phi, int log_diag,
+                        void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!u || !v || !w || !phi) return fail(OB_ERR_ARG, "project: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int de = p->diag_every;
+  if (log_diag) p->diag_every = 1;
+  int rc = DISPATCH(p,
+                    project_impl<double>(p, (double*)u, (double*)v, (double*)w, nullptr, -1.0,
+                                         (double*)u, (double*)v, (double*)w, (double*)phi,
+                                         OB_DIAG_LAST_COMPAT, OB_DIAG_LAST_DISC, st),
+                    project_impl<float>(p, (float*)u, (float*)v, (float*)w, nullptr, -1.0,
+                                        (float*)u, (float*)v, (float*)w, (float*)phi,
+                                        OB_DIAG_LAST_COMPAT, OB_DIAG_LAST_DISC, st));
+  p->diag_every = de;
+  return rc;
+}
+
+int oracle_b200_divergence(OraclePlan* p, const void* u, const void* v, const void* w, void* d,
+                           void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!u || !v || !w || !d) return fail(OB_ERR_ARG, "divergence: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p,
+                  divergence_impl<double>(p, (const double*)u, (const double*)v,
+                                          (const double*)w, (double*)d, st),
+                  divergence_impl<float>(p, (const float*)u, (const float*)v, (const float*)w,
+                                         (float*)d, st));
+}
+
+int oracle_b200_phi_gradient(OraclePlan* p, const void* phi, void* gx, void* gy, void* gz,
+                             void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!phi || !gx || !gy || !gz) return fail(OB_ERR_ARG, "phi_gradient: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p,
+                  gradient_impl<double>(p, (const double*)phi, (double*)gx, (double*)gy,
+                                        (double*)gz, st),
+                  gradient_impl<float>(p, (const float*)phi, (float*)gx, (float*)gy,
+                                       (float*)gz, st));
+}
+
+int oracle_b200_poisson_solve(OraclePlan* p, const void* d, void* phi, int log_diag,
+                              void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!d || !phi) return fail(OB_ERR_ARG, "poisson_solve: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p, solve_impl<double>(p, (const double*)d, (double*)phi, log_diag, st),
+                  solve_impl<float>(p, (const float*)d, (float*)phi, log_diag, st));
+}
+
+int oracle_b200_apply_operator(OraclePlan* p, const void* phi, void* out, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!phi || !out) return fail(OB_ERR_ARG, "apply_operator: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p, apply_op_impl<double>(p, (const double*)phi, (double*)out, st),
+                  apply_op_impl<float>(p, (const float*)phi, (float*)out, st));
+}
+
+int oracle_b200_buoyancy(OraclePlan* p, const void* th, void* dw, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!th || !dw) return fail(OB_ERR_ARG, "buoyancy: NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p, buoyancy_impl<double>(p, (const double*)th, (double*)dw, st),
+                  buoyancy_impl<float>(p, (const float*)th, (float*)dw, st));
+}
+
+int oracle_b200_tendency(OraclePlan* p, int mask, const OracleStatePtrs* s, void* du, void* dv,
+                         void* dw, void* dth, double dt_slow, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!s || !s->u || !s->v || !s->w || !s->theta_prime || !du || !dv || !dw || !dth)
+    return fail(OB_ERR_ARG, "tendency: NULL pointer");
+  if ((mask & OB_TEND_DAMPING) && p->damping && !(dt_slow != 0.0))
+    return fail(OB_ERR_ARG, "tendency: damping needs a non-zero dt_slow");
+  cudaStream_t st = (cudaStream_t)stream;
+  return DISPATCH(p,
+                  tendency_impl<double>(p, mask, s, (double*)du, (double*)dv, (double*)dw,
+                                        (double*)dth, dt_slow, st),
+                  tendency_impl<float>(p, mask, s, (float*)du, (float*)dv, (float*)dw,
+                                       (float*)dth, dt_slow, st));
+}
+
+int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!host_out || n < 0) return fail(OB_ERR_ARG, "read_diag: bad output");
+  if (n > OB_DIAG_COUNT) n = OB_DIAG_COUNT;
+  cudaStream_t st = (cudaStream_t)stream;
+  double buf[OB_DIAG_COUNT];
+  OB_CUDA(cudaMemcpyAsync(buf, p->diag, sizeof buf, cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  // discrete residual slots hold sum(w |r^|^2); rms = sqrt(sum / ((nx ny)^2 nz))
+  const double nxy = (double)p->g.nx * p->g.ny;
+  const double norm = nxy * nxy * p->g.nz;
+  for (int s : {OB_DIAG_DISC0, OB_DIAG_DISC0 + 1, OB_DIAG_DISC0 + 2, OB_DIAG_LAST_DISC})
+    buf[s] = std::sqrt(std::fmax(buf[s], 0.0) / norm);
+  std::memcpy(host_out, buf, n * sizeof(double));
+  return OB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+// Shared device helpers for the LH82 step kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ob {
+
+// Interleaved complex value; 8-byte (float) or 16-byte (double) aligned so a
+// warp moves it with one vector load per lane.
+template <class T>
+struct __align__(2 * sizeof(T)) cplx {
+  T x, y;
+};
+
+template <class T>
+__device__ __forceinline__ cplx<T> mk(T a, T b) {
+  cplx<T> c;
+  c.x = a;
+  c.y = b;
+  return c;
+}
+template <class T>
+__device__ __forceinline__ cplx<T> add(cplx<T> a, cplx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <class T>
+__device__ __forceinline__ cplx<T> sub(cplx<T> a, cplx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <class T>
+__device__ __forceinline__ cplx<T> mul(cplx<T> a, cplx<T> b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <class T>
+__device__ __forceinline__ cplx<T> conjg(cplx<T> a) { return mk<T>(a.x, -a.y); }
+template <class T>
+__device__ __forceinline__ cplx<T> scl(cplx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <class T, bool INV>
+__device__ __forceinline__ cplx<T> rot(cplx<T> a) {
+  return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
+}
+// i * k * a  (k real): the spectral derivative multiplier
+template <class T>
+__device__ __forceinline__ cplx<T> ik(T k, cplx<T> a) { return mk<T>(-k * a.y, k * a.x); }
+
+// Round-to-nearest arithmetic without FMA contraction, for the sequences
+// whose rounding must follow the reference's NumPy operation order.
+__device__ __forceinline__ double mrn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double arn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double srn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double drn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float mrn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float arn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float srn(float a, float b) { return __fsub_rn(a, b); }
+
+// Grid description passed by value to every kernel.
+struct GridK {
+  int nx, ny, nz;
+  int M;        // nx / 2 (length of the packed complex FFT along x)
+  int nxh;      // nx / 2 + 1 (R2C modes along x)
+  double dx, dy, dz;
+};
+
+// Mixed-radix factor list of a complex FFT length.
+struct FftPlan {
+  int M;
+  int np;
+  int r[20];
+};
+
+constexpr double kGravity = 9.81;  // oracle_v8/constants.py:25
+
+}  // namespace ob

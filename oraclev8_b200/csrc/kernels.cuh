@@ -1,0 +1,850 @@
+// Device kernels of the LH82 anelastic step.
+//
+// Projection pipeline (AnelasticProjection.apply_projection,
+// oracle_v8/solver/tendency.py:717-790), spectral layout [kx][y|ky][z] with
+// kx in [0, nx/2] (real FFT along x), z contiguous:
+//   k_fx     x-pencils (fixed y, z-chunk): rho-weighting, vertical flux
+//            divergence, R2C along x; emits X1 = i kx' FFTx(rho u) + FFTx(vd)
+//            and X2 = FFTx(rho v).
+//   k_fy     y-pencils (fixed kx, z-chunk): C2C along y; d^ = FFTy(X1) +
+//            i ky' FFTy(X2).
+//   k_thomas columns (kx, ky): batched Thomas in z with the zero mode solved on
+//            its reduced system; phi^ scaled by 1/(nx ny).
+//   k_iy     y-pencils: phi~ = IFFTy(phi^), psi~ = IFFTy(i ky' phi^).
+//   k_ix     x-pencils: C2R along x of phi~, i kx' phi~, psi~; applies the
+//            velocity correction u -= dphi/dx, v -= dphi/dy,
+//            w -= (phi_k - phi_{k-1})/dz and stores phi.
+// kx' and ky' are the wavenumbers with the Nyquist entry zeroed: the reference
+// takes real(ifft2(i k f^)), which removes exactly that component
+// (tendency.py:428-431, 487-491).
+#pragma once
+#include "fft.cuh"
+
+namespace ob {
+
+// ---------------------------------------------------------------------------
+// Buoyancy on half levels: b_half[k] = 0.5 (b[k-1] + b[k]), b = g theta'/theta0,
+// zero at surface and lid (equation_set.py:255-263, staggering.py:201-208).
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ double bhalf(const T* __restrict__ thc, int k, int nz,
+                                        const double* __restrict__ theta0) {
+  if (k <= 0 || k >= nz) return 0.0;
+  const double b0 = drn(mrn(kGravity, (double)thc[k - 1]), theta0[k - 1]);
+  const double b1 = drn(mrn(kGravity, (double)thc[k]), theta0[k]);
+  return mrn(0.5, arn(b0, b1));
+}
+
+// Stage provisional w: w_n + sdt * b_half (integrator.py:483-490).
+template <class T>
+__device__ __forceinline__ double stage_w(const T* __restrict__ wc, const T* __restrict__ thc,
+                                          int k, int nz, double sdt,
+                                          const double* __restrict__ theta0) {
+  return arn((double)wc[k], mrn(sdt, bhalf(thc, k, nz, theta0)));
+}
+
+enum FxMode { FX_DIV = 0, FX_DIV_STAGE = 1, FX_FIELDS = 2 };
+
+// x-pencil forward kernel.  grid = (ny, ceil(nz/zc)).  smem: 2 * (M+1) * B cplx.
+// FX_FIELDS transforms `nf` real fields f0..f2 (no weighting) into X0..X2.
+template <class T, int MODE>
+__global__ void __launch_bounds__(512) k_fx(GridK g, FftPlan px, int zc, int nf,
+                                            const T* __restrict__ f0, const T* __restrict__ f1,
+                                            const T* __restrict__ f2, const T* __restrict__ th,
+                                            double sdt, const double* __restrict__ rho,
+                                            const double* __restrict__ rhoh,
+                                            const double* __restrict__ theta0,
+                                            const double* __restrict__ kxd,
+                                            const cplx<T>* __restrict__ twx,
+                                            cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1,
+                                            cplx<T>* __restrict__ X2) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NF = (MODE == FX_FIELDS) ? nf : 3;
+  const int B = NF * zc;
+  const int M = g.M;
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* bufB = bufA + (size_t)(M + 1) * B;
+  const int y = blockIdx.x;
+  const int z0 = blockIdx.y * zc;
+  const int zn = min(zc, g.nz - z0);
+  const int nz = g.nz;
+  T* rA = reinterpret_cast<T*>(bufA);
+
+  const int nel = g.nx * zc;
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int x = e / zc;
+    const int zl = e - x * zc;
+    const int n = x >> 1, odd = x & 1;
+    const size_t col = (size_t)x * g.ny + y;
+    if (MODE == FX_FIELDS) {
+      for (int f = 0; f < NF; ++f) {
+        const T* src = f == 0 ? f0 : (f == 1 ? f1 : f2);
+        T val = (T)0;
+        if (zl < zn) val = src[col * nz + z0 + zl];
+        rA[2 * ((size_t)n * B + f * zc + zl) + odd] = val;
+      }
+    } else {
+      T a = 0, b = 0, c = 0;
+      if (zl < zn) {
+        const int z = z0 + zl;
+        const double r = rho[z];
+        a = (T)(r * (double)f0[col * nz + z]);
+        b = (T)(r * (double)f1[col * nz + z]);
+        const T* wc = f2 + col * (nz + 1);
+        double wl, wu;
+        if (MODE == FX_DIV_STAGE) {
+          const T* thc = th + col * nz;
+          wl = stage_w(wc, thc, z, nz, sdt, theta0);
+          wu = stage_w(wc, thc, z + 1, nz, sdt, theta0);
+        } else {
+          wl = (double)wc[z];
+          wu = (double)wc[z + 1];
+        }
+        c = (T)((rhoh[z + 1] * wu - rhoh[z] * wl) / g.dz);
+      }
+      rA[2 * ((size_t)n * B + zl) + odd] = a;
+      rA[2 * ((size_t)n * B + zc + zl) + odd] = b;
+      rA[2 * ((size_t)n * B + 2 * zc + zl) + odd] = c;
+    }
+  }
+  __syncthreads();
+  cplx<T>* Z = fft_smem<T, false>(bufA, bufB, B, px, twx, 2);
+  cplx<T>* X = (Z == bufA) ? bufB : bufA;
+  r2c_post<T>(Z, X, M, B, twx);
+  __syncthreads();
+
+  const int nout = (M + 1) * zc;
+  for (int e = threadIdx.x; e < nout; e += blockDim.x) {
+    const int k = e / zc;
+    const int zl = e - k * zc;
+    if (zl >= zn) continue;
+    const size_t o = ((size_t)k * g.ny + y) * nz + z0 + zl;
+    if (MODE == FX_FIELDS) {
+      for (int f = 0; f < NF; ++f) {
+        cplx<T>* dst = f == 0 ? X0 : (f == 1 ? X1 : X2);
+        dst[o] = X[(size_t)k * B + f * zc + zl];
+      }
+    } else {
+      const T kk = (k == M) ? (T)0 : (T)kxd[k];
+      const cplx<T> U = X[(size_t)k * B + zl];
+      const cplx<T> V = X[(size_t)k * B + zc + zl];
+      const cplx<T> D = X[(size_t)k * B + 2 * zc + zl];
+      X0[o] = add(ik(kk, U), D);
+      X1[o] = V;
+    }
+  }
+}
+
+enum FyMode { FY_DIV = 0, FY_FIELDS = 1, FY_HELM = 2 };
+
+// y-pencil forward kernel.  grid = (nxh, ceil(nz/zc)).  smem: 2 * ny * B cplx.
+// FY_DIV: out0 = FFTy(in0) + i ky' FFTy(in1).
+// FY_FIELDS: out_f = FFTy(in_f) for f < nf.
+// FY_HELM: the Helmholtz divergent-part multipliers (tendency.py:1800-1839),
+//   out0 = s (Kx^2/K^2 U + (KxKy/K^2)' V), out1 = s ((KxKy/K^2)' U + Ky^2/K^2 V),
+//   s = scale; the primed cross term is zero where exactly one of kx, ky is
+//   the Nyquist index (there the reference's real() drops it).
+template <class T, int MODE>
+__global__ void __launch_bounds__(512) k_fy(GridK g, FftPlan py, int zc, int nf,
+                                            const cplx<T>* __restrict__ in0,
+                                            const cplx<T>* __restrict__ in1,
+                                            const double* __restrict__ kxd,
+                                            const double* __restrict__ kyd,
+                                            const cplx<T>* __restrict__ twy, double scale,
+                                            cplx<T>* __restrict__ out0,
+                                            cplx<T>* __restrict__ out1) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NF = (MODE == FY_FIELDS) ? nf : 2;
+  const int B = NF * zc;
+  const int ny = g.ny, nz = g.nz;
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* bufB = bufA + (size_t)ny * B;
+  const int kx = blockIdx.x;
+  const int z0 = blockIdx.y * zc;
+  const int zn = min(zc, nz - z0);
+  const int nel = ny * zc;
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int y = e / zc;
+    const int zl = e - y * zc;
+    const size_t o = ((size_t)kx * ny + y) * nz + z0 + zl;
+    for (int f = 0; f < NF; ++f) {
+      const cplx<T>* src = f == 0 ? in0 : in1;
+      cplx<T> val = mk<T>((T)0, (T)0);
+      if (zl < zn) val = src[o];
+      bufA[(size_t)y * B + f * zc + zl] = val;
+    }
+  }
+  __syncthreads();
+  cplx<T>* R = fft_smem<T, false>(bufA, bufB, B, py, twy, 1);
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int ky = e / zc;
+    const int zl = e - ky * zc;
+    if (zl >= zn) continue;
+    const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
+    if (MODE == FY_DIV) {
+      const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
+      out0[o] = add(R[(size_t)ky * B + zl], ik(kk, R[(size_t)ky * B + zc + zl]));
+    } else if (MODE == FY_FIELDS) {
+      for (int f = 0; f < NF; ++f) (f == 0 ? out0 : out1)[o] = R[(size_t)ky * B + f * zc + zl];
+    } else {
+      const double Kx = kxd[kx], Ky = kyd[ky];
+      const double K2 = Kx * Kx + Ky * Ky;
+      double mxx = 0, myy = 0, mxy = 0;
+      if (K2 > 0) {
+        mxx = Kx * Kx / K2;
+        myy = Ky * Ky / K2;
+        const bool nyqx = (kx == g.nx / 2), nyqy = (ky == ny / 2);
+        mxy = (nyqx != nyqy) ? 0.0 : Kx * Ky / K2;
+      }
+      const cplx<T> U = R[(size_t)ky * B + zl];
+      const cplx<T> V = R[(size_t)ky * B + zc + zl];
+      const T sxx = (T)(scale * mxx), syy = (T)(scale * myy), sxy = (T)(scale * mxy);
+      out0[o] = mk<T>(sxx * U.x + sxy * V.x, sxx * U.y + sxy * V.y);
+      out1[o] = mk<T>(sxy * U.x + syy * V.x, sxy * U.y + syy * V.y);
+    }
+  }
+}
+
+// Thomas tables (double, device), built on the host exactly as
+// poisson.py:286-325 builds them.
+struct ThomasK {
+  const double* a;     // (nz) sub-diagonal, a[0] = 0
+  const double* c;     // (nz) super-diagonal, c[nz-1] = 0
+  const double* negs;  // (nz) mode-independent part of the diagonal
+  const double* rho;   // (nz) rho on full levels (multiplies k^2)
+  const double* rhoh;  // (nz+1) rho on half levels (residual operator)
+  const double* kx;    // (nx) 2 pi fftfreq
+  const double* ky;    // (ny)
+  const double* a0;    // (nz-1) zero-mode reduced system
+  const double* cp0;
+  const double* inv0;
+  double dz;
+  double scale;        // 1 / (nx ny): inverse-FFT normalisation folded in
+};
+
+// Batched Thomas, one thread per spectral column (kx, ky).  Columns are
+// staged through shared memory (coalesced loads of TC consecutive columns);
+// the recurrence runs in double with the reference's operation order and no
+// FMA contraction (poisson.py:334-383).  diag != nullptr records the
+// compatibility residual (poisson.py:233-236) in diag[slot_c] and the
+// Parseval form of the discrete-operator residual (poisson.py:263-268) as a
+// raw sum of weighted |r^|^2 in diag[slot_d] (normalised on the host).
+// dh and ph may alias: a CTA reads only its own columns before writing them.
+template <class T, int TC>
+__global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>* dh,
+                                               cplx<T>* ph, double* diag, int slot_c,
+                                               int slot_d) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nz = g.nz;
+  const int P = nz + 1;  // padded column stride (bank spread)
+  double* sre = reinterpret_cast<double*>(smem_raw);  // TC * P real parts
+  double* sim = sre + (size_t)TC * P;                   // TC * P imag parts
+  double* scp = sim + (size_t)TC * P;                   // TC * P c' factors
+  const long ncols = (long)g.nxh * g.ny;
+  const long c0 = (long)blockIdx.x * TC;
+  const int ncl = (int)min((long)TC, ncols - c0);
+  const long base = c0 * nz;
+  for (int e = threadIdx.x; e < ncl * nz; e += TC) {
+    const int cl = e / nz;
+    const int k = e - cl * nz;
+    const cplx<T> v = dh[base + e];
+    sre[cl * P + k] = (double)v.x;
+    sim[cl * P + k] = (double)v.y;
+  }
+  __syncthreads();
+  const int cl = threadIdx.x;
+  double resid = 0.0;
+  if (cl < ncl) {
+    const long col = c0 + cl;
+    const int kxi = (int)(col / g.ny);
+    const int kyi = (int)(col - (long)kxi * g.ny);
+    double* re = sre + cl * P;
+    double* im = sim + cl * P;
+    double* cp = scp + cl * P;
+    if (col == 0) {
+      // Zero mode (poisson.py:233-236, 256, 316-325, 367-383): compatibility
+      // residual, removal of the column mean, then the reduced (nz-1) system
+      // on levels 1..nz-1 with phi(0,0,0) pinned to 0.
+      double sr = 0, si = 0;
+      for (int k = 0; k < nz; ++k) {
+        sr = arn(sr, re[k]);
+        si = arn(si, im[k]);
+      }
+      if (diag) diag[slot_c] = hypot(mrn(sr, t.dz), mrn(si, t.dz));
+      const double mr = drn(sr, (double)nz), mi = drn(si, (double)nz);
+      for (int k = 0; k < nz; ++k) cp[k] = re[k];  // source, kept for the residual
+      const int n0 = nz - 1;
+      double pr = mrn(srn(re[1], mr), t.inv0[0]);
+      double pi = mrn(srn(im[1], mi), t.inv0[0]);
+      re[1] = pr;
+      im[1] = pi;
+      for (int j = 1; j < n0; ++j) {
+        pr = mrn(srn(srn(re[j + 1], mr), mrn(t.a0[j], pr)), t.inv0[j]);
+        pi = mrn(srn(srn(im[j + 1], mi), mrn(t.a0[j], pi)), t.inv0[j]);
+        re[j + 1] = pr;
+        im[j + 1] = pi;
+      }
+      double xr = pr, xi = pi;
+      for (int j = n0 - 2; j >= 0; --j) {
+        xr = srn(re[j + 1], mrn(t.cp0[j], xr));
+        xi = srn(im[j + 1], mrn(t.cp0[j], xi));
+        re[j + 1] = xr;
+        im[j + 1] = xi;
+      }
+      re[0] = 0.0;
+      im[0] = 0.0;
+      if (diag) {
+        // The zero mode of a real field is real.  Residual against the
+        // original source, with its z-mean (the domain mean of the physical
+        // residual) removed.
+        const double dz2 = t.dz * t.dz;
+        double rsum = 0, r2 = 0;
+        for (int k = 0; k < nz; ++k) {
+          const double fu = (k < nz - 1) ? t.rhoh[k + 1] * (re[k + 1] - re[k]) : 0.0;
+          const double fl = (k > 0) ? t.rhoh[k] * (re[k] - re[k - 1]) : 0.0;
+          const double r = (fu - fl) / dz2 - cp[k];
+          rsum += r;
+          r2 += r * r;
+        }
+        resid = r2 - rsum * rsum / nz;
+      }
+    } else {
+      const double kx = t.kx[kxi], ky = t.ky[kyi];
+      const double ksq = arn(mrn(kx, kx), mrn(ky, ky));
+      double b = srn(t.negs[0], mrn(ksq, t.rho[0]));
+      double inv = drn(1.0, b);
+      double cpp = mrn(t.c[0], inv);
+      cp[0] = cpp;
+      double pr = mrn(re[0], inv), pi = mrn(im[0], inv);
+      re[0] = pr;
+      im[0] = pi;
+      for (int k = 1; k < nz; ++k) {
+        b = srn(t.negs[k], mrn(ksq, t.rho[k]));
+        const double den = srn(b, mrn(t.a[k], cpp));
+        inv = drn(1.0, den);
+        if (k < nz - 1) {
+          cpp = mrn(t.c[k], inv);
+          cp[k] = cpp;
+        }
+        pr = mrn(srn(re[k], mrn(t.a[k], pr)), inv);
+        pi = mrn(srn(im[k], mrn(t.a[k], pi)), inv);
+        re[k] = pr;
+        im[k] = pi;
+      }
+      double xr = pr, xi = pi;
+      for (int k = nz - 2; k >= 0; --k) {
+        xr = srn(re[k], mrn(cp[k], xr));
+        xi = srn(im[k], mrn(cp[k], xi));
+        re[k] = xr;
+        im[k] = xi;
+      }
+      if (diag) {
+        // r^ = L phi^ - d^, source re-read from global memory
+        const double dz2 = t.dz * t.dz;
+        double acc = 0;
+        for (int k = 0; k < nz; ++k) {
+          const double fur = (k < nz - 1) ? t.rhoh[k + 1] * (re[k + 1] - re[k]) : 0.0;
+          const double fui = (k < nz - 1) ? t.rhoh[k + 1] * (im[k + 1] - im[k]) : 0.0;
+          const double flr = (k > 0) ? t.rhoh[k] * (re[k] - re[k - 1]) : 0.0;
+          const double fli = (k > 0) ? t.rhoh[k] * (im[k] - im[k - 1]) : 0.0;
+          const cplx<T> src = dh[(size_t)col * nz + k];
+          const double rr = (fur - flr) / dz2 - ksq * t.rho[k] * re[k] - (double)src.x;
+          const double ri = (fui - fli) / dz2 - ksq * t.rho[k] * im[k] - (double)src.y;
+          acc += rr * rr + ri * ri;
+        }
+        resid = ((kxi == 0 || 2 * kxi == g.nx) ? 1.0 : 2.0) * acc;
+      }
+    }
+  }
+  if (diag) {
+    for (int o = 16; o > 0; o >>= 1) resid += __shfl_xor_sync(0xffffffffu, resid, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&diag[slot_d], resid);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < ncl * nz; e += TC) {
+    const int c = e / nz;
+    const int k = e - c * nz;
+    ph[base + e] = mk<T>((T)(sre[c * P + k] * t.scale), (T)(sim[c * P + k] * t.scale));
+  }
+}
+
+enum IyMode { IY_GRAD = 0, IY_FIELDS = 1 };
+
+// y-pencil inverse kernel.  grid = (nxh, ceil(nz/zc)).  smem 2 * ny * B cplx.
+// IY_GRAD: out0 = IFFTy(in0), out1 = IFFTy(i ky' in0).
+// IY_FIELDS: out_f = IFFTy(scale * in_f), f < nf.
+template <class T, int MODE>
+__global__ void __launch_bounds__(512) k_iy(GridK g, FftPlan py, int zc, int nf,
+                                            const cplx<T>* __restrict__ in0,
+                                            const cplx<T>* __restrict__ in1,
+                                            const double* __restrict__ kyd,
+                                            const cplx<T>* __restrict__ twy, double scale,
+                                            cplx<T>* __restrict__ out0,
+                                            cplx<T>* __restrict__ out1) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NF = (MODE == IY_FIELDS) ? nf : 2;
+  const int B = NF * zc;
+  const int ny = g.ny, nz = g.nz;
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* bufB = bufA + (size_t)ny * B;
+  const int kx = blockIdx.x;
+  const int z0 = blockIdx.y * zc;
+  const int zn = min(zc, nz - z0);
+  const int nel = ny * zc;
+  const T s = (T)scale;
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int ky = e / zc;
+    const int zl = e - ky * zc;
+    const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
+    if (MODE == IY_GRAD) {
+      cplx<T> v = mk<T>((T)0, (T)0);
+      if (zl < zn) v = in0[o];
+      const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
+      bufA[(size_t)ky * B + zl] = v;
+      bufA[(size_t)ky * B + zc + zl] = ik(kk, v);
+    } else {
+      for (int f = 0; f < NF; ++f) {
+        cplx<T> v = mk<T>((T)0, (T)0);
+        if (zl < zn) v = scl((f == 0 ? in0 : in1)[o], s);
+        bufA[(size_t)ky * B + f * zc + zl] = v;
+      }
+    }
+  }
+  __syncthreads();
+  cplx<T>* R = fft_smem<T, true>(bufA, bufB, B, py, twy, 1);
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int y = e / zc;
+    const int zl = e - y * zc;
+    if (zl >= zn) continue;
+    const size_t o = ((size_t)kx * ny + y) * nz + z0 + zl;
+    out0[o] = R[(size_t)y * B + zl];
+    if (NF > 1) out1[o] = R[(size_t)y * B + zc + zl];
+  }
+}
+
+enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3 };
+
+// x-pencil inverse kernel.  grid = (ny, ceil(nz/zc)).  smem: (M+1)*B + M*B cplx,
+// B = 3 zc + 1 (correction/grad: phi with one halo level below, d/dx, d/dy)
+// or nf * zc (IX_FIELDS).
+//   IX_CORRECT: in place, u -= gx, v -= gy, w[k] -= (phi_k - phi_{k-1})/dz
+//               (1 <= k <= nz-1), phi stored (tendency.py:781-788).
+//   IX_STAGE:   u_out = u_n - gx, v_out = v_n - gy, w_out = w_n + sdt b_half
+//               - gz, phi_out = phi (the RK3 stage provisional state,
+//               integrator.py:483-500).
+//   IX_GRAD:    gx, gy (full levels), gz (nz+1 half levels, zero ends)
+//               (tendency.py:487-500).
+//   IX_FIELDS:  real outputs of nf spectra.
+template <class T, int MODE>
+__global__ void __launch_bounds__(512) k_ix(GridK g, FftPlan px, int zc, int nf,
+                                            const cplx<T>* __restrict__ phs,
+                                            const cplx<T>* __restrict__ psi,
+                                            const cplx<T>* __restrict__ s2,
+                                            const double* __restrict__ kxd,
+                                            const cplx<T>* __restrict__ twx,
+                                            const T* u_in, const T* v_in, const T* w_in,
+                                            const T* __restrict__ th, double sdt,
+                                            const double* __restrict__ theta0, T* u_out,
+                                            T* v_out, T* w_out, T* phi_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const bool fields = (MODE == IX_FIELDS);
+  const int B = fields ? nf * zc : 3 * zc + 1;
+  const int M = g.M;
+  const int nz = g.nz;
+  cplx<T>* bufX = reinterpret_cast<cplx<T>*>(smem_raw);  // (M+1) * B
+  cplx<T>* bufZ = bufX + (size_t)(M + 1) * B;             // M * B
+  const int y = blockIdx.x;
+  const int z0 = blockIdx.y * zc;
+  const int zn = min(zc, nz - z0);
+
+  // load spectra X[k][b]
+  const int nel = (M + 1) * B;
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int k = e / B;
+    const int bb = e - k * B;
+    cplx<T> v = mk<T>((T)0, (T)0);
+    const size_t rowo = ((size_t)k * g.ny + y) * nz;
+    if (fields) {
+      const int f = bb / zc, zl = bb - f * zc;
+      if (zl < zn) v = (f == 0 ? phs : (f == 1 ? psi : s2))[rowo + z0 + zl];
+    } else if (bb <= zc) {
+      // phi at level z0 - 1 + bb (bb = 0 is the halo below the chunk)
+      const int z = z0 - 1 + bb;
+      if (z >= 0 && bb <= zn) v = phs[rowo + z];
+    } else if (bb <= 2 * zc) {
+      const int zl = bb - zc - 1;
+      if (zl < zn) {
+        const T kk = (k == M) ? (T)0 : (T)kxd[k];
+        v = ik(kk, phs[rowo + z0 + zl]);
+      }
+    } else {
+      const int zl = bb - 2 * zc - 1;
+      if (zl < zn) v = psi[rowo + z0 + zl];
+    }
+    bufX[e] = v;
+  }
+  __syncthreads();
+  c2r_pre<T>(bufX, bufZ, M, B, twx);
+  __syncthreads();
+  cplx<T>* Zr = fft_smem<T, true>(bufZ, bufX, B, px, twx, 2);
+  const T* rz = reinterpret_cast<const T*>(Zr);
+  // real value of batch bb at x: rz[2 * ((x >> 1) * B + bb) + (x & 1)]
+
+  const int nout = g.nx * zc;
+  for (int e = threadIdx.x; e < nout; e += blockDim.x) {
+    const int x = e / zc;
+    const int zl = e - x * zc;
+    if (zl >= zn) continue;
+    const int z = z0 + zl;
+    const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
+    const size_t col = (size_t)x * g.ny + y;
+    const size_t idx = col * nz + z;
+    if (fields) {
+      for (int f = 0; f < nf; ++f) {
+        T* dst = f == 0 ? u_out : (f == 1 ? v_out : w_out);
+        dst[idx] = rz[rb + 2 * (f * zc + zl)];
+      }
+      continue;
+    }
+    const T phi = rz[rb + 2 * (zl + 1)];
+    const T phib = rz[rb + 2 * zl];
+    const T gx = rz[rb + 2 * (zc + 1 + zl)];
+    const T gy = rz[rb + 2 * (2 * zc + 1 + zl)];
+    const T gz = (z >= 1) ? (T)((phi - phib) / (T)g.dz) : (T)0;
+    const size_t wi = col * (nz + 1) + z;
+    if (MODE == IX_GRAD) {
+      u_out[idx] = gx;
+      v_out[idx] = gy;
+      w_out[wi] = gz;
+      if (z == nz - 1) w_out[wi + 1] = (T)0;
+    } else if (MODE == IX_CORRECT) {
+      u_out[idx] = u_in[idx] - gx;
+      v_out[idx] = v_in[idx] - gy;
+      w_out[wi] = w_in[wi] - gz;
+      if (z == nz - 1 && w_out != w_in) w_out[wi + 1] = w_in[wi + 1];
+      phi_out[idx] = phi;
+    } else {  // IX_STAGE
+      const T* wc = w_in + col * (nz + 1);
+      const T* thc = th + col * nz;
+      u_out[idx] = u_in[idx] - gx;
+      v_out[idx] = v_in[idx] - gy;
+      w_out[wi] = (T)stage_w(wc, thc, z, nz, sdt, theta0) - gz;
+      if (z == nz - 1) w_out[wi + 1] = (T)stage_w(wc, thc, nz, nz, sdt, theta0);
+      phi_out[idx] = phi;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused slow tendency + forward-Euler half step (integrator.py:346-370).
+// Components, summed in OperatorConfig slot order (operator_config.py:147-160):
+// advection (tendency.py:965-1062), Coriolis (tendency.py:1220-1234),
+// divergence damping (precomputed spectral tendency, added here) and
+// diabatic heating (tendency.py:1731-1732).
+// ---------------------------------------------------------------------------
+struct SlowK {
+  int adv;            // OB_ADV_*
+  int cor;            // 0 none, 1 f-plane, 2 beta-plane
+  int heat;
+  int damp;
+  double f0, u_env, v_env;
+  const double* fy;     // (ny)
+  const double* dth0;   // (nz) d theta0 / dz (tendency.py:1013-1016)
+  const double* heat_r; // (nx*ny)
+  const double* heat_z; // (nz)
+  double inv2dx, inv2dy, inv60dx, inv60dy, inv2dz, invdz;
+};
+
+template <class T>
+__device__ __forceinline__ double ddx_ws5(const T* __restrict__ q, size_t o, const size_t* off,
+                                          double a, double inv60d) {
+  // off[0..5] = offsets of i-3, i-2, i-1, i+1, i+2, i+3 relative to o
+  const double qm3 = q[o + off[0]], qm2 = q[o + off[1]], qm1 = q[o + off[2]];
+  const double q0 = q[o], qp1 = q[o + off[3]], qp2 = q[o + off[4]], qp3 = q[o + off[5]];
+  if (a >= 0.0)
+    return (-2.0 * qm3 + 15.0 * qm2 - 60.0 * qm1 + 20.0 * q0 + 30.0 * qp1 - 3.0 * qp2) * inv60d;
+  return (2.0 * qp3 - 15.0 * qp2 + 60.0 * qp1 - 20.0 * q0 - 30.0 * qm1 + 3.0 * qm2) * inv60d;
+}
+
+template <class T>
+__device__ __forceinline__ double ddx_c2(const T* __restrict__ q, size_t o, const size_t* off,
+                                         double inv2d) {
+  return ((double)q[o + off[3]] - (double)q[o + off[2]]) * inv2d;
+}
+
+// One thread per (i, j, k), k in [0, nz] (k = nz only updates w).
+// grid = (ceil(ny / blockDim.y), nx); blockDim.x strides k.
+// OUTMODE 0: out = in + dts * tendency (state update); 1: out = tendency.
+template <class T, int OUTMODE>
+__global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double dts,
+                                              const T* __restrict__ u, const T* __restrict__ v,
+                                              const T* __restrict__ w,
+                                              const T* __restrict__ th,
+                                              const T* __restrict__ dmp_u,
+                                              const T* __restrict__ dmp_v, T* __restrict__ uo,
+                                              T* __restrict__ vo, T* __restrict__ wo,
+                                              T* __restrict__ tho) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * blockDim.y + threadIdx.y;
+  if (j >= g.ny) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nzw = nz + 1;
+  const bool adv = (mask & 1) && s.adv;
+  const bool cor = (mask & 2) && s.cor;
+  const bool dmp = (mask & 4) && s.damp;
+  const bool heat = (mask & 8) && s.heat;
+  // periodic neighbour columns
+  int ix[6], jy[6];
+  const int dd[6] = {-3, -2, -1, 1, 2, 3};
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    int a = i + dd[r];
+    a += (a < 0) ? nx : 0;
+    a -= (a >= nx) ? nx : 0;
+    ix[r] = a;
+    int b = j + dd[r];
+    b += (b < 0) ? ny : 0;
+    b -= (b >= ny) ? ny : 0;
+    jy[r] = b;
+  }
+  const size_t col = (size_t)i * ny + j;
+  size_t offx[6], offy[6], offxw[6], offyw[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    offx[r] = ((size_t)ix[r] * ny + j) * nz - col * nz;
+    offy[r] = ((size_t)i * ny + jy[r]) * nz - col * nz;
+    offxw[r] = ((size_t)ix[r] * ny + j) * nzw - col * nzw;
+    offyw[r] = ((size_t)i * ny + jy[r]) * nzw - col * nzw;
+  }
+  const bool ws5 = (s.adv == 2);
+  for (int k = threadIdx.x; k <= nz; k += blockDim.x) {
+    const size_t o = col * nz + k;
+    const size_t ow = col * nzw + k;
+    if (k < nz) {
+      const double uc = u[o], vc = v[o], thc = th[o];
+      double tu = 0.0, tv = 0.0, tt = 0.0;
+      if (adv) {
+        const double wc = 0.5 * ((double)w[ow] + (double)w[ow + 1]);
+        double czu, czv, czt;
+        if (k == 0) {
+          czu = ((double)u[o + 1] - uc) * s.invdz;
+          czv = ((double)v[o + 1] - vc) * s.invdz;
+          czt = ((double)th[o + 1] - thc) * s.invdz;
+        } else if (k == nz - 1) {
+          czu = (uc - (double)u[o - 1]) * s.invdz;
+          czv = (vc - (double)v[o - 1]) * s.invdz;
+          czt = (thc - (double)th[o - 1]) * s.invdz;
+        } else {
+          czu = ((double)u[o + 1] - (double)u[o - 1]) * s.inv2dz;
+          czv = ((double)v[o + 1] - (double)v[o - 1]) * s.inv2dz;
+          czt = ((double)th[o + 1] - (double)th[o - 1]) * s.inv2dz;
+        }
+        double xu, yu, xv, yv, xt, yt;
+        if (ws5) {
+          xt = ddx_ws5(th, o, offx, uc, s.inv60dx);
+          yt = ddx_ws5(th, o, offy, vc, s.inv60dy);
+          xu = ddx_ws5(u, o, offx, uc, s.inv60dx);
+          yu = ddx_ws5(u, o, offy, vc, s.inv60dy);
+          xv = ddx_ws5(v, o, offx, uc, s.inv60dx);
+          yv = ddx_ws5(v, o, offy, vc, s.inv60dy);
+        } else {
+          xt = ddx_c2(th, o, offx, s.inv2dx);
+          yt = ddx_c2(th, o, offy, s.inv2dy);
+          xu = ddx_c2(u, o, offx, s.inv2dx);
+          yu = ddx_c2(u, o, offy, s.inv2dy);
+          xv = ddx_c2(v, o, offx, s.inv2dx);
+          yv = ddx_c2(v, o, offy, s.inv2dy);
+        }
+        tt = -(uc * xt + vc * yt + wc * (czt + s.dth0[k]));
+        tu = -(uc * xu + vc * yu + wc * czu);
+        tv = -(uc * xv + vc * yv + wc * czv);
+      }
+      if (cor) {
+        const double f = (s.cor == 2) ? s.fy[j] : s.f0;
+        tu = tu + f * (vc - s.v_env);
+        tv = tv + (-f) * (uc - s.u_env);
+      }
+      if (dmp) {
+        tu = tu + (double)dmp_u[o];
+        tv = tv + (double)dmp_v[o];
+      }
+      if (heat) tt = tt + s.heat_r[col] * s.heat_z[k];
+      if (OUTMODE == 0) {
+        uo[o] = (T)(uc + dts * tu);
+        vo[o] = (T)(vc + dts * tv);
+        tho[o] = (T)(thc + dts * tt);
+      } else {
+        uo[o] = (T)tu;
+        vo[o] = (T)tv;
+        tho[o] = (T)tt;
+      }
+    }
+    // w on half level k
+    {
+      const double wk = w[ow];
+      double tw = 0.0;
+      if (adv && k > 0 && k < nz) {
+        const double uh = 0.5 * ((double)u[o - 1] + (double)u[o]);
+        const double vh = 0.5 * ((double)v[o - 1] + (double)v[o]);
+        const double czw = ((double)w[ow + 1] - (double)w[ow - 1]) * s.inv2dz;
+        double xw, yw;
+        if (ws5) {
+          xw = ddx_ws5(w, ow, offxw, uh, s.inv60dx);
+          yw = ddx_ws5(w, ow, offyw, vh, s.inv60dy);
+        } else {
+          xw = ddx_c2(w, ow, offxw, s.inv2dx);
+          yw = ddx_c2(w, ow, offyw, s.inv2dy);
+        }
+        tw = -(uh * xw + vh * yw + wk * czw);
+      }
+      if (OUTMODE == 0)
+        wo[ow] = (T)(wk + dts * tw);
+      else
+        wo[ow] = (T)tw;
+    }
+  }
+}
+
+// dw_dt of the buoyancy component (nz+1 levels).
+template <class T>
+__global__ void k_buoyancy(GridK g, const T* __restrict__ th, const double* __restrict__ theta0,
+                           T* __restrict__ dw) {
+  const size_t ncol = (size_t)g.nx * g.ny;
+  const int nzw = g.nz + 1;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ncol * nzw;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t col = e / nzw;
+    const int k = (int)(e - col * nzw);
+    dw[e] = (T)bhalf(th + col * g.nz, k, g.nz, theta0);
+  }
+}
+
+// Vertical part of apply_operator plus rho * horizontal Laplacian term
+// (poisson.py:171-200): out = rho * lap + vert(phi).
+template <class T>
+__global__ void k_apply_vert(GridK g, const T* __restrict__ phi, const T* __restrict__ lap,
+                             const double* __restrict__ rho, const double* __restrict__ rhoh,
+                             T* __restrict__ out) {
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  const double dz2 = g.dz * g.dz;
+  const int nz = g.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % nz);
+    const double p = phi[e];
+    double vert;
+    const double fu = (k < nz - 1) ? rhoh[k + 1] * ((double)phi[e + 1] - p) : 0.0;
+    const double fl = (k > 0) ? rhoh[k] * (p - (double)phi[e - 1]) : 0.0;
+    if (k == 0)
+      vert = fu / dz2;
+    else if (k == nz - 1)
+      vert = -fl / dz2;
+    else
+      vert = (fu - fl) / dz2;
+    out[e] = (T)(rho[k] * (double)lap[e] + vert);
+  }
+}
+
+// k^2-weighted copy for the horizontal Laplacian: out = -k^2 * in.
+template <class T>
+__global__ void k_neg_ksq(GridK g, const cplx<T>* __restrict__ in, const double* __restrict__ kxd,
+                          const double* __restrict__ kyd, cplx<T>* __restrict__ out) {
+  const size_t n = (size_t)g.nxh * g.ny * g.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t col = e / g.nz;
+    const int kx = (int)(col / g.ny), ky = (int)(col - (size_t)kx * g.ny);
+    const double k2 = kxd[kx] * kxd[kx] + kyd[ky] * kyd[ky];
+    out[e] = scl(in[e], (T)(-k2));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Step diagnostics (integrator.py:287-295): max|u|, max|v|, max|w|, max|th|,
+// sum(phi), min/max phi[:, :, 0].  Two-stage deterministic reduction.
+// ---------------------------------------------------------------------------
+struct DiagPart {
+  double mu, mv, mw, mt, sp, pmin, pmax, pad;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restrict__ u,
+                                                      const T* __restrict__ v,
+                                                      const T* __restrict__ w,
+                                                      const T* __restrict__ th,
+                                                      const T* __restrict__ phi, DiagPart* part) {
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  const size_t nw = (size_t)g.nx * g.ny * (g.nz + 1);
+  double mu = 0, mv = 0, mw = 0, mt = 0, sp = 0, pmin = INFINITY, pmax = -INFINITY;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += stride) {
+    mu = fmax(mu, fabs((double)u[e]));
+    mv = fmax(mv, fabs((double)v[e]));
+    mt = fmax(mt, fabs((double)th[e]));
+    const double p = phi[e];
+    sp += p;
+    if (e % g.nz == 0) {
+      pmin = fmin(pmin, p);
+      pmax = fmax(pmax, p);
+    }
+  }
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nw; e += stride)
+    mw = fmax(mw, fabs((double)w[e]));
+  __shared__ double red[8][8];
+  double vals[7] = {mu, mv, mw, mt, sp, pmin, pmax};
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    double x = vals[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, x, o);
+      x = (q == 4) ? x + y : (q == 5 ? fmin(x, y) : fmax(x, y));
+    }
+    vals[q] = x;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int q = 0; q < 7; ++q) red[wid][q] = vals[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw_ = blockDim.x >> 5;
+    double r[7];
+    for (int q = 0; q < 7; ++q) r[q] = red[0][q];
+    for (int ww = 1; ww < nw_; ++ww)
+      for (int q = 0; q < 7; ++q)
+        r[q] = (q == 4) ? r[q] + red[ww][q]
+                        : (q == 5 ? fmin(r[q], red[ww][q]) : fmax(r[q], red[ww][q]));
+    DiagPart p;
+    p.mu = r[0];
+    p.mv = r[1];
+    p.mw = r[2];
+    p.mt = r[3];
+    p.sp = r[4];
+    p.pmin = r[5];
+    p.pmax = r[6];
+    p.pad = 0;
+    part[blockIdx.x] = p;
+  }
+}
+
+__global__ void k_diag_final(const DiagPart* part, int np, double ncell, double* diag) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double mu = 0, mv = 0, mw = 0, mt = 0, sp = 0, pmin = INFINITY, pmax = -INFINITY;
+  for (int b = 0; b < np; ++b) {
+    mu = fmax(mu, part[b].mu);
+    mv = fmax(mv, part[b].mv);
+    mw = fmax(mw, part[b].mw);
+    mt = fmax(mt, part[b].mt);
+    sp += part[b].sp;
+    pmin = fmin(pmin, part[b].pmin);
+    pmax = fmax(pmax, part[b].pmax);
+  }
+  const double mean = sp / ncell;
+  diag[0] = mu;
+  diag[1] = mv;
+  diag[2] = mw;
+  diag[3] = mt;
+  diag[4] = pmin - mean;
+  diag[5] = pmax - mean;
+}
+
+}  // namespace ob

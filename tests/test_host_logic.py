@@ -1,0 +1,115 @@
+"""Host-side logic of the B200 package that needs no GPU: configuration
+compilation, reference-identical host tables, guards and error types."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import lh82 as O
+
+
+def test_base_state_and_constants_identical():
+    from oraclev8_b200.production_config import build_base_state
+    for nz, Lz in ((32, 16e3), (64, 16e3), (80, 20e3), (7, 3e3)):
+        a = build_base_state(nz, Lz)
+        b = O.build_base_state(nz, Lz)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def test_coriolis_profile_identical():
+    from oraclev8_b200.solver import CoriolisComponent
+    for kw in (dict(f=4.99e-5, beta=2.15e-11, periodic_taper=True),
+               dict(f=6.164e-5, periodic_taper=False),
+               dict(f=3.7e-5, periodic_taper=True, y0=1e5)):
+        c = CoriolisComponent(mode="beta_plane", Ly=2.56e6, ny=128, **kw)
+        ref = O.coriolis_profile(kw["f"], "beta_plane", kw.get("beta"), 2.56e6, 128,
+                                 kw.get("y0"), kw["periodic_taper"])
+        assert np.array_equal(c.f_y, ref)
+    with pytest.raises(ValueError):
+        CoriolisComponent(mode="beta_plane")
+
+
+def test_heating_factors_reproduce_reference_field():
+    from oraclev8_b200.solver import DiabaticHeatingComponent
+    kw = dict(Q_max=3.0 / 3600.0, r_eyewall=40e3, width_r=math.sqrt(2.0) * 15e3, z_peak=6e3,
+              width_z=math.sqrt(2.0) * 2e3, nx=24, ny=20, nz=9, Lx=240e3, Ly=200e3, Lz=16e3)
+    h = DiabaticHeatingComponent(**kw)
+    r, z = h.heat_factors
+    assert np.array_equal(r[:, :, None] * z[None, None, :], O.heating_field(**kw))
+
+
+def _cfg(**extra):
+    from oraclev8_b200.solver import (AdvectionComponent, AnelasticProjection,
+                                      BuoyancyComponent, CoriolisComponent,
+                                      LH82AnelasticEquationSet, OperatorConfig)
+    from oraclev8_b200.grid import LorenzStaggering
+    kw = dict(equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
+              buoyancy=BuoyancyComponent(),
+              projection=AnelasticProjection(32, 24, 8, 640e3, 480e3, 16e3),
+              advection=AdvectionComponent(32, 24, 8, 640e3, 480e3, 16e3, scheme="upwind5h"),
+              coriolis=CoriolisComponent(f=4.99e-5, mode="beta_plane", beta=2.15e-11,
+                                         Ly=480e3, ny=24, periodic_taper=True))
+    kw.update(extra)
+    return OperatorConfig(**kw)
+
+
+def test_compile_config_maps_every_slot():
+    from oraclev8_b200 import _lib as L
+    from oraclev8_b200.solver.integrator import compile_config
+    from oraclev8_b200.solver import HelmholtzDivergenceDampingComponent, DiabaticHeatingComponent
+    from oraclev8_b200.production_config import BaseState
+    cfg = _cfg(divergence_damping=HelmholtzDivergenceDampingComponent(0.5, 640e3, 480e3, 32, 24),
+               diabatic_heating=DiabaticHeatingComponent(1e-3, 40e3, 20e3, 6e3, 3e3, 32, 24, 8,
+                                                         640e3, 480e3, 16e3))
+    spec = compile_config(cfg, BaseState(8, 16e3), "fp32")
+    assert (spec.nx, spec.ny, spec.nz) == (32, 24, 8)
+    assert spec.buoyancy and spec.projection and spec.damping and spec.heating
+    assert spec.advection == L.OB_ADV_UPWIND5H and spec.coriolis == L.OB_COR_BETA
+    assert spec.epsilon == 0.5 and spec.f_y.shape == (24,) and spec.precision == "fp32"
+
+
+def test_unsupported_components_raise_and_guards():
+    from oraclev8_b200.solver import (NewtonianCoolingComponent, PressureGradientComponent,
+                                      AdvectionComponent)
+    from oraclev8_b200.solver.integrator import compile_config
+    from oraclev8_b200.production_config import BaseState
+    with pytest.raises(NotImplementedError):
+        NewtonianCoolingComponent(tau=1800.0)
+    with pytest.raises(ValueError):
+        _cfg(pressure_gradient=PressureGradientComponent(32, 24, 8, 1, 1, 1))
+    cfg = _cfg(pressure_gradient=PressureGradientComponent(32, 24, 8, 1, 1, 1),
+               _unsafe_pgc_override=True)
+    with pytest.raises(NotImplementedError):
+        compile_config(cfg, BaseState(8, 16e3), "fp64")
+    with pytest.raises(ValueError):
+        AdvectionComponent(scheme="weno")
+
+
+def test_operator_config_slot_order_and_stages():
+    cfg = _cfg()
+    names = [c.name for c in cfg.active_components()]
+    assert names == ["buoyancy", "anelastic_projection", "advection", "coriolis"]
+    assert [c.name for c in cfg.fast_components()] == ["buoyancy"]
+    assert [c.name for c in cfg.slow_components()] == ["advection", "coriolis"]
+    d = cfg.to_log_dict()
+    assert d["n_pre_projection"] == 1 and d["n_slow"] == 2 and d["n_projection"] == 1
+
+
+def test_product_path_has_no_cpu_fallback():
+    """Without a CUDA device the backend refuses to run (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from oraclev8_b200.solver import RK3Integrator
+    from oraclev8_b200.production_config import BaseState
+    with pytest.raises(RuntimeError):
+        RK3Integrator(_cfg(), BaseState(8, 16e3))
+
+
+def test_product_package_never_imports_oracle():
+    import pathlib
+    import re
+    pkg = pathlib.Path(__file__).resolve().parents[1] / "oraclev8_b200"
+    for f in pkg.rglob("*.py"):
+        assert not re.search(r"^\s*(from|import)\s+oracle\b", f.read_text(), re.M), f
