@@ -1,0 +1,508 @@
+"""Benchmark of the LH82 anelastic RK3 step (cell-updates/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+                    [--workload config1|config0|config2] [--impl b200|reference]
+
+Default workload: the mid-size single run — 512 x 512 x 64 cells, dx = 5 km,
+0-16 km (dz = 250 m), beta-plane at 20N (f0 = 4.99e-5, beta = 2.15e-11,
+periodic taper), Holland vortex Vmax 50 m/s / Rmax 40 km / B 1.6 with wind
+decaying linearly to zero at 12 km, eyewall heating ring (3 K/h, r0 40 km,
+sigma_r 15 km, z0 6 km, sigma_z 2 km), seeded +-0.05 K theta' noise,
+WS5 advection, buoyancy, projection, dt = 20 s.  Synthetic inputs (the
+reference has no dataset); every field is > L2-sized (64-134 MB per field),
+so consecutive steps stream from HBM.
+
+One "step" = one full RK3Integrator.step: two Strang slow half steps (fused
+WS5 + Coriolis + heating tendency and forward Euler), three fast stages, five
+anelastic projections (FFT x/y + Thomas z + correction) and the device-side
+step diagnostics.  N > 1: N independent replicas, one per GPU (the path
+partitions into independent runs; no collective on the data path).
+
+--impl reference times the reference algorithm on the host CPU (the NumPy
+oracle; the reference is pure Python and cannot be installed on the GPU host)
+on a bounded sample of the same workload: the same 512 x 512 horizontal grid
+with 8 levels, one independent sample run per host core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "config1": dict(nx=512, ny=512, nz=64, dx=5e3, Lz=16e3, dt=20.0,
+                    vortex=dict(Vmax=50.0, Rmax=40e3, B=1.6, f=4.99e-5),
+                    coriolis=dict(f=4.99e-5, mode="beta_plane", beta=2.15e-11,
+                                  periodic_taper=True),
+                    heating=dict(Q_max=3.0 / 3600.0, r_eyewall=40e3,
+                                 width_r=math.sqrt(2.0) * 15e3, z_peak=6e3,
+                                 width_z=math.sqrt(2.0) * 2e3),
+                    noise_seed=20261203),
+    "config0": dict(nx=128, ny=128, nz=32, dx=20e3, Lz=16e3, dt=60.0,
+                    vortex=dict(Vmax=40.0, Rmax=50e3, B=1.5, f=4.99e-5),
+                    coriolis=dict(f=4.99e-5, mode="beta_plane", beta=2.15e-11,
+                                  periodic_taper=True), heating=None, noise_seed=None),
+    "config2": dict(nx=1024, ny=1024, nz=80, dx=4e3, Lz=20e3, dt=15.0,
+                    vortex=dict(Vmax=55.0, Rmax=30e3, B=1.8,
+                                f=2 * 7.2921e-5 * math.sin(math.radians(25.0)), u_env=-3.0),
+                    coriolis=dict(f=2 * 7.2921e-5 * math.sin(math.radians(25.0)),
+                                  mode="beta_plane",
+                                  beta=2 * 7.2921e-5 * math.cos(math.radians(25.0)) / 6.371e6,
+                                  periodic_taper=True, u_env=-3.0),
+                    heating=None, noise_seed=None),
+}
+# Algorithmic field passes per cell-update of one step (one read or write of
+# an nx*ny*nz field = 1 pass; w counts as nz; a half-spectrum complex field
+# as 1): slow halves 2 x 8, fast stages 3 x 1, projections 5 x 14 = 89, plus
+# 2 (heating factors read per slow half) when heating is on.
+PASSES_BASE, PASSES_HEAT = 89, 2
+SAMPLE_NZ = 8  # levels of the bounded CPU sample
+
+
+def grid_of(w):
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    return nx, ny, nz, nx * w["dx"], ny * w["dx"], w["Lz"]
+
+
+# ---------------------------------------------------------------------------
+# configuration builders
+# ---------------------------------------------------------------------------
+
+def b200_integrator(w, precision):
+    from oraclev8_b200.grid import LorenzStaggering
+    from oraclev8_b200.production_config import BaseState
+    from oraclev8_b200.solver import (AdvectionComponent, AnelasticProjection,
+                                      BuoyancyComponent, CoriolisComponent,
+                                      DiabaticHeatingComponent, LH82AnelasticEquationSet,
+                                      OperatorConfig, RK3Integrator)
+    nx, ny, nz, Lx, Ly, Lz = grid_of(w)
+    base = BaseState(nz, Lz)
+    kw = dict(equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
+              buoyancy=BuoyancyComponent(),
+              projection=AnelasticProjection(nx, ny, nz, Lx, Ly, Lz),
+              advection=AdvectionComponent(nx, ny, nz, Lx, Ly, Lz, scheme="upwind5h"),
+              coriolis=CoriolisComponent(Ly=Ly, ny=ny, **w["coriolis"]))
+    if w["heating"]:
+        kw["diabatic_heating"] = DiabaticHeatingComponent(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly,
+                                                          Lz=Lz, **w["heating"])
+    return RK3Integrator(OperatorConfig(**kw), base, precision=precision), base
+
+
+def host_initial_state(w, base):
+    from oraclev8_b200.vortex_init import HollandVortexInit
+    nx, ny, nz, Lx, Ly, Lz = grid_of(w)
+    s = HollandVortexInit(**w["vortex"], wind_decay_top=12e3).build_state(
+        nx, ny, nz, Lx, Ly, base, device=False)
+    if w["noise_seed"] is not None:
+        rng = np.random.default_rng(w["noise_seed"])
+        s.theta_prime = s.theta_prime + rng.uniform(-0.05, 0.05, (nx, ny, nz))
+    return s
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample (same nx, ny; SAMPLE_NZ levels)
+# ---------------------------------------------------------------------------
+
+def _sample_integrator(w):
+    from oracle import lh82 as O
+    nx, ny = w["nx"], w["ny"]
+    nz = SAMPLE_NZ
+    Lz = nz * (w["Lz"] / w["nz"])
+    Lx, Ly = nx * w["dx"], ny * w["dx"]
+    z, rho0, th0 = O.build_base_state(nz, Lz)
+    cor = dict(w["coriolis"], Ly=Ly, ny=ny)
+    cfg = O.StepConfig(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, Lz=Lz, coriolis=cor,
+                       heating=w["heating"])
+    s = O.Holland(**w["vortex"], wind_decay_top=12e3).build_state(nx, ny, nz, Lx, Ly, z,
+                                                                   rho0, th0)
+    return O.Integrator(cfg, z, rho0, th0), s, nx * ny * nz
+
+
+def _worker(conn, wname):
+    os.environ["OMP_NUM_THREADS"] = "1"
+    integ, s, cells = _sample_integrator(WORKLOADS[wname])
+    dt = WORKLOADS[wname]["dt"]
+    n = 0
+    while True:
+        cmd = conn.recv()
+        if cmd is None:
+            break
+        t0 = time.perf_counter()
+        s, _ = integ.step(s, dt, n)
+        n += 1
+        conn.send(time.perf_counter() - t0)
+
+
+def cpu_sample_rate(wname, procs, steps, warmup):
+    """Independent sample runs, one per process; returns (cell-updates/s list,
+    cells per sample)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    pipes, ps = [], []
+    for _ in range(procs):
+        a, b = ctx.Pipe()
+        p = ctx.Process(target=_worker, args=(b, wname), daemon=True)
+        p.start()
+        pipes.append(a)
+        ps.append(p)
+    cells = WORKLOADS[wname]["nx"] * WORKLOADS[wname]["ny"] * SAMPLE_NZ
+    rates = []
+    try:
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            for c in pipes:
+                c.send(1)
+            for c in pipes:
+                c.recv()
+            el = time.perf_counter() - t0
+            if i >= warmup:
+                rates.append(procs * cells / el)
+    finally:
+        for c in pipes:
+            try:
+                c.send(None)
+            except Exception:
+                pass
+        for p in ps:
+            p.join(timeout=10)
+    return rates, cells
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def mem_available_gb():
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable"):
+                return int(ln.split()[1]) / 1e6
+    except Exception:
+        pass
+    return 16.0
+
+
+def reference_procs():
+    return max(1, min(host_cores(), 32, int(mem_available_gb() // 2)))
+
+
+# ---------------------------------------------------------------------------
+# per-kernel algorithmic bytes (the kernel's own I/O contract)
+# ---------------------------------------------------------------------------
+
+def kernel_bytes(w, S, fast_stages=3, slow_projections=2):
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    n = nx * ny * nz
+    nw = nx * ny * (nz + 1)
+    ns = (nx // 2 + 1) * ny * nz  # complex half-spectrum elements
+    c = 2 * S
+    P = slow_projections + fast_stages
+    fx = (slow_projections * (2 * n * S + nw * S) + fast_stages * (3 * n * S + nw * S)) / P \
+        + 2 * ns * c
+    ix = 2 * ns * c + (slow_projections * (2 * (2 * n + nw) * S + n * S)
+                       + fast_stages * ((3 * n + nw) * S + (3 * n + nw) * S)) / P
+    heat = (nx * ny + nz) * 8 if w["heating"] else 0
+    return {
+        "fx": fx, "fy": 3 * ns * c, "thomas": 2 * ns * c, "iy": 3 * ns * c, "ix": ix,
+        "slow": 2 * (3 * n + nw) * S + heat, "diag": (4 * n + nw) * S,
+    }
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(wname, precision):
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return {}
+    try:
+        return json.loads(p.read_text()).get(f"{wname}/{precision}", {})
+    except Exception:
+        return {}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    w = WORKLOADS[args.workload]
+    from oraclev8_b200.solver import State
+    integ, base = b200_integrator(w, args.precision)
+    hs = host_initial_state(w, base)
+    dt = w["dt"]
+    dtype = integ.dtype
+    S = 8 if args.precision == "fp64" else 4
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def to_dev(a):
+        return torch.as_tensor(a, dtype=dtype).to(dev)
+
+    st = State(to_dev(hs.u), to_dev(hs.v), to_dev(hs.w), to_dev(hs.theta_prime),
+               to_dev(hs.projection_potential), 0.0)
+    for _ in range(args.warmup):
+        integ.step_(st, dt, want_diag=True)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    plan = integ.plan
+    plan.profile(True)
+    l0 = plan.launches
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        integ.step_(st, dt, want_diag=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = plan.launches - l0
+    prof = plan.profile_read()
+    plan.profile(False)
+    clk = clocks.stop()
+    if not bool(torch.isfinite(st.u).all()):
+        raise RuntimeError("non-finite state after the timed steps")
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = w["nx"] * w["ny"] * w["nz"]
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # ---- e2e through the public API with host buffers ---------------------
+    pinned = [torch.empty(tuple(x.shape), dtype=dtype, pin_memory=True)
+              for x in (st.u, st.v, st.w, st.theta_prime, st.projection_potential)]
+    outs = [torch.empty_like(p, pin_memory=True) for p in pinned]
+    for p, x in zip(pinned, (st.u, st.v, st.w, st.theta_prime, st.projection_potential)):
+        p.copy_(x)
+    h2d = sum(p.numel() * p.element_size() for p in pinned)
+    devbufs = [torch.empty_like(x) for x in (st.u, st.v, st.w, st.theta_prime,
+                                             st.projection_potential)]
+    k_e2e = args.steps
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s_in = None
+    for i in range(k_e2e):
+        for d_, p in zip(devbufs, pinned):
+            d_.copy_(p, non_blocking=True)
+        s_in = State(*devbufs, 0.0)
+        s_out, diag = integ.step(s_in, dt, step_number=i)  # reads diagnostics (host sync)
+        for o, x in zip(outs, (s_out.u, s_out.v, s_out.w, s_out.theta_prime,
+                               s_out.projection_potential)):
+            o.copy_(x, non_blocking=True)
+        torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * cells * k_e2e / t_e2e
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    peak, peak_kind = load_peaks()
+    kb = kernel_bytes(w, S)
+    dom = max((c for c in prof if prof[c][1] > 0 and c in kb), key=lambda c: prof[c][0])
+    dms, dn = prof[dom]
+    ach = kb[dom] / (dms / dn / 1e3) / 1e9
+    traffic = load_traffic(args.workload, args.precision).get(dom)
+    passes = PASSES_BASE + (PASSES_HEAT if w["heating"] else 0)
+    step_gbs = passes * S * cells * args.steps / (ms / 1e3) / 1e9
+    line = {
+        "metric": "cell-updates/s (RK3 step)",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic (seeded Holland vortex + theta' noise; no dataset in the reference)",
+        "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step, "
+                               f"WS5 + beta-plane + buoyancy + projection"
+                               + (" + heating" if w["heating"] else "") + f", dt={dt}s",
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (>= 67 MB per field, 5 fields)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "bytes_per_launch": kb[dom],
+                     "avg_launch_ms": dms / dn},
+        "step_roofline": {"passes_per_cell": passes, "achieved": step_gbs, "peak": peak,
+                          "unit": "GB/s", "frac": step_gbs / peak},
+        "kernels_ms_per_step": {c: prof[c][0] / args.steps for c in prof if prof[c][1]},
+        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d + 8 * 6,
+                "note": "public RK3Integrator.step per step: full state H2D from pinned host, "
+                        "step, StepDiagnostics read, full state D2H"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rates, sc = cpu_sample_rate(args.workload, 1, 1, 1)
+        line["cpu_baseline"] = {
+            "value": statistics.median(rates), "unit": "cell-updates/s", "cores": 1,
+            "kind": "port",
+            "sample": f"oracle (NumPy restatement of the reference, FP64) on "
+                      f"{w['nx']}x{w['ny']}x{SAMPLE_NZ} with the same physics, 1 warm-up + "
+                      f"1 timed step, 1 process"}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    procs = reference_procs()
+    rates, sc = cpu_sample_rate(args.workload, procs, args.steps, args.warmup)
+    v = statistics.median(rates)
+    cells = w["nx"] * w["ny"] * w["nz"]
+    line = {
+        "impl": "reference",
+        "metric": "cell-updates/s (RK3 step)",
+        "value": v,
+        "unit": "cell-updates/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": cells / v * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step",
+                   "parallelism": f"{procs} host processes"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "port",
+                         "sample": f"{procs} independent oracle runs (NumPy restatement of the "
+                                   f"reference, FP64), each {w['nx']}x{w['ny']}x{SAMPLE_NZ} "
+                                   f"with the workload's physics; one step per process per "
+                                   f"bench step"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

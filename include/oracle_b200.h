@@ -156,6 +156,28 @@ int oracle_b200_tendency(OraclePlan *plan, int mask, const OracleStatePtrs *stat
 /* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
 int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);
 
+/* Number of kernels this plan has launched since creation (launch accounting
+ * for benchmarks).  No counterpart in the reference (it launches through CuPy). */
+long oracle_b200_launch_count(const OraclePlan *plan);
+
+/* Per-kernel-class device timing for benchmarks (no counterpart in the
+ * reference, whose ORACLE_PROF timers are host wall clocks,
+ * integrator.py:59-69).  oracle_b200_profile(plan, 1) clears previous marks
+ * and brackets every later launch with CUDA events on its stream;
+ * oracle_b200_profile_read synchronises on them and returns the summed
+ * milliseconds and launch counts per class, index OB_PROF_*. */
+#define OB_PROF_FX 0      /* x-pencil forward FFT + divergence assembly */
+#define OB_PROF_FY 1      /* y-pencil forward FFT */
+#define OB_PROF_THOMAS 2  /* batched tridiagonal solve */
+#define OB_PROF_IY 3      /* y-pencil inverse FFT + d/dy */
+#define OB_PROF_IX 4      /* x-pencil inverse FFT + velocity correction */
+#define OB_PROF_SLOW 5    /* fused slow tendency + forward Euler */
+#define OB_PROF_DIAG 6    /* step diagnostics reductions */
+#define OB_PROF_OTHER 7
+#define OB_PROF_CLASSES 8
+int oracle_b200_profile(OraclePlan *plan, int enable);
+int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
+
 const char *oracle_b200_last_error(void);
 int oracle_b200_version(void);
 

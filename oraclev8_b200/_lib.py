@@ -27,8 +27,10 @@ EXPORTS = (
     "oracle_b200_step", "oracle_b200_project", "oracle_b200_divergence",
     "oracle_b200_phi_gradient", "oracle_b200_poisson_solve", "oracle_b200_apply_operator",
     "oracle_b200_buoyancy", "oracle_b200_tendency", "oracle_b200_read_diag",
-    "oracle_b200_last_error", "oracle_b200_version",
+    "oracle_b200_last_error", "oracle_b200_version", "oracle_b200_launch_count",
+    "oracle_b200_profile", "oracle_b200_profile_read",
 )
+PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other")
 
 
 class GridDesc(ctypes.Structure):
@@ -80,6 +82,9 @@ def load(path: Path | None = None):
         "oracle_b200_read_diag": ([vp, POINTER(c_double), c_int, vp], c_int),
         "oracle_b200_last_error": ([], ctypes.c_char_p),
         "oracle_b200_version": ([], c_int),
+        "oracle_b200_launch_count": ([vp], ctypes.c_long),
+        "oracle_b200_profile": ([vp, c_int], c_int),
+        "oracle_b200_profile_read": ([vp, POINTER(c_double), POINTER(ctypes.c_long), c_int], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -121,6 +121,20 @@ class Plan:
         L.check(self.lib.oracle_b200_step(self.handle, ctypes.byref(ins), ctypes.byref(outs),
                                           float(dt), int(want_diag), self._stream()))
 
+    @property
+    def launches(self) -> int:
+        return int(self.lib.oracle_b200_launch_count(self.handle))
+
+    def profile(self, enable: bool) -> None:
+        L.check(self.lib.oracle_b200_profile(self.handle, int(enable)))
+
+    def profile_read(self) -> dict:
+        n = len(L.PROF_CLASSES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_long * n)()
+        L.check(self.lib.oracle_b200_profile_read(self.handle, ms, cnt, n))
+        return {c: (float(ms[i]), int(cnt[i])) for i, c in enumerate(L.PROF_CLASSES)}
+
     def read_diag(self) -> np.ndarray:
         buf = (ctypes.c_double * L.DIAG_COUNT)()
         L.check(self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream()))

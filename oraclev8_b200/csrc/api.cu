@@ -117,6 +117,14 @@ struct OraclePlan {
   int nparts = 0;
   std::vector<void*> allocs;
   size_t scratch_bytes = 0;
+  // launch accounting and optional per-kernel-class event timing
+  long launches = 0;
+  int profiling = 0;
+  struct Mark {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
 };
 
 namespace {
@@ -193,6 +201,29 @@ ThomasK thomas_args(const OraclePlan* p) {
   return t;
 }
 
+// Brackets one kernel launch: counts it and, when profiling is on, records a
+// pair of events on the launch stream so per-class device time can be summed.
+struct Launch {
+  OraclePlan* p;
+  cudaStream_t st;
+  int cls;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Launch(OraclePlan* p_, int cls_, cudaStream_t st_) : p(p_), st(st_), cls(cls_) {
+    p->launches++;
+    if (p->profiling) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~Launch() {
+    if (a) {
+      cudaEventRecord(b, st);
+      p->marks.push_back({cls, a, b});
+    }
+  }
+};
+
 dim3 grid_x(const OraclePlan* p, int zc) { return dim3(p->g.ny, (p->g.nz + zc - 1) / zc); }
 dim3 grid_y(const OraclePlan* p, int zc) { return dim3(p->g.nxh, (p->g.nz + zc - 1) / zc); }
 
@@ -223,34 +254,34 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   }
   const bool stage = stage_sdt >= 0.0;
   if (stage)
-    k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+    { Launch L_(p, 0, st); k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
         g, p->px, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2, nullptr);
+        (const C*)p->twx, S1, S2, nullptr); }
   else
-    k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+    { Launch L_(p, 0, st); k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
         g, p->px, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2, nullptr);
+        (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
-  k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr);
+  { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   const long ncols = (long)g.nxh * g.ny;
-  k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+  { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
                              smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
-                                                   slot_d);
+                                                   slot_d); }
   OB_LAUNCHED();
-  k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2);
+  { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
   if (stage)
-    k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+    { Launch L_(p, 4, st); k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
         g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th,
-        stage_sdt, p->theta0, uo, vo, wo, phio);
+        stage_sdt, p->theta0, uo, vo, wo, phio); }
   else
-    k_ix<T, IX_CORRECT><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+    { Launch L_(p, 4, st); k_ix<T, IX_CORRECT><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
         g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th, 0.0,
-        p->theta0, uo, vo, wo, phio);
+        p->theta0, uo, vo, wo, phio); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -262,20 +293,20 @@ int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStrea
   const GridK g = p->g;
   C* S1 = (C*)p->S1;
   C* S2 = (C*)p->S2;
-  k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
+  { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
       g, p->px, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-      (const C*)p->twx, S1, S2, nullptr);
+      (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   const double scale = -(p->epsilon / dt_slow) / ((double)g.nx * (double)g.ny);
-  k_fy<T, FY_HELM><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2);
+  { Launch L_(p, 1, st); k_fy<T, FY_HELM><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2); }
   OB_LAUNCHED();
-  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-      g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2);
+  { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
-  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+  { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
       g, p->px, p->zc_ix, 2, S1, S2, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
-      nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr);
+      nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -307,8 +338,8 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
               const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
   dim3 blk(32, 8);
   dim3 grd((p->g.ny + 7) / 8, p->g.nx);
-  k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
-                                      (const T*)p->Dv, uo, vo, wo, tho);
+  { Launch L_(p, 5, st); k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                      (const T*)p->Dv, uo, vo, wo, tho); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -323,10 +354,10 @@ int copy_field(void* dst, const void* src, size_t n, cudaStream_t st) {
 template <class T>
 int diag_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th, const T* phi,
               cudaStream_t st) {
-  k_diag_partial<T><<<p->nparts, 256, 0, st>>>(p->g, u, v, w, th, phi, p->parts);
+  { Launch L_(p, 6, st); k_diag_partial<T><<<p->nparts, 256, 0, st>>>(p->g, u, v, w, th, phi, p->parts); }
   OB_LAUNCHED();
-  k_diag_final<<<1, 32, 0, st>>>(p->parts, p->nparts,
-                                 (double)p->g.nx * p->g.ny * p->g.nz, p->diag);
+  { Launch L_(p, 6, st); k_diag_final<<<1, 32, 0, st>>>(p->parts, p->nparts,
+                                 (double)p->g.nx * p->g.ny * p->g.nz, p->diag); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -430,20 +461,20 @@ int divergence_impl(OraclePlan* p, const T* u, const T* v, const T* w, T* d, cud
   C* S1 = (C*)p->S1;
   C* S2 = (C*)p->S2;
   C* S3 = (C*)p->S3;
-  k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+  { Launch L_(p, 0, st); k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
       g, p->px, p->zc_fx, 3, u, v, w, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-      (const C*)p->twx, S1, S2, nullptr);
+      (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
-  k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr);
+  { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
-  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+  { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 1, S3, nullptr, p->ky, (const C*)p->twy,
-      1.0 / ((double)g.nx * (double)g.ny), S1, nullptr);
+      1.0 / ((double)g.nx * (double)g.ny), S1, nullptr); }
   OB_LAUNCHED();
-  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+  { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
       g, p->px, p->zc_ix, 1, S1, nullptr, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
-      nullptr, nullptr, 0.0, p->theta0, d, nullptr, nullptr, nullptr);
+      nullptr, nullptr, 0.0, p->theta0, d, nullptr, nullptr, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -453,13 +484,13 @@ template <class T>
 int fwd_scalar(OraclePlan* p, const T* f, cudaStream_t st) {
   using C = cplx<T>;
   const GridK g = p->g;
-  k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
+  { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
       g, p->px, p->zc_fx, 1, f, nullptr, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0,
-      p->kx, (const C*)p->twx, (C*)p->S1, nullptr, nullptr);
+      p->kx, (const C*)p->twx, (C*)p->S1, nullptr, nullptr); }
   OB_LAUNCHED();
-  k_fy<T, FY_FIELDS><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+  { Launch L_(p, 1, st); k_fy<T, FY_FIELDS><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
       g, p->py, p->zc_fy, 1, (C*)p->S1, nullptr, p->kx, p->ky, (const C*)p->twy, 1.0,
-      (C*)p->S3, nullptr);
+      (C*)p->S3, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -469,13 +500,13 @@ template <class T>
 int inv_scalar(OraclePlan* p, double scale, T* out, cudaStream_t st) {
   using C = cplx<T>;
   const GridK g = p->g;
-  k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+  { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 1, (C*)p->S3, nullptr, p->ky, (const C*)p->twy, scale, (C*)p->S1,
-      nullptr);
+      nullptr); }
   OB_LAUNCHED();
-  k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+  { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
       g, p->px, p->zc_ix, 1, (C*)p->S1, nullptr, nullptr, p->kx, (const C*)p->twx, nullptr,
-      nullptr, nullptr, nullptr, 0.0, p->theta0, out, nullptr, nullptr, nullptr);
+      nullptr, nullptr, nullptr, 0.0, p->theta0, out, nullptr, nullptr, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -485,13 +516,13 @@ int gradient_impl(OraclePlan* p, const T* phi, T* gx, T* gy, T* gz, cudaStream_t
   using C = cplx<T>;
   const GridK g = p->g;
   RC(fwd_scalar<T>(p, phi, st));
-  k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+  { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 2, (C*)p->S3, nullptr, p->ky, (const C*)p->twy,
-      1.0 / ((double)g.nx * (double)g.ny), (C*)p->S1, (C*)p->S2);
+      1.0 / ((double)g.nx * (double)g.ny), (C*)p->S1, (C*)p->S2); }
   OB_LAUNCHED();
-  k_ix<T, IX_GRAD><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
+  { Launch L_(p, 4, st); k_ix<T, IX_GRAD><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
       g, p->px, p->zc_ix, 0, (C*)p->S1, (C*)p->S2, nullptr, p->kx, (const C*)p->twx, nullptr,
-      nullptr, nullptr, nullptr, 0.0, p->theta0, gx, gy, gz, nullptr);
+      nullptr, nullptr, nullptr, 0.0, p->theta0, gx, gy, gz, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -507,9 +538,9 @@ int solve_impl(OraclePlan* p, const T* d, T* phi, int log_diag, cudaStream_t st)
     OB_CUDA(cudaMemsetAsync(p->diag + OB_DIAG_LAST_DISC, 0, sizeof(double), st));
   }
   const long ncols = (long)g.nxh * g.ny;
-  k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+  { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
                              smem_thomas(p), st>>>(g, thomas_args(p), (C*)p->S3, (C*)p->S3,
-                                                   diag, OB_DIAG_LAST_COMPAT, OB_DIAG_LAST_DISC);
+                                                   diag, OB_DIAG_LAST_COMPAT, OB_DIAG_LAST_DISC); }
   OB_LAUNCHED();
   return inv_scalar<T>(p, 1.0, phi, st);
 }
@@ -520,13 +551,13 @@ int apply_op_impl(OraclePlan* p, const T* phi, T* out, cudaStream_t st) {
   const GridK g = p->g;
   RC(fwd_scalar<T>(p, phi, st));
   const size_t ns = (size_t)g.nxh * g.ny * g.nz;
-  k_neg_ksq<T><<<(unsigned)std::min<size_t>((ns + 255) / 256, 65535), 256, 0, st>>>(
-      g, (C*)p->S3, p->kx, p->ky, (C*)p->S3);
+  { Launch L_(p, 7, st); k_neg_ksq<T><<<(unsigned)std::min<size_t>((ns + 255) / 256, 65535), 256, 0, st>>>(
+      g, (C*)p->S3, p->kx, p->ky, (C*)p->S3); }
   OB_LAUNCHED();
   RC(inv_scalar<T>(p, 1.0 / ((double)g.nx * (double)g.ny), (T*)p->Du, st));
   const size_t n = (size_t)g.nx * g.ny * g.nz;
-  k_apply_vert<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
-      g, phi, (const T*)p->Du, p->rho, p->rhoh, out);
+  { Launch L_(p, 7, st); k_apply_vert<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
+      g, phi, (const T*)p->Du, p->rho, p->rhoh, out); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -534,8 +565,8 @@ int apply_op_impl(OraclePlan* p, const T* phi, T* out, cudaStream_t st) {
 template <class T>
 int buoyancy_impl(OraclePlan* p, const T* th, T* dw, cudaStream_t st) {
   const size_t n = (size_t)p->g.nx * p->g.ny * (p->g.nz + 1);
-  k_buoyancy<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
-      p->g, th, p->theta0, dw);
+  { Launch L_(p, 7, st); k_buoyancy<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, st>>>(
+      p->g, th, p->theta0, dw); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -570,6 +601,10 @@ size_t oracle_b200_plan_scratch_bytes(const OraclePlan* p) { return p ? p->scrat
 
 int oracle_b200_plan_destroy(OraclePlan* p) {
   if (!p) return OB_OK;
+  for (auto& m : p->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
   for (void* q : p->allocs) cudaFree(q);
   delete p;
   return OB_OK;
@@ -841,6 +876,36 @@ int oracle_b200_tendency(OraclePlan* p, int mask, const OracleStatePtrs* s, void
                                         (double*)dth, dt_slow, st),
                   tendency_impl<float>(p, mask, s, (float*)du, (float*)dv, (float*)dw,
                                        (float*)dth, dt_slow, st));
+}
+
+long oracle_b200_launch_count(const OraclePlan* p) { return p ? p->launches : -1; }
+
+int oracle_b200_profile(OraclePlan* p, int enable) {
+  if (int rc = check_plan(p)) return rc;
+  for (auto& m : p->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  p->marks.clear();
+  p->profiling = enable ? 1 : 0;
+  return OB_OK;
+}
+
+int oracle_b200_profile_read(OraclePlan* p, double* ms, long* counts, int ncls) {
+  if (int rc = check_plan(p)) return rc;
+  if (!ms || !counts || ncls < OB_PROF_CLASSES) return fail(OB_ERR_ARG, "profile_read: bad buffers");
+  for (int c = 0; c < ncls; ++c) {
+    ms[c] = 0.0;
+    counts[c] = 0;
+  }
+  for (auto& m : p->marks) {
+    OB_CUDA(cudaEventSynchronize(m.b));
+    float t = 0.f;
+    OB_CUDA(cudaEventElapsedTime(&t, m.a, m.b));
+    ms[m.cls] += t;
+    counts[m.cls] += 1;
+  }
+  return OB_OK;
 }
 
 int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) {

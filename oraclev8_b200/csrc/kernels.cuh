@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(512) k_iy(GridK g, FftPlan py, int zc, int nf,
     const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
     if (MODE == IY_GRAD) {
       cplx<T> v = mk<T>((T)0, (T)0);
-      if (zl < zn) v = in0[o];
+      if (zl < zn) v = scl(in0[o], s);
       const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
       bufA[(size_t)ky * B + zl] = v;
       bufA[(size_t)ky * B + zc + zl] = ik(kk, v);

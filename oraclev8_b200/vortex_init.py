@@ -1,0 +1,106 @@
+"""Holland (1980) balanced vortex initial state (oracle_v8/vortex_init.py:75-411).
+
+Host-side input preparation, run once per run: the radial gradient-wind
+integral, the hydrostatic theta', and the interpolation to the grid are
+FP64 NumPy, then the fields move to the device.  ``wind_decay_top`` selects the
+linear wind structure max(0, 1 - z/top) the beta-drift workloads use in place
+of exp(-z/H_wind).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .constants import GRAVITY
+from .backend import asarray, to_numpy
+
+
+class HollandVortexInit:
+    def __init__(self, Vmax, Rmax, B=1.5, f=5e-5, R_env=None, u_env=0.0, v_env=0.0,
+                 n_radial=4000, z_peak=8_000.0, sigma_z=4_000.0, H_wind=15_000.0,
+                 wind_taper=False, taper_start_frac=0.5, wind_decay_top=None):
+        self.Vmax, self.Rmax, self.B, self.f = float(Vmax), float(Rmax), float(B), float(f)
+        self.R_env = float(R_env) if R_env is not None else 10.0 * Rmax
+        self.u_env, self.v_env = float(u_env), float(v_env)
+        self.n_radial = int(n_radial)
+        self.z_peak, self.sigma_z, self.H_wind = float(z_peak), float(sigma_z), float(H_wind)
+        self.wind_taper = bool(wind_taper)
+        self.taper_start_frac = float(taper_start_frac)
+        self.wind_decay_top = None if wind_decay_top is None else float(wind_decay_top)
+        self._r1d = np.linspace(0.0, self.R_env, self.n_radial)
+
+    def tangential_wind(self, r):
+        """V = Vmax sqrt(x e^{1-x}), x = (Rmax/r)^B, V(0) = 0 (vortex_init.py:169-189)."""
+        r_safe = np.where(r > 0.0, r, 1.0)
+        x = (self.Rmax / r_safe) ** self.B
+        Vt = self.Vmax * np.sqrt(x * np.exp(1.0 - x))
+        Vt = np.where(r > 0.0, Vt, 0.0)
+        if self.wind_taper:
+            r0 = self.taper_start_frac * self.R_env
+            frac = np.clip((r - r0) / max(self.R_env - r0, 1e-9), 0.0, 1.0)
+            Vt = Vt * 0.5 * (1.0 + np.cos(np.pi * frac))
+        return Vt
+
+    def wind_vertical_structure(self, z):
+        if self.wind_decay_top is not None:
+            return np.maximum(0.0, 1.0 - z / self.wind_decay_top)
+        return np.exp(-z / self.H_wind)
+
+    def _pressure_deficit_1d(self, rho_z, S_z):
+        """Inward trapezoid of dP/dr = rho (V^2/r + f V) (vortex_init.py:223-255);
+        the recurrence is evaluated in closed form as a reversed cumulative sum of
+        the same trapezoid terms."""
+        r = self._r1d
+        Vt = self.tangential_wind(r) * S_z
+        r_safe = np.where(r > 0.0, r, 1.0)
+        dPdr = rho_z * (np.where(r > 0.0, Vt ** 2 / r_safe, 0.0) + self.f * Vt)
+        dr = r[1] - r[0]
+        P = np.zeros(self.n_radial)
+        terms = 0.5 * (dPdr[:-1] + dPdr[1:]) * dr
+        acc = 0.0
+        for i in range(self.n_radial - 2, -1, -1):
+            acc = acc - terms[i]
+            P[i] = acc
+        return P
+
+    def build_state(self, nx, ny, nz, Lx, Ly, base, x_c=None, y_c=None, device=True):
+        """Balanced State (vortex_init.py:261-370).  ``device=False`` returns
+        host NumPy fields (for pinned-buffer staging)."""
+        from .solver.tendency import State
+        x_c = x_c if x_c is not None else Lx / 2.0
+        y_c = y_c if y_c is not None else Ly / 2.0
+        dx, dy = Lx / nx, Ly / ny
+        x = (np.arange(nx) + 0.5) * dx
+        y = (np.arange(ny) + 0.5) * dy
+        X, Y = np.meshgrid(x, y, indexing="ij")
+        dX, dY = X - x_c, Y - y_c
+        R2d = np.sqrt(dX ** 2 + dY ** 2)
+        PHI = np.arctan2(dY, dX)
+        z = np.asarray(to_numpy(base.z), dtype=np.float64)
+        rho0 = np.asarray(to_numpy(base.rho0), dtype=np.float64)
+        theta0 = np.asarray(to_numpy(base.theta0), dtype=np.float64)
+        S = self.wind_vertical_structure(z)
+        Pp = np.zeros((self.n_radial, nz))
+        for k in range(nz):
+            Pp[:, k] = self._pressure_deficit_1d(float(rho0[k]), float(S[k]))
+        dP = np.empty_like(Pp)
+        dP[:, 1:-1] = (Pp[:, 2:] - Pp[:, :-2]) / (z[2:] - z[:-2])[None, :]
+        dP[:, 0] = (Pp[:, 1] - Pp[:, 0]) / (z[1] - z[0])
+        dP[:, -1] = (Pp[:, -1] - Pp[:, -2]) / (z[-1] - z[-2])
+        theta_rad = (theta0[None, :] / (rho0[None, :] * GRAVITY)) * dP
+        rf = R2d.ravel()
+        th = np.empty((nx, ny, nz))
+        for k in range(nz):
+            th[:, :, k] = np.interp(rf, self._r1d, theta_rad[:, k]).reshape(nx, ny)
+        sin_phi, cos_phi = np.sin(PHI), np.cos(PHI)
+        Vt0 = self.tangential_wind(R2d)
+        u = np.empty((nx, ny, nz))
+        v = np.empty((nx, ny, nz))
+        for k in range(nz):
+            Vt = Vt0 * float(S[k])
+            u[:, :, k] = -Vt * sin_phi + self.u_env
+            v[:, :, k] = +Vt * cos_phi + self.v_env
+        w = np.zeros((nx, ny, nz + 1))
+        phi = np.zeros((nx, ny, nz))
+        if not device:
+            return State(u, v, w, th, phi, 0.0)
+        return State(asarray(u), asarray(v), asarray(w), asarray(th), asarray(phi), 0.0)

@@ -113,3 +113,16 @@ def test_product_package_never_imports_oracle():
     pkg = pathlib.Path(__file__).resolve().parents[1] / "oraclev8_b200"
     for f in pkg.rglob("*.py"):
         assert not re.search(r"^\s*(from|import)\s+oracle\b", f.read_text(), re.M), f
+
+
+def test_vortex_init_identical_to_reference_restatement():
+    from oraclev8_b200.vortex_init import HollandVortexInit
+    from oraclev8_b200.production_config import BaseState
+    base = BaseState(8, 16e3)
+    for kw in (dict(Vmax=40.0, Rmax=50e3, B=1.5, f=4.99e-5, wind_decay_top=12e3),
+               dict(Vmax=55.0, Rmax=30e3, B=1.8, f=6.1e-5, u_env=-3.0, v_env=1.0,
+                    wind_taper=True)):
+        a = HollandVortexInit(**kw).build_state(32, 24, 8, 640e3, 480e3, base, device=False)
+        b = O.Holland(**kw).build_state(32, 24, 8, 640e3, 480e3, base.z, base.rho0, base.theta0)
+        for f in ("u", "v", "w", "theta_prime"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
