@@ -178,6 +178,28 @@ long oracle_b200_launch_count(const OraclePlan *plan);
 int oracle_b200_profile(OraclePlan *plan, int enable);
 int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
 
+/* Poisson solve that allocates no device memory.  No counterpart in the
+ * reference: it is an extra entry point for callers that cannot call
+ * cudaMalloc when they need a solve (a process whose own allocator already
+ * holds the GPU's memory, a framework whose pool must remain the only owner of
+ * device memory, or a latency-critical caller that cannot afford cudaMalloc's
+ * device synchronisation).  Same result as oracle_b200_poisson_solve on a plan
+ * of the same grid and rho0 (host array, nz values), without a plan.
+ *  - Working memory is one fixed 32 MiB array per device, reserved by the CUDA
+ *    module on every GPU that loads this library until the process exits.
+ *    Grids whose tables plus two half-spectrum buffers exceed it, or with
+ *    nx, ny > 2048 or nz > 512, are rejected with OB_ERR_ARG (e.g. 128x128x32
+ *    FP64 uses about 8.5 MB; 256x256x32 FP64 does not fit).
+ *  - The first call on each device looks up the array's address and sets
+ *    kernel attributes; make that first call before any stream capture.
+ *  - Every call shares the array and overwrites all of it that it reads, so
+ *    nothing carries over between calls; calls whose GPU work overlaps (other
+ *    streams, other host threads on the same device) race on it.
+ *  - The tables are copied from pageable host memory, so the call returns
+ *    after they are staged; the solve itself is enqueued on `stream`. */
+int oracle_b200_poisson_solve_noalloc(const OracleGridDesc *grid, const double *rho0,
+                                      const void *d, void *phi, void *stream);
+
 const char *oracle_b200_last_error(void);
 int oracle_b200_version(void);
 

@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -926,3 +927,228 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Poisson solve that allocates nothing
+// ===========================================================================
+//
+// Some callers cannot call cudaMalloc when they need a solve: a host program
+// whose own allocator has already reserved the GPU's memory, code that runs
+// inside a framework whose memory pool must stay the only owner of device
+// memory, or a caller on a latency-critical path where cudaMalloc's implicit
+// device synchronisation is not acceptable.  oracle_b200_poisson_solve_noalloc
+// serves them: it performs the same FFT + Thomas solve as
+// oracle_b200_poisson_solve, but every byte of working memory (spectral
+// buffers, wavenumber / twiddle / Thomas tables) lives in the fixed array
+// below.  The CUDA module reserves that array on every device that loads this
+// library, and it stays reserved until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 32ull << 20;  // 32 MiB per device
+constexpr int kNoAllocMaxDevices = 64;
+constexpr int kNoAllocMaxN = 2048;  // nx, ny limit (table sizes)
+constexpr int kNoAllocMaxNz = 512;
+
+}  // namespace
+
+// File-scope device scratch.  In host code this name is only a host-side
+// stand-in: its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_dev_base[kNoAllocMaxDevices] = {};
+// host staging of the tables (guarded by g_noalloc_mu)
+alignas(256) unsigned char g_noalloc_host[512 * 1024];
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Once per device, with that device current: look up the array's device
+// address and raise the kernels' shared-memory limits.
+int noalloc_base(unsigned char** out) {
+  int dev = 0;
+  OB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc: device index %d out of range", dev);
+  if (!g_noalloc_dev_base[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr)
+      return fail(OB_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch) failed: %s",
+                  cudaGetErrorString(e));
+    int rc = set_smem_attrs<double>();
+    if (rc) return rc;
+    rc = set_smem_attrs<float>();
+    if (rc) return rc;
+    g_noalloc_dev_base[dev] = static_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_dev_base[dev];
+  return OB_OK;
+}
+
+template <class T>
+int noalloc_solve(const OracleGridDesc* grid, const double* rho0, const T* d, T* phi,
+                  cudaStream_t st) {
+  const int nx = grid->nx, ny = grid->ny, nz = grid->nz;
+  OraclePlan p;  // stack descriptor; every pointer below aims into the fixed array
+  p.prec = grid->precision;
+  p.esz = sizeof(T);
+  p.g.nx = nx;
+  p.g.ny = ny;
+  p.g.nz = nz;
+  p.g.M = nx / 2;
+  p.g.nxh = nx / 2 + 1;
+  p.g.dx = grid->Lx / nx;
+  p.g.dy = grid->Ly / ny;
+  p.g.dz = grid->Lz / nz;
+  if (!factorize(nx / 2, p.px) || !factorize(ny, p.py))
+    return fail(OB_ERR_ARG, "nx/2=%d and ny=%d must factor into 2, 3, 5", nx / 2, ny);
+  const size_t ce = 2 * sizeof(T);
+  p.zc_fx = pick_zc(nz, 2ull * (p.g.M + 1) * 3 * ce, 0);
+  p.zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, 0);
+  p.zc_iy = p.zc_fy;
+  p.zc_ix = pick_zc(nz, (size_t)(2 * p.g.M + 1) * 3 * ce, (size_t)(2 * p.g.M + 1) * ce);
+  if (smem_fx(&p, 3) > kSmemMax || smem_fy(&p, 2, p.zc_fy) > kSmemMax ||
+      smem_ix(&p, 3 * p.zc_ix + 1) > kSmemMax || smem_thomas(&p) > kSmemMax)
+    return fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx, ny, nz);
+
+  // carve: [tables | twiddles | S1 | S3]
+  const size_t ns = (size_t)p.g.nxh * ny * nz;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += align256(bytes);
+    return o;
+  };
+  const size_t o_kx = take(nx * 8), o_ky = take(ny * 8), o_rho = take(nz * 8),
+               o_rhoh = take((nz + 1) * 8), o_a = take(nz * 8), o_c = take(nz * 8),
+               o_negs = take(nz * 8), o_a0 = take(nz * 8), o_cp0 = take(nz * 8),
+               o_inv0 = take(nz * 8), o_twx = take(nx * ce), o_twy = take(ny * ce);
+  const size_t table_bytes = off;
+  const size_t o_s1 = take(ns * ce), o_s3 = take(ns * ce);
+  if (off > kNoAllocScratchBytes)
+    return fail(OB_ERR_ARG,
+                "poisson_solve_noalloc: grid (%d, %d, %d) needs %zu bytes of scratch; the "
+                "no-allocation entry point holds at most %zu bytes (use oracle_b200_poisson_solve)",
+                nx, ny, nz, off, kNoAllocScratchBytes);
+  if (table_bytes > sizeof(g_noalloc_host))
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc: tables exceed the host staging buffer");
+
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  unsigned char* base = nullptr;
+  if (int rc = noalloc_base(&base)) return rc;
+
+  // host tables, built as oracle_b200_plan_create builds them (poisson.py:286-325)
+  unsigned char* h = g_noalloc_host;
+  std::memset(h, 0, table_bytes);
+  double* kx = (double*)(h + o_kx);
+  double* ky = (double*)(h + o_ky);
+  double* rf = (double*)(h + o_rho);
+  double* rh = (double*)(h + o_rhoh);
+  double* a = (double*)(h + o_a);
+  double* c = (double*)(h + o_c);
+  double* negs = (double*)(h + o_negs);
+  double* a0 = (double*)(h + o_a0);
+  double* cp0 = (double*)(h + o_cp0);
+  double* inv0 = (double*)(h + o_inv0);
+  {
+    const double dxk = grid->Lx / nx, dyk = grid->Ly / ny;
+    const double vx = 1.0 / ((double)nx * dxk), vy = 1.0 / ((double)ny * dyk);
+    for (int i = 0; i < nx; ++i) {
+      const long si = (i < (nx - 1) / 2 + 1) ? i : (long)i - nx;
+      kx[i] = (2.0 * M_PI) * ((double)si * vx);
+    }
+    for (int i = 0; i < ny; ++i) {
+      const long si = (i < (ny - 1) / 2 + 1) ? i : (long)i - ny;
+      ky[i] = (2.0 * M_PI) * ((double)si * vy);
+    }
+  }
+  for (int k = 0; k < nz; ++k) rf[k] = rho0[k];
+  for (int k = 1; k < nz; ++k) rh[k] = 0.5 * (rf[k - 1] + rf[k]);
+  rh[0] = rf[0];
+  rh[nz] = rf[nz - 1];
+  const double dz2 = p.g.dz * p.g.dz;
+  for (int k = 0; k < nz; ++k) {
+    const double rl = rh[k] / dz2, ru = rh[k + 1] / dz2;
+    a[k] = rl;
+    c[k] = ru;
+    negs[k] = -(rl + ru);
+  }
+  a[0] = 0.0;
+  c[nz - 1] = 0.0;
+  negs[0] = -(rh[1] / dz2);
+  negs[nz - 1] = -(rh[nz - 1] / dz2);
+  {
+    const int n0 = nz - 1;
+    double b0[kNoAllocMaxNz], c0[kNoAllocMaxNz];
+    for (int j = 0; j < n0; ++j) {
+      const double rl = rh[j + 1] / dz2, ru = rh[j + 2] / dz2;
+      a0[j] = rl;
+      b0[j] = -(rl + ru);
+      c0[j] = ru;
+    }
+    a0[0] = 0.0;
+    a0[n0 - 1] = rh[nz - 1] / dz2;
+    c0[n0 - 1] = 0.0;
+    b0[n0 - 1] = -(rh[nz - 1] / dz2);
+    inv0[0] = 1.0 / b0[0];
+    cp0[0] = c0[0] * inv0[0];
+    for (int j = 1; j < n0; ++j) {
+      const double den = b0[j] - a0[j] * cp0[j - 1];
+      inv0[j] = 1.0 / den;
+      cp0[j] = (j < n0 - 1) ? c0[j] * inv0[j] : 0.0;
+    }
+  }
+  for (int t = 0; t < nx; ++t) {
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * t / nx;
+    ((cplx<T>*)(h + o_twx))[t] = cplx<T>{(T)cosl(ang), (T)sinl(ang)};
+  }
+  for (int t = 0; t < ny; ++t) {
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * t / ny;
+    ((cplx<T>*)(h + o_twy))[t] = cplx<T>{(T)cosl(ang), (T)sinl(ang)};
+  }
+  // pageable source: the call returns once the bytes are staged, so the host
+  // buffer may be rewritten by the next call
+  OB_CUDA(cudaMemcpyAsync(base, h, table_bytes, cudaMemcpyHostToDevice, st));
+
+  p.kx = (double*)(base + o_kx);
+  p.ky = (double*)(base + o_ky);
+  p.rho = (double*)(base + o_rho);
+  p.rhoh = (double*)(base + o_rhoh);
+  p.ta = (double*)(base + o_a);
+  p.tc = (double*)(base + o_c);
+  p.tnegs = (double*)(base + o_negs);
+  p.ta0 = (double*)(base + o_a0);
+  p.tcp0 = (double*)(base + o_cp0);
+  p.tinv0 = (double*)(base + o_inv0);
+  p.theta0 = p.rho;  // not read by the solve kernels
+  p.twx = base + o_twx;
+  p.twy = base + o_twy;
+  p.S1 = base + o_s1;
+  p.S3 = base + o_s3;
+  return solve_impl<T>(&p, d, phi, 0, st);
+}
+
+}  // namespace
+
+extern "C" int oracle_b200_poisson_solve_noalloc(const OracleGridDesc* grid, const double* rho0,
+                                                 const void* d, void* phi, void* stream) {
+  if (!grid || !rho0 || !d || !phi) return fail(OB_ERR_ARG, "poisson_solve_noalloc: NULL argument");
+  const int nx = grid->nx, ny = grid->ny, nz = grid->nz;
+  if (nx < 4 || ny < 4 || (nx & 1) || (ny & 1) || nz < 3)
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc: need even nx, ny >= 4 and nz >= 3 (got %d, %d, %d)",
+                nx, ny, nz);
+  if (nx > kNoAllocMaxN || ny > kNoAllocMaxN || nz > kNoAllocMaxNz)
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc: grid (%d, %d, %d) exceeds the limits "
+                "nx, ny <= %d, nz <= %d", nx, ny, nz, kNoAllocMaxN, kNoAllocMaxNz);
+  if (!(grid->Lx > 0 && grid->Ly > 0 && grid->Lz > 0))
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc: domain lengths must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (grid->precision == OB_PREC_F64)
+    return noalloc_solve<double>(grid, rho0, (const double*)d, (double*)phi, st);
+  if (grid->precision == OB_PREC_F32)
+    return noalloc_solve<float>(grid, rho0, (const float*)d, (float*)phi, st);
+  return fail(OB_ERR_ARG, "poisson_solve_noalloc: unknown precision %d", grid->precision);
+}
