@@ -291,14 +291,17 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# ncu capture of this workload (profiles/ncu_projection_kernels_config1_fp64.md):
+# k_ix 1.163 GB in correction mode and 1.323 GB in stage mode, weighted 2:3 as
+# the five projections of a step use them.
+NCU_TRAFFIC = {
+    ("config1", "fp64"): {"ix": (2 * 1.163e9 + 3 * 1.323e9) / 5, "fy": 0.384e9, "iy": 0.356e9},
+}
+
+
 def load_traffic(wname, precision):
-    p = ROOT / "profiles" / "ncu_traffic.json"
-    if not p.exists():
-        return {}
-    try:
-        return json.loads(p.read_text()).get(f"{wname}/{precision}", {})
-    except Exception:
-        return {}
+    return NCU_TRAFFIC.get((wname, precision), {})
 
 
 def run_b200(args):

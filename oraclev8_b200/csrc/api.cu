@@ -2,6 +2,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -9,6 +11,7 @@
 
 #include "../../include/oracle_b200.h"
 #include "kernels.cuh"
+#include "pipe.cuh"
 
 using namespace ob;
 
@@ -47,21 +50,34 @@ constexpr int kFftThreads = 256;
 constexpr size_t kSmemBudget = 112 * 1024;  // two CTAs per SM
 constexpr size_t kSmemMax = 227 * 1024;
 
-bool factorize(int M, FftPlan& p) {
+bool factorize(int M, FftPlan& p, bool radix16 = true) {
   p.M = M;
   p.np = 0;
   int m = M;
-  while (m > 1 && m % 4 == 0) {
-    p.r[p.np++] = 4;
-    m /= 4;
-  }
+  auto push = [&](int r) {
+    if (p.np >= 16) return false;
+    p.r[p.np++] = r;
+    return true;
+  };
+  // large radices first: each pass is one trip through shared memory.  A
+  // stand-alone radix-8 pass is not used (see the kernel notes on the
+  // misaligned-address fault); 8 is factored as 4 x 2.
+  for (int r : {16, 4})
+    while (m > 1 && m % r == 0 && (radix16 || r != 16)) {
+      if (!push(r)) return false;
+      m /= r;
+    }
   const int rs[3] = {2, 3, 5};
   for (int r : rs)
     while (m % r == 0 && m > 1) {
-      if (p.np >= 20) return false;
-      p.r[p.np++] = r;
+      if (!push(r)) return false;
       m /= r;
     }
+  int ns = 1;
+  for (int s = 0; s < p.np; ++s) {
+    p.ns[s] = FastDiv((unsigned)ns);
+    ns *= p.r[s];
+  }
   return m == 1;
 }
 
@@ -99,8 +115,13 @@ struct OraclePlan {
   double f0 = 0, u_env = 0, v_env = 0, epsilon = 0;
   int diag_every = 60;
   long solve_count = 0;
-  FftPlan px{}, py{};
+  FftPlan px{}, py{};    // radix-16-first plans (inverse kernels)
+  FftPlan pxf{}, pyf{};  // radix-4-first plans (forward kernels: lower register pressure)
   int zc_fx = 1, zc_fy = 1, zc_iy = 1, zc_ix = 1;
+  // pipelined projection kernels: z-chunk and persistent grid size
+  int zc_fxp = 1, zc_fyp = 1, zc_iyp = 1, zc_ixp = 1;
+  int grid_fxp = 1, grid_fyp = 1, grid_iyp = 1, grid_ixp = 1;
+  int use_pipe = 0;  // projection through the persistent pipelined kernels
   size_t esz = 8;  // element size of T
   // device constants
   double *kx = nullptr, *ky = nullptr, *rho = nullptr, *rhoh = nullptr, *theta0 = nullptr;
@@ -159,12 +180,54 @@ int pick_zc(int nz, size_t per_zc, size_t fixed) {
   return best;
 }
 
+// bytes of a twiddle table of n complex entries staged at the start of the
+// FFT kernels' dynamic shared memory
+size_t tw_bytes(const OraclePlan* p, int n) { return ((size_t)n * 2 * p->esz + 15) & ~size_t(15); }
 size_t smem_fx(const OraclePlan* p, int nf) {
-  return 2ull * (p->g.M + 1) * nf * p->zc_fx * 2 * p->esz;
+  return tw_bytes(p, p->g.nx) + 2ull * (p->g.M + 1) * nf * p->zc_fx * 2 * p->esz;
 }
-size_t smem_fy(const OraclePlan* p, int nf, int zc) { return 2ull * p->g.ny * nf * zc * 2 * p->esz; }
-size_t smem_ix(const OraclePlan* p, int B) { return (size_t)(2 * p->g.M + 1) * B * 2 * p->esz; }
+size_t smem_fy(const OraclePlan* p, int nf, int zc) {
+  return tw_bytes(p, p->g.ny) + 2ull * p->g.ny * nf * zc * 2 * p->esz;
+}
+size_t smem_ix(const OraclePlan* p, int B) {
+  return tw_bytes(p, p->g.nx) + (size_t)(2 * p->g.M + 1) * B * 2 * p->esz;
+}
 size_t smem_thomas(const OraclePlan* p) { return 3ull * kThomasCols * (p->g.nz + 1) * 8; }
+
+constexpr int kPipeThreads = 256;
+
+size_t smem_fxp(const OraclePlan* p, int zc) {
+  const size_t raw = (fxp_raw_elems<double>(p->g.nx, zc, true) * p->esz + 15) & ~size_t(15);
+  return tw_bytes(p, p->g.nx) + 2 * raw + 2ull * (p->g.M + 1) * ((3 * zc) | 1) * 2 * p->esz;
+}
+size_t smem_fyp(const OraclePlan* p, int zc) {
+  return tw_bytes(p, p->g.ny) + 3ull * p->g.ny * ((2 * zc) | 1) * 2 * p->esz;
+}
+size_t smem_iyp(const OraclePlan* p, int zc) {
+  return tw_bytes(p, p->g.ny) + 2ull * p->g.ny * zc * 2 * p->esz +
+         2ull * p->g.ny * ((2 * zc) | 1) * 2 * p->esz;
+}
+size_t smem_ixp(const OraclePlan* p, int zc) {
+  const size_t raw = p->esz == 8 ? ixp_raw_bytes<double>(p->g.nx, zc, true)
+                                 : ixp_raw_bytes<float>(p->g.nx, zc, true);
+  return tw_bytes(p, p->g.nx) + 2 * raw + (size_t)(2 * p->g.M + 1) * ((3 * zc + 1) | 1) * 2 * p->esz;
+}
+
+// Largest z-chunk whose footprint lets `occ` CTAs share an SM (occ = 2 by
+// default; ORACLE_B200_PIPE_OCC=1 prefers one CTA with a deeper chunk);
+// falls back to one CTA per SM.
+template <class F>
+int pick_pipe_zc(int nz, F&& smem) {
+  int occ = 2;
+  if (const char* e = getenv("ORACLE_B200_PIPE_OCC")) occ = atoi(e) == 1 ? 1 : 2;
+  const size_t budget = occ == 2 ? (kSmemMax - 1024) / 2 : kSmemMax;
+  for (size_t lim : {budget, kSmemMax})
+    for (int zc : {8, 4, 2, 1}) {
+      if (zc > nz && zc > 1) continue;
+      if (smem(zc) <= lim) return zc;
+    }
+  return 0;
+}
 
 template <class T>
 int set_smem_attrs() {
@@ -182,6 +245,51 @@ int set_smem_attrs() {
   OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_thomas<T, kThomasCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fxp<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fxp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fyp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_iyp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ixp<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ixp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  return OB_OK;
+}
+
+// Persistent grid: resident CTAs per SM (occupancy API) x SMs, capped by items.
+template <class K>
+int persistent_grid(K kernel, size_t smem, int items, int* out) {
+  int dev = 0, nsm = 148, per = 1;
+  OB_CUDA(cudaGetDevice(&dev));
+  OB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  OB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPipeThreads, smem));
+  if (per < 1) return fail(OB_ERR_ARG, "pipelined kernel does not fit on an SM (smem %zu)", smem);
+  *out = std::max(1, std::min(items, per * nsm));
+  return OB_OK;
+}
+
+template <class T>
+int setup_pipes(OraclePlan* p) {
+  const int nz = p->g.nz;
+  p->zc_fxp = pick_pipe_zc(nz, [&](int zc) { return smem_fxp(p, zc); });
+  p->zc_fyp = pick_pipe_zc(nz, [&](int zc) { return smem_fyp(p, zc); });
+  p->zc_iyp = pick_pipe_zc(nz, [&](int zc) { return smem_iyp(p, zc); });
+  p->zc_ixp = pick_pipe_zc(nz, [&](int zc) { return smem_ixp(p, zc); });
+  if (!p->zc_fxp || !p->zc_fyp || !p->zc_iyp || !p->zc_ixp)
+    return fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds the pipelined kernels' shared memory",
+                p->g.nx, p->g.ny, nz);
+  auto nzc = [&](int zc) { return (nz + zc - 1) / zc; };
+  int rc;
+  if ((rc = persistent_grid(k_fxp<T, true>, smem_fxp(p, p->zc_fxp), p->g.ny * nzc(p->zc_fxp),
+                            &p->grid_fxp)))
+    return rc;
+  if ((rc = persistent_grid(k_fyp<T>, smem_fyp(p, p->zc_fyp), p->g.nxh * nzc(p->zc_fyp),
+                            &p->grid_fyp)))
+    return rc;
+  if ((rc = persistent_grid(k_iyp<T>, smem_iyp(p, p->zc_iyp), p->g.nxh * nzc(p->zc_iyp),
+                            &p->grid_iyp)))
+    return rc;
+  if ((rc = persistent_grid(k_ixp<T, true>, smem_ixp(p, p->zc_ixp), p->g.ny * nzc(p->zc_ixp),
+                            &p->grid_ixp)))
+    return rc;
   return OB_OK;
 }
 
@@ -225,8 +333,51 @@ struct Launch {
   }
 };
 
-dim3 grid_x(const OraclePlan* p, int zc) { return dim3(p->g.ny, (p->g.nz + zc - 1) / zc); }
-dim3 grid_y(const OraclePlan* p, int zc) { return dim3(p->g.nxh, (p->g.nz + zc - 1) / zc); }
+dim3 grid_x(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.ny); }
+dim3 grid_y(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.nxh); }
+
+// projection through the persistent pipelined kernels (pipe.cuh)
+template <class T>
+int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
+                 double stage_sdt, T* uo, T* vo, T* wo, T* phio, double* diag, int slot_c,
+                 int slot_d, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  C* S3 = (C*)p->S3;
+  const bool stage = stage_sdt >= 0.0;
+  if (stage)
+    { Launch L_(p, 0, st); k_fxp<T, true><<<p->grid_fxp, kPipeThreads, smem_fxp(p, p->zc_fxp), st>>>(
+        g, p->pxf, p->zc_fxp, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2); }
+  else
+    { Launch L_(p, 0, st); k_fxp<T, false><<<p->grid_fxp, kPipeThreads, smem_fxp(p, p->zc_fxp), st>>>(
+        g, p->pxf, p->zc_fxp, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2); }
+  OB_LAUNCHED();
+  { Launch L_(p, 1, st); k_fyp<T><<<p->grid_fyp, kPipeThreads, smem_fyp(p, p->zc_fyp), st>>>(
+      g, p->pyf, p->zc_fyp, S1, S2, p->ky, (const C*)p->twy, S3); }
+  OB_LAUNCHED();
+  const long ncols = (long)g.nxh * g.ny;
+  { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
+                                                   slot_d); }
+  OB_LAUNCHED();
+  { Launch L_(p, 3, st); k_iyp<T><<<p->grid_iyp, kPipeThreads, smem_iyp(p, p->zc_iyp), st>>>(
+      g, p->py, p->zc_iyp, S3, p->ky, (const C*)p->twy, 1.0, S1, S2); }
+  OB_LAUNCHED();
+  if (stage)
+    { Launch L_(p, 4, st); k_ixp<T, true><<<p->grid_ixp, kPipeThreads, smem_ixp(p, p->zc_ixp), st>>>(
+        g, p->px, p->zc_ixp, S1, S2, p->kx, (const C*)p->twx, u, v, w, th, stage_sdt,
+        p->theta0, uo, vo, wo, phio); }
+  else
+    { Launch L_(p, 4, st); k_ixp<T, false><<<p->grid_ixp, kPipeThreads, smem_ixp(p, p->zc_ixp), st>>>(
+        g, p->px, p->zc_ixp, S1, S2, p->kx, (const C*)p->twx, u, v, w, th, 0.0, p->theta0,
+        uo, vo, wo, phio); }
+  OB_LAUNCHED();
+  return OB_OK;
+}
 
 // ---- projection pipeline -------------------------------------------------
 // stage_sdt < 0: in-place projection of (u, v, w) with phi output.
@@ -254,17 +405,18 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
     OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
   }
   const bool stage = stage_sdt >= 0.0;
+  if (p->use_pipe) return project_pipe<T>(p, u, v, w, th, stage_sdt, uo, vo, wo, phio, diag, slot_c, slot_d, st);
   if (stage)
     { Launch L_(p, 0, st); k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
-        g, p->px, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
+        g, p->pxf, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
         (const C*)p->twx, S1, S2, nullptr); }
   else
     { Launch L_(p, 0, st); k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
-        g, p->px, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+        g, p->pxf, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
         (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
+      g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   const long ncols = (long)g.nxh * g.ny;
   { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
@@ -295,12 +447,12 @@ int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStrea
   C* S1 = (C*)p->S1;
   C* S2 = (C*)p->S2;
   { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
-      g, p->px, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+      g, p->pxf, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
       (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   const double scale = -(p->epsilon / dt_slow) / ((double)g.nx * (double)g.ny);
   { Launch L_(p, 1, st); k_fy<T, FY_HELM><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2); }
+      g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2); }
   OB_LAUNCHED();
   { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2); }
@@ -463,11 +615,11 @@ int divergence_impl(OraclePlan* p, const T* u, const T* v, const T* w, T* d, cud
   C* S2 = (C*)p->S2;
   C* S3 = (C*)p->S3;
   { Launch L_(p, 0, st); k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
-      g, p->px, p->zc_fx, 3, u, v, w, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+      g, p->pxf, p->zc_fx, 3, u, v, w, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
       (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
+      g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 1, S3, nullptr, p->ky, (const C*)p->twy,
@@ -486,11 +638,11 @@ int fwd_scalar(OraclePlan* p, const T* f, cudaStream_t st) {
   using C = cplx<T>;
   const GridK g = p->g;
   { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
-      g, p->px, p->zc_fx, 1, f, nullptr, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0,
+      g, p->pxf, p->zc_fx, 1, f, nullptr, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0,
       p->kx, (const C*)p->twx, (C*)p->S1, nullptr, nullptr); }
   OB_LAUNCHED();
   { Launch L_(p, 1, st); k_fy<T, FY_FIELDS><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->py, p->zc_fy, 1, (C*)p->S1, nullptr, p->kx, p->ky, (const C*)p->twy, 1.0,
+      g, p->pyf, p->zc_fy, 1, (C*)p->S1, nullptr, p->kx, p->ky, (const C*)p->twy, 1.0,
       (C*)p->S3, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
@@ -661,7 +813,8 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
   p->v_env = comp->v_env;
   p->epsilon = comp->epsilon;
   p->diag_every = comp->poisson_diag_every;
-  if (!factorize(nx / 2, p->px) || !factorize(ny, p->py))
+  if (!factorize(nx / 2, p->px) || !factorize(ny, p->py) || !factorize(nx / 2, p->pxf, false) ||
+      !factorize(ny, p->pyf, false))
     return bail(fail(OB_ERR_ARG, "nx/2=%d and ny=%d must factor into 2, 3, 5", nx / 2, ny));
 
   const double dz = p->g.dz;
@@ -740,6 +893,8 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
         cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs<double>())) return bail(rc);
+    if ((rc = setup_pipes<double>(p))) return bail(rc);
+    if (const char* e = getenv("ORACLE_B200_PIPE")) p->use_pipe = atoi(e) != 0;
   } else {
     auto tx = twiddles<float>(nx), ty = twiddles<float>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<float>)))) return bail(rc);
@@ -748,14 +903,17 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
         cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<float>), cudaMemcpyHostToDevice))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs<float>())) return bail(rc);
+    if ((rc = setup_pipes<float>(p))) return bail(rc);
+    if (const char* e = getenv("ORACLE_B200_PIPE")) p->use_pipe = atoi(e) != 0;
   }
 
   // chunk sizes: largest z-chunk whose shared-memory footprint allows two CTAs/SM
   const size_t ce = 2 * p->esz;  // complex element
-  p->zc_fx = pick_zc(nz, 2ull * (p->g.M + 1) * 3 * ce, 0);
-  p->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, 0);
+  p->zc_fx = pick_zc(nz, 2ull * (p->g.M + 1) * 3 * ce, tw_bytes(p, nx));
+  p->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, tw_bytes(p, ny));
   p->zc_iy = p->zc_fy;
-  p->zc_ix = pick_zc(nz, (size_t)(2 * p->g.M + 1) * 3 * ce, (size_t)(2 * p->g.M + 1) * ce);
+  p->zc_ix = pick_zc(nz, (size_t)(2 * p->g.M + 1) * 3 * ce,
+                     tw_bytes(p, nx) + (size_t)(2 * p->g.M + 1) * ce);
   if (smem_fx(p, 3) > kSmemMax || smem_fy(p, 2, p->zc_fy) > kSmemMax ||
       smem_ix(p, 3 * p->zc_ix + 1) > kSmemMax || smem_thomas(p) > kSmemMax)
     return bail(fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx,
@@ -1003,13 +1161,15 @@ int noalloc_solve(const OracleGridDesc* grid, const double* rho0, const T* d, T*
   p.g.dx = grid->Lx / nx;
   p.g.dy = grid->Ly / ny;
   p.g.dz = grid->Lz / nz;
-  if (!factorize(nx / 2, p.px) || !factorize(ny, p.py))
+  if (!factorize(nx / 2, p.px) || !factorize(ny, p.py) || !factorize(nx / 2, p.pxf, false) ||
+      !factorize(ny, p.pyf, false))
     return fail(OB_ERR_ARG, "nx/2=%d and ny=%d must factor into 2, 3, 5", nx / 2, ny);
   const size_t ce = 2 * sizeof(T);
-  p.zc_fx = pick_zc(nz, 2ull * (p.g.M + 1) * 3 * ce, 0);
-  p.zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, 0);
+  p.zc_fx = pick_zc(nz, 2ull * (p.g.M + 1) * 3 * ce, tw_bytes(&p, nx));
+  p.zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, tw_bytes(&p, ny));
   p.zc_iy = p.zc_fy;
-  p.zc_ix = pick_zc(nz, (size_t)(2 * p.g.M + 1) * 3 * ce, (size_t)(2 * p.g.M + 1) * ce);
+  p.zc_ix = pick_zc(nz, (size_t)(2 * p.g.M + 1) * 3 * ce,
+                    tw_bytes(&p, nx) + (size_t)(2 * p.g.M + 1) * ce);
   if (smem_fx(&p, 3) > kSmemMax || smem_fy(&p, 2, p.zc_fy) > kSmemMax ||
       smem_ix(&p, 3 * p.zc_ix + 1) > kSmemMax || smem_thomas(&p) > kSmemMax)
     return fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx, ny, nz);

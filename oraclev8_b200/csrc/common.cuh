@@ -58,11 +58,28 @@ struct GridK {
   double dx, dy, dz;
 };
 
-// Mixed-radix factor list of a complex FFT length.
+// Division by a runtime-invariant divisor d >= 1 as a multiply-high, add and
+// shift (Granlund & Montgomery, 1994): q = (umulhi(m, n) + n) >> l with
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1.  Exact for n < 2^31.
+struct FastDiv {
+  unsigned d, m, l;
+  __host__ __device__ FastDiv() : d(1), m(1), l(0) {}
+  __host__ __device__ explicit FastDiv(unsigned dd) : d(dd), m(1), l(0) {
+    while ((1u << l) < d) ++l;
+    m = (unsigned)((((unsigned long long)1 << 32) * ((1ull << l) - d)) / d + 1ull);
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi(m, (unsigned)n) + (unsigned)n) >> l);
+  }
+};
+
+// Mixed-radix factor list of a complex FFT length, with the invariant
+// divisors of each Stockham pass (Ns = product of the earlier radices).
 struct FftPlan {
   int M;
   int np;
-  int r[20];
+  int r[16];
+  FastDiv ns[16];
 };
 
 constexpr double kGravity = 9.81;  // oracle_v8/constants.py:25

@@ -43,12 +43,17 @@ __device__ __forceinline__ double stage_w(const T* __restrict__ wc, const T* __r
   return arn((double)wc[k], mrn(sdt, bhalf(thc, k, nz, theta0)));
 }
 
+// global loads each thread issues before consuming them (memory-level parallelism)
+constexpr int kLoadBatch = 4;
+// state values per thread k_ix prefetches ahead of its FFT
+constexpr int kIxPrefetch = 4;
+
 enum FxMode { FX_DIV = 0, FX_DIV_STAGE = 1, FX_FIELDS = 2 };
 
 // x-pencil forward kernel.  grid = (ny, ceil(nz/zc)).  smem: 2 * (M+1) * B cplx.
 // FX_FIELDS transforms `nf` real fields f0..f2 (no weighting) into X0..X2.
 template <class T, int MODE>
-__global__ void __launch_bounds__(512) k_fx(GridK g, FftPlan px, int zc, int nf,
+__global__ void __launch_bounds__(256, 2) k_fx(GridK g, FftPlan px, int zc, int nf,
                                             const T* __restrict__ f0, const T* __restrict__ f1,
                                             const T* __restrict__ f2, const T* __restrict__ th,
                                             double sdt, const double* __restrict__ rho,
@@ -58,59 +63,74 @@ __global__ void __launch_bounds__(512) k_fx(GridK g, FftPlan px, int zc, int nf,
                                             const cplx<T>* __restrict__ twx,
                                             cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1,
                                             cplx<T>* __restrict__ X2) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  // twiddle table staged in shared memory (off the butterflies' critical path)
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  for (int i = threadIdx.x; i < g.nx; i += blockDim.x) stw[i] = twx[i];
+  unsigned char* smem_raw = smem_dyn + ((((size_t)g.nx) * sizeof(cplx<T>) + 15) & ~size_t(15));
   const int NF = (MODE == FX_FIELDS) ? nf : 3;
   const int B = NF * zc;
   const int M = g.M;
   cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* bufB = bufA + (size_t)(M + 1) * B;
-  const int y = blockIdx.x;
-  const int z0 = blockIdx.y * zc;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * zc;
   const int zn = min(zc, g.nz - z0);
   const int nz = g.nz;
   T* rA = reinterpret_cast<T*>(bufA);
 
+  // Load phase: each thread gathers kLoadBatch elements into registers before
+  // writing shared memory, so that many global loads are in flight at once.
   const int nel = g.nx * zc;
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-    const int x = e / zc;
-    const int zl = e - x * zc;
-    const int n = x >> 1, odd = x & 1;
-    const size_t col = (size_t)x * g.ny + y;
-    if (MODE == FX_FIELDS) {
-      for (int f = 0; f < NF; ++f) {
-        const T* src = f == 0 ? f0 : (f == 1 ? f1 : f2);
-        T val = (T)0;
-        if (zl < zn) val = src[col * nz + z0 + zl];
-        rA[2 * ((size_t)n * B + f * zc + zl) + odd] = val;
-      }
-    } else {
-      T a = 0, b = 0, c = 0;
-      if (zl < zn) {
+  for (int e0 = threadIdx.x; e0 < nel; e0 += kLoadBatch * blockDim.x) {
+    T va[kLoadBatch][3];
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      va[q][0] = va[q][1] = va[q][2] = (T)0;
+      const int x = e / zc;
+      const int zl = e - x * zc;
+      if (e < nel && zl < zn) {
+        const size_t col = (size_t)x * g.ny + y;
         const int z = z0 + zl;
-        const double r = rho[z];
-        a = (T)(r * (double)f0[col * nz + z]);
-        b = (T)(r * (double)f1[col * nz + z]);
-        const T* wc = f2 + col * (nz + 1);
-        double wl, wu;
-        if (MODE == FX_DIV_STAGE) {
-          const T* thc = th + col * nz;
-          wl = stage_w(wc, thc, z, nz, sdt, theta0);
-          wu = stage_w(wc, thc, z + 1, nz, sdt, theta0);
+        if (MODE == FX_FIELDS) {
+          va[q][0] = f0[col * nz + z];
+          if (NF > 1) va[q][1] = f1[col * nz + z];
+          if (NF > 2) va[q][2] = f2[col * nz + z];
         } else {
-          wl = (double)wc[z];
-          wu = (double)wc[z + 1];
+          const double r = rho[z];
+          va[q][0] = (T)(r * (double)f0[col * nz + z]);
+          va[q][1] = (T)(r * (double)f1[col * nz + z]);
+          const T* wc = f2 + col * (nz + 1);
+          double wl, wu;
+          if (MODE == FX_DIV_STAGE) {
+            const T* thc = th + col * nz;
+            wl = stage_w(wc, thc, z, nz, sdt, theta0);
+            wu = stage_w(wc, thc, z + 1, nz, sdt, theta0);
+          } else {
+            wl = (double)wc[z];
+            wu = (double)wc[z + 1];
+          }
+          va[q][2] = (T)((rhoh[z + 1] * wu - rhoh[z] * wl) / g.dz);
         }
-        c = (T)((rhoh[z + 1] * wu - rhoh[z] * wl) / g.dz);
       }
-      rA[2 * ((size_t)n * B + zl) + odd] = a;
-      rA[2 * ((size_t)n * B + zc + zl) + odd] = b;
-      rA[2 * ((size_t)n * B + 2 * zc + zl) + odd] = c;
+    }
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      if (e >= nel) continue;
+      const int x = e / zc;
+      const int zl = e - x * zc;
+      const int n = x >> 1, odd = x & 1;
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+        if (f < NF) rA[2 * ((size_t)n * B + f * zc + zl) + odd] = va[q][f];
     }
   }
   __syncthreads();
-  cplx<T>* Z = fft_smem<T, false>(bufA, bufB, B, px, twx, 2);
+  cplx<T>* Z = fft_smem<T, false, 4>(bufA, bufB, B, px, stw, 2);
   cplx<T>* X = (Z == bufA) ? bufB : bufA;
-  r2c_post<T>(Z, X, M, B, twx);
+  r2c_post<T>(Z, X, M, B, stw);
   __syncthreads();
 
   const int nout = (M + 1) * zc;
@@ -145,7 +165,7 @@ enum FyMode { FY_DIV = 0, FY_FIELDS = 1, FY_HELM = 2 };
 //   s = scale; the primed cross term is zero where exactly one of kx, ky is
 //   the Nyquist index (there the reference's real() drops it).
 template <class T, int MODE>
-__global__ void __launch_bounds__(512) k_fy(GridK g, FftPlan py, int zc, int nf,
+__global__ void __launch_bounds__(256, 2) k_fy(GridK g, FftPlan py, int zc, int nf,
                                             const cplx<T>* __restrict__ in0,
                                             const cplx<T>* __restrict__ in1,
                                             const double* __restrict__ kxd,
@@ -153,29 +173,47 @@ __global__ void __launch_bounds__(512) k_fy(GridK g, FftPlan py, int zc, int nf,
                                             const cplx<T>* __restrict__ twy, double scale,
                                             cplx<T>* __restrict__ out0,
                                             cplx<T>* __restrict__ out1) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  // twiddle table staged in shared memory (off the butterflies' critical path)
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  for (int i = threadIdx.x; i < g.ny; i += blockDim.x) stw[i] = twy[i];
+  unsigned char* smem_raw = smem_dyn + ((((size_t)g.ny) * sizeof(cplx<T>) + 15) & ~size_t(15));
   const int NF = (MODE == FY_FIELDS) ? nf : 2;
   const int B = NF * zc;
   const int ny = g.ny, nz = g.nz;
   cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* bufB = bufA + (size_t)ny * B;
-  const int kx = blockIdx.x;
-  const int z0 = blockIdx.y * zc;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * zc;
   const int zn = min(zc, nz - z0);
   const int nel = ny * zc;
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-    const int y = e / zc;
-    const int zl = e - y * zc;
-    const size_t o = ((size_t)kx * ny + y) * nz + z0 + zl;
-    for (int f = 0; f < NF; ++f) {
-      const cplx<T>* src = f == 0 ? in0 : in1;
-      cplx<T> val = mk<T>((T)0, (T)0);
-      if (zl < zn) val = src[o];
-      bufA[(size_t)y * B + f * zc + zl] = val;
+  for (int e0 = threadIdx.x; e0 < nel; e0 += kLoadBatch * blockDim.x) {
+    cplx<T> va[kLoadBatch][2];
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      const int y = e / zc;
+      const int zl = e - y * zc;
+      va[q][0] = va[q][1] = mk<T>((T)0, (T)0);
+      if (e < nel && zl < zn) {
+        const size_t o = ((size_t)kx * ny + y) * nz + z0 + zl;
+        va[q][0] = in0[o];
+        if (NF > 1) va[q][1] = in1[o];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      if (e >= nel) continue;
+      const int y = e / zc;
+      const int zl = e - y * zc;
+#pragma unroll
+      for (int f = 0; f < 2; ++f)
+        if (f < NF) bufA[(size_t)y * B + f * zc + zl] = va[q][f];
     }
   }
   __syncthreads();
-  cplx<T>* R = fft_smem<T, false>(bufA, bufB, B, py, twy, 1);
+  cplx<T>* R = fft_smem<T, false, 4>(bufA, bufB, B, py, stw, 1);
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     const int ky = e / zc;
     const int zl = e - ky * zc;
@@ -374,44 +412,61 @@ enum IyMode { IY_GRAD = 0, IY_FIELDS = 1 };
 // IY_GRAD: out0 = IFFTy(in0), out1 = IFFTy(i ky' in0).
 // IY_FIELDS: out_f = IFFTy(scale * in_f), f < nf.
 template <class T, int MODE>
-__global__ void __launch_bounds__(512) k_iy(GridK g, FftPlan py, int zc, int nf,
+__global__ void __launch_bounds__(256, 2) k_iy(GridK g, FftPlan py, int zc, int nf,
                                             const cplx<T>* __restrict__ in0,
                                             const cplx<T>* __restrict__ in1,
                                             const double* __restrict__ kyd,
                                             const cplx<T>* __restrict__ twy, double scale,
                                             cplx<T>* __restrict__ out0,
                                             cplx<T>* __restrict__ out1) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  // twiddle table staged in shared memory (off the butterflies' critical path)
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  for (int i = threadIdx.x; i < g.ny; i += blockDim.x) stw[i] = twy[i];
+  unsigned char* smem_raw = smem_dyn + ((((size_t)g.ny) * sizeof(cplx<T>) + 15) & ~size_t(15));
   const int NF = (MODE == IY_FIELDS) ? nf : 2;
   const int B = NF * zc;
   const int ny = g.ny, nz = g.nz;
   cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* bufB = bufA + (size_t)ny * B;
-  const int kx = blockIdx.x;
-  const int z0 = blockIdx.y * zc;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * zc;
   const int zn = min(zc, nz - z0);
   const int nel = ny * zc;
   const T s = (T)scale;
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-    const int ky = e / zc;
-    const int zl = e - ky * zc;
-    const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
-    if (MODE == IY_GRAD) {
-      cplx<T> v = mk<T>((T)0, (T)0);
-      if (zl < zn) v = scl(in0[o], s);
-      const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
-      bufA[(size_t)ky * B + zl] = v;
-      bufA[(size_t)ky * B + zc + zl] = ik(kk, v);
-    } else {
-      for (int f = 0; f < NF; ++f) {
-        cplx<T> v = mk<T>((T)0, (T)0);
-        if (zl < zn) v = scl((f == 0 ? in0 : in1)[o], s);
-        bufA[(size_t)ky * B + f * zc + zl] = v;
+  for (int e0 = threadIdx.x; e0 < nel; e0 += kLoadBatch * blockDim.x) {
+    cplx<T> va[kLoadBatch][2];
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      const int ky = e / zc;
+      const int zl = e - ky * zc;
+      va[q][0] = va[q][1] = mk<T>((T)0, (T)0);
+      if (e < nel && zl < zn) {
+        const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
+        va[q][0] = scl(in0[o], s);
+        if (MODE == IY_FIELDS && NF > 1) va[q][1] = scl(in1[o], s);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      if (e >= nel) continue;
+      const int ky = e / zc;
+      const int zl = e - ky * zc;
+      if (MODE == IY_GRAD) {
+        const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
+        bufA[(size_t)ky * B + zl] = va[q][0];
+        bufA[(size_t)ky * B + zc + zl] = ik(kk, va[q][0]);
+      } else {
+#pragma unroll
+        for (int f = 0; f < 2; ++f)
+          if (f < NF) bufA[(size_t)ky * B + f * zc + zl] = va[q][f];
       }
     }
   }
   __syncthreads();
-  cplx<T>* R = fft_smem<T, true>(bufA, bufB, B, py, twy, 1);
+  cplx<T>* R = fft_smem<T, true>(bufA, bufB, B, py, stw, 1);
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     const int y = e / zc;
     const int zl = e - y * zc;
@@ -436,7 +491,7 @@ enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3 };
 //               (tendency.py:487-500).
 //   IX_FIELDS:  real outputs of nf spectra.
 template <class T, int MODE>
-__global__ void __launch_bounds__(512) k_ix(GridK g, FftPlan px, int zc, int nf,
+__global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int nf,
                                             const cplx<T>* __restrict__ phs,
                                             const cplx<T>* __restrict__ psi,
                                             const cplx<T>* __restrict__ s2,
@@ -446,52 +501,99 @@ __global__ void __launch_bounds__(512) k_ix(GridK g, FftPlan px, int zc, int nf,
                                             const T* __restrict__ th, double sdt,
                                             const double* __restrict__ theta0, T* u_out,
                                             T* v_out, T* w_out, T* phi_out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  // twiddle table staged in shared memory (off the butterflies' critical path)
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  for (int i = threadIdx.x; i < g.nx; i += blockDim.x) stw[i] = twx[i];
+  unsigned char* smem_raw = smem_dyn + ((((size_t)g.nx) * sizeof(cplx<T>) + 15) & ~size_t(15));
   const bool fields = (MODE == IX_FIELDS);
   const int B = fields ? nf * zc : 3 * zc + 1;
   const int M = g.M;
   const int nz = g.nz;
   cplx<T>* bufX = reinterpret_cast<cplx<T>*>(smem_raw);  // (M+1) * B
   cplx<T>* bufZ = bufX + (size_t)(M + 1) * B;             // M * B
-  const int y = blockIdx.x;
-  const int z0 = blockIdx.y * zc;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * zc;
   const int zn = min(zc, nz - z0);
 
-  // load spectra X[k][b]
+  // load spectra X[k][b], kLoadBatch elements per thread in flight
   const int nel = (M + 1) * B;
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-    const int k = e / B;
-    const int bb = e - k * B;
-    cplx<T> v = mk<T>((T)0, (T)0);
-    const size_t rowo = ((size_t)k * g.ny + y) * nz;
-    if (fields) {
-      const int f = bb / zc, zl = bb - f * zc;
-      if (zl < zn) v = (f == 0 ? phs : (f == 1 ? psi : s2))[rowo + z0 + zl];
-    } else if (bb <= zc) {
-      // phi at level z0 - 1 + bb (bb = 0 is the halo below the chunk)
-      const int z = z0 - 1 + bb;
-      if (z >= 0 && bb <= zn) v = phs[rowo + z];
-    } else if (bb <= 2 * zc) {
-      const int zl = bb - zc - 1;
-      if (zl < zn) {
-        const T kk = (k == M) ? (T)0 : (T)kxd[k];
-        v = ik(kk, phs[rowo + z0 + zl]);
+  for (int e0 = threadIdx.x; e0 < nel; e0 += kLoadBatch * blockDim.x) {
+    cplx<T> va[kLoadBatch];
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      const int k = e / B;
+      const int bb = e - k * B;
+      cplx<T> v = mk<T>((T)0, (T)0);
+      if (e < nel) {
+        const size_t rowo = ((size_t)k * g.ny + y) * nz;
+        if (fields) {
+          const int f = bb / zc, zl = bb - f * zc;
+          if (zl < zn) v = (f == 0 ? phs : (f == 1 ? psi : s2))[rowo + z0 + zl];
+        } else if (bb <= zc) {
+          // phi at level z0 - 1 + bb (bb = 0 is the halo below the chunk)
+          const int z = z0 - 1 + bb;
+          if (z >= 0 && bb <= zn) v = phs[rowo + z];
+        } else if (bb <= 2 * zc) {
+          const int zl = bb - zc - 1;
+          if (zl < zn) {
+            const T kk = (k == M) ? (T)0 : (T)kxd[k];
+            v = ik(kk, phs[rowo + z0 + zl]);
+          }
+        } else {
+          const int zl = bb - 2 * zc - 1;
+          if (zl < zn) v = psi[rowo + z0 + zl];
+        }
       }
-    } else {
-      const int zl = bb - 2 * zc - 1;
-      if (zl < zn) v = psi[rowo + z0 + zl];
+      va[q] = v;
     }
-    bufX[e] = v;
+#pragma unroll
+    for (int q = 0; q < kLoadBatch; ++q) {
+      const int e = e0 + q * blockDim.x;
+      if (e < nel) bufX[e] = va[q];
+    }
+  }
+  // Prefetch the state values this thread will correct, so their load
+  // latency overlaps the shared-memory FFT below (CORRECT / STAGE modes).
+  const int nout = g.nx * zc;
+  const bool pre = (MODE == IX_CORRECT || MODE == IX_STAGE) && nout <= kIxPrefetch * (int)blockDim.x;
+  T pu[kIxPrefetch], pv[kIxPrefetch], pw[kIxPrefetch], pt[kIxPrefetch];
+  if (pre) {
+#pragma unroll
+    for (int q = 0; q < kIxPrefetch; ++q) {
+      const int e = threadIdx.x + q * blockDim.x;
+      pu[q] = pv[q] = pw[q] = pt[q] = (T)0;
+      const int x = e / zc;
+      const int zl = e - x * zc;
+      if (e < nout && zl < zn) {
+        const int z = z0 + zl;
+        const size_t col = (size_t)x * g.ny + y;
+        const size_t idx = col * nz + z;
+        const size_t wi = col * (nz + 1) + z;
+        pu[q] = u_in[idx];
+        pv[q] = v_in[idx];
+        if (MODE == IX_CORRECT) {
+          pw[q] = w_in[wi];
+          if (z == nz - 1) pt[q] = w_in[wi + 1];
+        } else {
+          const T* wc = w_in + col * (nz + 1);
+          const T* thc = th + col * nz;
+          pw[q] = (T)stage_w(wc, thc, z, nz, sdt, theta0);
+          if (z == nz - 1) pt[q] = (T)stage_w(wc, thc, nz, nz, sdt, theta0);
+        }
+      }
+    }
   }
   __syncthreads();
-  c2r_pre<T>(bufX, bufZ, M, B, twx);
+  c2r_pre<T>(bufX, bufZ, M, B, stw);
   __syncthreads();
-  cplx<T>* Zr = fft_smem<T, true>(bufZ, bufX, B, px, twx, 2);
+  cplx<T>* Zr = fft_smem<T, true>(bufZ, bufX, B, px, stw, 2);
   const T* rz = reinterpret_cast<const T*>(Zr);
   // real value of batch bb at x: rz[2 * ((x >> 1) * B + bb) + (x & 1)]
 
-  const int nout = g.nx * zc;
-  for (int e = threadIdx.x; e < nout; e += blockDim.x) {
+#pragma unroll 1
+  for (int e = threadIdx.x, q = 0; e < nout; e += blockDim.x, ++q) {
     const int x = e / zc;
     const int zl = e - x * zc;
     if (zl >= zn) continue;
@@ -517,21 +619,34 @@ __global__ void __launch_bounds__(512) k_ix(GridK g, FftPlan px, int zc, int nf,
       v_out[idx] = gy;
       w_out[wi] = gz;
       if (z == nz - 1) w_out[wi + 1] = (T)0;
-    } else if (MODE == IX_CORRECT) {
-      u_out[idx] = u_in[idx] - gx;
-      v_out[idx] = v_in[idx] - gy;
-      w_out[wi] = w_in[wi] - gz;
-      if (z == nz - 1 && w_out != w_in) w_out[wi + 1] = w_in[wi + 1];
-      phi_out[idx] = phi;
-    } else {  // IX_STAGE
-      const T* wc = w_in + col * (nz + 1);
-      const T* thc = th + col * nz;
-      u_out[idx] = u_in[idx] - gx;
-      v_out[idx] = v_in[idx] - gy;
-      w_out[wi] = (T)stage_w(wc, thc, z, nz, sdt, theta0) - gz;
-      if (z == nz - 1) w_out[wi + 1] = (T)stage_w(wc, thc, nz, nz, sdt, theta0);
-      phi_out[idx] = phi;
+      continue;
     }
+    T uc, vc, wc, wt;
+    if (pre) {
+      // q < kIxPrefetch whenever pre holds; select the register without
+      // dynamic indexing of the arrays
+      uc = pu[0]; vc = pv[0]; wc = pw[0]; wt = pt[0];
+#pragma unroll
+      for (int r = 1; r < kIxPrefetch; ++r)
+        if (q == r) { uc = pu[r]; vc = pv[r]; wc = pw[r]; wt = pt[r]; }
+    } else {
+      uc = u_in[idx];
+      vc = v_in[idx];
+      if (MODE == IX_CORRECT) {
+        wc = w_in[wi];
+        wt = (z == nz - 1) ? w_in[wi + 1] : (T)0;
+      } else {
+        const T* wcol = w_in + col * (nz + 1);
+        const T* thc = th + col * nz;
+        wc = (T)stage_w(wcol, thc, z, nz, sdt, theta0);
+        wt = (z == nz - 1) ? (T)stage_w(wcol, thc, nz, nz, sdt, theta0) : (T)0;
+      }
+    }
+    u_out[idx] = uc - gx;
+    v_out[idx] = vc - gy;
+    w_out[wi] = wc - gz;
+    if (z == nz - 1 && (MODE == IX_STAGE || w_out != w_in)) w_out[wi + 1] = wt;
+    phi_out[idx] = phi;
   }
 }
 
@@ -555,6 +670,10 @@ struct SlowK {
   double inv2dx, inv2dy, inv60dx, inv60dy, inv2dz, invdz;
 };
 
+// WS5 upwind derivative along one horizontal axis.  cols[r] are the linear
+// column indices of the neighbours i-3, i-2, i-1, i+1, i+2, i+3 (periodic);
+// the value at neighbour r, level k is q[cols[r] * nzk + k].  Only the six
+// points of the stencil a selects are loaded (tendency.py:940-959).
 template <class T>
 __device__ __forceinline__ double ddx_ws5(const T* __restrict__ q, size_t o, const size_t* off,
                                           double a, double inv60d) {
