@@ -1,6 +1,6 @@
 """Benchmark of the LH82 anelastic RK3 step (cell-updates/s) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32r|fp64|fp32]
                     [--workload config1|config0|config2] [--impl b200|reference]
 
 Default workload: the mid-size single run — 512 x 512 x 64 cells, dx = 5 km,
@@ -15,7 +15,15 @@ so consecutive steps stream from HBM.
 One "step" = one full RK3Integrator.step: two Strang slow half steps (fused
 WS5 + Coriolis + heating tendency and forward Euler), three fast stages, five
 anelastic projections (FFT x/y + Thomas z + correction) and the device-side
-step diagnostics.  N > 1: N independent replicas, one per GPU (the path
+step diagnostics.
+
+Precision (the metric is FP32-refined against plain FP64): the default
+``fp32r`` runs the step on an FP32 state and, after its final projection, one
+defect correction whose residual divergence is formed in FP64.  The same line
+then carries ``fp64_plain`` (the plain FP64 step timed the same way on the
+same workload, and the ratio) and ``accuracy`` (per-field error of the FP32
+run against the FP64 run after the same steps, and the FP64-evaluated
+divergence of both).  ``--precision fp64`` times the plain FP64 step alone.  N > 1: N independent replicas, one per GPU (the path
 partitions into independent runs; no collective on the data path).
 
 --impl reference times the reference algorithm on the host CPU (the NumPy
@@ -304,6 +312,65 @@ def load_traffic(wname, precision):
     return NCU_TRAFFIC.get((wname, precision), {})
 
 
+def _timed_steps(integ, st, dt, steps, warmup, barrier):
+    """W untimed steps, then K steps bracketed by barrier + synchronize and
+    timed with CUDA events on the launching stream; per-class kernel times
+    from the plan's own launch events."""
+    import torch
+    for _ in range(warmup):
+        integ.step_(st, dt, want_diag=True)
+    torch.cuda.synchronize()
+    plan = integ.plan
+    plan.profile(True)
+    l0 = plan.launches
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        integ.step_(st, dt, want_diag=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = plan.launches - l0
+    prof = plan.profile_read()
+    plan.profile(False)
+    if not bool(torch.isfinite(st.u).all()):
+        raise RuntimeError("non-finite state after the timed steps")
+    return ms, launches, prof
+
+
+def _non_nyquist_max(d):
+    """max |d| after removing the Nyquist rows of the horizontal spectrum
+    (measurement only; the spectral derivative of the reference cannot act
+    on them)."""
+    import torch
+    nx, ny = d.shape[:2]
+    D = torch.fft.fft2(d, dim=(0, 1))
+    D[nx // 2] = 0
+    D[:, ny // 2] = 0
+    return float(torch.fft.ifft2(D, dim=(0, 1)).real.abs().max())
+
+
+def _precision_report(st, st64, plan64):
+    """Per-field error of a single-precision run against the FP64 run from the
+    same initial state and step count (max |a - b| / max |b|), and the FP64
+    evaluation of the post-step anelastic divergence of both."""
+    fields = ("u", "v", "w", "theta_prime", "projection_potential")
+    err = {}
+    for f in fields:
+        a, b = getattr(st, f).double(), getattr(st64, f)
+        err[f] = float((a - b).abs().max() / b.abs().max().clamp_min(1e-300))
+    d32 = plan64.divergence(st.u.double(), st.v.double(), st.w.double())
+    d64 = plan64.divergence(st64.u, st64.v, st64.w)
+    return {"rel_err_vs_fp64": err,
+            "divergence_non_nyquist_max": {"this": _non_nyquist_max(d32),
+                                           "fp64": _non_nyquist_max(d64)},
+            "divergence_max": {"this": float(d32.abs().max()), "fp64": float(d64.abs().max())}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -326,45 +393,37 @@ def run_b200(args):
     S = 8 if args.precision == "fp64" else 4
     dev = torch.device("cuda", torch.cuda.current_device())
 
-    def to_dev(a):
-        return torch.as_tensor(a, dtype=dtype).to(dev)
-
-    st = State(to_dev(hs.u), to_dev(hs.v), to_dev(hs.w), to_dev(hs.theta_prime),
-               to_dev(hs.projection_potential), 0.0)
-    for _ in range(args.warmup):
-        integ.step_(st, dt, want_diag=True)
-    torch.cuda.synchronize()
+    def to_dev(a, dt_=None):
+        return torch.as_tensor(a, dtype=dt_ or dtype).to(dev)
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    st = State(to_dev(hs.u), to_dev(hs.v), to_dev(hs.w), to_dev(hs.theta_prime),
+               to_dev(hs.projection_potential), 0.0)
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
-    plan = integ.plan
-    plan.profile(True)
-    l0 = plan.launches
-    stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        integ.step_(st, dt, want_diag=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1)
-    launches = plan.launches - l0
-    prof = plan.profile_read()
-    plan.profile(False)
+    ms, launches, prof = _timed_steps(integ, st, dt, args.steps, args.warmup, barrier)
+    companion = None
+    if args.precision != "fp64":
+        # the plain FP64 step on the same workload, timed the same way, and the
+        # error of this run against it after the same number of steps
+        integ64, _ = b200_integrator(w, "fp64")
+        f64 = torch.float64
+        st64 = State(to_dev(hs.u, f64), to_dev(hs.v, f64), to_dev(hs.w, f64),
+                     to_dev(hs.theta_prime, f64), to_dev(hs.projection_potential, f64), 0.0)
+        ms64, _, _ = _timed_steps(integ64, st64, dt, args.steps, args.warmup, barrier)
+        companion = (ms64, _precision_report(st, st64, integ64.plan))
+        del st64, integ64
     clk = clocks.stop()
-    if not bool(torch.isfinite(st.u).all()):
-        raise RuntimeError("non-finite state after the timed steps")
     if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        t = torch.tensor([ms] + ([companion[0]] if companion else []), device=dev,
+                         dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = float(t[0].item())
+        if companion:
+            companion = (float(t[1].item()), companion[1])
     cells = w["nx"] * w["ny"] * w["nz"]
     value = world * cells * args.steps / (ms / 1e3)
 
@@ -418,7 +477,8 @@ def run_b200(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "dtype": "f64" if args.precision == "fp64" else "f32 (f64 residual)" if
+        args.precision == "fp32r" else "f32",
         "data": "synthetic (seeded Holland vortex + theta' noise; no dataset in the reference)",
         "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step, "
                                f"WS5 + beta-plane + buoyancy + projection"
@@ -439,6 +499,16 @@ def run_b200(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if companion:
+        v64 = world * cells * args.steps / (companion[0] / 1e3)
+        line["fp64_plain"] = {"value": v64, "unit": "cell-updates/s",
+                              "ms_per_step": companion[0] / args.steps,
+                              "ratio": value / v64,
+                              "note": "plain FP64 step on the same workload and GPU, timed "
+                                      "the same way (W warm-up + K timed steps)"}
+        line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
+                                note="this run vs the FP64 run from the same initial state; "
+                                     "divergence = anelastic divergence evaluated in FP64")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rates, sc = cpu_sample_rate(args.workload, 1, 1, 1)
         line["cpu_baseline"] = {
@@ -495,7 +565,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp32r", choices=["fp64", "fp32", "fp32r"])
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

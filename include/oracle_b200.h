@@ -156,6 +156,17 @@ int oracle_b200_tendency(OraclePlan *plan, int mask, const OracleStatePtrs *stat
 /* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
 int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);
 
+/* FP64 defect correction of single-precision plans (BASELINE precision
+ * scheme; no counterpart in the reference, which is FP64 throughout).  After
+ * the final projection of every `every`-th step, `passes` correction passes
+ * run: the divergence of the stored FP32 velocity is formed in FP64, the
+ * correction potential solved with the FP64 Thomas sweep, and u, v, w -=
+ * grad(dphi), phi += dphi.  passes = 0 (the default) gives the plain FP32 step. */
+int oracle_b200_set_refinement(OraclePlan *plan, int passes, int every);
+
+/* One defect-correction pass on a projected FP32 state, in place. */
+int oracle_b200_refine(OraclePlan *plan, void *u, void *v, void *w, void *phi, void *stream);
+
 /* Number of kernels this plan has launched since creation (launch accounting
  * for benchmarks).  No counterpart in the reference (it launches through CuPy). */
 long oracle_b200_launch_count(const OraclePlan *plan);
@@ -174,7 +185,8 @@ long oracle_b200_launch_count(const OraclePlan *plan);
 #define OB_PROF_SLOW 5    /* fused slow tendency + forward Euler */
 #define OB_PROF_DIAG 6    /* step diagnostics reductions */
 #define OB_PROF_OTHER 7
-#define OB_PROF_CLASSES 8
+#define OB_PROF_REFINE 8  /* defect-correction passes of single-precision plans */
+#define OB_PROF_CLASSES 9
 int oracle_b200_profile(OraclePlan *plan, int enable);
 int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
 

@@ -29,8 +29,9 @@ EXPORTS = (
     "oracle_b200_buoyancy", "oracle_b200_tendency", "oracle_b200_read_diag",
     "oracle_b200_last_error", "oracle_b200_version", "oracle_b200_launch_count",
     "oracle_b200_profile", "oracle_b200_profile_read", "oracle_b200_poisson_solve_noalloc",
+    "oracle_b200_set_refinement", "oracle_b200_refine",
 )
-PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other")
+PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
 
 class GridDesc(ctypes.Structure):
@@ -86,6 +87,8 @@ def load(path: Path | None = None):
         "oracle_b200_profile": ([vp, c_int], c_int),
         "oracle_b200_profile_read": ([vp, POINTER(c_double), POINTER(ctypes.c_long), c_int], c_int),
         "oracle_b200_poisson_solve_noalloc": ([POINTER(GridDesc), POINTER(c_double), vp, vp, vp], c_int),
+        "oracle_b200_set_refinement": ([vp, c_int, c_int], c_int),
+        "oracle_b200_refine": ([vp, vp, vp, vp, vp, vp], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -135,6 +135,17 @@ class Plan:
         L.check(self.lib.oracle_b200_profile_read(self.handle, ms, cnt, n))
         return {c: (float(ms[i]), int(cnt[i])) for i, c in enumerate(L.PROF_CLASSES)}
 
+    def set_refinement(self, passes: int, every: int = 1) -> None:
+        """FP64 defect correction of the final projection of every `every`-th
+        step (single-precision plans)."""
+        L.check(self.lib.oracle_b200_set_refinement(self.handle, int(passes), int(every)))
+
+    def refine(self, u, v, w, phi):
+        s = self.shape
+        L.check(self.lib.oracle_b200_refine(self.handle, self._ptr(u, s), self._ptr(v, s),
+                                            self._ptr(w, self.wshape), self._ptr(phi, s),
+                                            self._stream()))
+
     def read_diag(self) -> np.ndarray:
         buf = (ctypes.c_double * L.DIAG_COUNT)()
         L.check(self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream()))

@@ -3,7 +3,8 @@
 The reference selects NumPy or CuPy as ``xp``; this backend keeps every
 prognostic field as a CUDA ``torch.Tensor`` (z contiguous, C order) and runs
 the step through the sm_100a library.  ``ORACLE_B200_PRECISION`` selects the
-default device dtype: ``fp64`` (default) or ``fp32``.
+default device dtype: ``fp64`` (default), ``fp32``, or ``fp32r`` (FP32 state
+with one FP64-residual defect correction of the projection per step).
 """
 from __future__ import annotations
 
@@ -14,8 +15,8 @@ import torch as xp  # device arrays are torch tensors
 
 GPU_AVAILABLE: bool = bool(xp.cuda.is_available())
 PRECISION: str = _os.environ.get("ORACLE_B200_PRECISION", "fp64")
-if PRECISION not in ("fp64", "fp32"):
-    raise ValueError(f"ORACLE_B200_PRECISION must be fp64 or fp32, got {PRECISION!r}")
+if PRECISION not in ("fp64", "fp32", "fp32r"):
+    raise ValueError(f"ORACLE_B200_PRECISION must be fp64, fp32 or fp32r, got {PRECISION!r}")
 DTYPE = xp.float64 if PRECISION == "fp64" else xp.float32
 
 

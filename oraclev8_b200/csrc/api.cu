@@ -122,6 +122,11 @@ struct OraclePlan {
   int zc_fxp = 1, zc_fyp = 1, zc_iyp = 1, zc_ixp = 1;
   int grid_fxp = 1, grid_fyp = 1, grid_iyp = 1, grid_ixp = 1;
   int use_pipe = 0;  // projection through the persistent pipelined kernels
+  // FP64 defect correction of single-precision plans: a double-precision
+  // shadow descriptor (own twiddles and spectral buffers, shared tables)
+  OraclePlan* dbl = nullptr;
+  int refine_passes = 0, refine_every = 1;
+  long step_count = 0;
   size_t esz = 8;  // element size of T
   // device constants
   double *kx = nullptr, *ky = nullptr, *rho = nullptr, *rhoh = nullptr, *theta0 = nullptr;
@@ -251,6 +256,9 @@ int set_smem_attrs() {
   OB_CUDA(cudaFuncSetAttribute(k_iyp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ixp<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ixp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fx<double, FX_DIV, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_fy<double, FY_RESID, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  OB_CUDA(cudaFuncSetAttribute(k_ix<float, IX_REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   return OB_OK;
 }
 
@@ -439,6 +447,82 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   return OB_OK;
 }
 
+// Defect correction of a projected single-precision state (in place).  The
+// residual -- the anelastic divergence of the stored (u, v, w) outside the
+// Nyquist rows -- is formed in double (x and y transforms of the FP32 fields
+// in FP64, tendency.py:717-790 operator order) and rounded to float only once
+// the cancellation between its terms has happened; the correction potential
+// is then solved and applied in single precision (it is small, so its
+// relative FP32 error is negligible against the state):
+// u, v, w -= grad(dphi), phi += dphi.
+int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStream_t st) {
+  OraclePlan* q = p->dbl;
+  if (!q) return fail(OB_ERR_UNSUPPORTED, "defect correction needs a single-precision plan");
+  using Cd = cplx<double>;
+  using Cf = cplx<float>;
+  const GridK g = p->g;
+  Cd* R1 = (Cd*)q->S1;
+  Cd* R2 = (Cd*)q->S2;
+  Cf* S1 = (Cf*)p->S1;
+  Cf* S2 = (Cf*)p->S2;
+  Cf* S3 = (Cf*)p->S3;
+  { Launch L_(p, OB_PROF_REFINE, st); k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
+      g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
+      (const Cd*)q->twx, R1, R2, nullptr); }
+  OB_LAUNCHED();
+  { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
+      g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
+  OB_LAUNCHED();
+  const long ncols = (long)g.nxh * g.ny;
+  { Launch L_(p, OB_PROF_REFINE, st); k_thomas<float, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
+                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, nullptr, 0, 0); }
+  OB_LAUNCHED();
+  { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
+  OB_LAUNCHED();
+  { Launch L_(p, OB_PROF_REFINE, st); k_ix<float, IX_REFINE><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
+      g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const Cf*)p->twx, u, v, w, nullptr, 0.0,
+      p->theta0, u, v, w, phi); }
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// Double-precision companion of a single-precision plan for the residual
+// transforms: FP64 twiddles and two FP64 half-spectrum buffers; the FFT
+// plans, wavenumbers and reference profiles are shared with the plan.
+int make_refiner(OraclePlan* p) {
+  OraclePlan* q = new OraclePlan();
+  p->dbl = q;
+  q->prec = OB_PREC_F64;
+  q->esz = 8;
+  q->g = p->g;
+  q->px = p->px;
+  q->py = p->py;
+  q->pxf = p->pxf;
+  q->pyf = p->pyf;
+  q->kx = p->kx;
+  q->ky = p->ky;
+  q->rho = p->rho;
+  q->rhoh = p->rhoh;
+  q->theta0 = p->theta0;
+  const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz;
+  const size_t ce = 16;
+  q->zc_fx = pick_zc(nz, 2ull * (q->g.M + 1) * 3 * ce, tw_bytes(q, nx));
+  q->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, tw_bytes(q, ny));
+  if (smem_fx(q, 3) > kSmemMax || smem_fy(q, 2, q->zc_fy) > kSmemMax)
+    return fail(OB_ERR_ARG, "grid too large for the FP64 residual kernels");
+  auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
+  int rc;
+  if ((rc = dalloc(p, &q->twx, nx * sizeof(cplx<double>))) ||
+      (rc = dalloc(p, &q->twy, ny * sizeof(cplx<double>))))
+    return rc;
+  OB_CUDA(cudaMemcpy(q->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice));
+  OB_CUDA(cudaMemcpy(q->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice));
+  const size_t ns = (size_t)p->g.nxh * ny * nz;
+  if ((rc = dalloc(p, &q->S1, ns * ce)) || (rc = dalloc(p, &q->S2, ns * ce))) return rc;
+  return set_smem_attrs<double>();
+}
+
 // Helmholtz divergence damping tendency (tendency.py:1800-1839) into Du, Dv.
 template <class T>
 int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStream_t st) {
@@ -601,6 +685,13 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
     RC(copy_field<T>(out->theta_prime, ath, n, st));
     RC(copy_field<T>(out->phi, sphi, n, st));
   }
+  // FP64 defect correction of the step's final projection (single precision)
+  if constexpr (sizeof(T) == 4) {
+    if (p->projection && p->refine_passes > 0 && p->step_count % p->refine_every == 0)
+      for (int r = 0; r < p->refine_passes; ++r)
+        RC(refine_impl(p, (float*)out->u, (float*)out->v, (float*)out->w, (float*)out->phi, st));
+  }
+  p->step_count += 1;
   if (want_diag)
     RC(diag_impl<T>(p, (const T*)out->u, (const T*)out->v, (const T*)out->w,
                     (const T*)out->theta_prime, sphi, st));
@@ -754,6 +845,7 @@ size_t oracle_b200_plan_scratch_bytes(const OraclePlan* p) { return p ? p->scrat
 
 int oracle_b200_plan_destroy(OraclePlan* p) {
   if (!p) return OB_OK;
+  delete p->dbl;  // owns no allocations: its buffers are in p->allocs
   for (auto& m : p->marks) {
     cudaEventDestroy(m.a);
     cudaEventDestroy(m.b);
@@ -937,6 +1029,7 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   p->nparts = nsm * 4;
   if ((rc = dalloc(p, &p->parts, p->nparts * sizeof(DiagPart)))) return bail(rc);
+  if (p->prec == OB_PREC_F32 && (rc = make_refiner(p))) return bail(rc);
   *out = p;
   return OB_OK;
 }
@@ -1038,6 +1131,25 @@ int oracle_b200_tendency(OraclePlan* p, int mask, const OracleStatePtrs* s, void
 }
 
 long oracle_b200_launch_count(const OraclePlan* p) { return p ? p->launches : -1; }
+
+int oracle_b200_set_refinement(OraclePlan* p, int passes, int every) {
+  if (int rc = check_plan(p)) return rc;
+  if (passes < 0 || passes > 4 || every < 1)
+    return fail(OB_ERR_ARG, "set_refinement: need 0 <= passes <= 4 and every >= 1");
+  if (passes > 0 && p->prec != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "set_refinement: defect correction applies to single-precision plans");
+  p->refine_passes = passes;
+  p->refine_every = every;
+  return OB_OK;
+}
+
+int oracle_b200_refine(OraclePlan* p, void* u, void* v, void* w, void* phi, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!u || !v || !w || !phi) return fail(OB_ERR_ARG, "refine: NULL pointer");
+  if (p->prec != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "refine: defect correction applies to single-precision plans");
+  return refine_impl(p, (float*)u, (float*)v, (float*)w, (float*)phi, (cudaStream_t)stream);
+}
 
 int oracle_b200_profile(OraclePlan* p, int enable) {
   if (int rc = check_plan(p)) return rc;

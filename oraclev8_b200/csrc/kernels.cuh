@@ -43,6 +43,15 @@ __device__ __forceinline__ double stage_w(const T* __restrict__ wc, const T* __r
   return arn((double)wc[k], mrn(sdt, bhalf(thc, k, nz, theta0)));
 }
 
+// Non-deduced alias: template arguments given explicitly (or defaulted) are not
+// re-deduced from pointer arguments, so nullptr can be passed for unused ones.
+template <class X>
+struct nd {
+  using type = X;
+};
+template <class X>
+using nd_t = typename nd<X>::type;
+
 // global loads each thread issues before consuming them (memory-level parallelism)
 constexpr int kLoadBatch = 4;
 // state values per thread k_ix prefetches ahead of its FFT
@@ -52,10 +61,12 @@ enum FxMode { FX_DIV = 0, FX_DIV_STAGE = 1, FX_FIELDS = 2 };
 
 // x-pencil forward kernel.  grid = (ny, ceil(nz/zc)).  smem: 2 * (M+1) * B cplx.
 // FX_FIELDS transforms `nf` real fields f0..f2 (no weighting) into X0..X2.
-template <class T, int MODE>
+template <class T, int MODE, class TS = T>
 __global__ void __launch_bounds__(256, 2) k_fx(GridK g, FftPlan px, int zc, int nf,
-                                            const T* __restrict__ f0, const T* __restrict__ f1,
-                                            const T* __restrict__ f2, const T* __restrict__ th,
+                                            const nd_t<TS>* __restrict__ f0,
+                                            const nd_t<TS>* __restrict__ f1,
+                                            const nd_t<TS>* __restrict__ f2,
+                                            const nd_t<TS>* __restrict__ th,
                                             double sdt, const double* __restrict__ rho,
                                             const double* __restrict__ rhoh,
                                             const double* __restrict__ theta0,
@@ -94,17 +105,17 @@ __global__ void __launch_bounds__(256, 2) k_fx(GridK g, FftPlan px, int zc, int 
         const size_t col = (size_t)x * g.ny + y;
         const int z = z0 + zl;
         if (MODE == FX_FIELDS) {
-          va[q][0] = f0[col * nz + z];
-          if (NF > 1) va[q][1] = f1[col * nz + z];
-          if (NF > 2) va[q][2] = f2[col * nz + z];
+          va[q][0] = (T)f0[col * nz + z];
+          if (NF > 1) va[q][1] = (T)f1[col * nz + z];
+          if (NF > 2) va[q][2] = (T)f2[col * nz + z];
         } else {
           const double r = rho[z];
           va[q][0] = (T)(r * (double)f0[col * nz + z]);
           va[q][1] = (T)(r * (double)f1[col * nz + z]);
-          const T* wc = f2 + col * (nz + 1);
+          const TS* wc = f2 + col * (nz + 1);
           double wl, wu;
           if (MODE == FX_DIV_STAGE) {
-            const T* thc = th + col * nz;
+            const TS* thc = th + col * nz;
             wl = stage_w(wc, thc, z, nz, sdt, theta0);
             wu = stage_w(wc, thc, z + 1, nz, sdt, theta0);
           } else {
@@ -155,23 +166,31 @@ __global__ void __launch_bounds__(256, 2) k_fx(GridK g, FftPlan px, int zc, int 
   }
 }
 
-enum FyMode { FY_DIV = 0, FY_FIELDS = 1, FY_HELM = 2 };
+enum FyMode { FY_DIV = 0, FY_FIELDS = 1, FY_HELM = 2, FY_RESID = 3 };
 
 // y-pencil forward kernel.  grid = (nxh, ceil(nz/zc)).  smem: 2 * ny * B cplx.
 // FY_DIV: out0 = FFTy(in0) + i ky' FFTy(in1).
+// FY_RESID: FY_DIV with the Nyquist rows (kx = nx/2 or ky = ny/2) set to
+//   zero: the residual of a defect correction.  The projection cannot make
+//   those modes divergence-free (the spectral derivative drops them), so a
+//   second projection would only move them; the correction leaves them as
+//   the first projection put them.
 // FY_FIELDS: out_f = FFTy(in_f) for f < nf.
 // FY_HELM: the Helmholtz divergent-part multipliers (tendency.py:1800-1839),
 //   out0 = s (Kx^2/K^2 U + (KxKy/K^2)' V), out1 = s ((KxKy/K^2)' U + Ky^2/K^2 V),
 //   s = scale; the primed cross term is zero where exactly one of kx, ky is
 //   the Nyquist index (there the reference's real() drops it).
-template <class T, int MODE>
+// TO: type of the FY_DIV output (narrower than T for the defect correction,
+// whose residual divergence is formed in double and handed to a
+// single-precision solve); the other modes write T.
+template <class T, int MODE, class TO = T>
 __global__ void __launch_bounds__(256, 2) k_fy(GridK g, FftPlan py, int zc, int nf,
                                             const cplx<T>* __restrict__ in0,
                                             const cplx<T>* __restrict__ in1,
                                             const double* __restrict__ kxd,
                                             const double* __restrict__ kyd,
                                             const cplx<T>* __restrict__ twy, double scale,
-                                            cplx<T>* __restrict__ out0,
+                                            cplx<nd_t<TO>>* __restrict__ out0,
                                             cplx<T>* __restrict__ out1) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   // twiddle table staged in shared memory (off the butterflies' critical path)
@@ -219,10 +238,12 @@ __global__ void __launch_bounds__(256, 2) k_fy(GridK g, FftPlan py, int zc, int 
     const int zl = e - ky * zc;
     if (zl >= zn) continue;
     const size_t o = ((size_t)kx * ny + ky) * nz + z0 + zl;
-    if (MODE == FY_DIV) {
+    if (MODE == FY_DIV || MODE == FY_RESID) {
       const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
-      out0[o] = add(R[(size_t)ky * B + zl], ik(kk, R[(size_t)ky * B + zc + zl]));
-    } else if (MODE == FY_FIELDS) {
+      cplx<T> d = add(R[(size_t)ky * B + zl], ik(kk, R[(size_t)ky * B + zc + zl]));
+      if (MODE == FY_RESID && (ky == ny / 2 || kx == g.nx / 2)) d = mk<T>((T)0, (T)0);
+      out0[o] = mk<TO>((TO)d.x, (TO)d.y);
+    } else if constexpr (MODE == FY_FIELDS) {
       for (int f = 0; f < NF; ++f) (f == 0 ? out0 : out1)[o] = R[(size_t)ky * B + f * zc + zl];
     } else {
       const double Kx = kxd[kx], Ky = kyd[ky];
@@ -237,7 +258,7 @@ __global__ void __launch_bounds__(256, 2) k_fy(GridK g, FftPlan py, int zc, int 
       const cplx<T> U = R[(size_t)ky * B + zl];
       const cplx<T> V = R[(size_t)ky * B + zc + zl];
       const T sxx = (T)(scale * mxx), syy = (T)(scale * myy), sxy = (T)(scale * mxy);
-      out0[o] = mk<T>(sxx * U.x + sxy * V.x, sxx * U.y + sxy * V.y);
+      out0[o] = mk<TO>(sxx * U.x + sxy * V.x, sxx * U.y + sxy * V.y);
       out1[o] = mk<T>(sxy * U.x + syy * V.x, sxy * U.y + syy * V.y);
     }
   }
@@ -477,7 +498,7 @@ __global__ void __launch_bounds__(256, 2) k_iy(GridK g, FftPlan py, int zc, int 
   }
 }
 
-enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3 };
+enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3, IX_REFINE = 4 };
 
 // x-pencil inverse kernel.  grid = (ny, ceil(nz/zc)).  smem: (M+1)*B + M*B cplx,
 // B = 3 zc + 1 (correction/grad: phi with one halo level below, d/dx, d/dy)
@@ -490,17 +511,19 @@ enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3 };
 //   IX_GRAD:    gx, gy (full levels), gz (nz+1 half levels, zero ends)
 //               (tendency.py:487-500).
 //   IX_FIELDS:  real outputs of nf spectra.
-template <class T, int MODE>
+template <class T, int MODE, class TS = T>
 __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int nf,
                                             const cplx<T>* __restrict__ phs,
                                             const cplx<T>* __restrict__ psi,
                                             const cplx<T>* __restrict__ s2,
                                             const double* __restrict__ kxd,
                                             const cplx<T>* __restrict__ twx,
-                                            const T* u_in, const T* v_in, const T* w_in,
-                                            const T* __restrict__ th, double sdt,
-                                            const double* __restrict__ theta0, T* u_out,
-                                            T* v_out, T* w_out, T* phi_out) {
+                                            const nd_t<TS>* u_in, const nd_t<TS>* v_in,
+                                            const nd_t<TS>* w_in,
+                                            const nd_t<TS>* __restrict__ th, double sdt,
+                                            const double* __restrict__ theta0, nd_t<TS>* u_out,
+                                            nd_t<TS>* v_out, nd_t<TS>* w_out,
+                                            nd_t<TS>* phi_out) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   // twiddle table staged in shared memory (off the butterflies' critical path)
   cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
@@ -557,13 +580,14 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
   // Prefetch the state values this thread will correct, so their load
   // latency overlaps the shared-memory FFT below (CORRECT / STAGE modes).
   const int nout = g.nx * zc;
-  const bool pre = (MODE == IX_CORRECT || MODE == IX_STAGE) && nout <= kIxPrefetch * (int)blockDim.x;
-  T pu[kIxPrefetch], pv[kIxPrefetch], pw[kIxPrefetch], pt[kIxPrefetch];
+  const bool pre = (MODE == IX_CORRECT || MODE == IX_STAGE || MODE == IX_REFINE) &&
+                   nout <= kIxPrefetch * (int)blockDim.x;
+  TS pu[kIxPrefetch], pv[kIxPrefetch], pw[kIxPrefetch], pt[kIxPrefetch];
   if (pre) {
 #pragma unroll
     for (int q = 0; q < kIxPrefetch; ++q) {
       const int e = threadIdx.x + q * blockDim.x;
-      pu[q] = pv[q] = pw[q] = pt[q] = (T)0;
+      pu[q] = pv[q] = pw[q] = pt[q] = (TS)0;
       const int x = e / zc;
       const int zl = e - x * zc;
       if (e < nout && zl < zn) {
@@ -573,14 +597,14 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
         const size_t wi = col * (nz + 1) + z;
         pu[q] = u_in[idx];
         pv[q] = v_in[idx];
-        if (MODE == IX_CORRECT) {
+        if (MODE != IX_STAGE) {
           pw[q] = w_in[wi];
           if (z == nz - 1) pt[q] = w_in[wi + 1];
         } else {
-          const T* wc = w_in + col * (nz + 1);
-          const T* thc = th + col * nz;
-          pw[q] = (T)stage_w(wc, thc, z, nz, sdt, theta0);
-          if (z == nz - 1) pt[q] = (T)stage_w(wc, thc, nz, nz, sdt, theta0);
+          const TS* wc = w_in + col * (nz + 1);
+          const TS* thc = th + col * nz;
+          pw[q] = (TS)stage_w(wc, thc, z, nz, sdt, theta0);
+          if (z == nz - 1) pt[q] = (TS)stage_w(wc, thc, nz, nz, sdt, theta0);
         }
       }
     }
@@ -603,8 +627,8 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
     const size_t idx = col * nz + z;
     if (fields) {
       for (int f = 0; f < nf; ++f) {
-        T* dst = f == 0 ? u_out : (f == 1 ? v_out : w_out);
-        dst[idx] = rz[rb + 2 * (f * zc + zl)];
+        TS* dst = f == 0 ? u_out : (f == 1 ? v_out : w_out);
+        dst[idx] = (TS)rz[rb + 2 * (f * zc + zl)];
       }
       continue;
     }
@@ -615,13 +639,13 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
     const T gz = (z >= 1) ? (T)((phi - phib) / (T)g.dz) : (T)0;
     const size_t wi = col * (nz + 1) + z;
     if (MODE == IX_GRAD) {
-      u_out[idx] = gx;
-      v_out[idx] = gy;
-      w_out[wi] = gz;
-      if (z == nz - 1) w_out[wi + 1] = (T)0;
+      u_out[idx] = (TS)gx;
+      v_out[idx] = (TS)gy;
+      w_out[wi] = (TS)gz;
+      if (z == nz - 1) w_out[wi + 1] = (TS)0;
       continue;
     }
-    T uc, vc, wc, wt;
+    TS uc, vc, wc, wt;
     if (pre) {
       // q < kIxPrefetch whenever pre holds; select the register without
       // dynamic indexing of the arrays
@@ -632,21 +656,26 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
     } else {
       uc = u_in[idx];
       vc = v_in[idx];
-      if (MODE == IX_CORRECT) {
+      if (MODE != IX_STAGE) {
         wc = w_in[wi];
-        wt = (z == nz - 1) ? w_in[wi + 1] : (T)0;
+        wt = (z == nz - 1) ? w_in[wi + 1] : (TS)0;
       } else {
-        const T* wcol = w_in + col * (nz + 1);
-        const T* thc = th + col * nz;
-        wc = (T)stage_w(wcol, thc, z, nz, sdt, theta0);
-        wt = (z == nz - 1) ? (T)stage_w(wcol, thc, nz, nz, sdt, theta0) : (T)0;
+        const TS* wcol = w_in + col * (nz + 1);
+        const TS* thc = th + col * nz;
+        wc = (TS)stage_w(wcol, thc, z, nz, sdt, theta0);
+        wt = (z == nz - 1) ? (TS)stage_w(wcol, thc, nz, nz, sdt, theta0) : (TS)0;
       }
     }
-    u_out[idx] = uc - gx;
-    v_out[idx] = vc - gy;
-    w_out[wi] = wc - gz;
+    // the spectral type T may be wider than the state type TS (defect
+    // correction of a single-precision state): subtract in T, store in TS
+    u_out[idx] = (TS)((T)uc - gx);
+    v_out[idx] = (TS)((T)vc - gy);
+    w_out[wi] = (TS)((T)wc - gz);
     if (z == nz - 1 && (MODE == IX_STAGE || w_out != w_in)) w_out[wi + 1] = wt;
-    phi_out[idx] = phi;
+    if (MODE == IX_REFINE)
+      phi_out[idx] = (TS)((T)phi_out[idx] + phi);
+    else
+      phi_out[idx] = (TS)phi;
   }
 }
 

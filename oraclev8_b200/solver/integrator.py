@@ -112,12 +112,25 @@ class RK3Integrator:
     """integrator.py:140-311."""
     _STAGE_ALPHAS = (1.0 / 3.0, 1.0 / 2.0, 1.0)
 
-    def __init__(self, config, base, precision: str | None = None) -> None:
+    def __init__(self, config, base, precision: str | None = None,
+                 refine_passes: int | None = None, refine_every: int = 1) -> None:
+        """precision: "fp64", "fp32" or "fp32r".  "fp32r" is the FP32 step
+        followed, every ``refine_every`` steps, by ``refine_passes`` (default 1)
+        defect corrections of the final projection whose residual divergence
+        is formed in FP64."""
         self.config = config
         self.base = wrap_base(base)
         self.precision = precision or backend.PRECISION
-        self.spec = compile_config(config, self.base, self.precision)
+        if self.precision not in ("fp64", "fp32", "fp32r"):
+            raise ValueError(f"precision must be fp64, fp32 or fp32r, got {self.precision!r}")
+        plan_prec = "fp64" if self.precision == "fp64" else "fp32"
+        if refine_passes is None:
+            refine_passes = 1 if self.precision == "fp32r" else 0
+        self.spec = compile_config(config, self.base, plan_prec)
         self.plan = Plan(self.spec)
+        self.refine_passes, self.refine_every = int(refine_passes), int(refine_every)
+        if self.refine_passes:
+            self.plan.set_refinement(self.refine_passes, self.refine_every)
         self.dtype = self.plan.dtype
         self._fast = self.spec.buoyancy and self.spec.projection
 

@@ -1,0 +1,164 @@
+"""Single-precision step and its FP64-residual defect correction, measured
+against the plain FP64 GPU step (itself held to the reference at 1e-12 by
+test_gpu_parity.py).
+
+The FP32 state cannot be more accurate than its own rounding, so the
+correction is judged against that floor: the non-Nyquist anelastic
+divergence (evaluated in FP64) of the FP64 projection rounded to FP32.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lh82 as O
+from tests.gpu_helpers import Base, b200_config, dev, host, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _non_nyquist(a):
+    nx, ny = a.shape[:2]
+    ah = np.fft.fft2(a, axes=(0, 1))
+    ah[nx // 2, :, :] = 0
+    ah[:, ny // 2, :] = 0
+    return np.real(np.fft.ifft2(ah, axes=(0, 1)))
+
+
+def _plans(nx, ny, nz, Lx, Ly, Lz):
+    from oraclev8_b200._plan import Plan, PlanSpec
+    z, rho0, th0 = O.build_base_state(nz, Lz)
+    mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
+                                    projection=True))
+    return mk("fp64"), mk("fp32")
+
+
+def _div64(p64, u, v, w):
+    """max |non-Nyquist anelastic divergence| of FP32 fields, in FP64."""
+    d = p64.divergence(u.double(), v.double(), w.double())
+    return float(np.max(np.abs(_non_nyquist(host(d)))))
+
+
+def _smooth_state(nx, ny, nz, seed):
+    """Band-limited random flow (Gaussian horizontal spectrum) with w = 0 at
+    the surface and the lid."""
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(nx)[:, None, None]
+    ky = np.fft.fftfreq(ny)[None, :, None]
+    filt = np.exp(-(kx ** 2 + ky ** 2) / 0.02)
+
+    def field(shape, amp):
+        f = np.fft.fft2(rng.standard_normal(shape), axes=(0, 1)) * filt
+        return amp * np.real(np.fft.ifft2(f, axes=(0, 1)))
+    u = field((nx, ny, nz), 30.0)
+    v = field((nx, ny, nz), 30.0)
+    w = field((nx, ny, nz + 1), 0.5)
+    w[:, :, 0] = 0.0
+    w[:, :, -1] = 0.0
+    return u, v, w
+
+
+@pytest.mark.parametrize("shape", [(128, 96, 16), (192, 160, 24)])
+def test_refinement_reaches_fp32_storage_floor(shape):
+    nx, ny, nz = shape
+    Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
+    p64, p32 = _plans(nx, ny, nz, Lx, Ly, Lz)
+    u, v, w = _smooth_state(nx, ny, nz, seed=nx + ny + nz)
+    # FP64 projection of the same (FP32-representable) input
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    u64, v64, w64 = dev(f32(u)), dev(f32(v)), dev(f32(w))
+    phi64 = torch.empty_like(u64)
+    d_in = _div64(p64, u64, v64, w64)
+    p64.project(u64, v64, w64, phi64)
+    floor = _div64(p64, u64.float(), v64.float(), w64.float())
+    # plain FP32 projection, then one and two correction passes
+    mk32 = lambda a: dev(a, torch.float32)
+    u32, v32, w32 = mk32(u), mk32(v), mk32(w)
+    phi32 = torch.empty_like(u32)
+    p32.project(u32, v32, w32, phi32)
+    d_plain = _div64(p64, u32, v32, w32)
+    e_phi_plain = rel(phi32, host(phi64))
+    w_nyq = host(w32).astype(np.float64) - _non_nyquist(host(w32).astype(np.float64))
+    p32.refine(u32, v32, w32, phi32)
+    # the correction leaves the Nyquist rows (which no projection controls) alone
+    w_nyq1 = host(w32).astype(np.float64) - _non_nyquist(host(w32).astype(np.float64))
+    d_r1 = _div64(p64, u32, v32, w32)
+    e_phi_r1 = rel(phi32, host(phi64))
+    p32.refine(u32, v32, w32, phi32)
+    d_r2 = _div64(p64, u32, v32, w32)
+    print(f"{shape}: div in {d_in:.3e} plain {d_plain:.3e} refined {d_r1:.3e} / {d_r2:.3e} "
+          f"floor {floor:.3e}; phi rel err plain {e_phi_plain:.3e} refined {e_phi_r1:.3e}")
+    assert d_r1 <= 2.0 * floor and d_r2 <= 2.0 * floor
+    assert d_r1 < d_plain
+    assert e_phi_r1 <= e_phi_plain
+    # the corrected velocity is the FP64 projection to FP32 storage accuracy:
+    # the rounding of the stored horizontal wind (a few ulp of max |u, v|)
+    # reaches every component through the projection, w included
+    scale = max(float(u64.abs().max()), float(v64.abs().max()))
+    assert float(np.max(np.abs(w_nyq1 - w_nyq))) <= 1e-7 * scale
+    for a, r in ((u32, u64), (v32, v64), (w32, w64)):
+        assert float((a.double() - r).abs().max()) <= 4e-7 * scale
+
+
+def _vortex_case(nx, ny, nz):
+    return dict(nx=nx, ny=ny, nz=nz, Lx=nx * 10e3, Ly=ny * 10e3, Lz=16e3, dt=30.0,
+                vortex=dict(Vmax=50.0, Rmax=40e3, B=1.6, f=5.0e-5),
+                coriolis=dict(f=5.0e-5, mode="beta_plane", beta=2.0e-11, periodic_taper=True),
+                advection="upwind5h", buoyancy=True,
+                heating=dict(Q_max=3.0 / 3600.0, r_eyewall=40e3, width_r=math.sqrt(2.0) * 15e3,
+                             z_peak=6e3, width_z=math.sqrt(2.0) * 2e3), noise_seed=3)
+
+
+def test_fp32_steps_track_fp64():
+    """Ten full steps of the vortex configuration in FP32, FP32 with one
+    correction per step, and FP64: per-field error of the single-precision
+    runs, relative to each field's max |.|, and the post-step divergence."""
+    from oraclev8_b200.solver import RK3Integrator, State
+    from tests.test_oracle_golden import oracle_initial_state
+    c = _vortex_case(96, 72, 16)
+    s0, _ = oracle_initial_state(c)
+    base = Base(c["nz"], c["Lz"])
+    cfg = b200_config(c)
+    p64, _ = _plans(c["nx"], c["ny"], c["nz"], c["Lx"], c["Ly"], c["Lz"])
+    runs = {}
+    for prec in ("fp64", "fp32", "fp32r"):
+        dt = torch.float64 if prec == "fp64" else torch.float32
+        integ = RK3Integrator(cfg, base, precision=prec)
+        s = State(dev(s0.u, dt), dev(s0.v, dt), dev(s0.w, dt), dev(s0.theta_prime, dt),
+                  dev(s0.projection_potential, dt), 0.0)
+        for n in range(10):
+            s, _ = integ.step(s, c["dt"], n)
+        runs[prec] = s
+    ref = runs["fp64"]
+    fields = ("u", "v", "w", "theta_prime", "projection_potential")
+    err = {p: {f: rel(getattr(runs[p], f), host(getattr(ref, f))) for f in fields}
+           for p in ("fp32", "fp32r")}
+    div = {p: _div64(p64, runs[p].u.float(), runs[p].v.float(), runs[p].w.float())
+           for p in ("fp32", "fp32r")}
+    print("errors vs fp64:", err, "non-Nyquist divergence:", div)
+    # after ten steps (50 projections) the FP32 runs carry a few 1e-6 of the
+    # wind scale; w, whose own scale is ~1/100 of the wind's, is held to the
+    # same absolute level through a looser relative bound
+    bound = dict(u=2e-5, v=2e-5, w=1e-3, theta_prime=2e-5, projection_potential=1e-3)
+    for p in ("fp32", "fp32r"):
+        for f in fields:
+            assert err[p][f] <= bound[f], (p, f, err[p][f])
+    assert div["fp32r"] <= div["fp32"]
+
+
+def test_refinement_controls():
+    from oraclev8_b200._plan import Plan, PlanSpec
+    p64, p32 = _plans(16, 12, 8, 16e4, 12e4, 16e3)
+    with pytest.raises(ValueError):
+        p64.set_refinement(1)
+    with pytest.raises(ValueError):
+        p32.set_refinement(5)
+    with pytest.raises(ValueError):
+        p32.set_refinement(1, every=0)
+    p32.set_refinement(2, every=3)
+    p32.set_refinement(0)
+    u = torch.zeros((16, 12, 8), dtype=torch.float64, device="cuda")
+    w = torch.zeros((16, 12, 9), dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        p64.refine(u, u.clone(), w, u.clone())
