@@ -190,6 +190,48 @@ long oracle_b200_launch_count(const OraclePlan *plan);
 int oracle_b200_profile(OraclePlan *plan, int enable);
 int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
 
+/* ---- storm tracker reductions (oracle_v8/storm_tracker.py) -------------- */
+/* Device half of find_storm_centre (storm_tracker.py:232-394): the theta'
+ * surface-pressure proxy and its masked argmin run on the GPU; the scalar
+ * decisions (parabolic refine, continuity gate, fall-backs) stay on the host. */
+typedef struct OracleTracker OracleTracker;
+
+/* Result of one theta' fix.  Indices are C-order cell indices ix * ny + iy, as
+ * numpy's argmin returns them; the *_nb arrays hold the field at (ix, iy),
+ * (ix-1, iy), (ix+1, iy), (ix, iy-1), (ix, iy+1) (0 outside the grid). */
+typedef struct OracleTrackFix {
+  double mean;             /* domain mean of p_sfc (storm_tracker.py:72) */
+  double raw_min, raw_max; /* interior minimum / field maximum of the anomaly */
+  long long raw_idx;       /* masked argmin of the anomaly (:191-203) */
+  double raw_nb[5];
+  double win_min, win_max; /* the same for the Gaussian-windowed anomaly (:76-98) */
+  long long win_idx;       /* == raw_idx when there is no previous fix */
+  double win_nb[5];
+} OracleTrackFix;
+
+/* z, rho0, theta0: host arrays of nz values (the base state's levels and
+ * profiles, storm_tracker.py:69-71).  Replaces the per-call profile reads of
+ * _theta_prime_proxy (storm_tracker.py:64-73). */
+int oracle_b200_tracker_create(int nx, int ny, int nz, const double *z, const double *rho0,
+                               const double *theta0, OracleTracker **out);
+int oracle_b200_tracker_destroy(OracleTracker *tracker);
+
+/* theta_prime: device (nx, ny, nz) field of `precision` (OB_PREC_*).
+ * margin: cells masked at every edge.  has_last != 0 applies the window
+ * exp(-r^2 / (2 r0^2)) about (last_ix, last_iy) in cells.  Blocks until
+ * `out` (host) holds the result.  Replaces _theta_prime_proxy,
+ * _gaussian_weight and _masked_argmin (storm_tracker.py:64-98,191-203). */
+int oracle_b200_track_theta(OracleTracker *tracker, const void *theta_prime, int precision,
+                            int margin, int has_last, double last_ix, double last_iy,
+                            double r0_cells, OracleTrackFix *out, void *stream);
+
+/* Column mean over the lower nz/2 levels of max(dv/dx - du/dy, 0) (periodic
+ * centred differences, spacing dx on both axes) into zcol_host (nx * ny
+ * doubles, C order).  Blocks until it is copied.  Replaces the field part of
+ * _vorticity_centre (storm_tracker.py:115-139). */
+int oracle_b200_track_vorticity(OracleTracker *tracker, const void *u, const void *v,
+                                int precision, double dx, double *zcol_host, void *stream);
+
 /* Poisson solve that allocates no device memory.  No counterpart in the
  * reference: it is an extra entry point for callers that cannot call
  * cudaMalloc when they need a solve (a process whose own allocator already

@@ -30,6 +30,8 @@ EXPORTS = (
     "oracle_b200_last_error", "oracle_b200_version", "oracle_b200_launch_count",
     "oracle_b200_profile", "oracle_b200_profile_read", "oracle_b200_poisson_solve_noalloc",
     "oracle_b200_set_refinement", "oracle_b200_refine",
+    "oracle_b200_tracker_create", "oracle_b200_tracker_destroy", "oracle_b200_track_theta",
+    "oracle_b200_track_vorticity",
 )
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
@@ -51,6 +53,13 @@ class ComponentDesc(ctypes.Structure):
 class StatePtrs(ctypes.Structure):
     _fields_ = [("u", c_void_p), ("v", c_void_p), ("w", c_void_p),
                 ("theta_prime", c_void_p), ("phi", c_void_p)]
+
+
+class TrackFix(ctypes.Structure):
+    _fields_ = [("mean", c_double), ("raw_min", c_double), ("raw_max", c_double),
+                ("raw_idx", ctypes.c_longlong), ("raw_nb", c_double * 5),
+                ("win_min", c_double), ("win_max", c_double),
+                ("win_idx", ctypes.c_longlong), ("win_nb", c_double * 5)]
 
 
 _lib = None
@@ -89,6 +98,12 @@ def load(path: Path | None = None):
         "oracle_b200_poisson_solve_noalloc": ([POINTER(GridDesc), POINTER(c_double), vp, vp, vp], c_int),
         "oracle_b200_set_refinement": ([vp, c_int, c_int], c_int),
         "oracle_b200_refine": ([vp, vp, vp, vp, vp, vp], c_int),
+        "oracle_b200_tracker_create": ([c_int, c_int, c_int, POINTER(c_double), POINTER(c_double),
+                                        POINTER(c_double), POINTER(vp)], c_int),
+        "oracle_b200_tracker_destroy": ([vp], c_int),
+        "oracle_b200_track_theta": ([vp, vp, c_int, c_int, c_int, c_double, c_double, c_double,
+                                     POINTER(TrackFix), vp], c_int),
+        "oracle_b200_track_vorticity": ([vp, vp, vp, c_int, c_double, POINTER(c_double), vp], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

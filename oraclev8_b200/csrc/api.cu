@@ -12,6 +12,7 @@
 #include "../../include/oracle_b200.h"
 #include "kernels.cuh"
 #include "pipe.cuh"
+#include "tracker.cuh"
 
 using namespace ob;
 
@@ -836,6 +837,139 @@ int check_plan(const OraclePlan* p) {
 // ===========================================================================
 
 extern "C" {
+
+// ---- storm tracker --------------------------------------------------------
+struct OracleTracker {
+  int nx = 0, ny = 0, nz = 0;
+  int npsfc = 1, nmin = 1;  // CTAs of the two grid-wide kernels
+  double *z = nullptr, *rho0 = nullptr, *theta0 = nullptr;
+  double *p = nullptr, *part = nullptr, *zcol = nullptr;
+  TrackPart* parts = nullptr;
+  TrackFixD* fix = nullptr;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int tracker_alloc(OracleTracker* t, void** out, size_t bytes) {
+  void* q = nullptr;
+  OB_CUDA(cudaMalloc(&q, bytes));
+  t->allocs.push_back(q);
+  *out = q;
+  return OB_OK;
+}
+
+void tracker_free(OracleTracker* t) {
+  for (void* q : t->allocs) cudaFree(q);
+  delete t;
+}
+
+int check_tracker_call(const OracleTracker* t, int precision, const void* a, const void* b) {
+  if (!t) return fail(OB_ERR_ARG, "tracker is NULL");
+  if (!a || !b) return fail(OB_ERR_ARG, "tracker: NULL pointer");
+  if (precision != OB_PREC_F64 && precision != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "tracker: precision must be OB_PREC_F64 or OB_PREC_F32");
+  return OB_OK;
+}
+
+}  // namespace
+
+int oracle_b200_tracker_create(int nx, int ny, int nz, const double* z, const double* rho0,
+                               const double* theta0, OracleTracker** out) {
+  if (!out) return fail(OB_ERR_ARG, "tracker_create: out is NULL");
+  *out = nullptr;
+  if (nx < 3 || ny < 3 || nz < 2 || (long long)nx * ny > (1LL << 30))
+    return fail(OB_ERR_ARG, "tracker_create: need nx, ny >= 3, nz >= 2 (got %d, %d, %d)", nx,
+                ny, nz);
+  if (!z || !rho0 || !theta0) return fail(OB_ERR_ARG, "tracker_create: NULL profile");
+  OracleTracker* t = new OracleTracker();
+  t->nx = nx;
+  t->ny = ny;
+  t->nz = nz;
+  int dev = 0, nsm = 148;
+  OB_CUDA(cudaGetDevice(&dev));
+  OB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long long ncol = (long long)nx * ny;
+  t->npsfc = (int)std::min<long long>((ncol + 7) / 8, 8LL * nsm);
+  t->nmin = (int)std::min<long long>((ncol + kTrackThreads - 1) / kTrackThreads, 2LL * nsm);
+  int rc;
+  auto A = [&](void** q, size_t bytes) { return tracker_alloc(t, q, bytes); };
+  if ((rc = A((void**)&t->z, nz * sizeof(double))) || (rc = A((void**)&t->rho0, nz * sizeof(double))) ||
+      (rc = A((void**)&t->theta0, nz * sizeof(double))) ||
+      (rc = A((void**)&t->p, ncol * sizeof(double))) ||
+      (rc = A((void**)&t->zcol, ncol * sizeof(double))) ||
+      (rc = A((void**)&t->part, t->npsfc * sizeof(double))) ||
+      (rc = A((void**)&t->parts, t->nmin * sizeof(TrackPart))) ||
+      (rc = A((void**)&t->fix, sizeof(TrackFixD)))) {
+    tracker_free(t);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(t->z, z, nz * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->rho0, rho0, nz * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->theta0, theta0, nz * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    tracker_free(t);
+    return fail(OB_ERR_CUDA, "tracker_create: copy of the profiles failed: %s", cudaGetErrorString(e));
+  }
+  *out = t;
+  return OB_OK;
+}
+
+int oracle_b200_tracker_destroy(OracleTracker* t) {
+  if (t) tracker_free(t);
+  return OB_OK;
+}
+
+int oracle_b200_track_theta(OracleTracker* t, const void* th, int precision, int margin,
+                            int has_last, double last_ix, double last_iy, double r0_cells,
+                            OracleTrackFix* out, void* stream) {
+  if (int rc = check_tracker_call(t, precision, th, out)) return rc;
+  if (margin < 0) return fail(OB_ERR_ARG, "track_theta: margin must be >= 0");
+  if (has_last && !(r0_cells > 0.0))
+    return fail(OB_ERR_ARG, "track_theta: r0_cells must be > 0");
+  static_assert(sizeof(TrackFixD) == sizeof(OracleTrackFix), "TrackFixD layout");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int ncol = t->nx * t->ny;
+  if (precision == OB_PREC_F64)
+    k_track_psfc<double><<<t->npsfc, kTrackThreads, 0, st>>>(
+        ncol, t->nz, (const double*)th, t->z, t->rho0, t->theta0, t->p, t->part);
+  else
+    k_track_psfc<float><<<t->npsfc, kTrackThreads, 0, st>>>(
+        ncol, t->nz, (const float*)th, t->z, t->rho0, t->theta0, t->p, t->part);
+  OB_LAUNCHED();
+  TrackWin win{has_last ? 1 : 0, last_ix, last_iy, r0_cells};
+  k_track_min<<<t->nmin, kTrackThreads, 0, st>>>(t->nx, t->ny, margin, win, t->p, t->part,
+                                                  t->npsfc, t->parts);
+  OB_LAUNCHED();
+  k_track_final<<<1, kTrackThreads, 0, st>>>(t->nx, t->ny, win, t->p, t->part, t->npsfc,
+                                              t->parts, t->nmin, t->fix);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(out, t->fix, sizeof(TrackFixD), cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_track_vorticity(OracleTracker* t, const void* u, const void* v, int precision,
+                                double dx, double* zcol_host, void* stream) {
+  if (int rc = check_tracker_call(t, precision, u, v)) return rc;
+  if (!zcol_host || !(dx > 0.0)) return fail(OB_ERR_ARG, "track_vorticity: bad output or dx");
+  if (t->nz < 2) return fail(OB_ERR_ARG, "track_vorticity: need nz >= 2");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == OB_PREC_F64)
+    k_track_zcol<double><<<t->npsfc, kTrackThreads, 0, st>>>(t->nx, t->ny, t->nz,
+                                                           (const double*)u, (const double*)v,
+                                                           dx, t->zcol);
+  else
+    k_track_zcol<float><<<t->npsfc, kTrackThreads, 0, st>>>(t->nx, t->ny, t->nz,
+                                                          (const float*)u, (const float*)v,
+                                                          dx, t->zcol);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(zcol_host, t->zcol, (size_t)t->nx * t->ny * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
 
 const char* oracle_b200_last_error(void) { return g_err.c_str(); }
 

@@ -126,3 +126,26 @@ def test_vortex_init_identical_to_reference_restatement():
         b = O.Holland(**kw).build_state(32, 24, 8, 640e3, 480e3, base.z, base.rho0, base.theta0)
         for f in ("u", "v", "w", "theta_prime"):
             assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
+def test_tracker_host_logic_matches_oracle():
+    """The host half of the B200 tracker (sub-cell refine from the device's
+    5-point neighbourhood, vorticity fall-back on the device's column means)
+    gives the oracle's answers on the same fields."""
+    from oraclev8_b200 import storm_tracker as T
+    rng = np.random.default_rng(4)
+    nx, ny, nz, dx = 20, 16, 6, 10e3
+    p = rng.standard_normal((nx, ny))
+    for ix, iy in ((5, 7), (0, 3), (nx - 1, ny - 1), (10, 0)):
+        nb = [p[ix, iy]] + [p[x, y] if 0 <= x < nx and 0 <= y < ny else 0.0
+                            for x, y in ((ix - 1, iy), (ix + 1, iy), (ix, iy - 1), (ix, iy + 1))]
+        assert T._refine(nb, ix, iy, nx, ny) == O.parabolic_refine(p, ix, iy)
+    u = 5 * rng.standard_normal((nx, ny, nz))
+    v = 5 * rng.standard_normal((nx, ny, nz))
+    h = nz // 2
+    dvdx = (np.roll(v[:, :, :h], -1, 0) - np.roll(v[:, :, :h], 1, 0)) / (2.0 * dx)
+    dudy = (np.roll(u[:, :, :h], -1, 1) - np.roll(u[:, :, :h], 1, 1)) / (2.0 * dx)
+    zcol = np.mean(np.maximum(dvdx - dudy, 0.0), axis=2)
+    for last in (None, (80e3, 70e3), (150e3, 20e3)):
+        assert T._vorticity_centre(zcol, nx, ny, dx, last) == \
+            O.vorticity_centre(u, v, nx, ny, dx, last_pos=last)
