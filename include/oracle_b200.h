@@ -111,6 +111,22 @@ int oracle_b200_plan_create(const OracleGridDesc *grid, const OracleComponentDes
                             OraclePlan **out);
 int oracle_b200_plan_destroy(OraclePlan *plan);
 
+/* ---- captured steps --------------------------------------------------------
+ * A CUDA graph of `nsteps` consecutive in-place steps of one state: the kernel
+ * sequence of oracle_b200_step (want_diag = 0) recorded once, then replayed
+ * with a single launch per call, so a run's whole step costs one host call.
+ * No reference counterpart (the reference steps from Python, integrator.py:
+ * 189-311).  The graph holds the state pointers, dt and the plan's scratch:
+ * replays of graphs of one plan must not overlap, and the plan must outlive
+ * its graphs.  Solver-residual logging is off inside graphs; with a
+ * refinement cadence `every` > 1, nsteps should be a multiple of it. */
+typedef struct OracleStepGraph OracleStepGraph;
+int oracle_b200_step_graph_create(OraclePlan *plan, const OracleStatePtrs *state, double dt,
+                                  int nsteps, OracleStepGraph **out);
+int oracle_b200_step_graph_launch(OracleStepGraph *graph, void *stream);
+long oracle_b200_step_graph_kernels(const OracleStepGraph *graph);
+int oracle_b200_step_graph_destroy(OracleStepGraph *graph);
+
 /* Bytes of device scratch the plan holds. */
 size_t oracle_b200_plan_scratch_bytes(const OraclePlan *plan);
 
@@ -189,6 +205,19 @@ long oracle_b200_launch_count(const OraclePlan *plan);
 #define OB_PROF_CLASSES 9
 int oracle_b200_profile(OraclePlan *plan, int enable);
 int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
+
+/* ---- vortex initial state (oracle_v8/vortex_init.py) --------------------- */
+/* Per-cell part of HollandVortexInit.build_state (vortex_init.py:330-370) on
+ * the device, from tables the host computes once (all device pointers, FP64):
+ * col: 4 * nx * ny values (r, V_t(r), sin phi, cos phi) per (x, y) column in
+ * C order; S: nz wind-structure factors; rr: nr increasing radii; tab: nr x nz
+ * theta' radial profiles.  Writes theta' = numpy.interp(r, rr, tab[:, k]),
+ * u = -V_t S sin + u_env, v = V_t S cos + v_env and w = phi = 0 into `out`
+ * (device fields of `precision`), with numpy's rounding. */
+int oracle_b200_vortex_fill(int nx, int ny, int nz, int precision, const double *col,
+                            const double *S, const double *rr, const double *tab, int nr,
+                            double u_env, double v_env, const OracleStatePtrs *out,
+                            void *stream);
 
 /* ---- storm tracker reductions (oracle_v8/storm_tracker.py) -------------- */
 /* Device half of find_storm_centre (storm_tracker.py:232-394): the theta'

@@ -31,7 +31,9 @@ EXPORTS = (
     "oracle_b200_profile", "oracle_b200_profile_read", "oracle_b200_poisson_solve_noalloc",
     "oracle_b200_set_refinement", "oracle_b200_refine",
     "oracle_b200_tracker_create", "oracle_b200_tracker_destroy", "oracle_b200_track_theta",
-    "oracle_b200_track_vorticity",
+    "oracle_b200_track_vorticity", "oracle_b200_step_graph_create",
+    "oracle_b200_step_graph_launch", "oracle_b200_step_graph_kernels",
+    "oracle_b200_step_graph_destroy", "oracle_b200_vortex_fill",
 )
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
@@ -104,6 +106,12 @@ def load(path: Path | None = None):
         "oracle_b200_track_theta": ([vp, vp, c_int, c_int, c_int, c_double, c_double, c_double,
                                      POINTER(TrackFix), vp], c_int),
         "oracle_b200_track_vorticity": ([vp, vp, vp, c_int, c_double, POINTER(c_double), vp], c_int),
+        "oracle_b200_step_graph_create": ([vp, POINTER(StatePtrs), c_double, c_int, POINTER(vp)], c_int),
+        "oracle_b200_step_graph_launch": ([vp, vp], c_int),
+        "oracle_b200_step_graph_kernels": ([vp], ctypes.c_long),
+        "oracle_b200_step_graph_destroy": ([vp], c_int),
+        "oracle_b200_vortex_fill": ([c_int, c_int, c_int, c_int, vp, vp, vp, vp, c_int, c_double,
+                                     c_double, POINTER(StatePtrs), vp], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

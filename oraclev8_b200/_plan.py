@@ -146,6 +146,9 @@ class Plan:
                                             self._ptr(w, self.wshape), self._ptr(phi, s),
                                             self._stream()))
 
+    def step_graph(self, ptrs: L.StatePtrs, dt: float, nsteps: int) -> "StepGraph":
+        return StepGraph(self, ptrs, dt, nsteps)
+
     def read_diag(self) -> np.ndarray:
         buf = (ctypes.c_double * L.DIAG_COUNT)()
         L.check(self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream()))
@@ -204,6 +207,35 @@ class Plan:
                                               self._ptr(dw, self.wshape), self._ptr(dth, s),
                                               float(dt_slow), self._stream()))
         return du, dv, dw, dth
+
+
+class StepGraph:
+    """``nsteps`` in-place steps of one state recorded as a CUDA graph
+    (oracle_b200_step_graph_create); ``launch`` replays them with one call.
+    Holds the plan so that the plan outlives the graph; the state tensors
+    behind ``ptrs`` must stay alive while the graph is used."""
+
+    def __init__(self, plan: Plan, ptrs: L.StatePtrs, dt: float, nsteps: int):
+        self.plan, self.lib, self.nsteps = plan, plan.lib, int(nsteps)
+        h = ctypes.c_void_p()
+        L.check(self.lib.oracle_b200_step_graph_create(plan.handle, ctypes.byref(ptrs),
+                                                       float(dt), self.nsteps, ctypes.byref(h)))
+        self.handle = h
+        self.kernels = int(self.lib.oracle_b200_step_graph_kernels(h))
+
+    def launch(self, stream=None) -> None:
+        s = stream if stream is not None else torch.cuda.current_stream(self.plan.device)
+        L.check(self.lib.oracle_b200_step_graph_launch(self.handle,
+                                                       ctypes.c_void_p(s.cuda_stream)))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.oracle_b200_step_graph_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
 
 
 # ---------------------------------------------------------------------------

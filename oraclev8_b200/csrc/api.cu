@@ -13,6 +13,7 @@
 #include "kernels.cuh"
 #include "pipe.cuh"
 #include "tracker.cuh"
+#include "init.cuh"
 
 using namespace ob;
 
@@ -128,6 +129,7 @@ struct OraclePlan {
   OraclePlan* dbl = nullptr;
   int refine_passes = 0, refine_every = 1;
   long step_count = 0;
+  int capturing = 0;  // recording a step graph: no solver-residual logging
   size_t esz = 8;  // element size of T
   // device constants
   double *kx = nullptr, *ky = nullptr, *rho = nullptr, *rhoh = nullptr, *theta0 = nullptr;
@@ -404,7 +406,7 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   C* S3 = (C*)p->S3;
   p->solve_count += 1;
   const int de = p->diag_every < 1 ? 1 : p->diag_every;
-  const bool log = (de == 1) || (p->solve_count % de == 1);
+  const bool log = !p->capturing && ((de == 1) || (p->solve_count % de == 1));
   double* diag = nullptr;
   if (log) {
     diag = p->diag;
@@ -874,6 +876,34 @@ int check_tracker_call(const OracleTracker* t, int precision, const void* a, con
 
 }  // namespace
 
+int oracle_b200_vortex_fill(int nx, int ny, int nz, int precision, const double* col,
+                            const double* S, const double* rr, const double* tab, int nr,
+                            double u_env, double v_env, const OracleStatePtrs* out, void* stream) {
+  if (nx < 1 || ny < 1 || nz < 1 || nr < 2 || (long long)nx * ny > (1LL << 30))
+    return fail(OB_ERR_ARG, "vortex_fill: bad sizes (%d, %d, %d, nr %d)", nx, ny, nz, nr);
+  if (!col || !S || !rr || !tab || !out || !out->u || !out->v || !out->w ||
+      !out->theta_prime || !out->phi)
+    return fail(OB_ERR_ARG, "vortex_fill: NULL pointer");
+  if (precision != OB_PREC_F64 && precision != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "vortex_fill: precision must be OB_PREC_F64 or OB_PREC_F32");
+  const int ncol = nx * ny;
+  int dev = 0, nsm = 148;
+  OB_CUDA(cudaGetDevice(&dev));
+  OB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = (int)std::min<long long>((ncol + 7) / 8, 16LL * nsm);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == OB_PREC_F64)
+    k_vortex_fill<double><<<blocks, 256, 0, st>>>(
+        ncol, nz, nr, col, S, rr, tab, u_env, v_env, (double*)out->u, (double*)out->v,
+        (double*)out->w, (double*)out->theta_prime, (double*)out->phi);
+  else
+    k_vortex_fill<float><<<blocks, 256, 0, st>>>(
+        ncol, nz, nr, col, S, rr, tab, u_env, v_env, (float*)out->u, (float*)out->v,
+        (float*)out->w, (float*)out->theta_prime, (float*)out->phi);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
 int oracle_b200_tracker_create(int nx, int ny, int nz, const double* z, const double* rho0,
                                const double* theta0, OracleTracker** out) {
   if (!out) return fail(OB_ERR_ARG, "tracker_create: out is NULL");
@@ -1180,6 +1210,82 @@ int oracle_b200_step(OraclePlan* p, const OracleStatePtrs* in, const OracleState
   cudaStream_t st = (cudaStream_t)stream;
   return DISPATCH(p, step_impl<double>(p, in, out, dt, want_diag, st),
                   step_impl<float>(p, in, out, dt, want_diag, st));
+}
+
+struct OracleStepGraph {
+  OraclePlan* plan = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long kernels = 0;  // kernel launches recorded in the graph
+};
+
+int oracle_b200_step_graph_create(OraclePlan* p, const OracleStatePtrs* state, double dt,
+                                  int nsteps, OracleStepGraph** out) {
+  if (int rc = check_plan(p)) return rc;
+  if (!out) return fail(OB_ERR_ARG, "step_graph_create: out is NULL");
+  *out = nullptr;
+  if (!state || !state->u || !state->v || !state->w || !state->theta_prime || !state->phi)
+    return fail(OB_ERR_ARG, "step_graph_create: NULL state pointer");
+  if (!std::isfinite(dt)) return fail(OB_ERR_ARG, "step_graph_create: dt must be finite");
+  if (nsteps < 1 || nsteps > 4096)
+    return fail(OB_ERR_ARG, "step_graph_create: need 1 <= nsteps <= 4096");
+  if (p->profiling) return fail(OB_ERR_ARG, "step_graph_create: switch profiling off first");
+  // record on a private stream: nothing executes while capturing, and the
+  // graph can then be launched on any stream
+  cudaStream_t cs = nullptr;
+  OB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return fail(OB_ERR_CUDA, "step_graph_create: begin capture failed: %s", cudaGetErrorString(e));
+  }
+  const long l0 = p->launches;
+  p->capturing = 1;
+  int rc = OB_OK;
+  for (int s = 0; s < nsteps && rc == OB_OK; ++s)
+    rc = DISPATCH(p, step_impl<double>(p, state, state, dt, 0, cs),
+                  step_impl<float>(p, state, state, dt, 0, cs));
+  p->capturing = 0;
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);
+  cudaStreamDestroy(cs);
+  if (rc != OB_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc != OB_OK ? rc
+                       : fail(OB_ERR_CUDA, "step_graph_create: capture failed: %s",
+                              cudaGetErrorString(e));
+  }
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(OB_ERR_CUDA, "step_graph_create: instantiate failed: %s", cudaGetErrorString(e));
+  }
+  OracleStepGraph* gr = new OracleStepGraph();
+  gr->plan = p;
+  gr->graph = graph;
+  gr->exec = exec;
+  gr->kernels = p->launches - l0;
+  p->launches = l0;  // counted when the graph is launched
+  *out = gr;
+  return OB_OK;
+}
+
+int oracle_b200_step_graph_launch(OracleStepGraph* g, void* stream) {
+  if (!g) return fail(OB_ERR_ARG, "step_graph_launch: graph is NULL");
+  OB_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  g->plan->launches += g->kernels;
+  return OB_OK;
+}
+
+long oracle_b200_step_graph_kernels(const OracleStepGraph* g) { return g ? g->kernels : -1; }
+
+int oracle_b200_step_graph_destroy(OracleStepGraph* g) {
+  if (!g) return OB_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return OB_OK;
 }
 
 int oracle_b200_project(OraclePlan* p, void* u, void* v, void* w, void* phi, int log_diag,

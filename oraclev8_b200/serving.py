@@ -1,0 +1,310 @@
+"""Ensemble and serving loop for many independent vortex runs on one GPU.
+
+The runs come from a request stream (vortex parameters, grid, run length,
+precision).  Each run keeps its whole state and its plan resident in HBM from
+admission to retirement.  Its steps are recorded once as a CUDA graph of
+``chunk`` steps (``RK3Integrator.capture``) and replayed on the run's own
+stream, so runs of different sizes overlap on the device.  Admission is by
+HBM footprint against a budget; finished runs retire and free their slot for
+the next queued request (continuous batching).  Per run the loop records
+arrival, admission and completion times; the summary gives p50/p95/p99
+time-to-completion, queueing delay and aggregate cell-updates/s.
+
+Request distributions (vortex parameters, grids and CFL time step) follow the
+ensemble and serving workloads of the LH82 beta-drift study:
+nx = ny in {96, 128, 192, 256, 384} at dx = 10 km, nz in {32, 48, 64} over
+16 km, Vmax ~ U(25, 65) m/s, Rmax ~ U(20, 80) km, B ~ U(1, 2), latitude ~
+U(10, 30) N giving f0 = 2 Omega sin(lat) and beta = 2 Omega cos(lat) / R
+(tendency.py:1160-1164), dt = 0.8 dx / Vmax (run_storm.py:91) rounded down so
+that an integer number of steps fills the run.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+OMEGA = 7.2921e-5
+R_EARTH = 6.371e6
+SIZES = (96, 128, 192, 256, 384)
+LEVELS = (32, 48, 64)
+
+
+@dataclass
+class RunRequest:
+    rid: int
+    n: int                  # nx = ny
+    nz: int
+    vmax: float
+    rmax: float
+    b: float
+    lat_deg: float
+    hours: float
+    precision: str = "fp32r"  # "fp64" or "fp32r"
+    arrival_s: float = 0.0
+    dx: float = 10e3
+    lz: float = 16e3
+
+    @property
+    def f0(self) -> float:
+        return 2.0 * OMEGA * math.sin(math.radians(self.lat_deg))
+
+    @property
+    def beta(self) -> float:
+        return 2.0 * OMEGA * math.cos(math.radians(self.lat_deg)) / R_EARTH
+
+    @property
+    def nsteps(self) -> int:
+        return max(1, math.ceil(self.hours * 3600.0 / (0.8 * self.dx / self.vmax) - 1e-9))
+
+    @property
+    def dt(self) -> float:
+        return self.hours * 3600.0 / self.nsteps
+
+    @property
+    def cells(self) -> int:
+        return self.n * self.n * self.nz
+
+    @property
+    def cell_updates(self) -> int:
+        return self.cells * self.nsteps
+
+
+def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: float = 0.0,
+                  fp32r_frac: float = 1.0) -> "list[RunRequest]":
+    """``count`` requests from a seeded stream.  ``hours``: a fixed run length
+    or a (lo, hi) uniform range.  ``rate`` > 0 gives Poisson arrivals at that
+    many requests per second (else all arrive at 0); ``fp32r_frac`` < 1 tags
+    that fraction FP32-refined and the rest FP64 (``precision`` ignored)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for i in range(count):
+        n = int(rng.choice(SIZES))
+        nz = int(rng.choice(LEVELS))
+        vmax = float(rng.uniform(25.0, 65.0))
+        rmax = float(rng.uniform(20e3, 80e3))
+        b = float(rng.uniform(1.0, 2.0))
+        lat = float(rng.uniform(10.0, 30.0))
+        h = float(rng.uniform(*hours)) if isinstance(hours, tuple) else float(hours)
+        prec = precision
+        if fp32r_frac < 1.0:
+            prec = "fp32r" if rng.uniform() < fp32r_frac else "fp64"
+        if rate > 0.0:
+            t += float(rng.exponential(1.0 / rate))
+        out.append(RunRequest(i, n, nz, vmax, rmax, b, lat, h, prec, t))
+    return out
+
+
+def build_run(req: RunRequest, device_dtype=None):
+    """Integrator and device initial state of a request: WS5 advection,
+    beta-plane Coriolis (periodic taper), buoyancy and the anelastic
+    projection; Holland vortex at the domain centre with the 12-km linear
+    wind decay."""
+    from .grid import LorenzStaggering
+    from .production_config import BaseState
+    from .solver import (AdvectionComponent, AnelasticProjection, BuoyancyComponent,
+                         CoriolisComponent, LH82AnelasticEquationSet, OperatorConfig,
+                         RK3Integrator)
+    from .vortex_init import HollandVortexInit
+    n, nz = req.n, req.nz
+    L = n * req.dx
+    base = BaseState(nz, req.lz)
+    cfg = OperatorConfig(
+        equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
+        buoyancy=BuoyancyComponent(), projection=AnelasticProjection(n, n, nz, L, L, req.lz),
+        advection=AdvectionComponent(n, n, nz, L, L, req.lz, scheme="upwind5h"),
+        coriolis=CoriolisComponent(f=req.f0, mode="beta_plane", beta=req.beta, Ly=L, ny=n,
+                                   periodic_taper=True))
+    integ = RK3Integrator(cfg, base, precision=req.precision)
+    state = HollandVortexInit(req.vmax, req.rmax, req.b, f=req.f0, wind_decay_top=12e3
+                              ).build_state(n, n, nz, L, L, base, dtype=integ.dtype)
+    return integ, state, base
+
+
+def footprint_bytes(req: RunRequest) -> int:
+    """HBM a resident run holds: 5 state fields and the plan's scratch (3
+    half-spectrum buffers, 5 anchor and 4 stage fields, 2 temporaries; plus
+    two FP64 spectra for the FP32-refined correction), in the state dtype."""
+    S = 8 if req.precision == "fp64" else 4
+    n = req.cells
+    ns = (req.n // 2 + 1) * req.n * req.nz
+    b = S * (5 * n + 11 * n) + 3 * ns * 2 * S
+    if req.precision != "fp64":
+        b += 2 * ns * 16
+    return int(b * 1.05) + (8 << 20)
+
+
+@dataclass
+class RunRecord:
+    rid: int
+    n: int
+    nz: int
+    precision: str
+    steps: int
+    cells: int
+    arrival_s: float
+    admit_s: float = math.nan
+    done_s: float = math.nan
+    final: Optional[dict] = None
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.arrival_s
+
+    @property
+    def queue_s(self) -> float:
+        return self.admit_s - self.arrival_s
+
+
+@dataclass
+class _Active:
+    req: RunRequest
+    rec: RunRecord
+    integ: object
+    state: object
+    stream: torch.cuda.Stream
+    graphs: dict
+    left: int
+    events: list = field(default_factory=list)
+    bytes: int = 0
+
+
+class ServingEngine:
+    """Continuous-batching loop over a request stream on the current GPU.
+
+    hbm_budget: bytes of resident runs admitted at once.  chunk: steps per
+    graph launch.  depth: graph launches kept in flight per run.  realtime:
+    honour the arrival times (else every request is available at once).
+    keep_final: copy each run's final state to the host when it retires."""
+
+    def __init__(self, hbm_budget: float = 150e9, chunk: int = 16, depth: int = 2,
+                 realtime: bool = True, keep_final: bool = False, max_active: int = 256):
+        self.budget = float(hbm_budget)
+        self.chunk, self.depth = int(chunk), int(depth)
+        self.realtime, self.keep_final = bool(realtime), bool(keep_final)
+        self.max_active = int(max_active)
+
+    # -- run lifecycle ---------------------------------------------------------
+    def _admit(self, req: RunRequest, now: float) -> _Active:
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            integ, state, _ = build_run(req)
+            graphs = {}
+            full = min(self.chunk, req.nsteps)
+            graphs[full] = integ.capture(state, req.dt, full)
+            tail = req.nsteps % full
+            if tail:
+                graphs[tail] = integ.capture(state, req.dt, tail)
+        rec = RunRecord(req.rid, req.n, req.nz, req.precision, req.nsteps, req.cells,
+                        req.arrival_s, admit_s=now)
+        return _Active(req, rec, integ, state, stream, graphs, req.nsteps,
+                       bytes=footprint_bytes(req))
+
+    def _launch(self, a: _Active) -> None:
+        k = min(self.chunk, a.left)
+        a.graphs[k].launch(a.stream)
+        ev = torch.cuda.Event()
+        ev.record(a.stream)
+        a.events.append(ev)
+        a.left -= k
+
+    def _retire(self, a: _Active, now: float) -> RunRecord:
+        a.rec.done_s = now
+        if self.keep_final:
+            with torch.cuda.stream(a.stream):
+                s = a.state
+                a.rec.final = {f: getattr(s, f).detach().cpu().numpy() for f in
+                               ("u", "v", "w", "theta_prime", "projection_potential")}
+        return a.rec
+
+    # -- main loop -------------------------------------------------------------
+    def run(self, requests: "list[RunRequest]") -> "list[RunRecord]":
+        pending = sorted(requests, key=lambda r: (r.arrival_s, r.rid))
+        queue: "list[RunRequest]" = []
+        active: "list[_Active]" = []
+        done: "list[RunRecord]" = []
+        graveyard: "list[_Active]" = []
+        used = 0      # bytes of active runs (the admission budget)
+        held = 0      # bytes of retired runs not yet released
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while pending or queue or active:
+            now = time.perf_counter() - t0
+            while pending and (not self.realtime or pending[0].arrival_s <= now):
+                queue.append(pending.pop(0))
+            # admission (FIFO with backfill: a request that fits may pass one
+            # that does not)
+            i = 0
+            while i < len(queue) and len(active) < self.max_active:
+                fb = footprint_bytes(queue[i])
+                if used + fb <= self.budget and used + held + fb > self.budget:
+                    # release retired runs' device memory in one batch (a
+                    # cudaFree synchronises the device, so not once per run)
+                    graveyard.clear()
+                    held = 0
+                if used + fb <= self.budget or not active:
+                    req = queue.pop(i)
+                    a = self._admit(req, time.perf_counter() - t0)
+                    active.append(a)
+                    used += a.bytes
+                else:
+                    i += 1
+            # keep every run's stream fed
+            progressed = False
+            for a in list(active):
+                a.events = [e for e in a.events if not e.query()]
+                while a.left > 0 and len(a.events) < self.depth:
+                    self._launch(a)
+                    progressed = True
+                if a.left == 0 and not a.events:
+                    done.append(self._retire(a, time.perf_counter() - t0))
+                    active.remove(a)
+                    used -= a.bytes
+                    held += a.bytes
+                    graveyard.append(a)
+                    progressed = True
+            if not progressed:
+                time.sleep(50e-6)
+        graveyard.clear()
+        return done
+
+
+def summarize(records: "list[RunRecord]", makespan_s: Optional[float] = None) -> dict:
+    lat = np.array([r.latency_s for r in records])
+    q = np.array([r.queue_s for r in records])
+    cu = float(sum(r.cells * r.steps for r in records))
+    span = makespan_s if makespan_s is not None else float(max(r.done_s for r in records))
+    pct = lambda a, p: float(np.percentile(a, p))
+    return {"runs": len(records), "cell_updates": cu, "makespan_s": span,
+            "cell_updates_per_s": cu / span,
+            "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99),
+                          "max": float(lat.max())},
+            "queue_s": {"p50": pct(q, 50), "p95": pct(q, 95), "p99": pct(q, 99)}}
+
+
+def serve_serial_plain(requests: "list[RunRequest]", realtime: bool = True
+                       ) -> "list[RunRecord]":
+    """The comparison the serving loop is measured against: the same stream
+    served one run at a time, each in plain FP64 through the public
+    ``RK3Integrator.step`` (a new State per step), in arrival order."""
+    recs = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for req in sorted(requests, key=lambda r: (r.arrival_s, r.rid)):
+        if realtime:
+            while time.perf_counter() - t0 < req.arrival_s:
+                time.sleep(1e-3)
+        r64 = RunRequest(**{**req.__dict__, "precision": "fp64"})
+        admit = time.perf_counter() - t0
+        integ, state, _ = build_run(r64)
+        for n in range(r64.nsteps):
+            state, _ = integ.step(state, r64.dt, n)
+        torch.cuda.synchronize()
+        recs.append(RunRecord(req.rid, req.n, req.nz, "fp64", r64.nsteps, r64.cells,
+                              req.arrival_s, admit_s=admit, done_s=time.perf_counter() - t0))
+        del integ, state
+    return recs

@@ -190,5 +190,14 @@ class RK3Integrator:
             state.t = state.t + dt
         return state
 
+    def capture(self, state: State, dt: float, nsteps: int = 1):
+        """Record ``nsteps`` in-place steps of ``state`` (device tensors of the
+        plan's dtype) as a CUDA graph; ``graph.launch(stream)`` then advances
+        the state by nsteps * dt with one host call.  The model time
+        ``state.t`` is not advanced by graph launches (the caller owns it)."""
+        ptrs = self.plan.state_ptrs(state.u, state.v, state.w, state.theta_prime,
+                                    state.projection_potential)
+        return self.plan.step_graph(ptrs, dt, nsteps)
+
     def read_diagnostics(self, step_number: int = 0, t: float = 0.0, dt: float = 0.0):
         return self._diagnostics(step_number, t, dt, True)

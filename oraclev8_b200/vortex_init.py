@@ -1,8 +1,9 @@
 """Holland (1980) balanced vortex initial state (oracle_v8/vortex_init.py:75-411).
 
-Host-side input preparation, run once per run: the radial gradient-wind
-integral, the hydrostatic theta', and the interpolation to the grid are
-FP64 NumPy, then the fields move to the device.  ``wind_decay_top`` selects the
+The radial gradient-wind integral and the hydrostatic theta' profiles are
+FP64 NumPy tables on the host (O(n_radial nz + nx ny)); the per-cell
+interpolation and wind expansion run on the device (``oracle_b200_vortex_fill``)
+with numpy's rounding, so both paths give the same fields.  ``wind_decay_top`` selects the
 linear wind structure max(0, 1 - z/top) the beta-drift workloads use in place
 of exp(-z/H_wind).
 """
@@ -62,10 +63,9 @@ class HollandVortexInit:
             P[i] = acc
         return P
 
-    def build_state(self, nx, ny, nz, Lx, Ly, base, x_c=None, y_c=None, device=True):
-        """Balanced State (vortex_init.py:261-370).  ``device=False`` returns
-        host NumPy fields (for pinned-buffer staging)."""
-        from .solver.tendency import State
+    def _tables(self, nx, ny, nz, Lx, Ly, base, x_c, y_c):
+        """Column tables (r, V_t(r), sin, cos) and theta' radial profiles
+        (vortex_init.py:261-329), FP64 on the host: O(nx ny + n_radial nz)."""
         x_c = x_c if x_c is not None else Lx / 2.0
         y_c = y_c if y_c is not None else Ly / 2.0
         dx, dy = Lx / nx, Ly / ny
@@ -87,12 +87,24 @@ class HollandVortexInit:
         dP[:, 0] = (Pp[:, 1] - Pp[:, 0]) / (z[1] - z[0])
         dP[:, -1] = (Pp[:, -1] - Pp[:, -2]) / (z[-1] - z[-2])
         theta_rad = (theta0[None, :] / (rho0[None, :] * GRAVITY)) * dP
+        return R2d, self.tangential_wind(R2d), np.sin(PHI), np.cos(PHI), S, theta_rad
+
+    def build_state(self, nx, ny, nz, Lx, Ly, base, x_c=None, y_c=None, device=True,
+                    dtype=None):
+        """Balanced State (vortex_init.py:261-370).  ``device=True`` expands the
+        host tables into the device fields with one kernel (identical values to
+        the host path); ``device=False`` returns host NumPy fields.  ``dtype``:
+        device dtype (default the backend's)."""
+        from .solver.tendency import State
+        R2d, Vt0, sin_phi, cos_phi, S, theta_rad = self._tables(nx, ny, nz, Lx, Ly, base,
+                                                                x_c, y_c)
+        if device:
+            return self._fill_device(nx, ny, nz, R2d, Vt0, sin_phi, cos_phi, S, theta_rad,
+                                     dtype)
         rf = R2d.ravel()
         th = np.empty((nx, ny, nz))
         for k in range(nz):
             th[:, :, k] = np.interp(rf, self._r1d, theta_rad[:, k]).reshape(nx, ny)
-        sin_phi, cos_phi = np.sin(PHI), np.cos(PHI)
-        Vt0 = self.tangential_wind(R2d)
         u = np.empty((nx, ny, nz))
         v = np.empty((nx, ny, nz))
         for k in range(nz):
@@ -101,6 +113,33 @@ class HollandVortexInit:
             v[:, :, k] = +Vt * cos_phi + self.v_env
         w = np.zeros((nx, ny, nz + 1))
         phi = np.zeros((nx, ny, nz))
-        if not device:
-            return State(u, v, w, th, phi, 0.0)
-        return State(asarray(u), asarray(v), asarray(w), asarray(th), asarray(phi), 0.0)
+        return State(u, v, w, th, phi, 0.0)
+
+    def _fill_device(self, nx, ny, nz, R2d, Vt0, sin_phi, cos_phi, S, theta_rad, dtype):
+        import ctypes
+
+        import torch
+
+        from . import _lib as L
+        from .backend import DTYPE, _device
+        from .solver.tendency import State
+        dev = _device()
+        dtype = dtype or DTYPE
+        lib = L.load()
+        f64 = dict(dtype=torch.float64, device=dev)
+        col = torch.as_tensor(np.stack([R2d, Vt0, sin_phi, cos_phi], axis=-1).reshape(-1),
+                              **f64)
+        S_d = torch.as_tensor(np.ascontiguousarray(S, dtype=np.float64), **f64)
+        rr = torch.as_tensor(self._r1d, **f64)
+        tab = torch.as_tensor(np.ascontiguousarray(theta_rad), **f64)
+        u = torch.empty((nx, ny, nz), dtype=dtype, device=dev)
+        v, th, phi = torch.empty_like(u), torch.empty_like(u), torch.empty_like(u)
+        w = torch.empty((nx, ny, nz + 1), dtype=dtype, device=dev)
+        prec = {torch.float64: L.OB_PREC_F64, torch.float32: L.OB_PREC_F32}[dtype]
+        ptrs = L.StatePtrs(*(ctypes.c_void_p(t.data_ptr()) for t in (u, v, w, th, phi)))
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+        L.check(lib.oracle_b200_vortex_fill(
+            nx, ny, nz, prec, vp(col), vp(S_d), vp(rr), vp(tab), int(self.n_radial),
+            self.u_env, self.v_env, ctypes.byref(ptrs),
+            ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+        return State(u, v, w, th, phi, 0.0)
