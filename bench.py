@@ -23,8 +23,18 @@ defect correction whose residual divergence is formed in FP64.  The same line
 then carries ``fp64_plain`` (the plain FP64 step timed the same way on the
 same workload, and the ratio) and ``accuracy`` (per-field error of the FP32
 run against the FP64 run after the same steps, and the FP64-evaluated
-divergence of both).  ``--precision fp64`` times the plain FP64 step alone.  N > 1: N independent replicas, one per GPU (the path
-partitions into independent runs; no collective on the data path).
+divergence of both).  ``--precision fp64`` times the plain FP64 step alone.
+
+Ensemble and serving (the metric's latency half, at N = 1): ``ensemble``
+serves a sample of the mixed 256-run ensemble through the serving loop
+(resident runs, captured step graphs, one stream per run) next to the same
+runs served serially in plain FP64; ``serving`` replays a Poisson request
+stream with HBM admission and reports p50/p95/p99 time-to-completion.  Sizes
+are set by ``--ensemble-runs/--ensemble-hours`` and
+``--serving-requests/--serving-scale``; ``--no-ensemble`` skips both.
+
+N > 1: N independent replicas, one per GPU (the path partitions into
+independent runs; no collective on the data path).
 
 --impl reference times the reference algorithm on the host CPU (the NumPy
 oracle; the reference is pure Python and cannot be installed on the GPU host)
@@ -509,6 +519,8 @@ def run_b200(args):
         line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
                                 note="this run vs the FP64 run from the same initial state; "
                                      "divergence = anelastic divergence evaluated in FP64")
+    if world == 1 and not args.no_ensemble:
+        line["ensemble"], line["serving"] = ensemble_report(args, load_peaks()[0])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rates, sc = cpu_sample_rate(args.workload, 1, 1, 1)
         line["cpu_baseline"] = {
@@ -521,6 +533,51 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def ensemble_report(args, peak_gbs):
+    """Ensemble and serving measurements through ``oraclev8_b200.serving``.
+
+    Ensemble: ``--ensemble-runs`` draws of the mixed ensemble (seed 3), each
+    ``--ensemble-hours`` long at its CFL time step, FP32-refined, all arriving
+    at once; against the same runs served one at a time in plain FP64 through
+    ``RK3Integrator.step``.  Serving: ``--serving-requests`` Poisson arrivals
+    at 2/s (seed 4), run length U(6, 72) h divided by ``--serving-scale``,
+    80% FP32-refined / 20% FP64, 150 GB HBM budget; against the same stream
+    served serially in plain FP64."""
+    from oraclev8_b200.serving import (ServingEngine, draw_requests, serve_serial_plain,
+                                       summarize)
+    # library, kernels and the plan pool warm before timing
+    ServingEngine(realtime=False).run(draw_requests(6, 99, hours=0.2, fp32r_frac=0.5))
+    serve_serial_plain(draw_requests(2, 98, hours=0.1), realtime=False)
+    reqs = draw_requests(args.ensemble_runs, 3, hours=args.ensemble_hours)
+    eng = summarize(ServingEngine(realtime=False).run(reqs))
+    ser = summarize(serve_serial_plain(reqs, realtime=False))
+    passes = PASSES_BASE  # no heating in the ensemble draws
+    ens = {
+        "workload": f"{len(reqs)} runs drawn from the mixed ensemble (seed 3): nx=ny in "
+                    f"{{96,128,192,256,384}} at dx 10 km, nz in {{32,48,64}} over 16 km, "
+                    f"Vmax U(25,65), Rmax U(20,80) km, B U(1,2), lat U(10,30)N; "
+                    f"{args.ensemble_hours:g} h each at dt = 0.8 dx / Vmax; WS5 + beta-plane + "
+                    f"buoyancy + projection; all arrive at t = 0",
+        "precision": "fp32r", "engine": eng, "serial_plain_fp64": ser,
+        "throughput_ratio_vs_serial_plain": eng["cell_updates_per_s"] / ser["cell_updates_per_s"],
+        "roofline": {"bound": "hbm", "passes_per_cell": passes, "bytes_per_cell": passes * 4,
+                     "achieved": passes * 4 * eng["cell_updates_per_s"] / 1e9, "peak": peak_gbs,
+                     "unit": "GB/s",
+                     "frac": passes * 4 * eng["cell_updates_per_s"] / 1e9 / peak_gbs}}
+    r4 = draw_requests(args.serving_requests, 4, hours=(6.0 / args.serving_scale,
+                                                        72.0 / args.serving_scale),
+                       rate=2.0, fp32r_frac=0.8)
+    eng4 = summarize(ServingEngine(hbm_budget=150e9, realtime=True).run(r4))
+    ser4 = summarize(serve_serial_plain(r4, realtime=True))
+    serving = {
+        "workload": f"{len(r4)} requests, Poisson arrivals at 2/s (seed 4), ensemble draws, "
+                    f"run length U(6,72) h / {args.serving_scale:g}, 80% fp32r / 20% fp64, "
+                    f"150 GB HBM admission budget",
+        "engine": eng4, "serial_plain_fp64": ser4,
+        "p99_ratio_serial_over_engine": ser4["latency_s"]["p99"] / eng4["latency_s"]["p99"]}
+    return ens, serving
 
 
 def run_reference(args):
@@ -568,6 +625,11 @@ def main():
     ap.add_argument("--precision", default="fp32r", choices=["fp64", "fp32", "fp32r"])
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-runs", type=int, default=64)
+    ap.add_argument("--ensemble-hours", type=float, default=6.0)
+    ap.add_argument("--serving-requests", type=int, default=32)
+    ap.add_argument("--serving-scale", type=float, default=4.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

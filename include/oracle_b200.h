@@ -110,6 +110,13 @@ typedef struct OraclePlan OraclePlan;
 int oracle_b200_plan_create(const OracleGridDesc *grid, const OracleComponentDesc *comp,
                             OraclePlan **out);
 int oracle_b200_plan_destroy(OraclePlan *plan);
+/* Plans draw their device memory from a per-device pool that keeps released
+ * blocks for the next plan.  plan_destroy waits for all device work first
+ * (as cudaFree would); plan_release instead returns the memory in the order
+ * of `stream`, without synchronising: every kernel that uses the plan must
+ * have been queued on `stream` or have completed.  No reference counterpart
+ * (the reference's solvers are garbage-collected Python objects). */
+int oracle_b200_plan_release(OraclePlan *plan, void *stream);
 
 /* ---- captured steps --------------------------------------------------------
  * A CUDA graph of `nsteps` consecutive in-place steps of one state: the kernel

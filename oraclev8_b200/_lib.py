@@ -33,7 +33,7 @@ EXPORTS = (
     "oracle_b200_tracker_create", "oracle_b200_tracker_destroy", "oracle_b200_track_theta",
     "oracle_b200_track_vorticity", "oracle_b200_step_graph_create",
     "oracle_b200_step_graph_launch", "oracle_b200_step_graph_kernels",
-    "oracle_b200_step_graph_destroy", "oracle_b200_vortex_fill",
+    "oracle_b200_step_graph_destroy", "oracle_b200_vortex_fill", "oracle_b200_plan_release",
 )
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
@@ -82,6 +82,7 @@ def load(path: Path | None = None):
     sig = {
         "oracle_b200_plan_create": ([POINTER(GridDesc), POINTER(ComponentDesc), POINTER(vp)], c_int),
         "oracle_b200_plan_destroy": ([vp], c_int),
+        "oracle_b200_plan_release": ([vp, vp], c_int),
         "oracle_b200_plan_scratch_bytes": ([vp], c_size_t),
         "oracle_b200_step": ([vp, POINTER(StatePtrs), POINTER(StatePtrs), c_double, c_int, vp], c_int),
         "oracle_b200_project": ([vp, vp, vp, vp, vp, c_int, vp], c_int),

@@ -89,6 +89,17 @@ class Plan:
                 pass
             self.handle = None
 
+    def release(self, stream=None) -> None:
+        """Give the plan's device memory back to the pool in the order of
+        ``stream`` (default: the current stream) without synchronising; every
+        kernel that used the plan must have been queued on that stream or be
+        complete.  The plan is unusable afterwards."""
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            s = stream if stream is not None else torch.cuda.current_stream(self.device)
+            self.lib.oracle_b200_plan_release(h, ctypes.c_void_p(s.cuda_stream))
+            self.handle = None
+
     # -- helpers -------------------------------------------------------------
     @property
     def scratch_bytes(self) -> int:

@@ -147,6 +147,8 @@ struct OraclePlan {
   int nparts = 0;
   std::vector<void*> allocs;
   size_t scratch_bytes = 0;
+  cudaMemPool_t pool = nullptr;   // device memory pool (plan_pool)
+  cudaStream_t astream = nullptr; // private stream ordering set-up work
   // launch accounting and optional per-kernel-class event timing
   long launches = 0;
   int profiling = 0;
@@ -159,10 +161,52 @@ struct OraclePlan {
 
 namespace {
 
+// Plan memory comes from one stream-ordered pool per device that keeps the
+// blocks it is given back (release threshold = max).  A loop that retires
+// and creates plans (a serving loop) then reuses the same device memory: no
+// page mapping per plan, and no device-wide synchronisation on release, which
+// cudaFree implies.
+std::mutex g_pool_mu;
+constexpr int kMaxDevices = 64;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+int plan_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  OB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(OB_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    OB_CUDA(cudaMemPoolCreate(&pool, &props));
+    unsigned long long keep = ~0ull;
+    OB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return OB_OK;
+}
+
+// Allocations are ordered on the plan's private set-up stream; plan_create
+// synchronises that stream before returning, after which the memory may be
+// used on any stream.
 template <class P>
 int dalloc(OraclePlan* p, P** out, size_t bytes) {
   void* q = nullptr;
-  OB_CUDA(cudaMalloc(&q, bytes));
+  cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, p->pool, p->astream);
+  if (e == cudaErrorMemoryAllocation) {
+    // give blocks the pool holds for reuse back to the device, then retry
+    cudaGetLastError();
+    OB_CUDA(cudaStreamSynchronize(p->astream));
+    OB_CUDA(cudaMemPoolTrimTo(p->pool, 0));
+    e = cudaMallocFromPoolAsync(&q, bytes, p->pool, p->astream);
+  }
+  if (e != cudaSuccess)
+    return fail(OB_ERR_CUDA, "plan allocation of %zu bytes failed: %s", bytes,
+                cudaGetErrorString(e));
   p->allocs.push_back(q);
   p->scratch_bytes += bytes;
   *out = reinterpret_cast<P*>(q);
@@ -172,8 +216,21 @@ int dalloc(OraclePlan* p, P** out, size_t bytes) {
 int upload(OraclePlan* p, double** out, const double* host, size_t n) {
   int rc = dalloc(p, out, n * sizeof(double));
   if (rc) return rc;
-  OB_CUDA(cudaMemcpy(*out, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  OB_CUDA(cudaMemcpyAsync(*out, host, n * sizeof(double), cudaMemcpyHostToDevice, p->astream));
   return OB_OK;
+}
+
+// Release a plan's memory in the order of `st` (the pool reuses it once the
+// work queued on `st` before this point is done) and free the descriptor.
+void release_plan(OraclePlan* p, cudaStream_t st) {
+  delete p->dbl;  // owns no allocations: its buffers are in p->allocs
+  for (auto& m : p->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  for (void* q : p->allocs) cudaFreeAsync(q, st);
+  if (p->astream) cudaStreamDestroy(p->astream);
+  delete p;
 }
 
 int pick_zc(int nz, size_t per_zc, size_t fixed) {
@@ -519,8 +576,10 @@ int make_refiner(OraclePlan* p) {
   if ((rc = dalloc(p, &q->twx, nx * sizeof(cplx<double>))) ||
       (rc = dalloc(p, &q->twy, ny * sizeof(cplx<double>))))
     return rc;
-  OB_CUDA(cudaMemcpy(q->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice));
-  OB_CUDA(cudaMemcpy(q->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice));
+  OB_CUDA(cudaMemcpyAsync(q->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice,
+                          p->astream));
+  OB_CUDA(cudaMemcpyAsync(q->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice,
+                          p->astream));
   const size_t ns = (size_t)p->g.nxh * ny * nz;
   if ((rc = dalloc(p, &q->S1, ns * ce)) || (rc = dalloc(p, &q->S2, ns * ce))) return rc;
   return set_smem_attrs<double>();
@@ -1009,13 +1068,16 @@ size_t oracle_b200_plan_scratch_bytes(const OraclePlan* p) { return p ? p->scrat
 
 int oracle_b200_plan_destroy(OraclePlan* p) {
   if (!p) return OB_OK;
-  delete p->dbl;  // owns no allocations: its buffers are in p->allocs
-  for (auto& m : p->marks) {
-    cudaEventDestroy(m.a);
-    cudaEventDestroy(m.b);
-  }
-  for (void* q : p->allocs) cudaFree(q);
-  delete p;
+  // wait for all device work, as cudaFree would, so that no queued kernel
+  // still uses the memory when the pool hands it out again
+  cudaDeviceSynchronize();
+  release_plan(p, p->astream);
+  return OB_OK;
+}
+
+int oracle_b200_plan_release(OraclePlan* p, void* stream) {
+  if (!p) return OB_OK;
+  release_plan(p, (cudaStream_t)stream);
   return OB_OK;
 }
 
@@ -1048,6 +1110,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     oracle_b200_plan_destroy(p);
     return rc;
   };
+  if (int rc = plan_pool(&p->pool)) return bail(rc);
+  if (cudaStreamCreateWithFlags(&p->astream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(OB_ERR_CUDA, "plan_create: stream creation failed"));
   p->prec = grid->precision;
   p->esz = p->prec == OB_PREC_F64 ? 8 : 4;
   p->g.nx = nx;
@@ -1145,8 +1210,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<double>)))) return bail(rc);
     if ((rc = dalloc(p, &p->twy, ny * sizeof(cplx<double>)))) return bail(rc);
-    if (cudaMemcpy(p->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice) ||
-        cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice))
+    if (cudaMemcpyAsync(p->twx, tx.data(), nx * sizeof(cplx<double>), cudaMemcpyHostToDevice,
+                        p->astream) ||
+        cudaMemcpyAsync(p->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice,
+                        p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs<double>())) return bail(rc);
     if ((rc = setup_pipes<double>(p))) return bail(rc);
@@ -1155,8 +1222,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     auto tx = twiddles<float>(nx), ty = twiddles<float>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<float>)))) return bail(rc);
     if ((rc = dalloc(p, &p->twy, ny * sizeof(cplx<float>)))) return bail(rc);
-    if (cudaMemcpy(p->twx, tx.data(), nx * sizeof(cplx<float>), cudaMemcpyHostToDevice) ||
-        cudaMemcpy(p->twy, ty.data(), ny * sizeof(cplx<float>), cudaMemcpyHostToDevice))
+    if (cudaMemcpyAsync(p->twx, tx.data(), nx * sizeof(cplx<float>), cudaMemcpyHostToDevice,
+                        p->astream) ||
+        cudaMemcpyAsync(p->twy, ty.data(), ny * sizeof(cplx<float>), cudaMemcpyHostToDevice,
+                        p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs<float>())) return bail(rc);
     if ((rc = setup_pipes<float>(p))) return bail(rc);
@@ -1194,6 +1263,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
   p->nparts = nsm * 4;
   if ((rc = dalloc(p, &p->parts, p->nparts * sizeof(DiagPart)))) return bail(rc);
   if (p->prec == OB_PREC_F32 && (rc = make_refiner(p))) return bail(rc);
+  // allocations and table copies complete: the memory is usable on any stream
+  if (cudaStreamSynchronize(p->astream) != cudaSuccess)
+    return bail(fail(OB_ERR_CUDA, "plan_create: set-up stream failed"));
   *out = p;
   return OB_OK;
 }

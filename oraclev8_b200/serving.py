@@ -6,7 +6,8 @@ admission to retirement.  Its steps are recorded once as a CUDA graph of
 ``chunk`` steps (``RK3Integrator.capture``) and replayed on the run's own
 stream, so runs of different sizes overlap on the device.  Admission is by
 HBM footprint against a budget; finished runs retire and free their slot for
-the next queued request (continuous batching).  Per run the loop records
+the next queued request (continuous batching).  Resident runs are fed
+shortest-remaining-work first, as many at a time as it takes to fill the GPU.  Per run the loop records
 arrival, admission and completion times; the summary gives p50/p95/p99
 time-to-completion, queueing delay and aggregate cell-updates/s.
 
@@ -21,6 +22,8 @@ that an integer number of steps fills the run.
 from __future__ import annotations
 
 import math
+import queue as _queue
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Optional
@@ -179,17 +182,25 @@ class ServingEngine:
     hbm_budget: bytes of resident runs admitted at once.  chunk: steps per
     graph launch.  depth: graph launches kept in flight per run.  realtime:
     honour the arrival times (else every request is available at once).
-    keep_final: copy each run's final state to the host when it retires."""
+    keep_final: copy each run's final state to the host when it retires.
+    prepare_ahead: admitted runs being set up at once on the preparation
+    thread.  inflight_cells: cells of the runs allowed work on the device at
+    once; runs are fed shortest remaining work first."""
 
     def __init__(self, hbm_budget: float = 150e9, chunk: int = 16, depth: int = 2,
-                 realtime: bool = True, keep_final: bool = False, max_active: int = 256):
+                 realtime: bool = True, keep_final: bool = False, max_active: int = 256,
+                 prepare_ahead: int = 4, inflight_cells: float = 8e6):
         self.budget = float(hbm_budget)
+        self.inflight_cells = float(inflight_cells)
+        self.prepare_ahead = int(prepare_ahead)
         self.chunk, self.depth = int(chunk), int(depth)
         self.realtime, self.keep_final = bool(realtime), bool(keep_final)
         self.max_active = int(max_active)
 
     # -- run lifecycle ---------------------------------------------------------
-    def _admit(self, req: RunRequest, now: float) -> _Active:
+    def _prepare(self, req: RunRequest) -> _Active:
+        """Set a run up (plan, device initial state, step graphs): host work,
+        done on the preparation thread while the main loop feeds the GPU."""
         stream = torch.cuda.Stream()
         with torch.cuda.stream(stream):
             integ, state, _ = build_run(req)
@@ -200,7 +211,7 @@ class ServingEngine:
             if tail:
                 graphs[tail] = integ.capture(state, req.dt, tail)
         rec = RunRecord(req.rid, req.n, req.nz, req.precision, req.nsteps, req.cells,
-                        req.arrival_s, admit_s=now)
+                        req.arrival_s)
         return _Active(req, rec, integ, state, stream, graphs, req.nsteps,
                        bytes=footprint_bytes(req))
 
@@ -219,57 +230,102 @@ class ServingEngine:
                 s = a.state
                 a.rec.final = {f: getattr(s, f).detach().cpu().numpy() for f in
                                ("u", "v", "w", "theta_prime", "projection_potential")}
+        # the run's work is complete: hand its plan memory back to the pool
+        # without a device-wide synchronisation
+        a.graphs.clear()
+        a.integ.plan.release(a.stream)
+        a.integ = a.state = None
         return a.rec
 
     # -- main loop -------------------------------------------------------------
     def run(self, requests: "list[RunRequest]") -> "list[RunRecord]":
+        """Serve ``requests`` to completion; returns one record per run.
+
+        The main thread admits requests against the HBM budget (FIFO with
+        backfill: a request that fits may pass one that does not) and keeps
+        every active run's stream fed with graph launches; a preparation
+        thread sets admitted runs up, so host set-up overlaps device work."""
         pending = sorted(requests, key=lambda r: (r.arrival_s, r.rid))
         queue: "list[RunRequest]" = []
         active: "list[_Active]" = []
         done: "list[RunRecord]" = []
-        graveyard: "list[_Active]" = []
-        used = 0      # bytes of active runs (the admission budget)
-        held = 0      # bytes of retired runs not yet released
+        used = 0      # bytes of admitted runs (the admission budget)
+        todo: "_queue.Queue" = _queue.Queue()
+        ready: "_queue.Queue" = _queue.Queue()
+        device = torch.cuda.current_device()
+
+        def worker():
+            torch.cuda.set_device(device)
+            while True:
+                item = todo.get()
+                if item is None:
+                    return
+                req, t_admit = item
+                try:
+                    a = self._prepare(req)
+                    a.rec.admit_s = t_admit
+                    ready.put(a)
+                except BaseException as e:  # surfaced on the main thread
+                    ready.put(e)
+
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
+        preparing = 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        while pending or queue or active:
-            now = time.perf_counter() - t0
-            while pending and (not self.realtime or pending[0].arrival_s <= now):
-                queue.append(pending.pop(0))
-            # admission (FIFO with backfill: a request that fits may pass one
-            # that does not)
-            i = 0
-            while i < len(queue) and len(active) < self.max_active:
-                fb = footprint_bytes(queue[i])
-                if used + fb <= self.budget and used + held + fb > self.budget:
-                    # release retired runs' device memory in one batch (a
-                    # cudaFree synchronises the device, so not once per run)
-                    graveyard.clear()
-                    held = 0
-                if used + fb <= self.budget or not active:
-                    req = queue.pop(i)
-                    a = self._admit(req, time.perf_counter() - t0)
+        try:
+            while pending or queue or active or preparing:
+                now = time.perf_counter() - t0
+                while pending and (not self.realtime or pending[0].arrival_s <= now):
+                    queue.append(pending.pop(0))
+                i = 0
+                while (i < len(queue) and len(active) + preparing < self.max_active
+                       and preparing < self.prepare_ahead):
+                    fb = footprint_bytes(queue[i])
+                    if used + fb <= self.budget or not (active or preparing):
+                        todo.put((queue.pop(i), time.perf_counter() - t0))
+                        used += fb
+                        preparing += 1
+                    else:
+                        i += 1
+                progressed = False
+                while True:
+                    try:
+                        a = ready.get_nowait()
+                    except _queue.Empty:
+                        break
+                    preparing -= 1
+                    if isinstance(a, BaseException):
+                        raise a
                     active.append(a)
-                    used += a.bytes
-                else:
-                    i += 1
-            # keep every run's stream fed
-            progressed = False
-            for a in list(active):
-                a.events = [e for e in a.events if not e.query()]
-                while a.left > 0 and len(a.events) < self.depth:
-                    self._launch(a)
                     progressed = True
-                if a.left == 0 and not a.events:
-                    done.append(self._retire(a, time.perf_counter() - t0))
-                    active.remove(a)
-                    used -= a.bytes
-                    held += a.bytes
-                    graveyard.append(a)
-                    progressed = True
-            if not progressed:
-                time.sleep(50e-6)
-        graveyard.clear()
+                # feed the runs with the least remaining work first (shortest
+                # remaining processing time), while the cells of runs with
+                # work in flight stay under `inflight_cells`: enough
+                # concurrent runs to fill the GPU, without slowing every
+                # resident run down by sharing the GPU among all of them
+                for a in active:
+                    a.events = [e for e in a.events if not e.query()]
+                busy = sum(a.req.cells for a in active if a.events)
+                for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
+                    if a.left > 0 and (a.events or busy < self.inflight_cells):
+                        if not a.events:
+                            busy += a.req.cells
+                        while a.left > 0 and len(a.events) < self.depth:
+                            self._launch(a)
+                            progressed = True
+                for a in list(active):
+                    if a.left == 0 and not a.events:
+                        done.append(self._retire(a, time.perf_counter() - t0))
+                        active.remove(a)
+                        used -= a.bytes
+                        progressed = True
+                if not progressed:
+                    time.sleep(50e-6)
+        finally:
+            todo.put(None)
+            th.join()
+            torch.cuda.synchronize()
         return done
 
 

@@ -47,20 +47,21 @@ class HollandVortexInit:
         return np.exp(-z / self.H_wind)
 
     def _pressure_deficit_1d(self, rho_z, S_z):
-        """Inward trapezoid of dP/dr = rho (V^2/r + f V) (vortex_init.py:223-255);
-        the recurrence is evaluated in closed form as a reversed cumulative sum of
-        the same trapezoid terms."""
+        """Inward trapezoid of dP/dr = rho (V^2/r + f V) (vortex_init.py:223-255).
+        The reference's recurrence P[i] = P[i+1] - term[i] (from P = 0 at the
+        outer edge) is a strictly sequential running sum of -term from the
+        outside in, which numpy's cumulative sum evaluates in the same order
+        (add.accumulate is sequential), so the values are identical."""
         r = self._r1d
-        Vt = self.tangential_wind(r) * S_z
+        if getattr(self, "_vt1d", None) is None:
+            self._vt1d = self.tangential_wind(r)
+        Vt = self._vt1d * S_z
         r_safe = np.where(r > 0.0, r, 1.0)
         dPdr = rho_z * (np.where(r > 0.0, Vt ** 2 / r_safe, 0.0) + self.f * Vt)
         dr = r[1] - r[0]
         P = np.zeros(self.n_radial)
         terms = 0.5 * (dPdr[:-1] + dPdr[1:]) * dr
-        acc = 0.0
-        for i in range(self.n_radial - 2, -1, -1):
-            acc = acc - terms[i]
-            P[i] = acc
+        P[:-1] = np.cumsum(-terms[::-1])[::-1]
         return P
 
     def _tables(self, nx, ny, nz, Lx, Ly, base, x_c, y_c):
