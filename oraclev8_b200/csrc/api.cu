@@ -12,6 +12,7 @@
 #include "../../include/oracle_b200.h"
 #include "kernels.cuh"
 #include "pipe.cuh"
+#include "pencil.cuh"
 #include "tracker.cuh"
 #include "init.cuh"
 
@@ -83,6 +84,25 @@ bool factorize(int M, FftPlan& p, bool radix16 = true) {
   return m == 1;
 }
 
+// Radix-8-first factorisation for the kernels compiled with fft_smem<.., 8>.
+bool factorize8(int M, FftPlan& p) {
+  p.M = M;
+  p.np = 0;
+  int m = M;
+  for (int r : {8, 4, 2, 3, 5})
+    while (m > 1 && m % r == 0) {
+      if (p.np >= 16) return false;
+      p.r[p.np++] = r;
+      m /= r;
+    }
+  int ns = 1;
+  for (int s = 0; s < p.np; ++s) {
+    p.ns[s] = FastDiv((unsigned)ns);
+    ns *= p.r[s];
+  }
+  return m == 1;
+}
+
 // 2 pi fftfreq(n, d=L/n), with NumPy's operation order (numpy/fft/_helper.py).
 std::vector<double> wavenumbers(int n, double L) {
   const double d = L / n;
@@ -124,6 +144,9 @@ struct OraclePlan {
   int zc_fxp = 1, zc_fyp = 1, zc_iyp = 1, zc_ixp = 1;
   int grid_fxp = 1, grid_fyp = 1, grid_iyp = 1, grid_ixp = 1;
   int use_pipe = 0;  // projection through the persistent pipelined kernels
+  // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
+  FftPlan px8{};
+  int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0;
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -294,6 +317,40 @@ int pick_pipe_zc(int nz, F&& smem) {
   return 0;
 }
 
+// x2 pencil kernels: allow the full shared-memory carve-out so that the
+// target number of CTAs fits on an SM.
+template <class K>
+int x2_attr(K kernel) {
+  OB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+  OB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  return OB_OK;
+}
+
+template <class T, class TS, int ZC>
+int x2_attrs_zc() {
+  int rc;
+  if ((rc = x2_attr(k_fx2<T, false, TS, ZC>)) || (rc = x2_attr(k_fx2<T, true, TS, ZC>)) ||
+      (rc = x2_attr(k_ix2<T, IX_CORRECT, TS, ZC>)) || (rc = x2_attr(k_ix2<T, IX_STAGE, TS, ZC>)))
+    return rc;
+  if constexpr (sizeof(TS) == 4)
+    if ((rc = x2_attr(k_ix2<T, IX_REFINE, TS, ZC>))) return rc;
+  return OB_OK;
+}
+
+template <class T>
+int set_x2_attrs() {
+  int rc;
+  if ((rc = x2_attrs_zc<T, T, 1>()) || (rc = x2_attrs_zc<T, T, 2>()) ||
+      (rc = x2_attrs_zc<T, T, 4>()) || (rc = x2_attrs_zc<T, T, 8>()))
+    return rc;
+  if constexpr (sizeof(T) == 8) {  // residual transforms of the FP32 defect correction
+    for (auto k : {k_fx2<double, false, float, 1>, k_fx2<double, false, float, 2>,
+                   k_fx2<double, false, float, 4>, k_fx2<double, false, float, 8>})
+      if ((rc = x2_attr(k))) return rc;
+  }
+  return OB_OK;
+}
+
 template <class T>
 int set_smem_attrs() {
   const int mx = (int)kSmemMax;
@@ -319,7 +376,7 @@ int set_smem_attrs() {
   OB_CUDA(cudaFuncSetAttribute(k_fx<double, FX_DIV, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_fy<double, FY_RESID, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ix<float, IX_REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  return OB_OK;
+  return set_x2_attrs<T>();
 }
 
 // Persistent grid: resident CTAs per SM (occupancy API) x SMs, capped by items.
@@ -404,6 +461,89 @@ struct Launch {
 dim3 grid_x(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.ny); }
 dim3 grid_y(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.nxh); }
 
+// ---- x2 pencil kernels (pencil.cuh) ----------------------------------------
+// shared memory per CTA for the pencil_min_blocks<T>() CTAs per SM
+template <class T>
+size_t x2_smem_budget() {
+  if (const char* e = getenv("ORACLE_B200_X2_SMEM_KB")) return (size_t)atoi(e) * 1024;
+  return sizeof(T) == 8 ? 112 * 1024 : 74 * 1024;
+}
+
+// Dynamic shared memory of a k_fx2 (kind 0), staged k_fx2 (kind 1) or k_ix2
+// (kind 2) launch with z-chunk zc.
+template <class T, class TS>
+size_t x2_smem(int kind, int zc, int nx) {
+  switch (zc) {
+#define OB_X2_CASE(Z)                                                                  \
+  case Z:                                                                              \
+    return kind == 0 ? fx2_layout<T, TS, Z, false>(nx).total                           \
+                     : kind == 1 ? fx2_layout<T, TS, Z, true>(nx).total : ix2_layout<T, Z>(nx).total;
+    OB_X2_CASE(1)
+    OB_X2_CASE(2)
+    OB_X2_CASE(4)
+    OB_X2_CASE(8)
+#undef OB_X2_CASE
+  }
+  return ~size_t(0);
+}
+
+// Largest z-chunk in {8, 4, 2, 1} (no larger than nz) whose tile fits the
+// per-CTA budget of the kernels' target occupancy, else the largest that fits
+// one CTA; 0 when none fits.
+template <class T, class TS>
+int pick_x2_zc(int kind, int nx, int nz) {
+  if (const char* e = getenv("ORACLE_B200_X2"))
+    if (atoi(e) == 0) return 0;
+  for (size_t cap : {x2_smem_budget<T>(), kSmemMax})
+    for (int zc : {8, 4, 2, 1}) {
+      if (zc > 1 && zc > nz) continue;
+      if (x2_smem<T, TS>(kind, zc, nx) <= cap) return zc;
+    }
+  return 0;
+}
+
+template <class T, bool STAGE, class TS, int ZC>
+void fx2_launch(const OraclePlan* q, const TS* u, const TS* v, const TS* w, const TS* th,
+                double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
+  const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
+  k_fx2<T, STAGE, TS, ZC><<<grid, kPencilThreads, fx2_layout<T, TS, ZC, STAGE>(q->g.nx).total,
+                            st>>>(q->g, q->px8, u, v, w, th, sdt, q->rho, q->rhoh, q->theta0,
+                                  q->kx, (const cplx<T>*)q->twx, X0, X1);
+}
+
+template <class T, bool STAGE, class TS>
+void fx2(const OraclePlan* q, int zc, const TS* u, const TS* v, const TS* w, const TS* th,
+         double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
+  switch (zc) {
+    case 1: fx2_launch<T, STAGE, TS, 1>(q, u, v, w, th, sdt, X0, X1, st); break;
+    case 2: fx2_launch<T, STAGE, TS, 2>(q, u, v, w, th, sdt, X0, X1, st); break;
+    case 4: fx2_launch<T, STAGE, TS, 4>(q, u, v, w, th, sdt, X0, X1, st); break;
+    default: fx2_launch<T, STAGE, TS, 8>(q, u, v, w, th, sdt, X0, X1, st); break;
+  }
+}
+
+template <class T, int MODE, class TS, int ZC>
+void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
+                const TS* v, const TS* w, const TS* th, double sdt, TS* uo, TS* vo, TS* wo,
+                TS* phio, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
+  k_ix2<T, MODE, TS, ZC><<<grid, kPencilThreads, ix2_layout<T, ZC>(p->g.nx).total, st>>>(
+      p->g, p->px8, phs, psi, p->kx, (const cplx<T>*)p->twx, u, v, w, th, sdt, p->theta0, uo,
+      vo, wo, phio);
+}
+
+template <class T, int MODE, class TS>
+void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
+         const TS* v, const TS* w, const TS* th, double sdt, TS* uo, TS* vo, TS* wo, TS* phio,
+         cudaStream_t st) {
+  switch (zc) {
+    case 1: ix2_launch<T, MODE, TS, 1>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
+    case 2: ix2_launch<T, MODE, TS, 2>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
+    case 4: ix2_launch<T, MODE, TS, 4>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
+    default: ix2_launch<T, MODE, TS, 8>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
+  }
+}
+
 // projection through the persistent pipelined kernels (pipe.cuh)
 template <class T>
 int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
@@ -474,7 +614,11 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   }
   const bool stage = stage_sdt >= 0.0;
   if (p->use_pipe) return project_pipe<T>(p, u, v, w, th, stage_sdt, uo, vo, wo, phio, diag, slot_c, slot_d, st);
-  if (stage)
+  if (stage && p->zc2_fxs)
+    { Launch L_(p, 0, st); fx2<T, true, T>(p, p->zc2_fxs, u, v, w, th, stage_sdt, S1, S2, st); }
+  else if (!stage && p->zc2_fx)
+    { Launch L_(p, 0, st); fx2<T, false, T>(p, p->zc2_fx, u, v, w, th, 0.0, S1, S2, st); }
+  else if (stage)
     { Launch L_(p, 0, st); k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
         g, p->pxf, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
         (const C*)p->twx, S1, S2, nullptr); }
@@ -495,7 +639,11 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
       g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
-  if (stage)
+  if (p->zc2_ix && stage)
+    { Launch L_(p, 4, st); ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, th, stage_sdt, uo, vo, wo, phio, st); }
+  else if (p->zc2_ix)
+    { Launch L_(p, 4, st); ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, th, 0.0, uo, vo, wo, phio, st); }
+  else if (stage)
     { Launch L_(p, 4, st); k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
         g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th,
         stage_sdt, p->theta0, uo, vo, wo, phio); }
@@ -526,9 +674,12 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
   Cf* S1 = (Cf*)p->S1;
   Cf* S2 = (Cf*)p->S2;
   Cf* S3 = (Cf*)p->S3;
-  { Launch L_(p, OB_PROF_REFINE, st); k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
-      g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
-      (const Cd*)q->twx, R1, R2, nullptr); }
+  if (q->zc2_fx)
+    { Launch L_(p, OB_PROF_REFINE, st); fx2<double, false, float>(q, q->zc2_fx, u, v, w, nullptr, 0.0, R1, R2, st); }
+  else
+    { Launch L_(p, OB_PROF_REFINE, st); k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
+        g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
+        (const Cd*)q->twx, R1, R2, nullptr); }
   OB_LAUNCHED();
   { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
       g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
@@ -540,9 +691,12 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
   { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
-  { Launch L_(p, OB_PROF_REFINE, st); k_ix<float, IX_REFINE><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
-      g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const Cf*)p->twx, u, v, w, nullptr, 0.0,
-      p->theta0, u, v, w, phi); }
+  if (p->zc2_ix)
+    { Launch L_(p, OB_PROF_REFINE, st); ix2<float, IX_REFINE, float>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
+  else
+    { Launch L_(p, OB_PROF_REFINE, st); k_ix<float, IX_REFINE><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
+        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const Cf*)p->twx, u, v, w, nullptr, 0.0,
+        p->theta0, u, v, w, phi); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -560,6 +714,7 @@ int make_refiner(OraclePlan* p) {
   q->py = p->py;
   q->pxf = p->pxf;
   q->pyf = p->pyf;
+  q->px8 = p->px8;
   q->kx = p->kx;
   q->ky = p->ky;
   q->rho = p->rho;
@@ -569,6 +724,7 @@ int make_refiner(OraclePlan* p) {
   const size_t ce = 16;
   q->zc_fx = pick_zc(nz, 2ull * (q->g.M + 1) * 3 * ce, tw_bytes(q, nx));
   q->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, tw_bytes(q, ny));
+  q->zc2_fx = pick_x2_zc<double, float>(0, nx, nz);
   if (smem_fx(q, 3) > kSmemMax || smem_fy(q, 2, q->zc_fy) > kSmemMax)
     return fail(OB_ERR_ARG, "grid too large for the FP64 residual kernels");
   auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
@@ -1243,6 +1399,18 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       smem_ix(p, 3 * p->zc_ix + 1) > kSmemMax || smem_thomas(p) > kSmemMax)
     return bail(fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx,
                      ny, nz));
+  // compile-time-chunk x-pencil kernels where their tiles fit
+  if (factorize8(nx / 2, p->px8)) {
+    if (p->prec == OB_PREC_F64) {
+      p->zc2_fx = pick_x2_zc<double, double>(0, nx, nz);
+      p->zc2_fxs = pick_x2_zc<double, double>(1, nx, nz);
+      p->zc2_ix = pick_x2_zc<double, double>(2, nx, nz);
+    } else {
+      p->zc2_fx = pick_x2_zc<float, float>(0, nx, nz);
+      p->zc2_fxs = pick_x2_zc<float, float>(1, nx, nz);
+      p->zc2_ix = pick_x2_zc<float, float>(2, nx, nz);
+    }
+  }
 
   const size_t n = (size_t)nx * ny * nz, nw = (size_t)nx * ny * (nz + 1);
   const size_t ns = (size_t)p->g.nxh * ny * nz;

@@ -159,7 +159,8 @@ __device__ __forceinline__ void stockham_pass(const cplx<T>* __restrict__ in,
 // before (input ready); this returns after a barrier.
 // MAXR: largest radix compiled into the caller.  Kernels whose plans stop at
 // radix 4 instantiate fft_smem<.., 4> so the 16-point butterfly (and its
-// register pressure) is not part of them.
+// register pressure) is not part of them; MAXR = 8 compiles radices 2-5 and 8
+// (plans from a radix-8-first factorisation) and not 16.
 template <class T, bool INV, int MAXR = 16>
 __device__ cplx<T>* fft_smem(cplx<T>* a, cplx<T>* b, int B, int Bs, const FftPlan& p,
                              const cplx<T>* __restrict__ tw, int tws) {
@@ -172,6 +173,9 @@ __device__ cplx<T>* fft_smem(cplx<T>* a, cplx<T>* b, int B, int Bs, const FftPla
       case 2: stockham_pass<T, 2, INV>(a, b, p.M, B, Bs, fB, Ns, p.ns[s], tw, step); break;
       case 3: stockham_pass<T, 3, INV>(a, b, p.M, B, Bs, fB, Ns, p.ns[s], tw, step); break;
       case 4: stockham_pass<T, 4, INV>(a, b, p.M, B, Bs, fB, Ns, p.ns[s], tw, step); break;
+      case 8:
+        if constexpr (MAXR == 8) stockham_pass<T, 8, INV>(a, b, p.M, B, Bs, fB, Ns, p.ns[s], tw, step);
+        break;
       case 16:
         if constexpr (MAXR >= 16) stockham_pass<T, 16, INV>(a, b, p.M, B, Bs, fB, Ns, p.ns[s], tw, step);
         break;

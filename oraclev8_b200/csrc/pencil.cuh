@@ -1,0 +1,331 @@
+// x-pencil kernels of the projection with compile-time z-chunks.
+//
+// Same arithmetic as k_fx (FX_DIV / FX_DIV_STAGE) and k_ix (IX_CORRECT /
+// IX_STAGE / IX_REFINE) in kernels.cuh; the data movement is reorganised for
+// memory-level parallelism and fewer instructions:
+//  * every global input of a CTA is requested at once with cp.async
+//    (global -> shared, no register staging), so a CTA's whole tile is in
+//    flight in one memory round trip instead of one per batch of loads;
+//  * the z-chunk ZC is a template parameter and threads own rows (x or kx)
+//    and loop over the ZC levels of the row, so no index needs a division;
+//  * k_ix2 loads phi~ once and forms the i kx' phi~ column in its C2R
+//    pre-process instead of loading phi~ twice;
+//  * launch bounds of three CTAs per SM in FP32 and two in FP64, with the
+//    z-chunk chosen so that that many tiles fit in shared memory.
+// Layouts are those of kernels.cuh: state (x, y, z) with z contiguous, w on
+// nz + 1 levels; spectra [kx][y][z] with kx in [0, nx/2].
+#pragma once
+#include "kernels.cuh"
+#include "pipe.cuh"
+
+namespace ob {
+
+constexpr int kPencilThreads = 256;
+// CTAs per SM the launch bounds target: three in FP32; two in FP64, whose
+// radix-8 butterflies need more than the 80 registers three CTAs leave.
+template <class T>
+constexpr int pencil_min_blocks() { return sizeof(T) == 8 ? 2 : 3; }
+
+// Shared-memory layout of k_fx2 (bytes from the dynamic base), shared by the
+// kernel and the host's launch sizing.
+struct Fx2Layout {
+  size_t tw, bufA, bufB, raw_u, raw_v, raw_w, raw_t, total;
+};
+template <class T, class TS, int ZC, bool STAGE>
+__host__ __device__ inline Fx2Layout fx2_layout(int nx) {
+  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const int M = nx / 2;
+  const size_t B = 3 * ZC;
+  Fx2Layout L;
+  L.tw = 0;
+  L.bufA = al((size_t)nx * sizeof(cplx<T>));
+  const size_t buf = al((size_t)(M + 1) * B * sizeof(cplx<T>));
+  L.bufB = L.bufA + buf;
+  // raw tiles share the second FFT buffer's space (dead until the first pass)
+  L.raw_u = L.bufB;
+  L.raw_v = L.raw_u + al((size_t)nx * ZC * sizeof(TS));
+  L.raw_w = L.raw_v + al((size_t)nx * ZC * sizeof(TS));
+  L.raw_t = L.raw_w + al((size_t)nx * (ZC + 1) * sizeof(TS));
+  const size_t raw_end = L.raw_t + (STAGE ? al((size_t)nx * (ZC + 2) * sizeof(TS)) : 0);
+  L.total = (L.bufB + buf > raw_end) ? L.bufB + buf : raw_end;
+  return L;
+}
+
+// x-pencil forward kernel: rho-weighting, vertical flux divergence (STAGE:
+// of w + sdt b_half), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd),
+// X1 = FFTx(rho v).  grid = (ceil(nz/ZC), ny).
+template <class T, bool STAGE, class TS, int ZC>
+__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
+    GridK g, FftPlan px, const TS* __restrict__ u, const TS* __restrict__ v,
+    const TS* __restrict__ w, const TS* __restrict__ th, double sdt,
+    const double* __restrict__ rho, const double* __restrict__ rhoh,
+    const double* __restrict__ theta0, const double* __restrict__ kxd,
+    const cplx<T>* __restrict__ twx, cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  const Fx2Layout L = fx2_layout<T, TS, ZC, STAGE>(g.nx);
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufA);
+  cplx<T>* bufB = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufB);
+  TS* U = reinterpret_cast<TS*>(smem_dyn + L.raw_u);
+  TS* V = reinterpret_cast<TS*>(smem_dyn + L.raw_v);
+  TS* W = reinterpret_cast<TS*>(smem_dyn + L.raw_w);
+  TS* TH = reinterpret_cast<TS*>(smem_dyn + L.raw_t);
+  const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
+  constexpr int B = 3 * ZC;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+
+  // 1. the whole tile in flight at once.  Consecutive threads take
+  //    consecutive levels of a row, so a warp's requests cover whole runs of
+  //    each row's contiguous z segment (divisions by compile-time widths).
+  for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    const size_t gi = ((size_t)x * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&U[e], u + gi, ok);
+    copy_or_zero(&V[e], v + gi, ok);
+  }
+  for (int e = threadIdx.x; e < nx * (ZC + 1); e += kPencilThreads) {
+    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+    const int z = z0 + j;  // w levels z0 .. z0+ZC
+    const bool ok = z <= nz;
+    copy_or_zero(&W[e], w + ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
+  }
+  if (STAGE) {
+    for (int e = threadIdx.x; e < nx * (ZC + 2); e += kPencilThreads) {
+      const int x = e / (ZC + 2), j = e - x * (ZC + 2);
+      const int z = z0 - 1 + j;  // theta' levels z0-1 .. z0+ZC
+      const bool ok = z >= 0 && z < nz;
+      copy_or_zero(&TH[e], th + ((size_t)x * ny + y) * nz + (ok ? z : 0), ok);
+    }
+  }
+  cp_commit();
+  for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
+  cp_wait<0>();
+  __syncthreads();
+
+  // 2. pack rows (2n, 2n+1) into complex inputs z[n] = f[2n] + i f[2n+1]
+  const double dz = g.dz;
+  for (int n = threadIdx.x; n < M; n += kPencilThreads) {
+#pragma unroll
+    for (int j = 0; j < ZC; ++j) {
+      const int z = z0 + j;
+      const bool ok = z < nz;
+      const double r = ok ? rho[z] : 0.0;
+      const double rl = ok ? rhoh[z] : 0.0, ru = ok ? rhoh[z + 1] : 0.0;
+      T fu[2], fv[2], fd[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int x = 2 * n + h;
+        fu[h] = (T)(r * (double)U[x * ZC + j]);
+        fv[h] = (T)(r * (double)V[x * ZC + j]);
+        double wl, wu;
+        if (STAGE) {
+          const TS* wc = W + x * (ZC + 1) - z0;      // wc[k] = w at level k
+          const TS* tc = TH + x * (ZC + 2) - (z0 - 1);  // tc[k] = theta' at level k
+          wl = ok ? stage_w(wc, tc, z, nz, sdt, theta0) : 0.0;
+          wu = ok ? stage_w(wc, tc, z + 1, nz, sdt, theta0) : 0.0;
+        } else {
+          wl = (double)W[x * (ZC + 1) + j];
+          wu = (double)W[x * (ZC + 1) + j + 1];
+        }
+        fd[h] = ok ? (T)((ru * wu - rl * wl) / dz) : (T)0;
+      }
+      bufA[(size_t)n * B + j] = mk<T>(fu[0], fu[1]);
+      bufA[(size_t)n * B + ZC + j] = mk<T>(fv[0], fv[1]);
+      bufA[(size_t)n * B + 2 * ZC + j] = mk<T>(fd[0], fd[1]);
+    }
+  }
+  __syncthreads();
+
+  // 3. M-point FFTs of the packed rows, then the real-to-complex split
+  cplx<T>* Z = fft_smem<T, false, 8>(bufA, bufB, B, px, stw, 2);
+  cplx<T>* X = (Z == bufA) ? bufB : bufA;
+  r2c_post<T>(Z, X, M, B, stw);
+  __syncthreads();
+
+  // 4. X0 = i kx' U + D, X1 = V (consecutive threads on consecutive levels)
+  for (int e = threadIdx.x; e < (M + 1) * ZC; e += kPencilThreads) {
+    const int k = e / ZC, j = e - k * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const T kk = (k == M) ? (T)0 : (T)kxd[k];
+    const size_t o = ((size_t)k * ny + y) * nz + z;
+    const cplx<T> Uk = X[(size_t)k * B + j];
+    const cplx<T> Vk = X[(size_t)k * B + ZC + j];
+    const cplx<T> Dk = X[(size_t)k * B + 2 * ZC + j];
+    X0[o] = add(ik(kk, Uk), Dk);
+    X1[o] = Vk;
+  }
+}
+
+// Shared-memory layout of k_ix2.
+struct Ix2Layout {
+  size_t tw, bufX, bufZ, total;
+};
+template <class T, int ZC>
+__host__ __device__ inline Ix2Layout ix2_layout(int nx) {
+  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const int M = nx / 2;
+  const size_t B = 3 * ZC + 1;
+  Ix2Layout L;
+  L.tw = 0;
+  L.bufX = al((size_t)nx * sizeof(cplx<T>));
+  L.bufZ = L.bufX + al((size_t)(M + 1) * B * sizeof(cplx<T>));
+  L.total = L.bufZ + al((size_t)M * B * sizeof(cplx<T>));
+  return L;
+}
+
+// x-pencil inverse kernel with the velocity correction.  Columns of the batch
+// (B = 3 ZC + 1): [0, ZC] phi at levels z0-1 .. z0+ZC-1 (one halo level for
+// the vertical difference), [ZC+1, 2ZC] d/dx phi, [2ZC+1, 3ZC] d/dy phi.
+//   IX_CORRECT: u -= gx, v -= gy, w[k] -= (phi_k - phi_{k-1}) / dz (k >= 1),
+//               phi stored (tendency.py:781-788); out may alias in.
+//   IX_STAGE:   out = (u_n - gx, v_n - gy, w_n + sdt b_half - gz, phi)
+//               (integrator.py:483-500).
+//   IX_REFINE:  as IX_CORRECT but phi_out += phi (a correction potential).
+// grid = (ceil(nz/ZC), ny).
+template <class T, int MODE, class TS, int ZC>
+__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
+    GridK g, FftPlan px, const cplx<T>* __restrict__ phs, const cplx<T>* __restrict__ psi,
+    const double* __restrict__ kxd, const cplx<T>* __restrict__ twx, const TS* u_in,
+    const TS* v_in, const TS* w_in, const TS* __restrict__ th, double sdt,
+    const double* __restrict__ theta0, TS* u_out, TS* v_out, TS* w_out, TS* phi_out) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  const Ix2Layout L = ix2_layout<T, ZC>(g.nx);
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
+  cplx<T>* bufX = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufX);
+  cplx<T>* bufZ = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufZ);
+  const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
+  constexpr int B = 3 * ZC + 1;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+
+  // 1. phi~ (with the halo level) and psi~ rows, all in flight at once;
+  //    consecutive threads on consecutive levels of a row
+  constexpr int BI = 2 * ZC + 1;  // loaded columns per row
+  for (int e = threadIdx.x; e < (M + 1) * BI; e += kPencilThreads) {
+    const int k = e / BI, b = e - k * BI;
+    const size_t ob = ((size_t)k * ny + y) * nz;
+    if (b <= ZC) {
+      const int z = z0 - 1 + b;
+      const bool ok = z >= 0 && z < nz;
+      copy_or_zero(&bufX[(size_t)k * B + b], phs + ob + (ok ? z : 0), ok);
+    } else {
+      const int j = b - ZC - 1;
+      const int z = z0 + j;
+      const bool ok = z < nz;
+      copy_or_zero(&bufX[(size_t)k * B + 2 * ZC + 1 + j], psi + ob + (ok ? z : 0), ok);
+    }
+  }
+  cp_commit();
+  for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
+  // state this thread corrects in its first kIxPrefetch output iterations:
+  // loaded now, so the latency overlaps the transforms below
+  TS pu[kIxPrefetch], pv[kIxPrefetch], pw[kIxPrefetch], pt[kIxPrefetch];
+#pragma unroll
+  for (int q = 0; q < kIxPrefetch; ++q) {
+    const int e = threadIdx.x + q * kPencilThreads;
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    pu[q] = pv[q] = pw[q] = pt[q] = (TS)0;
+    if (e < nx * ZC && z < nz) {
+      const size_t col = (size_t)x * ny + y;
+      const TS* wc = w_in + col * (nz + 1);
+      pu[q] = u_in[col * nz + z];
+      pv[q] = v_in[col * nz + z];
+      if (MODE == IX_STAGE) {
+        const TS* tc = th + col * nz;
+        pw[q] = (TS)stage_w(wc, tc, z, nz, sdt, theta0);
+        if (z == nz - 1) pt[q] = (TS)stage_w(wc, tc, nz, nz, sdt, theta0);
+      } else {
+        pw[q] = wc[z];
+        if (z == nz - 1) pt[q] = wc[nz];
+      }
+    }
+  }
+  cp_wait<0>();
+  __syncthreads();
+
+  // 2. C2R pre-process of every column; the d/dx columns come from the phi~
+  //    columns times i kx' (kx' = 0 at the Nyquist index M)
+  for (int m = threadIdx.x; m < M; m += kPencilThreads) {
+    const cplx<T> twc = conjg(stw[m]);
+    const T km = (T)kxd[m];
+    const T kc = (m == 0) ? (T)0 : (T)kxd[M - m];  // kx'[M] = 0
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      cplx<T> xm, xc;
+      if (c >= ZC + 1 && c <= 2 * ZC) {
+        const int src = c - ZC;  // phi~ column of the same level
+        xm = ik(km, bufX[(size_t)m * B + src]);
+        xc = ik(kc, bufX[(size_t)(M - m) * B + src]);
+      } else {
+        xm = bufX[(size_t)m * B + c];
+        xc = bufX[(size_t)(M - m) * B + c];
+      }
+      if (m == 0) {
+        xm.y = (T)0;
+        xc.y = (T)0;
+      }
+      xc = conjg(xc);
+      const cplx<T> S = add(xm, xc);
+      const cplx<T> D = mul(sub(xm, xc), twc);
+      bufZ[(size_t)m * B + c] = mk<T>(S.x - D.y, S.y + D.x);
+    }
+  }
+  __syncthreads();
+
+  // 3. inverse M-point FFTs: row x of column c is rz[2 ((x>>1) B + c) + (x&1)]
+  cplx<T>* Zr = fft_smem<T, true, 8>(bufZ, bufX, B, px, stw, 2);
+  const T* rz = reinterpret_cast<const T*>(Zr);
+
+  // 4. velocity correction; consecutive threads on consecutive levels
+  const double dz = g.dz;
+#pragma unroll 1
+  for (int e = threadIdx.x, q = 0; e < nx * ZC; e += kPencilThreads, ++q) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    if (z < nz) {
+      const size_t col = (size_t)x * ny + y;
+      const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
+      const TS* wc = w_in + col * (nz + 1);
+      const TS* tc = (MODE == IX_STAGE) ? th + col * nz : nullptr;
+      const size_t idx = col * nz + z;
+      const T phi = rz[rb + 2 * (j + 1)];
+      const T phib = rz[rb + 2 * j];
+      const T gx = rz[rb + 2 * (ZC + 1 + j)];
+      const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
+      const T gz = (z >= 1) ? (T)((phi - phib) / (T)dz) : (T)0;
+      TS uc, vc, wcz, wt = (TS)0;
+      if (q < kIxPrefetch) {
+        // select the prefetched registers without dynamic array indexing
+        uc = pu[0]; vc = pv[0]; wcz = pw[0]; wt = pt[0];
+#pragma unroll
+        for (int r = 1; r < kIxPrefetch; ++r)
+          if (q == r) { uc = pu[r]; vc = pv[r]; wcz = pw[r]; wt = pt[r]; }
+      } else {
+        uc = u_in[idx];
+        vc = v_in[idx];
+        if (MODE == IX_STAGE) {
+          wcz = (TS)stage_w(wc, tc, z, nz, sdt, theta0);
+          if (z == nz - 1) wt = (TS)stage_w(wc, tc, nz, nz, sdt, theta0);
+        } else {
+          wcz = wc[z];
+          if (z == nz - 1) wt = wc[nz];
+        }
+      }
+      u_out[idx] = (TS)((T)uc - gx);
+      v_out[idx] = (TS)((T)vc - gy);
+      w_out[col * (nz + 1) + z] = (TS)((T)wcz - gz);
+      if (z == nz - 1 && (MODE == IX_STAGE || w_out != w_in)) w_out[col * (nz + 1) + nz] = wt;
+      if (MODE == IX_REFINE)
+        phi_out[idx] = (TS)((T)phi_out[idx] + phi);
+      else
+        phi_out[idx] = (TS)phi;
+    }
+  }
+}
+
+}  // namespace ob
