@@ -165,6 +165,7 @@ struct OraclePlan {
   void *Au = nullptr, *Av = nullptr, *Aw = nullptr, *Ath = nullptr, *Aphi = nullptr;
   void *Su = nullptr, *Sv = nullptr, *Sw = nullptr, *Sphi = nullptr;
   void *Du = nullptr, *Dv = nullptr;                         // damper / temp
+  void* Bh = nullptr;  // half-level buoyancy of the step's anchor theta' (nz + 1 levels)
   double* diag = nullptr;
   DiagPart* parts = nullptr;
   int nparts = 0;
@@ -502,45 +503,46 @@ int pick_x2_zc(int kind, int nx, int nz) {
   return 0;
 }
 
+// bh: the step's half-level buoyancy field (STAGE only)
 template <class T, bool STAGE, class TS, int ZC>
-void fx2_launch(const OraclePlan* q, const TS* u, const TS* v, const TS* w, const TS* th,
+void fx2_launch(const OraclePlan* q, const TS* u, const TS* v, const TS* w, const TS* bh,
                 double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
   const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
   k_fx2<T, STAGE, TS, ZC><<<grid, kPencilThreads, fx2_layout<T, TS, ZC, STAGE>(q->g.nx).total,
-                            st>>>(q->g, q->px8, u, v, w, th, sdt, q->rho, q->rhoh, q->theta0,
-                                  q->kx, (const cplx<T>*)q->twx, X0, X1);
+                            st>>>(q->g, q->px8, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx,
+                                  (const cplx<T>*)q->twx, X0, X1);
 }
 
 template <class T, bool STAGE, class TS>
-void fx2(const OraclePlan* q, int zc, const TS* u, const TS* v, const TS* w, const TS* th,
+void fx2(const OraclePlan* q, int zc, const TS* u, const TS* v, const TS* w, const TS* bh,
          double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
   switch (zc) {
-    case 1: fx2_launch<T, STAGE, TS, 1>(q, u, v, w, th, sdt, X0, X1, st); break;
-    case 2: fx2_launch<T, STAGE, TS, 2>(q, u, v, w, th, sdt, X0, X1, st); break;
-    case 4: fx2_launch<T, STAGE, TS, 4>(q, u, v, w, th, sdt, X0, X1, st); break;
-    default: fx2_launch<T, STAGE, TS, 8>(q, u, v, w, th, sdt, X0, X1, st); break;
+    case 1: fx2_launch<T, STAGE, TS, 1>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    case 2: fx2_launch<T, STAGE, TS, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    case 4: fx2_launch<T, STAGE, TS, 4>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    default: fx2_launch<T, STAGE, TS, 8>(q, u, v, w, bh, sdt, X0, X1, st); break;
   }
 }
 
 template <class T, int MODE, class TS, int ZC>
 void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
-                const TS* v, const TS* w, const TS* th, double sdt, TS* uo, TS* vo, TS* wo,
+                const TS* v, const TS* w, const TS* bh, double sdt, TS* uo, TS* vo, TS* wo,
                 TS* phio, cudaStream_t st) {
   const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
   k_ix2<T, MODE, TS, ZC><<<grid, kPencilThreads, ix2_layout<T, ZC>(p->g.nx).total, st>>>(
-      p->g, p->px8, phs, psi, p->kx, (const cplx<T>*)p->twx, u, v, w, th, sdt, p->theta0, uo,
-      vo, wo, phio);
+      p->g, p->px8, phs, psi, p->kx, (const cplx<T>*)p->twx, u, v, w, bh, sdt, uo, vo, wo,
+      phio);
 }
 
 template <class T, int MODE, class TS>
 void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
-         const TS* v, const TS* w, const TS* th, double sdt, TS* uo, TS* vo, TS* wo, TS* phio,
+         const TS* v, const TS* w, const TS* bh, double sdt, TS* uo, TS* vo, TS* wo, TS* phio,
          cudaStream_t st) {
   switch (zc) {
-    case 1: ix2_launch<T, MODE, TS, 1>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
-    case 2: ix2_launch<T, MODE, TS, 2>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
-    case 4: ix2_launch<T, MODE, TS, 4>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
-    default: ix2_launch<T, MODE, TS, 8>(p, phs, psi, u, v, w, th, sdt, uo, vo, wo, phio, st); break;
+    case 1: ix2_launch<T, MODE, TS, 1>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    case 2: ix2_launch<T, MODE, TS, 2>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    case 4: ix2_launch<T, MODE, TS, 4>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    default: ix2_launch<T, MODE, TS, 8>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
   }
 }
 
@@ -595,7 +597,7 @@ int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
 template <class T>
 int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
                  double stage_sdt, T* uo, T* vo, T* wo, T* phio, int slot_c, int slot_d,
-                 cudaStream_t st) {
+                 cudaStream_t st, const T* bh = nullptr) {
   using C = cplx<T>;
   const GridK g = p->g;
   C* S1 = (C*)p->S1;
@@ -614,8 +616,8 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   }
   const bool stage = stage_sdt >= 0.0;
   if (p->use_pipe) return project_pipe<T>(p, u, v, w, th, stage_sdt, uo, vo, wo, phio, diag, slot_c, slot_d, st);
-  if (stage && p->zc2_fxs)
-    { Launch L_(p, 0, st); fx2<T, true, T>(p, p->zc2_fxs, u, v, w, th, stage_sdt, S1, S2, st); }
+  if (stage && p->zc2_fxs && bh)
+    { Launch L_(p, 0, st); fx2<T, true, T>(p, p->zc2_fxs, u, v, w, bh, stage_sdt, S1, S2, st); }
   else if (!stage && p->zc2_fx)
     { Launch L_(p, 0, st); fx2<T, false, T>(p, p->zc2_fx, u, v, w, th, 0.0, S1, S2, st); }
   else if (stage)
@@ -639,10 +641,10 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
       g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
-  if (p->zc2_ix && stage)
-    { Launch L_(p, 4, st); ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, th, stage_sdt, uo, vo, wo, phio, st); }
-  else if (p->zc2_ix)
-    { Launch L_(p, 4, st); ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, th, 0.0, uo, vo, wo, phio, st); }
+  if (p->zc2_ix && stage && bh)
+    { Launch L_(p, 4, st); ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, bh, stage_sdt, uo, vo, wo, phio, st); }
+  else if (p->zc2_ix && !stage)
+    { Launch L_(p, 4, st); ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st); }
   else if (stage)
     { Launch L_(p, 4, st); k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
         g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th,
@@ -856,10 +858,19 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
   const T *su = au, *sv = av, *sw = aw, *sphi = aphi;
   if (p->buoyancy && p->projection) {
     const double alphas[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
+    // the three stages share the buoyancy of the anchor theta'
+    const T* bh = nullptr;
+    if (p->Bh && (p->zc2_fxs || p->zc2_ix)) {
+      const long ncol = (long)p->g.nx * p->g.ny;
+      { Launch L_(p, 7, st); k_bhalf<T><<<(unsigned)std::min<long>((ncol + 7) / 8, 65535), 256, 0, st>>>(
+          p->g, ath, p->theta0, (T*)p->Bh); }
+      OB_LAUNCHED();
+      bh = (const T*)p->Bh;
+    }
     for (int s = 0; s < 3; ++s) {
       const double sdt = alphas[s] * dt;
       RC(project_impl<T>(p, au, av, aw, ath, sdt, (T*)p->Su, (T*)p->Sv, (T*)p->Sw,
-                         (T*)p->Sphi, OB_DIAG_COMPAT0 + s, OB_DIAG_DISC0 + s, st));
+                         (T*)p->Sphi, OB_DIAG_COMPAT0 + s, OB_DIAG_DISC0 + s, st, bh));
     }
     su = (const T*)p->Su;
     sv = (const T*)p->Sv;
@@ -1423,8 +1434,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       (rc = dalloc(p, &p->Sw, nw * e)) || (rc = dalloc(p, &p->Sphi, n * e)) ||
       (rc = dalloc(p, &p->Du, n * e)) || (rc = dalloc(p, &p->Dv, n * e)))
     return bail(rc);
+  if (p->buoyancy && p->projection && (rc = dalloc(p, &p->Bh, nw * e))) return bail(rc);
   if ((rc = dalloc(p, &p->diag, 64 * sizeof(double)))) return bail(rc);
-  OB_CUDA(cudaMemset(p->diag, 0, 64 * sizeof(double)));
+  // ordered after the allocation on the set-up stream
+  OB_CUDA(cudaMemsetAsync(p->diag, 0, 64 * sizeof(double), p->astream));
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

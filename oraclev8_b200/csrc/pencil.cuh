@@ -46,20 +46,21 @@ __host__ __device__ inline Fx2Layout fx2_layout(int nx) {
   L.raw_v = L.raw_u + al((size_t)nx * ZC * sizeof(TS));
   L.raw_w = L.raw_v + al((size_t)nx * ZC * sizeof(TS));
   L.raw_t = L.raw_w + al((size_t)nx * (ZC + 1) * sizeof(TS));
-  const size_t raw_end = L.raw_t + (STAGE ? al((size_t)nx * (ZC + 2) * sizeof(TS)) : 0);
+  const size_t raw_end = L.raw_t + (STAGE ? al((size_t)nx * (ZC + 1) * sizeof(TS)) : 0);
   L.total = (L.bufB + buf > raw_end) ? L.bufB + buf : raw_end;
   return L;
 }
 
 // x-pencil forward kernel: rho-weighting, vertical flux divergence (STAGE:
-// of w + sdt b_half), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd),
-// X1 = FFTx(rho v).  grid = (ceil(nz/ZC), ny).
+// of w + sdt b_half, with b_half = g theta'/theta0 on half levels given as the
+// field bh), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd), X1 = FFTx(rho v).
+// grid = (ceil(nz/ZC), ny).
 template <class T, bool STAGE, class TS, int ZC>
 __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
     GridK g, FftPlan px, const TS* __restrict__ u, const TS* __restrict__ v,
-    const TS* __restrict__ w, const TS* __restrict__ th, double sdt,
+    const TS* __restrict__ w, const TS* __restrict__ bh, double sdt,
     const double* __restrict__ rho, const double* __restrict__ rhoh,
-    const double* __restrict__ theta0, const double* __restrict__ kxd,
+    const double* __restrict__ kxd,
     const cplx<T>* __restrict__ twx, cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   const Fx2Layout L = fx2_layout<T, TS, ZC, STAGE>(g.nx);
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   TS* U = reinterpret_cast<TS*>(smem_dyn + L.raw_u);
   TS* V = reinterpret_cast<TS*>(smem_dyn + L.raw_v);
   TS* W = reinterpret_cast<TS*>(smem_dyn + L.raw_w);
-  TS* TH = reinterpret_cast<TS*>(smem_dyn + L.raw_t);
+  TS* BH = reinterpret_cast<TS*>(smem_dyn + L.raw_t);
   const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
   constexpr int B = 3 * ZC;
   const int y = blockIdx.y;
@@ -88,17 +89,11 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   }
   for (int e = threadIdx.x; e < nx * (ZC + 1); e += kPencilThreads) {
     const int x = e / (ZC + 1), j = e - x * (ZC + 1);
-    const int z = z0 + j;  // w levels z0 .. z0+ZC
+    const int z = z0 + j;  // half levels z0 .. z0+ZC
     const bool ok = z <= nz;
-    copy_or_zero(&W[e], w + ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
-  }
-  if (STAGE) {
-    for (int e = threadIdx.x; e < nx * (ZC + 2); e += kPencilThreads) {
-      const int x = e / (ZC + 2), j = e - x * (ZC + 2);
-      const int z = z0 - 1 + j;  // theta' levels z0-1 .. z0+ZC
-      const bool ok = z >= 0 && z < nz;
-      copy_or_zero(&TH[e], th + ((size_t)x * ny + y) * nz + (ok ? z : 0), ok);
-    }
+    const size_t gi = ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0);
+    copy_or_zero(&W[e], w + gi, ok);
+    if (STAGE) copy_or_zero(&BH[e], bh + gi, ok);
   }
   cp_commit();
   for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
@@ -106,7 +101,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   __syncthreads();
 
   // 2. pack rows (2n, 2n+1) into complex inputs z[n] = f[2n] + i f[2n+1]
-  const double dz = g.dz;
+  const double idz = 1.0 / g.dz;
   for (int n = threadIdx.x; n < M; n += kPencilThreads) {
 #pragma unroll
     for (int j = 0; j < ZC; ++j) {
@@ -120,17 +115,13 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
         const int x = 2 * n + h;
         fu[h] = (T)(r * (double)U[x * ZC + j]);
         fv[h] = (T)(r * (double)V[x * ZC + j]);
-        double wl, wu;
-        if (STAGE) {
-          const TS* wc = W + x * (ZC + 1) - z0;      // wc[k] = w at level k
-          const TS* tc = TH + x * (ZC + 2) - (z0 - 1);  // tc[k] = theta' at level k
-          wl = ok ? stage_w(wc, tc, z, nz, sdt, theta0) : 0.0;
-          wu = ok ? stage_w(wc, tc, z + 1, nz, sdt, theta0) : 0.0;
-        } else {
-          wl = (double)W[x * (ZC + 1) + j];
-          wu = (double)W[x * (ZC + 1) + j + 1];
+        double wl = (double)W[x * (ZC + 1) + j];
+        double wu = (double)W[x * (ZC + 1) + j + 1];
+        if (STAGE) {  // provisional stage w (integrator.py:483-490)
+          wl = arn(wl, mrn(sdt, (double)BH[x * (ZC + 1) + j]));
+          wu = arn(wu, mrn(sdt, (double)BH[x * (ZC + 1) + j + 1]));
         }
-        fd[h] = ok ? (T)((ru * wu - rl * wl) / dz) : (T)0;
+        fd[h] = ok ? (T)((ru * wu - rl * wl) * idz) : (T)0;
       }
       bufA[(size_t)n * B + j] = mk<T>(fu[0], fu[1]);
       bufA[(size_t)n * B + ZC + j] = mk<T>(fv[0], fv[1]);
@@ -183,15 +174,15 @@ __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
 //   IX_CORRECT: u -= gx, v -= gy, w[k] -= (phi_k - phi_{k-1}) / dz (k >= 1),
 //               phi stored (tendency.py:781-788); out may alias in.
 //   IX_STAGE:   out = (u_n - gx, v_n - gy, w_n + sdt b_half - gz, phi)
-//               (integrator.py:483-500).
+//               (integrator.py:483-500), b_half given as the field bh.
 //   IX_REFINE:  as IX_CORRECT but phi_out += phi (a correction potential).
 // grid = (ceil(nz/ZC), ny).
 template <class T, int MODE, class TS, int ZC>
 __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     GridK g, FftPlan px, const cplx<T>* __restrict__ phs, const cplx<T>* __restrict__ psi,
     const double* __restrict__ kxd, const cplx<T>* __restrict__ twx, const TS* u_in,
-    const TS* v_in, const TS* w_in, const TS* __restrict__ th, double sdt,
-    const double* __restrict__ theta0, TS* u_out, TS* v_out, TS* w_out, TS* phi_out) {
+    const TS* v_in, const TS* w_in, const TS* __restrict__ bh, double sdt,
+    TS* u_out, TS* v_out, TS* w_out, TS* phi_out) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   const Ix2Layout L = ix2_layout<T, ZC>(g.nx);
   cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
@@ -236,9 +227,9 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       pu[q] = u_in[col * nz + z];
       pv[q] = v_in[col * nz + z];
       if (MODE == IX_STAGE) {
-        const TS* tc = th + col * nz;
-        pw[q] = (TS)stage_w(wc, tc, z, nz, sdt, theta0);
-        if (z == nz - 1) pt[q] = (TS)stage_w(wc, tc, nz, nz, sdt, theta0);
+        const TS* bc = bh + col * (nz + 1);
+        pw[q] = (TS)arn((double)wc[z], mrn(sdt, (double)bc[z]));
+        if (z == nz - 1) pt[q] = (TS)arn((double)wc[nz], mrn(sdt, (double)bc[nz]));
       } else {
         pw[q] = wc[z];
         if (z == nz - 1) pt[q] = wc[nz];
@@ -282,7 +273,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
   const T* rz = reinterpret_cast<const T*>(Zr);
 
   // 4. velocity correction; consecutive threads on consecutive levels
-  const double dz = g.dz;
+  const T idz = (T)(1.0 / g.dz);
 #pragma unroll 1
   for (int e = threadIdx.x, q = 0; e < nx * ZC; e += kPencilThreads, ++q) {
     const int x = e / ZC, j = e - x * ZC;
@@ -291,13 +282,13 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       const size_t col = (size_t)x * ny + y;
       const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
       const TS* wc = w_in + col * (nz + 1);
-      const TS* tc = (MODE == IX_STAGE) ? th + col * nz : nullptr;
+      const TS* bc = (MODE == IX_STAGE) ? bh + col * (nz + 1) : nullptr;
       const size_t idx = col * nz + z;
       const T phi = rz[rb + 2 * (j + 1)];
       const T phib = rz[rb + 2 * j];
       const T gx = rz[rb + 2 * (ZC + 1 + j)];
       const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
-      const T gz = (z >= 1) ? (T)((phi - phib) / (T)dz) : (T)0;
+      const T gz = (z >= 1) ? (T)((phi - phib) * idz) : (T)0;
       TS uc, vc, wcz, wt = (TS)0;
       if (q < kIxPrefetch) {
         // select the prefetched registers without dynamic array indexing
@@ -309,8 +300,8 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
         uc = u_in[idx];
         vc = v_in[idx];
         if (MODE == IX_STAGE) {
-          wcz = (TS)stage_w(wc, tc, z, nz, sdt, theta0);
-          if (z == nz - 1) wt = (TS)stage_w(wc, tc, nz, nz, sdt, theta0);
+          wcz = (TS)arn((double)wc[z], mrn(sdt, (double)bc[z]));
+          if (z == nz - 1) wt = (TS)arn((double)wc[nz], mrn(sdt, (double)bc[nz]));
         } else {
           wcz = wc[z];
           if (z == nz - 1) wt = wc[nz];
@@ -326,6 +317,22 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
         phi_out[idx] = (TS)phi;
     }
   }
+}
+
+// Half-level buoyancy field b_half (nz + 1 levels, zero at surface and lid)
+// of theta' (equation_set.py:255-263, staggering.py:201-208), with the
+// operation order of bhalf(): the fast stages of a step all use the buoyancy
+// of the same theta', so it is formed once per step.  One warp per column.
+template <class T>
+__global__ void __launch_bounds__(256) k_bhalf(GridK g, const T* __restrict__ th,
+                                               const double* __restrict__ theta0,
+                                               T* __restrict__ bh) {
+  const int lane = threadIdx.x & 31;
+  const long ncol = (long)g.nx * g.ny;
+  const int nz = g.nz;
+  for (long c = (long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < ncol;
+       c += (long)gridDim.x * (blockDim.x / 32))
+    for (int k = lane; k <= nz; k += 32) bh[c * (nz + 1) + k] = (T)bhalf(th + c * nz, k, nz, theta0);
 }
 
 }  // namespace ob
