@@ -463,22 +463,26 @@ dim3 grid_x(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, 
 dim3 grid_y(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.nxh); }
 
 // ---- x2 pencil kernels (pencil.cuh) ----------------------------------------
-// shared memory per CTA for the pencil_min_blocks<T>() CTAs per SM
+// Shared memory per CTA the z-chunk choice aims at: three CTAs per SM for the
+// FP32 forward kernel, two otherwise (the inverse kernel's z-chunk of four
+// FP32 levels, with its state tiles, measured faster at two CTAs per SM than
+// a chunk of two at three).
 template <class T>
-size_t x2_smem_budget() {
+size_t x2_smem_budget(int kind) {
   if (const char* e = getenv("ORACLE_B200_X2_SMEM_KB")) return (size_t)atoi(e) * 1024;
-  return sizeof(T) == 8 ? 112 * 1024 : 74 * 1024;
+  return (sizeof(T) == 4 && kind < 2) ? 74 * 1024 : 112 * 1024;
 }
 
-// Dynamic shared memory of a k_fx2 (kind 0), staged k_fx2 (kind 1) or k_ix2
-// (kind 2) launch with z-chunk zc.
+// Dynamic shared memory of a k_fx2 (kind 0), staged k_fx2 (kind 1) or staged
+// k_ix2 (kind 2, the larger of its layouts) launch with z-chunk zc.
 template <class T, class TS>
 size_t x2_smem(int kind, int zc, int nx) {
   switch (zc) {
 #define OB_X2_CASE(Z)                                                                  \
   case Z:                                                                              \
     return kind == 0 ? fx2_layout<T, TS, Z, false>(nx).total                           \
-                     : kind == 1 ? fx2_layout<T, TS, Z, true>(nx).total : ix2_layout<T, Z>(nx).total;
+                     : kind == 1 ? fx2_layout<T, TS, Z, true>(nx).total                \
+                                 : ix2_layout<T, TS, Z, true>(nx).total;
     OB_X2_CASE(1)
     OB_X2_CASE(2)
     OB_X2_CASE(4)
@@ -495,7 +499,7 @@ template <class T, class TS>
 int pick_x2_zc(int kind, int nx, int nz) {
   if (const char* e = getenv("ORACLE_B200_X2"))
     if (atoi(e) == 0) return 0;
-  for (size_t cap : {x2_smem_budget<T>(), kSmemMax})
+  for (size_t cap : {x2_smem_budget<T>(kind), kSmemMax})
     for (int zc : {8, 4, 2, 1}) {
       if (zc > 1 && zc > nz) continue;
       if (x2_smem<T, TS>(kind, zc, nx) <= cap) return zc;
@@ -529,7 +533,8 @@ void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, con
                 const TS* v, const TS* w, const TS* bh, double sdt, TS* uo, TS* vo, TS* wo,
                 TS* phio, cudaStream_t st) {
   const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
-  k_ix2<T, MODE, TS, ZC><<<grid, kPencilThreads, ix2_layout<T, ZC>(p->g.nx).total, st>>>(
+  k_ix2<T, MODE, TS, ZC><<<grid, kPencilThreads,
+                           ix2_layout<T, TS, ZC, MODE == IX_STAGE>(p->g.nx).total, st>>>(
       p->g, p->px8, phs, psi, p->kx, (const cplx<T>*)p->twx, u, v, w, bh, sdt, uo, vo, wo,
       phio);
 }

@@ -151,11 +151,13 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   }
 }
 
-// Shared-memory layout of k_ix2.
+// Shared-memory layout of k_ix2: twiddles, the two FFT buffers, and the
+// state tiles the correction reads (u, v on ZC levels; w and, for STAGE, the
+// half-level buoyancy on ZC + 1 levels), fetched with the spectra.
 struct Ix2Layout {
-  size_t tw, bufX, bufZ, total;
+  size_t tw, bufX, bufZ, su, sv, sw, sb, total;
 };
-template <class T, int ZC>
+template <class T, class TS, int ZC, bool STAGE>
 __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   const int M = nx / 2;
@@ -164,7 +166,11 @@ __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
   L.tw = 0;
   L.bufX = al((size_t)nx * sizeof(cplx<T>));
   L.bufZ = L.bufX + al((size_t)(M + 1) * B * sizeof(cplx<T>));
-  L.total = L.bufZ + al((size_t)M * B * sizeof(cplx<T>));
+  L.su = L.bufZ + al((size_t)M * B * sizeof(cplx<T>));
+  L.sv = L.su + al((size_t)nx * ZC * sizeof(TS));
+  L.sw = L.sv + al((size_t)nx * ZC * sizeof(TS));
+  L.sb = L.sw + al((size_t)nx * (ZC + 1) * sizeof(TS));
+  L.total = L.sb + (STAGE ? al((size_t)nx * (ZC + 1) * sizeof(TS)) : 0);
   return L;
 }
 
@@ -183,19 +189,24 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     const double* __restrict__ kxd, const cplx<T>* __restrict__ twx, const TS* u_in,
     const TS* v_in, const TS* w_in, const TS* __restrict__ bh, double sdt,
     TS* u_out, TS* v_out, TS* w_out, TS* phi_out) {
+  constexpr bool STAGE = (MODE == IX_STAGE);
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  const Ix2Layout L = ix2_layout<T, ZC>(g.nx);
+  const Ix2Layout L = ix2_layout<T, TS, ZC, STAGE>(g.nx);
   cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
   cplx<T>* bufX = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufX);
   cplx<T>* bufZ = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufZ);
+  TS* SU = reinterpret_cast<TS*>(smem_dyn + L.su);
+  TS* SV = reinterpret_cast<TS*>(smem_dyn + L.sv);
+  TS* SW = reinterpret_cast<TS*>(smem_dyn + L.sw);
+  TS* SB = reinterpret_cast<TS*>(smem_dyn + L.sb);
   const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
   constexpr int B = 3 * ZC + 1;
   const int y = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
 
-  // 1. phi~ (with the halo level) and psi~ rows, all in flight at once;
-  //    consecutive threads on consecutive levels of a row
-  constexpr int BI = 2 * ZC + 1;  // loaded columns per row
+  // 1. phi~ (with the halo level) and psi~ rows, and the state tiles, all in
+  //    flight at once; consecutive threads on consecutive levels of a row
+  constexpr int BI = 2 * ZC + 1;  // loaded spectral columns per row
   for (int e = threadIdx.x; e < (M + 1) * BI; e += kPencilThreads) {
     const int k = e / BI, b = e - k * BI;
     const size_t ob = ((size_t)k * ny + y) * nz;
@@ -210,32 +221,24 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       copy_or_zero(&bufX[(size_t)k * B + 2 * ZC + 1 + j], psi + ob + (ok ? z : 0), ok);
     }
   }
-  cp_commit();
-  for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
-  // state this thread corrects in its first kIxPrefetch output iterations:
-  // loaded now, so the latency overlaps the transforms below
-  TS pu[kIxPrefetch], pv[kIxPrefetch], pw[kIxPrefetch], pt[kIxPrefetch];
-#pragma unroll
-  for (int q = 0; q < kIxPrefetch; ++q) {
-    const int e = threadIdx.x + q * kPencilThreads;
+  for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
-    pu[q] = pv[q] = pw[q] = pt[q] = (TS)0;
-    if (e < nx * ZC && z < nz) {
-      const size_t col = (size_t)x * ny + y;
-      const TS* wc = w_in + col * (nz + 1);
-      pu[q] = u_in[col * nz + z];
-      pv[q] = v_in[col * nz + z];
-      if (MODE == IX_STAGE) {
-        const TS* bc = bh + col * (nz + 1);
-        pw[q] = (TS)arn((double)wc[z], mrn(sdt, (double)bc[z]));
-        if (z == nz - 1) pt[q] = (TS)arn((double)wc[nz], mrn(sdt, (double)bc[nz]));
-      } else {
-        pw[q] = wc[z];
-        if (z == nz - 1) pt[q] = wc[nz];
-      }
-    }
+    const bool ok = z < nz;
+    const size_t gi = ((size_t)x * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&SU[e], u_in + gi, ok);
+    copy_or_zero(&SV[e], v_in + gi, ok);
   }
+  for (int e = threadIdx.x; e < nx * (ZC + 1); e += kPencilThreads) {
+    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+    const int z = z0 + j;  // half levels z0 .. z0+ZC
+    const bool ok = z <= nz;
+    const size_t gi = ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0);
+    copy_or_zero(&SW[e], w_in + gi, ok);
+    if (STAGE) copy_or_zero(&SB[e], bh + gi, ok);
+  }
+  cp_commit();
+  for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
   cp_wait<0>();
   __syncthreads();
 
@@ -274,48 +277,33 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
 
   // 4. velocity correction; consecutive threads on consecutive levels
   const T idz = (T)(1.0 / g.dz);
-#pragma unroll 1
-  for (int e = threadIdx.x, q = 0; e < nx * ZC; e += kPencilThreads, ++q) {
+  for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
-    if (z < nz) {
-      const size_t col = (size_t)x * ny + y;
-      const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
-      const TS* wc = w_in + col * (nz + 1);
-      const TS* bc = (MODE == IX_STAGE) ? bh + col * (nz + 1) : nullptr;
-      const size_t idx = col * nz + z;
-      const T phi = rz[rb + 2 * (j + 1)];
-      const T phib = rz[rb + 2 * j];
-      const T gx = rz[rb + 2 * (ZC + 1 + j)];
-      const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
-      const T gz = (z >= 1) ? (T)((phi - phib) * idz) : (T)0;
-      TS uc, vc, wcz, wt = (TS)0;
-      if (q < kIxPrefetch) {
-        // select the prefetched registers without dynamic array indexing
-        uc = pu[0]; vc = pv[0]; wcz = pw[0]; wt = pt[0];
-#pragma unroll
-        for (int r = 1; r < kIxPrefetch; ++r)
-          if (q == r) { uc = pu[r]; vc = pv[r]; wcz = pw[r]; wt = pt[r]; }
-      } else {
-        uc = u_in[idx];
-        vc = v_in[idx];
-        if (MODE == IX_STAGE) {
-          wcz = (TS)arn((double)wc[z], mrn(sdt, (double)bc[z]));
-          if (z == nz - 1) wt = (TS)arn((double)wc[nz], mrn(sdt, (double)bc[nz]));
-        } else {
-          wcz = wc[z];
-          if (z == nz - 1) wt = wc[nz];
-        }
-      }
-      u_out[idx] = (TS)((T)uc - gx);
-      v_out[idx] = (TS)((T)vc - gy);
-      w_out[col * (nz + 1) + z] = (TS)((T)wcz - gz);
-      if (z == nz - 1 && (MODE == IX_STAGE || w_out != w_in)) w_out[col * (nz + 1) + nz] = wt;
-      if (MODE == IX_REFINE)
-        phi_out[idx] = (TS)((T)phi_out[idx] + phi);
-      else
-        phi_out[idx] = (TS)phi;
+    if (z >= nz) continue;
+    const size_t col = (size_t)x * ny + y;
+    const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
+    const size_t idx = col * nz + z;
+    const T phi = rz[rb + 2 * (j + 1)];
+    const T phib = rz[rb + 2 * j];
+    const T gx = rz[rb + 2 * (ZC + 1 + j)];
+    const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
+    const T gz = (z >= 1) ? (T)((phi - phib) * idz) : (T)0;
+    const int sw = x * (ZC + 1) + j;
+    TS wcz = SW[sw], wt = (TS)0;
+    if (STAGE) wcz = (TS)arn((double)wcz, mrn(sdt, (double)SB[sw]));
+    if (z == nz - 1) {
+      wt = SW[sw + 1];
+      if (STAGE) wt = (TS)arn((double)wt, mrn(sdt, (double)SB[sw + 1]));
     }
+    u_out[idx] = (TS)((T)SU[e] - gx);
+    v_out[idx] = (TS)((T)SV[e] - gy);
+    w_out[col * (nz + 1) + z] = (TS)((T)wcz - gz);
+    if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[col * (nz + 1) + nz] = wt;
+    if (MODE == IX_REFINE)
+      phi_out[idx] = (TS)((T)phi_out[idx] + phi);
+    else
+      phi_out[idx] = (TS)phi;
   }
 }
 
