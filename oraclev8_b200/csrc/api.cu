@@ -145,8 +145,8 @@ struct OraclePlan {
   int grid_fxp = 1, grid_fyp = 1, grid_iyp = 1, grid_ixp = 1;
   int use_pipe = 0;  // projection through the persistent pipelined kernels
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
-  FftPlan px8{};
-  int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0;
+  FftPlan px8{}, py8{};
+  int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -330,6 +330,9 @@ int x2_attr(K kernel) {
 template <class T, class TS, int ZC>
 int x2_attrs_zc() {
   int rc;
+  if constexpr (sizeof(TS) == sizeof(T)) {
+    if ((rc = x2_attr(k_fy2<T, FY_DIV, T, ZC>)) || (rc = x2_attr(k_iy2<T, ZC>))) return rc;
+  }
   if ((rc = x2_attr(k_fx2<T, false, TS, ZC>)) || (rc = x2_attr(k_fx2<T, true, TS, ZC>)) ||
       (rc = x2_attr(k_ix2<T, IX_CORRECT, TS, ZC>)) || (rc = x2_attr(k_ix2<T, IX_STAGE, TS, ZC>)))
     return rc;
@@ -347,6 +350,9 @@ int set_x2_attrs() {
   if constexpr (sizeof(T) == 8) {  // residual transforms of the FP32 defect correction
     for (auto k : {k_fx2<double, false, float, 1>, k_fx2<double, false, float, 2>,
                    k_fx2<double, false, float, 4>, k_fx2<double, false, float, 8>})
+      if ((rc = x2_attr(k))) return rc;
+    for (auto k : {k_fy2<double, FY_RESID, float, 1>, k_fy2<double, FY_RESID, float, 2>,
+                   k_fy2<double, FY_RESID, float, 4>, k_fy2<double, FY_RESID, float, 8>})
       if ((rc = x2_attr(k))) return rc;
   }
   return OB_OK;
@@ -508,6 +514,67 @@ int pick_x2_zc(int kind, int nx, int nz) {
 }
 
 // bh: the step's half-level buoyancy field (STAGE only)
+template <class T>
+size_t y2_smem_zc(int zc, int ny) {
+  switch (zc) {
+    case 1: return y2_smem<T, 1>(ny);
+    case 2: return y2_smem<T, 2>(ny);
+    case 4: return y2_smem<T, 4>(ny);
+    case 8: return y2_smem<T, 8>(ny);
+  }
+  return ~size_t(0);
+}
+
+template <class T>
+int pick_y2_zc(int ny, int nz) {
+  if (const char* e = getenv("ORACLE_B200_X2"))
+    if (atoi(e) == 0) return 0;
+  for (size_t cap : {x2_smem_budget<T>(0), kSmemMax})
+    for (int zc : {8, 4, 2, 1}) {
+      if (zc > 1 && zc > nz) continue;
+      if (y2_smem_zc<T>(zc, ny) <= cap) return zc;
+    }
+  return 0;
+}
+
+template <class T, int MODE, class TO>
+void fy2(const OraclePlan* q, int zc, const cplx<T>* in0, const cplx<T>* in1, cplx<TO>* out,
+         cudaStream_t st) {
+  const GridK& g = q->g;
+  const cplx<T>* tw = (const cplx<T>*)q->twy;
+  switch (zc) {
+#define OB_FY2(Z)                                                                             \
+  case Z:                                                                                     \
+    k_fy2<T, MODE, TO, Z><<<dim3((g.nz + Z - 1) / Z, g.nxh), kPencilThreads, y2_smem<T, Z>(g.ny), \
+                           st>>>(g, q->py8, in0, in1, q->ky, tw, out);                        \
+    break;
+    OB_FY2(1)
+    OB_FY2(2)
+    OB_FY2(4)
+    OB_FY2(8)
+#undef OB_FY2
+  }
+}
+
+template <class T>
+void iy2(const OraclePlan* p, int zc, const cplx<T>* in0, cplx<T>* out0, cplx<T>* out1,
+         cudaStream_t st) {
+  const GridK& g = p->g;
+  const cplx<T>* tw = (const cplx<T>*)p->twy;
+  switch (zc) {
+#define OB_IY2(Z)                                                                             \
+  case Z:                                                                                     \
+    k_iy2<T, Z><<<dim3((g.nz + Z - 1) / Z, g.nxh), kPencilThreads, y2_smem<T, Z>(g.ny), st>>>( \
+        g, p->py8, in0, p->ky, tw, out0, out1);                                               \
+    break;
+    OB_IY2(1)
+    OB_IY2(2)
+    OB_IY2(4)
+    OB_IY2(8)
+#undef OB_IY2
+  }
+}
+
 template <class T, bool STAGE, class TS, int ZC>
 void fx2_launch(const OraclePlan* q, const TS* u, const TS* v, const TS* w, const TS* bh,
                 double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
@@ -634,16 +701,22 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
         g, p->pxf, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
         (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
-  { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-      g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
+  if (p->zc2_fy)
+    { Launch L_(p, 1, st); fy2<T, FY_DIV, T>(p, p->zc2_fy, S1, S2, S3, st); }
+  else
+    { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+        g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   const long ncols = (long)g.nxh * g.ny;
   { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
                              smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
                                                    slot_d); }
   OB_LAUNCHED();
-  { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
+  if (p->zc2_iy)
+    { Launch L_(p, 3, st); iy2<T>(p, p->zc2_iy, S3, S1, S2, st); }
+  else
+    { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+        g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
   if (p->zc2_ix && stage && bh)
@@ -688,15 +761,21 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
         g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
         (const Cd*)q->twx, R1, R2, nullptr); }
   OB_LAUNCHED();
-  { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
-      g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
+  if (q->zc2_fy)
+    { Launch L_(p, OB_PROF_REFINE, st); fy2<double, FY_RESID, float>(q, q->zc2_fy, R1, R2, S3, st); }
+  else
+    { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
+        g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   const long ncols = (long)g.nxh * g.ny;
   { Launch L_(p, OB_PROF_REFINE, st); k_thomas<float, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
                              smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, nullptr, 0, 0); }
   OB_LAUNCHED();
-  { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-      g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
+  if (p->zc2_iy)
+    { Launch L_(p, OB_PROF_REFINE, st); iy2<float>(p, p->zc2_iy, S3, S1, S2, st); }
+  else
+    { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+        g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   if (p->zc2_ix)
     { Launch L_(p, OB_PROF_REFINE, st); ix2<float, IX_REFINE, float>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
@@ -722,6 +801,7 @@ int make_refiner(OraclePlan* p) {
   q->pxf = p->pxf;
   q->pyf = p->pyf;
   q->px8 = p->px8;
+  q->py8 = p->py8;
   q->kx = p->kx;
   q->ky = p->ky;
   q->rho = p->rho;
@@ -732,6 +812,7 @@ int make_refiner(OraclePlan* p) {
   q->zc_fx = pick_zc(nz, 2ull * (q->g.M + 1) * 3 * ce, tw_bytes(q, nx));
   q->zc_fy = pick_zc(nz, 2ull * ny * 2 * ce, tw_bytes(q, ny));
   q->zc2_fx = pick_x2_zc<double, float>(0, nx, nz);
+  q->zc2_fy = p->zc2_fy ? pick_y2_zc<double>(ny, nz) : 0;
   if (smem_fx(q, 3) > kSmemMax || smem_fy(q, 2, q->zc_fy) > kSmemMax)
     return fail(OB_ERR_ARG, "grid too large for the FP64 residual kernels");
   auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
@@ -1416,6 +1497,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     return bail(fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx,
                      ny, nz));
   // compile-time-chunk x-pencil kernels where their tiles fit
+  if (factorize8(ny, p->py8)) {
+    p->zc2_fy = p->prec == OB_PREC_F64 ? pick_y2_zc<double>(ny, nz) : pick_y2_zc<float>(ny, nz);
+    p->zc2_iy = p->zc2_fy;
+  }
   if (factorize8(nx / 2, p->px8)) {
     if (p->prec == OB_PREC_F64) {
       p->zc2_fx = pick_x2_zc<double, double>(0, nx, nz);

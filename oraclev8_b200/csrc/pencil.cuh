@@ -307,6 +307,96 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
   }
 }
 
+// ---- y pencils ---------------------------------------------------------------
+// Same arithmetic as k_fy (FY_DIV / FY_RESID) and k_iy (IY_GRAD), with the
+// data movement of the x2 kernels: cp.async tiles, compile-time z-chunk,
+// level-fastest thread mapping.  grid = (ceil(nz/ZC), nx/2 + 1).
+template <class T, int ZC>
+__host__ __device__ inline size_t y2_smem(int ny) {
+  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  return al((size_t)ny * sizeof(cplx<T>)) + 2 * al((size_t)ny * 2 * ZC * sizeof(cplx<T>));
+}
+
+// d^ = FFTy(X1) + i ky' FFTy(X2) (FY_DIV); FY_RESID also zeroes the Nyquist
+// rows (kx = nx/2 or ky = ny/2) and may round the result to TO.
+template <class T, int MODE, class TO, int ZC>
+__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fy2(
+    GridK g, FftPlan py, const cplx<T>* __restrict__ in0, const cplx<T>* __restrict__ in1,
+    const double* __restrict__ kyd, const cplx<T>* __restrict__ twy,
+    cplx<nd_t<TO>>* __restrict__ out0) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  constexpr int B = 2 * ZC;
+  const int ny = g.ny, nz = g.nz;
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_dyn + (((size_t)ny * sizeof(cplx<T>) + 15) & ~size_t(15)));
+  cplx<T>* bufB = bufA + (size_t)ny * B;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  for (int e = threadIdx.x; e < ny * B; e += kPencilThreads) {
+    const int y = e / B, b = e - y * B;
+    const int f = b / ZC, j = b - f * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    const size_t o = ((size_t)kx * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&bufA[e], (f == 0 ? in0 : in1) + o, ok);
+  }
+  cp_commit();
+  for (int i = threadIdx.x; i < ny; i += kPencilThreads) stw[i] = twy[i];
+  cp_wait<0>();
+  __syncthreads();
+  cplx<T>* R = fft_smem<T, false, 8>(bufA, bufB, B, py, stw, 1);
+  for (int e = threadIdx.x; e < ny * ZC; e += kPencilThreads) {
+    const int ky = e / ZC, j = e - ky * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
+    cplx<T> d = add(R[(size_t)ky * B + j], ik(kk, R[(size_t)ky * B + ZC + j]));
+    if (MODE == FY_RESID && (ky == ny / 2 || kx == g.nx / 2)) d = mk<T>((T)0, (T)0);
+    out0[((size_t)kx * ny + ky) * nz + z] = mk<TO>((TO)d.x, (TO)d.y);
+  }
+}
+
+// phi~ = IFFTy(phi^), psi~ = IFFTy(i ky' phi^) (IY_GRAD with unit scale).
+template <class T, int ZC>
+__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_iy2(
+    GridK g, FftPlan py, const cplx<T>* __restrict__ in0, const double* __restrict__ kyd,
+    const cplx<T>* __restrict__ twy, cplx<T>* __restrict__ out0, cplx<T>* __restrict__ out1) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  constexpr int B = 2 * ZC;
+  const int ny = g.ny, nz = g.nz;
+  cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_dyn + (((size_t)ny * sizeof(cplx<T>) + 15) & ~size_t(15)));
+  cplx<T>* bufB = bufA + (size_t)ny * B;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  for (int e = threadIdx.x; e < ny * ZC; e += kPencilThreads) {
+    const int ky = e / ZC, j = e - ky * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    copy_or_zero(&bufA[(size_t)ky * B + j], in0 + ((size_t)kx * ny + ky) * nz + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  for (int i = threadIdx.x; i < ny; i += kPencilThreads) stw[i] = twy[i];
+  cp_wait<0>();
+  __syncthreads();
+  // the d/dy columns: i ky' phi^ (ky' = 0 at the Nyquist row)
+  for (int e = threadIdx.x; e < ny * ZC; e += kPencilThreads) {
+    const int ky = e / ZC, j = e - ky * ZC;
+    const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
+    bufA[(size_t)ky * B + ZC + j] = ik(kk, bufA[(size_t)ky * B + j]);
+  }
+  __syncthreads();
+  cplx<T>* R = fft_smem<T, true, 8>(bufA, bufB, B, py, stw, 1);
+  for (int e = threadIdx.x; e < ny * ZC; e += kPencilThreads) {
+    const int y = e / ZC, j = e - y * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const size_t o = ((size_t)kx * ny + y) * nz + z;
+    out0[o] = R[(size_t)y * B + j];
+    out1[o] = R[(size_t)y * B + ZC + j];
+  }
+}
+
 // Half-level buoyancy field b_half (nz + 1 levels, zero at surface and lid)
 // of theta' (equation_set.py:255-263, staggering.py:201-208), with the
 // operation order of bhalf(): the fast stages of a step all use the buoyancy
