@@ -309,12 +309,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# ncu capture of this workload (profiles/ncu_projection_kernels_config1_fp64.md):
-# k_ix 1.163 GB in correction mode and 1.323 GB in stage mode, weighted 2:3 as
-# the five projections of a step use them.
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernel class from one ncu capture of this workload
+# (profiles/ncu_pencil_kernels_config1_fp32r.md): k_ix2 moves 0.556 GB in
+# correction mode and 0.649 GB in stage mode, weighted 2:3 as the five
+# projections of a step use them.
 NCU_TRAFFIC = {
-    ("config1", "fp64"): {"ix": (2 * 1.163e9 + 3 * 1.323e9) / 5, "fy": 0.384e9, "iy": 0.356e9},
+    ("config1", "fp32r"): {"ix": (2 * 0.5563e9 + 3 * 0.6495e9) / 5},
 }
 
 
@@ -416,7 +417,7 @@ def run_b200(args):
     clocks.start()
     ms, launches, prof = _timed_steps(integ, st, dt, args.steps, args.warmup, barrier)
     companion = None
-    if args.precision != "fp64":
+    if args.precision != "fp64" and not args.no_fp64_companion:
         # the plain FP64 step on the same workload, timed the same way, and the
         # error of this run against it after the same number of steps
         integ64, _ = b200_integrator(w, "fp64")
@@ -626,6 +627,8 @@ def main():
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-fp64-companion", action="store_true",
+                    help="skip the plain-FP64 timing and accuracy report (profiling runs)")
     ap.add_argument("--ensemble-runs", type=int, default=64)
     ap.add_argument("--ensemble-hours", type=float, default=6.0)
     ap.add_argument("--serving-requests", type=int, default=32)

@@ -929,15 +929,17 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
     mu = fmax(mu, fabs((double)u[e]));
     mv = fmax(mv, fabs((double)v[e]));
     mt = fmax(mt, fabs((double)th[e]));
-    const double p = phi[e];
-    sp += p;
-    if (e % g.nz == 0) {
-      pmin = fmin(pmin, p);
-      pmax = fmax(pmax, p);
-    }
+    sp += (double)phi[e];
   }
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nw; e += stride)
     mw = fmax(mw, fabs((double)w[e]));
+  // surface level k = 0 of every column
+  const size_t ncol = (size_t)g.nx * g.ny;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncol; c += stride) {
+    const double p = phi[c * g.nz];
+    pmin = fmin(pmin, p);
+    pmax = fmax(pmax, p);
+  }
   __shared__ double red[8][8];
   double vals[7] = {mu, mv, mw, mt, sp, pmin, pmax};
 #pragma unroll
@@ -974,18 +976,31 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
   }
 }
 
+// One warp combines the per-CTA partials (fixed order: lane-strided, then a
+// butterfly), so the result does not depend on timing.
 __global__ void k_diag_final(const DiagPart* part, int np, double ncell, double* diag) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   double mu = 0, mv = 0, mw = 0, mt = 0, sp = 0, pmin = INFINITY, pmax = -INFINITY;
-  for (int b = 0; b < np; ++b) {
-    mu = fmax(mu, part[b].mu);
-    mv = fmax(mv, part[b].mv);
-    mw = fmax(mw, part[b].mw);
-    mt = fmax(mt, part[b].mt);
-    sp += part[b].sp;
-    pmin = fmin(pmin, part[b].pmin);
-    pmax = fmax(pmax, part[b].pmax);
+  for (int b = threadIdx.x; b < np; b += 32) {
+    const DiagPart q = part[b];
+    mu = fmax(mu, q.mu);
+    mv = fmax(mv, q.mv);
+    mw = fmax(mw, q.mw);
+    mt = fmax(mt, q.mt);
+    sp += q.sp;
+    pmin = fmin(pmin, q.pmin);
+    pmax = fmax(pmax, q.pmax);
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+    mt = fmax(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+    sp += __shfl_xor_sync(0xffffffffu, sp, o);
+    pmin = fmin(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
+    pmax = fmax(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+  }
+  if (threadIdx.x != 0) return;
   const double mean = sp / ncell;
   diag[0] = mu;
   diag[1] = mv;

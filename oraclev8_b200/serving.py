@@ -130,12 +130,13 @@ def build_run(req: RunRequest, device_dtype=None):
 
 def footprint_bytes(req: RunRequest) -> int:
     """HBM a resident run holds: 5 state fields and the plan's scratch (3
-    half-spectrum buffers, 5 anchor and 4 stage fields, 2 temporaries; plus
-    two FP64 spectra for the FP32-refined correction), in the state dtype."""
+    half-spectrum buffers, 5 anchor and 4 stage fields, 2 temporaries and the
+    half-level buoyancy; plus two FP64 spectra for the FP32-refined
+    correction), in the state dtype."""
     S = 8 if req.precision == "fp64" else 4
     n = req.cells
     ns = (req.n // 2 + 1) * req.n * req.nz
-    b = S * (5 * n + 11 * n) + 3 * ns * 2 * S
+    b = S * (5 * n + 12 * n) + 3 * ns * 2 * S
     if req.precision != "fp64":
         b += 2 * ns * 16
     return int(b * 1.05) + (8 << 20)
