@@ -281,7 +281,10 @@ size_t smem_fy(const OraclePlan* p, int nf, int zc) {
 size_t smem_ix(const OraclePlan* p, int B) {
   return tw_bytes(p, p->g.nx) + (size_t)(2 * p->g.M + 1) * B * 2 * p->esz;
 }
-size_t smem_thomas(const OraclePlan* p) { return 3ull * kThomasCols * (p->g.nz + 1) * 8; }
+// staging in the plan's type plus the zero mode's double region (k_thomas)
+size_t smem_thomas(const OraclePlan* p) {
+  return 3ull * kThomasCols * (p->g.nz + 1) * p->esz + 3ull * (p->g.nz + 1) * 8;
+}
 
 constexpr int kPipeThreads = 256;
 

@@ -49,6 +49,7 @@ __device__ __forceinline__ double drn(double a, double b) { return __ddiv_rn(a, 
 __device__ __forceinline__ float mrn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float arn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float srn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float drn(float a, float b) { return __fdiv_rn(a, b); }
 
 // Grid description passed by value to every kernel.
 struct GridK {

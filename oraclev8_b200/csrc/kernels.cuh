@@ -289,16 +289,24 @@ struct ThomasK {
 // Parseval form of the discrete-operator residual (poisson.py:263-268) as a
 // raw sum of weighted |r^|^2 in diag[slot_d] (normalised on the host).
 // dh and ph may alias: a CTA reads only its own columns before writing them.
+// The non-zero modes are staged and swept in the plan's type T (FP64 plans:
+// double, the reference's arithmetic; FP32 plans: single precision, half the
+// shared memory per column and so twice the columns in flight per SM); the
+// zero mode is always solved in double, in its own shared-memory region.
 template <class T, int TC>
 __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>* dh,
                                                cplx<T>* ph, double* diag, int slot_c,
                                                int slot_d) {
+  using R = T;  // staging and sweep type of the non-zero modes
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nz = g.nz;
   const int P = nz + 1;  // padded column stride (bank spread)
-  double* sre = reinterpret_cast<double*>(smem_raw);  // TC * P real parts
-  double* sim = sre + (size_t)TC * P;                   // TC * P imag parts
-  double* scp = sim + (size_t)TC * P;                   // TC * P c' factors
+  double* zre = reinterpret_cast<double*>(smem_raw);  // zero mode: P real parts
+  double* zim = zre + P;                                // P imag parts
+  double* zcp = zim + P;                                // P source copy
+  R* sre = reinterpret_cast<R*>(zcp + P);               // TC * P real parts
+  R* sim = sre + (size_t)TC * P;                        // TC * P imag parts
+  R* scp = sim + (size_t)TC * P;                        // TC * P c' factors
   const long ncols = (long)g.nxh * g.ny;
   const long c0 = (long)blockIdx.x * TC;
   const int ncl = (int)min((long)TC, ncols - c0);
@@ -307,8 +315,8 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
     const int cl = e / nz;
     const int k = e - cl * nz;
     const cplx<T> v = dh[base + e];
-    sre[cl * P + k] = (double)v.x;
-    sim[cl * P + k] = (double)v.y;
+    sre[cl * P + k] = (R)v.x;
+    sim[cl * P + k] = (R)v.y;
   }
   __syncthreads();
   const int cl = threadIdx.x;
@@ -317,10 +325,14 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
     const long col = c0 + cl;
     const int kxi = (int)(col / g.ny);
     const int kyi = (int)(col - (long)kxi * g.ny);
-    double* re = sre + cl * P;
-    double* im = sim + cl * P;
-    double* cp = scp + cl * P;
     if (col == 0) {
+      double* re = zre;
+      double* im = zim;
+      double* cp = zcp;
+      for (int k = 0; k < nz; ++k) {
+        re[k] = (double)sre[k];
+        im[k] = (double)sim[k];
+      }
       // Zero mode (poisson.py:233-236, 256, 316-325, 367-383): compatibility
       // residual, removal of the column mean, then the reduced (nz-1) system
       // on levels 1..nz-1 with phi(0,0,0) pinned to 0.
@@ -367,30 +379,38 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
         }
         resid = r2 - rsum * rsum / nz;
       }
+      for (int k = 0; k < nz; ++k) {
+        sre[k] = (R)re[k];
+        sim[k] = (R)im[k];
+      }
     } else {
+      R* re = sre + cl * P;
+      R* im = sim + cl * P;
+      R* cp = scp + cl * P;
       const double kx = t.kx[kxi], ky = t.ky[kyi];
       const double ksq = arn(mrn(kx, kx), mrn(ky, ky));
-      double b = srn(t.negs[0], mrn(ksq, t.rho[0]));
-      double inv = drn(1.0, b);
-      double cpp = mrn(t.c[0], inv);
+      R b = (R)srn(t.negs[0], mrn(ksq, t.rho[0]));
+      R inv = drn((R)1, b);
+      R cpp = mrn((R)t.c[0], inv);
       cp[0] = cpp;
-      double pr = mrn(re[0], inv), pi = mrn(im[0], inv);
+      R pr = mrn(re[0], inv), pi = mrn(im[0], inv);
       re[0] = pr;
       im[0] = pi;
       for (int k = 1; k < nz; ++k) {
-        b = srn(t.negs[k], mrn(ksq, t.rho[k]));
-        const double den = srn(b, mrn(t.a[k], cpp));
-        inv = drn(1.0, den);
+        b = (R)srn(t.negs[k], mrn(ksq, t.rho[k]));
+        const R ak = (R)t.a[k];
+        const R den = srn(b, mrn(ak, cpp));
+        inv = drn((R)1, den);
         if (k < nz - 1) {
-          cpp = mrn(t.c[k], inv);
+          cpp = mrn((R)t.c[k], inv);
           cp[k] = cpp;
         }
-        pr = mrn(srn(re[k], mrn(t.a[k], pr)), inv);
-        pi = mrn(srn(im[k], mrn(t.a[k], pi)), inv);
+        pr = mrn(srn(re[k], mrn(ak, pr)), inv);
+        pi = mrn(srn(im[k], mrn(ak, pi)), inv);
         re[k] = pr;
         im[k] = pi;
       }
-      double xr = pr, xi = pi;
+      R xr = pr, xi = pi;
       for (int k = nz - 2; k >= 0; --k) {
         xr = srn(re[k], mrn(cp[k], xr));
         xi = srn(im[k], mrn(cp[k], xi));
@@ -423,7 +443,7 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   for (int e = threadIdx.x; e < ncl * nz; e += TC) {
     const int c = e / nz;
     const int k = e - c * nz;
-    ph[base + e] = mk<T>((T)(sre[c * P + k] * t.scale), (T)(sim[c * P + k] * t.scale));
+    ph[base + e] = mk<T>((T)((double)sre[c * P + k] * t.scale), (T)((double)sim[c * P + k] * t.scale));
   }
 }
 
