@@ -48,6 +48,12 @@ int fail(int code, const char* fmt, ...) {
                   __FILE__, __LINE__);                                                   \
   } while (0)
 
+#define RC(x)            \
+  do {                   \
+    int rc_ = (x);       \
+    if (rc_) return rc_; \
+  } while (0)
+
 constexpr int kThomasCols = 32;
 constexpr int kFftThreads = 256;
 constexpr size_t kSmemBudget = 112 * 1024;  // two CTAs per SM
@@ -173,6 +179,14 @@ struct OraclePlan {
   size_t scratch_bytes = 0;
   cudaMemPool_t pool = nullptr;   // device memory pool (plan_pool)
   cudaStream_t astream = nullptr; // private stream ordering set-up work
+  // split FP32 Thomas solve: the column blocks holding a long-wave mode
+  // (k^2 Lz^2 < 1), as a list and as per-block flags, and the side stream
+  // and fork/join events that run their double launch beside the rest
+  int* lw_blocks = nullptr;
+  unsigned char* lw_flag = nullptr;
+  int n_lw = 0;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // launch accounting and optional per-kernel-class event timing
   long launches = 0;
   int profiling = 0;
@@ -254,6 +268,9 @@ void release_plan(OraclePlan* p, cudaStream_t st) {
   }
   for (void* q : p->allocs) cudaFreeAsync(q, st);
   if (p->astream) cudaStreamDestroy(p->astream);
+  if (p->aux) cudaStreamDestroy(p->aux);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   delete p;
 }
 
@@ -281,9 +298,9 @@ size_t smem_fy(const OraclePlan* p, int nf, int zc) {
 size_t smem_ix(const OraclePlan* p, int B) {
   return tw_bytes(p, p->g.nx) + (size_t)(2 * p->g.M + 1) * B * 2 * p->esz;
 }
-// staging in the plan's type plus the zero mode's double region (k_thomas)
-size_t smem_thomas(const OraclePlan* p) {
-  return 3ull * kThomasCols * (p->g.nz + 1) * p->esz + 3ull * (p->g.nz + 1) * 8;
+// staging in the sweep type plus the zero mode's double region (k_thomas)
+size_t smem_thomas(const OraclePlan* p, size_t rsz = 8) {
+  return 3ull * kThomasCols * (p->g.nz + 1) * rsz + 3ull * (p->g.nz + 1) * 8;
 }
 
 constexpr int kPipeThreads = 256;
@@ -621,6 +638,36 @@ void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, co
   }
 }
 
+// The batched Thomas solve of a projection, in place on S3: FP64 plans in one
+// double launch; FP32 plans as a double launch over the blocks holding a
+// long-wave mode and a single-precision launch over the rest (k_thomas).
+template <class T>
+int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, int slot_d,
+                 cudaStream_t st) {
+  const long ncols = (long)p->g.nxh * p->g.ny;
+  const unsigned nb = (unsigned)((ncols + kThomasCols - 1) / kThomasCols);
+  if (sizeof(T) == 8 || !p->lw_blocks) {
+    { Launch L_(p, cls, st); k_thomas<T, kThomasCols><<<nb, kThomasCols, smem_thomas(p), st>>>(
+          p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d); }
+    OB_LAUNCHED();
+  } else {
+    // the two launches touch disjoint columns: the short double launch (a
+    // few blocks, among them the serial zero mode) runs on the plan's side
+    // stream, beside the single-precision one
+    OB_CUDA(cudaEventRecord(p->ev_fork, st));
+    OB_CUDA(cudaStreamWaitEvent(p->aux, p->ev_fork, 0));
+    { Launch L_(p, cls, p->aux); k_thomas<T, kThomasCols, double><<<(unsigned)p->n_lw, kThomasCols, smem_thomas(p, 8), p->aux>>>(
+          p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, p->lw_blocks, nullptr); }
+    OB_LAUNCHED();
+    { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
+          p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, nullptr, p->lw_flag); }
+    OB_LAUNCHED();
+    OB_CUDA(cudaEventRecord(p->ev_join, p->aux));
+    OB_CUDA(cudaStreamWaitEvent(st, p->ev_join, 0));
+  }
+  return OB_OK;
+}
+
 // projection through the persistent pipelined kernels (pipe.cuh)
 template <class T>
 int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
@@ -644,11 +691,7 @@ int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   { Launch L_(p, 1, st); k_fyp<T><<<p->grid_fyp, kPipeThreads, smem_fyp(p, p->zc_fyp), st>>>(
       g, p->pyf, p->zc_fyp, S1, S2, p->ky, (const C*)p->twy, S3); }
   OB_LAUNCHED();
-  const long ncols = (long)g.nxh * g.ny;
-  { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
-                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
-                                                   slot_d); }
-  OB_LAUNCHED();
+  RC(thomas_solve<T>(p, 2, S3, diag, slot_c, slot_d, st));
   { Launch L_(p, 3, st); k_iyp<T><<<p->grid_iyp, kPipeThreads, smem_iyp(p, p->zc_iyp), st>>>(
       g, p->py, p->zc_iyp, S3, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
@@ -710,11 +753,7 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
     { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
         g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
-  const long ncols = (long)g.nxh * g.ny;
-  { Launch L_(p, 2, st); k_thomas<T, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
-                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, diag, slot_c,
-                                                   slot_d); }
-  OB_LAUNCHED();
+  RC(thomas_solve<T>(p, 2, S3, diag, slot_c, slot_d, st));
   if (p->zc2_iy)
     { Launch L_(p, 3, st); iy2<T>(p, p->zc2_iy, S3, S1, S2, st); }
   else
@@ -770,10 +809,7 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
     { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
         g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
-  const long ncols = (long)g.nxh * g.ny;
-  { Launch L_(p, OB_PROF_REFINE, st); k_thomas<float, kThomasCols><<<(unsigned)((ncols + kThomasCols - 1) / kThomasCols), kThomasCols,
-                             smem_thomas(p), st>>>(g, thomas_args(p), S3, S3, nullptr, 0, 0); }
-  OB_LAUNCHED();
+  RC(thomas_solve<float>(p, OB_PROF_REFINE, S3, nullptr, 0, 0, st));
   if (p->zc2_iy)
     { Launch L_(p, OB_PROF_REFINE, st); iy2<float>(p, p->zc2_iy, S3, S1, S2, st); }
   else
@@ -908,11 +944,6 @@ int diag_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th, co
   return OB_OK;
 }
 
-#define RC(x)            \
-  do {                   \
-    int rc_ = (x);       \
-    if (rc_) return rc_; \
-  } while (0)
 
 template <class T>
 int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* out, double dt,
@@ -1367,8 +1398,11 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     return rc;
   };
   if (int rc = plan_pool(&p->pool)) return bail(rc);
-  if (cudaStreamCreateWithFlags(&p->astream, cudaStreamNonBlocking) != cudaSuccess)
-    return bail(fail(OB_ERR_CUDA, "plan_create: stream creation failed"));
+  if (cudaStreamCreateWithFlags(&p->astream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(OB_ERR_CUDA, "plan_create: stream or event creation failed"));
   p->prec = grid->precision;
   p->esz = p->prec == OB_PREC_F64 ? 8 : 4;
   p->g.nx = nx;
@@ -1528,6 +1562,27 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       (rc = dalloc(p, &p->Du, n * e)) || (rc = dalloc(p, &p->Dv, n * e)))
     return bail(rc);
   if (p->buoyancy && p->projection && (rc = dalloc(p, &p->Bh, nw * e))) return bail(rc);
+  if (p->prec == OB_PREC_F32) {
+    const long ncols = (long)p->g.nxh * ny;
+    const long nblk = (ncols + kThomasCols - 1) / kThomasCols;
+    std::vector<unsigned char> flag(nblk, 0);
+    std::vector<int> lw;
+    const double Lz = grid->Lz;
+    for (long c = 0; c < ncols; ++c) {
+      const int ix = (int)(c / ny), iy = (int)(c - (long)ix * ny);
+      if ((kx[ix] * kx[ix] + ky[iy] * ky[iy]) * (Lz * Lz) < 1.0) flag[c / kThomasCols] = 1;
+    }
+    for (long b = 0; b < nblk; ++b)
+      if (flag[b]) lw.push_back((int)b);
+    p->n_lw = (int)lw.size();  // >= 1: the zero mode's block
+    if ((rc = dalloc(p, &p->lw_flag, nblk)) || (rc = dalloc(p, &p->lw_blocks, lw.size() * sizeof(int))))
+      return bail(rc);
+    OB_CUDA(cudaMemcpyAsync(p->lw_flag, flag.data(), nblk, cudaMemcpyHostToDevice, p->astream));
+    OB_CUDA(cudaMemcpyAsync(p->lw_blocks, lw.data(), lw.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, p->astream));
+    // the vectors must outlive the copies: pageable copies are staged before
+    // the call returns
+  }
   if ((rc = dalloc(p, &p->diag, 64 * sizeof(double)))) return bail(rc);
   // ordered after the allocation on the set-up stream
   OB_CUDA(cudaMemsetAsync(p->diag, 0, 64 * sizeof(double), p->astream));

@@ -289,16 +289,23 @@ struct ThomasK {
 // Parseval form of the discrete-operator residual (poisson.py:263-268) as a
 // raw sum of weighted |r^|^2 in diag[slot_d] (normalised on the host).
 // dh and ph may alias: a CTA reads only its own columns before writing them.
-// The non-zero modes are staged and swept in the plan's type T (FP64 plans:
-// double, the reference's arithmetic; FP32 plans: single precision, half the
-// shared memory per column and so twice the columns in flight per SM); the
-// zero mode is always solved in double, in its own shared-memory region.
-template <class T, int TC>
+// The modes are staged and swept in R.  FP64 plans use double throughout (the
+// reference's arithmetic).  FP32 plans run two launches over disjoint column
+// blocks: the blocks holding a long-wave mode, k^2 Lz^2 < 1, in double, since
+// these nearly singular columns amplify rounding by about 1/(k Lz)^2, and
+// all other blocks in single precision, with half the shared memory per
+// column and so twice the columns in flight per SM.  `blocks` (optional)
+// lists the column blocks of the launch (blockIdx.x indexes it); `skip`
+// (optional) flags blocks the launch leaves alone.  The zero mode (in the
+// first block) is always solved in double, in its own region.
+template <class T, int TC, class R = double>
 __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>* dh,
                                                cplx<T>* ph, double* diag, int slot_c,
-                                               int slot_d) {
-  using R = T;  // staging and sweep type of the non-zero modes
+                                               int slot_d, const int* blocks = nullptr,
+                                               const unsigned char* skip = nullptr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long blk = blocks ? (long)blocks[blockIdx.x] : (long)blockIdx.x;
+  if (skip && skip[blk]) return;  // uniform across the block
   const int nz = g.nz;
   const int P = nz + 1;  // padded column stride (bank spread)
   double* zre = reinterpret_cast<double*>(smem_raw);  // zero mode: P real parts
@@ -308,7 +315,7 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   R* sim = sre + (size_t)TC * P;                        // TC * P imag parts
   R* scp = sim + (size_t)TC * P;                        // TC * P c' factors
   const long ncols = (long)g.nxh * g.ny;
-  const long c0 = (long)blockIdx.x * TC;
+  const long c0 = blk * TC;
   const int ncl = (int)min((long)TC, ncols - c0);
   const long base = c0 * nz;
   for (int e = threadIdx.x; e < ncl * nz; e += TC) {
