@@ -100,11 +100,13 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   cp_wait<0>();
   __syncthreads();
 
-  // 2. pack rows (2n, 2n+1) into complex inputs z[n] = f[2n] + i f[2n+1]
-  const double idz = 1.0 / g.dz;
-  for (int n = threadIdx.x; n < M; n += kPencilThreads) {
-#pragma unroll
-    for (int j = 0; j < ZC; ++j) {
+  // 2. pack rows (2n, 2n+1) into complex inputs z[n] = f[2n] + i f[2n+1];
+  //    consecutive threads on consecutive levels (shared-memory rows of B
+  //    elements are not read or written with a stride of B across a warp)
+  const double dz = g.dz;
+  for (int e = threadIdx.x; e < M * ZC; e += kPencilThreads) {
+    const int n = e / ZC, j = e - n * ZC;
+    {
       const int z = z0 + j;
       const bool ok = z < nz;
       const double r = ok ? rho[z] : 0.0;
@@ -121,7 +123,8 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
           wl = arn(wl, mrn(sdt, (double)BH[x * (ZC + 1) + j]));
           wu = arn(wu, mrn(sdt, (double)BH[x * (ZC + 1) + j + 1]));
         }
-        fd[h] = ok ? (T)((ru * wu - rl * wl) * idz) : (T)0;
+        // the reference's operation order, rounded step by step (no FMA)
+        fd[h] = ok ? (T)drn(srn(mrn(ru, wu), mrn(rl, wl)), dz) : (T)0;
       }
       bufA[(size_t)n * B + j] = mk<T>(fu[0], fu[1]);
       bufA[(size_t)n * B + ZC + j] = mk<T>(fv[0], fv[1]);
@@ -276,7 +279,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
   const T* rz = reinterpret_cast<const T*>(Zr);
 
   // 4. velocity correction; consecutive threads on consecutive levels
-  const T idz = (T)(1.0 / g.dz);
+  const T dzt = (T)g.dz;
   for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     const T phib = rz[rb + 2 * j];
     const T gx = rz[rb + 2 * (ZC + 1 + j)];
     const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
-    const T gz = (z >= 1) ? (T)((phi - phib) * idz) : (T)0;
+    const T gz = (z >= 1) ? (T)drn(srn(phi, phib), dzt) : (T)0;
     const int sw = x * (ZC + 1) + j;
     TS wcz = SW[sw], wt = (TS)0;
     if (STAGE) wcz = (TS)arn((double)wcz, mrn(sdt, (double)SB[sw]));
