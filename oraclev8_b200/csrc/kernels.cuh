@@ -731,7 +731,7 @@ struct SlowK {
 // the value at neighbour r, level k is q[cols[r] * nzk + k].  Only the six
 // points of the stencil a selects are loaded (tendency.py:940-959).
 template <class T>
-__device__ __forceinline__ double ddx_ws5(const T* __restrict__ q, size_t o, const size_t* off,
+__device__ __forceinline__ double ddx_ws5(const T* __restrict__ q, int o, const int* off,
                                           double a, double inv60d) {
   // off[0..5] = offsets of i-3, i-2, i-1, i+1, i+2, i+3 relative to o
   const double qm3 = q[o + off[0]], qm2 = q[o + off[1]], qm1 = q[o + off[2]];
@@ -742,7 +742,7 @@ __device__ __forceinline__ double ddx_ws5(const T* __restrict__ q, size_t o, con
 }
 
 template <class T>
-__device__ __forceinline__ double ddx_c2(const T* __restrict__ q, size_t o, const size_t* off,
+__device__ __forceinline__ double ddx_c2(const T* __restrict__ q, int o, const int* off,
                                          double inv2d) {
   return ((double)q[o + off[3]] - (double)q[o + off[2]]) * inv2d;
 }
@@ -782,19 +782,20 @@ __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double
     b -= (b >= ny) ? ny : 0;
     jy[r] = b;
   }
-  const size_t col = (size_t)i * ny + j;
-  size_t offx[6], offy[6], offxw[6], offyw[6];
+  // 32-bit element offsets: plan_create bounds nx * ny * (nz + 1) by 2^31
+  const int col = i * ny + j;
+  int offx[6], offy[6], offxw[6], offyw[6];
 #pragma unroll
   for (int r = 0; r < 6; ++r) {
-    offx[r] = ((size_t)ix[r] * ny + j) * nz - col * nz;
-    offy[r] = ((size_t)i * ny + jy[r]) * nz - col * nz;
-    offxw[r] = ((size_t)ix[r] * ny + j) * nzw - col * nzw;
-    offyw[r] = ((size_t)i * ny + jy[r]) * nzw - col * nzw;
+    offx[r] = (ix[r] - i) * ny * nz;
+    offy[r] = (jy[r] - j) * nz;
+    offxw[r] = (ix[r] - i) * ny * nzw;
+    offyw[r] = (jy[r] - j) * nzw;
   }
   const bool ws5 = (s.adv == 2);
   for (int k = threadIdx.x; k <= nz; k += blockDim.x) {
-    const size_t o = col * nz + k;
-    const size_t ow = col * nzw + k;
+    const int o = col * nz + k;
+    const int ow = col * nzw + k;
     if (k < nz) {
       const double uc = u[o], vc = v[o], thc = th[o];
       double tu = 0.0, tv = 0.0, tt = 0.0;
