@@ -13,7 +13,8 @@
 //  * launch bounds of three CTAs per SM in FP32 and two in FP64, with the
 //    z-chunk chosen so that that many tiles fit in shared memory.
 // Layouts are those of kernels.cuh: state (x, y, z) with z contiguous, w on
-// nz + 1 levels; spectra [kx][y][z] with kx in [0, nx/2].
+// nz + 1 levels; spectra [kx][y][z] with kx in [0, nx/2].  Element indices
+// are 32-bit: plan_create bounds nx * ny * (nz + 1) by 2^31.
 #pragma once
 #include "kernels.cuh"
 #include "pipe.cuh"
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
     const bool ok = z < nz;
-    const size_t gi = ((size_t)x * ny + y) * nz + (ok ? z : 0);
+    const int gi = (x * ny + y) * nz + (ok ? z : 0);
     copy_or_zero(&U[e], u + gi, ok);
     copy_or_zero(&V[e], v + gi, ok);
   }
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
     const int x = e / (ZC + 1), j = e - x * (ZC + 1);
     const int z = z0 + j;  // half levels z0 .. z0+ZC
     const bool ok = z <= nz;
-    const size_t gi = ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0);
+    const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
     copy_or_zero(&W[e], w + gi, ok);
     if (STAGE) copy_or_zero(&BH[e], bh + gi, ok);
   }
@@ -126,9 +127,9 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
         // the reference's operation order, rounded step by step (no FMA)
         fd[h] = ok ? (T)drn(srn(mrn(ru, wu), mrn(rl, wl)), dz) : (T)0;
       }
-      bufA[(size_t)n * B + j] = mk<T>(fu[0], fu[1]);
-      bufA[(size_t)n * B + ZC + j] = mk<T>(fv[0], fv[1]);
-      bufA[(size_t)n * B + 2 * ZC + j] = mk<T>(fd[0], fd[1]);
+      bufA[n * B + j] = mk<T>(fu[0], fu[1]);
+      bufA[n * B + ZC + j] = mk<T>(fv[0], fv[1]);
+      bufA[n * B + 2 * ZC + j] = mk<T>(fd[0], fd[1]);
     }
   }
   __syncthreads();
@@ -145,10 +146,10 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
     const int z = z0 + j;
     if (z >= nz) continue;
     const T kk = (k == M) ? (T)0 : (T)kxd[k];
-    const size_t o = ((size_t)k * ny + y) * nz + z;
-    const cplx<T> Uk = X[(size_t)k * B + j];
-    const cplx<T> Vk = X[(size_t)k * B + ZC + j];
-    const cplx<T> Dk = X[(size_t)k * B + 2 * ZC + j];
+    const int o = (k * ny + y) * nz + z;
+    const cplx<T> Uk = X[k * B + j];
+    const cplx<T> Vk = X[k * B + ZC + j];
+    const cplx<T> Dk = X[k * B + 2 * ZC + j];
     X0[o] = add(ik(kk, Uk), Dk);
     X1[o] = Vk;
   }
@@ -212,23 +213,23 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
   constexpr int BI = 2 * ZC + 1;  // loaded spectral columns per row
   for (int e = threadIdx.x; e < (M + 1) * BI; e += kPencilThreads) {
     const int k = e / BI, b = e - k * BI;
-    const size_t ob = ((size_t)k * ny + y) * nz;
+    const int ob = (k * ny + y) * nz;
     if (b <= ZC) {
       const int z = z0 - 1 + b;
       const bool ok = z >= 0 && z < nz;
-      copy_or_zero(&bufX[(size_t)k * B + b], phs + ob + (ok ? z : 0), ok);
+      copy_or_zero(&bufX[k * B + b], phs + ob + (ok ? z : 0), ok);
     } else {
       const int j = b - ZC - 1;
       const int z = z0 + j;
       const bool ok = z < nz;
-      copy_or_zero(&bufX[(size_t)k * B + 2 * ZC + 1 + j], psi + ob + (ok ? z : 0), ok);
+      copy_or_zero(&bufX[k * B + 2 * ZC + 1 + j], psi + ob + (ok ? z : 0), ok);
     }
   }
   for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
     const bool ok = z < nz;
-    const size_t gi = ((size_t)x * ny + y) * nz + (ok ? z : 0);
+    const int gi = (x * ny + y) * nz + (ok ? z : 0);
     copy_or_zero(&SU[e], u_in + gi, ok);
     copy_or_zero(&SV[e], v_in + gi, ok);
   }
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     const int x = e / (ZC + 1), j = e - x * (ZC + 1);
     const int z = z0 + j;  // half levels z0 .. z0+ZC
     const bool ok = z <= nz;
-    const size_t gi = ((size_t)x * ny + y) * (nz + 1) + (ok ? z : 0);
+    const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
     copy_or_zero(&SW[e], w_in + gi, ok);
     if (STAGE) copy_or_zero(&SB[e], bh + gi, ok);
   }
@@ -256,11 +257,11 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       cplx<T> xm, xc;
       if (c >= ZC + 1 && c <= 2 * ZC) {
         const int src = c - ZC;  // phi~ column of the same level
-        xm = ik(km, bufX[(size_t)m * B + src]);
-        xc = ik(kc, bufX[(size_t)(M - m) * B + src]);
+        xm = ik(km, bufX[m * B + src]);
+        xc = ik(kc, bufX[(M - m) * B + src]);
       } else {
-        xm = bufX[(size_t)m * B + c];
-        xc = bufX[(size_t)(M - m) * B + c];
+        xm = bufX[m * B + c];
+        xc = bufX[(M - m) * B + c];
       }
       if (m == 0) {
         xm.y = (T)0;
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       xc = conjg(xc);
       const cplx<T> S = add(xm, xc);
       const cplx<T> D = mul(sub(xm, xc), twc);
-      bufZ[(size_t)m * B + c] = mk<T>(S.x - D.y, S.y + D.x);
+      bufZ[m * B + c] = mk<T>(S.x - D.y, S.y + D.x);
     }
   }
   __syncthreads();
@@ -284,9 +285,9 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
     if (z >= nz) continue;
-    const size_t col = (size_t)x * ny + y;
-    const size_t rb = 2 * ((size_t)(x >> 1) * B) + (x & 1);
-    const size_t idx = col * nz + z;
+    const int col = x * ny + y;
+    const int rb = 2 * ((x >> 1) * B) + (x & 1);
+    const int idx = col * nz + z;
     const T phi = rz[rb + 2 * (j + 1)];
     const T phib = rz[rb + 2 * j];
     const T gx = rz[rb + 2 * (ZC + 1 + j)];
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fy2(
     const int f = b / ZC, j = b - f * ZC;
     const int z = z0 + j;
     const bool ok = z < nz;
-    const size_t o = ((size_t)kx * ny + y) * nz + (ok ? z : 0);
+    const int o = (kx * ny + y) * nz + (ok ? z : 0);
     copy_or_zero(&bufA[e], (f == 0 ? in0 : in1) + o, ok);
   }
   cp_commit();
@@ -353,9 +354,9 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fy2(
     const int z = z0 + j;
     if (z >= nz) continue;
     const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
-    cplx<T> d = add(R[(size_t)ky * B + j], ik(kk, R[(size_t)ky * B + ZC + j]));
+    cplx<T> d = add(R[ky * B + j], ik(kk, R[ky * B + ZC + j]));
     if (MODE == FY_RESID && (ky == ny / 2 || kx == g.nx / 2)) d = mk<T>((T)0, (T)0);
-    out0[((size_t)kx * ny + ky) * nz + z] = mk<TO>((TO)d.x, (TO)d.y);
+    out0[(kx * ny + ky) * nz + z] = mk<TO>((TO)d.x, (TO)d.y);
   }
 }
 
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_iy2(
     const int ky = e / ZC, j = e - ky * ZC;
     const int z = z0 + j;
     const bool ok = z < nz;
-    copy_or_zero(&bufA[(size_t)ky * B + j], in0 + ((size_t)kx * ny + ky) * nz + (ok ? z : 0), ok);
+    copy_or_zero(&bufA[ky * B + j], in0 + (kx * ny + ky) * nz + (ok ? z : 0), ok);
   }
   cp_commit();
   for (int i = threadIdx.x; i < ny; i += kPencilThreads) stw[i] = twy[i];
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_iy2(
   for (int e = threadIdx.x; e < ny * ZC; e += kPencilThreads) {
     const int ky = e / ZC, j = e - ky * ZC;
     const T kk = (ky == ny / 2) ? (T)0 : (T)kyd[ky];
-    bufA[(size_t)ky * B + ZC + j] = ik(kk, bufA[(size_t)ky * B + j]);
+    bufA[ky * B + ZC + j] = ik(kk, bufA[ky * B + j]);
   }
   __syncthreads();
   cplx<T>* R = fft_smem<T, true, 8>(bufA, bufB, B, py, stw, 1);
@@ -394,9 +395,9 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_iy2(
     const int y = e / ZC, j = e - y * ZC;
     const int z = z0 + j;
     if (z >= nz) continue;
-    const size_t o = ((size_t)kx * ny + y) * nz + z;
-    out0[o] = R[(size_t)y * B + j];
-    out1[o] = R[(size_t)y * B + ZC + j];
+    const int o = (kx * ny + y) * nz + z;
+    out0[o] = R[y * B + j];
+    out1[o] = R[y * B + ZC + j];
   }
 }
 
