@@ -323,6 +323,18 @@ def load_traffic(wname, precision):
     return NCU_TRAFFIC.get((wname, precision), {})
 
 
+def max_over_ranks(vals, device):
+    """Element-wise maximum of `vals` over the ranks of the default process
+    group (the slowest replica's time); the values themselves at one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(x) for x in vals]
+    t = torch.tensor([float(x) for x in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def _timed_steps(integ, st, dt, steps, warmup, barrier):
     """W untimed steps, then K steps bracketed by barrier + synchronize and
     timed with CUDA events on the launching stream; per-class kernel times
@@ -428,13 +440,10 @@ def run_b200(args):
         companion = (ms64, _precision_report(st, st64, integ64.plan))
         del st64, integ64
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms] + ([companion[0]] if companion else []), device=dev,
-                         dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0].item())
-        if companion:
-            companion = (float(t[1].item()), companion[1])
+    red = max_over_ranks([ms] + ([companion[0]] if companion else []), dev)
+    ms = red[0]
+    if companion:
+        companion = (red[1], companion[1])
     cells = w["nx"] * w["ny"] * w["nz"]
     value = world * cells * args.steps / (ms / 1e3)
 
@@ -485,10 +494,7 @@ def run_b200(args):
                 o.copy_(x, non_blocking=True)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks([t_e2e], dev)[0]
     e2e = world * cells * k_e2e / t_e2e
 
     # ---- roofline of the dominant kernel ------------------------------------
@@ -544,8 +550,10 @@ def run_b200(args):
         line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
                                 note="this run vs the FP64 run from the same initial state; "
                                      "divergence = anelastic divergence evaluated in FP64")
-    if world == 1 and not args.no_ensemble:
-        line["ensemble"], line["serving"] = ensemble_report(args, load_peaks()[0])
+    if not args.no_ensemble:
+        ens = ensemble_report(args, load_peaks()[0])
+        if rank == 0:
+            line["ensemble"], line["serving"] = ens
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rates, sc = cpu_sample_rate(args.workload, 1, 1, 1)
         line["cpu_baseline"] = {
@@ -570,17 +578,32 @@ def ensemble_report(args, peak_gbs):
     at 2/s (seed 4), run length U(6, 72) h divided by ``--serving-scale``,
     80% FP32-refined / 20% FP64, 150 GB HBM budget; against the same stream
     served serially in plain FP64."""
-    from oraclev8_b200.serving import (ServingEngine, draw_requests, serve_serial_plain,
-                                       summarize)
+    import torch.distributed as dist
+    from oraclev8_b200.serving import (ServingEngine, draw_requests, gather_records,
+                                       serve_serial_plain, shard_requests, summarize)
+    rank = dist.get_rank() if dist.is_available() and dist.is_initialized() else 0
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
     # library, kernels and the plan pool warm before timing
     ServingEngine(realtime=False).run(draw_requests(6, 99, hours=0.2, fp32r_frac=0.5))
     serve_serial_plain(draw_requests(2, 98, hours=0.1), realtime=False)
+    # N > 1: whole runs are dealt to the GPUs (no exchange between runs)
     reqs = draw_requests(args.ensemble_runs, 3, hours=args.ensemble_hours)
-    eng = summarize(ServingEngine(realtime=False).run(reqs))
-    ser = summarize(serve_serial_plain(reqs, realtime=False))
+    mine = shard_requests(reqs, rank, world)
+    eng = gather_records(ServingEngine(realtime=False).run(mine))
+    ser = gather_records(serve_serial_plain(mine, realtime=False))
+    if eng is None:  # not rank 0
+        r4 = shard_requests(draw_requests(args.serving_requests, 4,
+                                          hours=(6.0 / args.serving_scale,
+                                                 72.0 / args.serving_scale),
+                                          rate=2.0, fp32r_frac=0.8), rank, world)
+        gather_records(ServingEngine(hbm_budget=150e9, realtime=True).run(r4))
+        gather_records(serve_serial_plain(r4, realtime=True))
+        return None
+    eng, ser = summarize(eng), summarize(ser)
     passes = PASSES_BASE  # no heating in the ensemble draws
     ens = {
-        "workload": f"{len(reqs)} runs drawn from the mixed ensemble (seed 3): nx=ny in "
+        "workload": f"{len(reqs)} runs drawn from the mixed ensemble (seed 3), dealt to "
+                    f"{world} GPU(s): nx=ny in "
                     f"{{96,128,192,256,384}} at dx 10 km, nz in {{32,48,64}} over 16 km, "
                     f"Vmax U(25,65), Rmax U(20,80) km, B U(1,2), lat U(10,30)N; "
                     f"{args.ensemble_hours:g} h each at dt = 0.8 dx / Vmax; WS5 + beta-plane + "
@@ -591,11 +614,11 @@ def ensemble_report(args, peak_gbs):
                      "achieved": passes * 4 * eng["cell_updates_per_s"] / 1e9, "peak": peak_gbs,
                      "unit": "GB/s",
                      "frac": passes * 4 * eng["cell_updates_per_s"] / 1e9 / peak_gbs}}
-    r4 = draw_requests(args.serving_requests, 4, hours=(6.0 / args.serving_scale,
-                                                        72.0 / args.serving_scale),
-                       rate=2.0, fp32r_frac=0.8)
-    eng4 = summarize(ServingEngine(hbm_budget=150e9, realtime=True).run(r4))
-    ser4 = summarize(serve_serial_plain(r4, realtime=True))
+    r4 = shard_requests(draw_requests(args.serving_requests, 4,
+                                      hours=(6.0 / args.serving_scale, 72.0 / args.serving_scale),
+                                      rate=2.0, fp32r_frac=0.8), rank, world)
+    eng4 = summarize(gather_records(ServingEngine(hbm_budget=150e9, realtime=True).run(r4)))
+    ser4 = summarize(gather_records(serve_serial_plain(r4, realtime=True)))
     serving = {
         "workload": f"{len(r4)} requests, Poisson arrivals at 2/s (seed 4), ensemble draws, "
                     f"run length U(6,72) h / {args.serving_scale:g}, 80% fp32r / 20% fp64, "

@@ -330,6 +330,37 @@ class ServingEngine:
         return done
 
 
+def shard_requests(requests: "list[RunRequest]", rank: int, world: int
+                   ) -> "list[RunRequest]":
+    """This rank's share of a request stream served by `world` GPUs: whole runs
+    are dealt out (runs never exchange data), largest cell-update count first
+    to the least-loaded rank (deterministic on every rank)."""
+    if world <= 1:
+        return list(requests)
+    load = [0] * world
+    mine = []
+    for r in sorted(requests, key=lambda q: (-q.cell_updates, q.rid)):
+        g = min(range(world), key=lambda i: (load[i], i))
+        load[g] += r.cell_updates
+        if g == rank:
+            mine.append(r)
+    return sorted(mine, key=lambda q: (q.arrival_s, q.rid))
+
+
+def gather_records(records: "list[RunRecord]"):
+    """All ranks' records on rank 0 (None elsewhere); the records themselves
+    without a process group.  Final states are not sent."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return records
+    slim = [RunRecord(**{**r.__dict__, "final": None}) for r in records]
+    out = [None] * dist.get_world_size() if dist.get_rank() == 0 else None
+    dist.gather_object(slim, out, dst=0)
+    if dist.get_rank() != 0:
+        return None
+    return [r for part in out for r in part]
+
+
 def summarize(records: "list[RunRecord]", makespan_s: Optional[float] = None) -> dict:
     lat = np.array([r.latency_s for r in records])
     q = np.array([r.queue_s for r in records])
