@@ -406,6 +406,21 @@ int set_smem_attrs() {
   return set_x2_attrs<T>();
 }
 
+// Kernel attributes are per function and device: set them once per device.
+template <class T>
+int set_smem_attrs_once() {
+  static std::mutex mu;
+  static bool done[kMaxDevices] = {};
+  int dev = 0;
+  OB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  const bool known = dev >= 0 && dev < kMaxDevices;
+  if (known && done[dev]) return OB_OK;
+  if (int rc = set_smem_attrs<T>()) return rc;
+  if (known) done[dev] = true;
+  return OB_OK;
+}
+
 // Persistent grid: resident CTAs per SM (occupancy API) x SMs, capped by items.
 template <class K>
 int persistent_grid(K kernel, size_t smem, int items, int* out) {
@@ -865,7 +880,7 @@ int make_refiner(OraclePlan* p) {
                           p->astream));
   const size_t ns = (size_t)p->g.nxh * ny * nz;
   if ((rc = dalloc(p, &q->S1, ns * ce)) || (rc = dalloc(p, &q->S2, ns * ce))) return rc;
-  return set_smem_attrs<double>();
+  return set_smem_attrs_once<double>();
 }
 
 // Helmholtz divergence damping tendency (tendency.py:1800-1839) into Du, Dv.
@@ -1505,9 +1520,11 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
         cudaMemcpyAsync(p->twy, ty.data(), ny * sizeof(cplx<double>), cudaMemcpyHostToDevice,
                         p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
-    if ((rc = set_smem_attrs<double>())) return bail(rc);
-    if ((rc = setup_pipes<double>(p))) return bail(rc);
-    if (const char* e = getenv("ORACLE_B200_PIPE")) p->use_pipe = atoi(e) != 0;
+    if ((rc = set_smem_attrs_once<double>())) return bail(rc);
+    // the persistent pipelined projection is optional (ORACLE_B200_PIPE=1):
+    // sized only when asked for, and left off where its tiles do not fit
+    if (const char* e = getenv("ORACLE_B200_PIPE"))
+      if (atoi(e) != 0) p->use_pipe = setup_pipes<double>(p) == OB_OK;
   } else {
     auto tx = twiddles<float>(nx), ty = twiddles<float>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<float>)))) return bail(rc);
@@ -1517,9 +1534,11 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
         cudaMemcpyAsync(p->twy, ty.data(), ny * sizeof(cplx<float>), cudaMemcpyHostToDevice,
                         p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
-    if ((rc = set_smem_attrs<float>())) return bail(rc);
-    if ((rc = setup_pipes<float>(p))) return bail(rc);
-    if (const char* e = getenv("ORACLE_B200_PIPE")) p->use_pipe = atoi(e) != 0;
+    if ((rc = set_smem_attrs_once<float>())) return bail(rc);
+    // the persistent pipelined projection is optional (ORACLE_B200_PIPE=1):
+    // sized only when asked for, and left off where its tiles do not fit
+    if (const char* e = getenv("ORACLE_B200_PIPE"))
+      if (atoi(e) != 0) p->use_pipe = setup_pipes<float>(p) == OB_OK;
   }
 
   // chunk sizes: largest z-chunk whose shared-memory footprint allows two CTAs/SM

@@ -7,9 +7,10 @@ admission to retirement.  Its steps are recorded once as a CUDA graph of
 stream, so runs of different sizes overlap on the device.  Admission is by
 HBM footprint against a budget; finished runs retire and free their slot for
 the next queued request (continuous batching).  Resident runs are fed
-shortest-remaining-work first, as many at a time as it takes to fill the GPU.  Per run the loop records
-arrival, admission and completion times; the summary gives p50/p95/p99
-time-to-completion, queueing delay and aggregate cell-updates/s.
+shortest-remaining-work first, as many at a time as it takes to fill the GPU.
+Per run the loop records arrival, admission and completion times; the summary
+gives p50/p95/p99 time-to-completion, queueing delay and aggregate
+cell-updates/s.
 
 Request distributions (vortex parameters, grids and CFL time step) follow the
 ensemble and serving workloads of the LH82 beta-drift study:
@@ -306,7 +307,8 @@ class ServingEngine:
                 # concurrent runs to fill the GPU, without slowing every
                 # resident run down by sharing the GPU among all of them
                 for a in active:
-                    a.events = [e for e in a.events if not e.query()]
+                    if a.events:
+                        a.events = [e for e in a.events if not e.query()]
                 busy = sum(a.req.cells for a in active if a.events)
                 for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
                     if a.left > 0 and (a.events or busy < self.inflight_cells):
@@ -321,7 +323,12 @@ class ServingEngine:
                         active.remove(a)
                         used -= a.bytes
                         progressed = True
-                if not progressed:
+                if preparing:
+                    # the preparation thread needs the interpreter: yield it
+                    # (a busy feeding loop would otherwise hold it for whole
+                    # switch intervals and starve the set-up of queued runs)
+                    time.sleep(200e-6)
+                elif not progressed:
                     time.sleep(50e-6)
         finally:
             todo.put(None)
