@@ -191,7 +191,7 @@ class ServingEngine:
 
     def __init__(self, hbm_budget: float = 150e9, chunk: int = 16, depth: int = 2,
                  realtime: bool = True, keep_final: bool = False, max_active: int = 256,
-                 prepare_ahead: int = 4, inflight_cells: float = 8e6):
+                 prepare_ahead: int = 16, inflight_cells: float = 64e6):
         self.budget = float(hbm_budget)
         self.inflight_cells = float(inflight_cells)
         self.prepare_ahead = int(prepare_ahead)
@@ -323,13 +323,14 @@ class ServingEngine:
                         active.remove(a)
                         used -= a.bytes
                         progressed = True
-                if preparing:
-                    # the preparation thread needs the interpreter: yield it
-                    # (a busy feeding loop would otherwise hold it for whole
-                    # switch intervals and starve the set-up of queued runs)
-                    time.sleep(200e-6)
-                elif not progressed:
-                    time.sleep(50e-6)
+                # Yield the interpreter: the preparation thread needs it, and
+                # a busy polling loop would starve the set-up of queued runs.
+                # Every fed run has `depth` graph launches queued, so a poll
+                # every millisecond leaves the GPU no gap.
+                if not progressed:
+                    time.sleep(1e-3)
+                elif preparing:
+                    time.sleep(100e-6)
         finally:
             todo.put(None)
             th.join()
