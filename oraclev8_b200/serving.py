@@ -191,7 +191,7 @@ class ServingEngine:
 
     def __init__(self, hbm_budget: float = 150e9, chunk: int = 16, depth: int = 2,
                  realtime: bool = True, keep_final: bool = False, max_active: int = 256,
-                 prepare_ahead: int = 16, inflight_cells: float = 64e6):
+                 prepare_ahead: int = 32, inflight_cells: float = 64e6):
         self.budget = float(hbm_budget)
         self.inflight_cells = float(inflight_cells)
         self.prepare_ahead = int(prepare_ahead)
