@@ -504,26 +504,32 @@ dim3 grid_x(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, 
 dim3 grid_y(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, p->g.nxh); }
 
 // ---- x2 pencil kernels (pencil.cuh) ----------------------------------------
-// Shared memory per CTA the z-chunk choice aims at: three CTAs per SM for the
-// FP32 forward kernel, two otherwise (the inverse kernel's z-chunk of four
-// FP32 levels, with its state tiles, measured faster at two CTAs per SM than
-// a chunk of two at three).
+// Shared memory per CTA the x-pencil z-chunk choice aims at.  k_ix2's time
+// follows the bytes it moves per global sector (a row's ZC levels are one
+// run): at nx = 512, FP32, 5.9 / 2.3 / 1.66 ms per step at ZC = 2 / 4 / 8,
+// the last at two CTAs per SM, so it gets two CTAs' worth.  The FP32 forward
+// kernel measured faster at ZC = 4 with three or more CTAs per SM (1.41 ms
+// per step) than at ZC = 8 with two (1.48 ms).
 template <class T>
 size_t x2_smem_budget(int kind) {
   if (const char* e = getenv("ORACLE_B200_X2_SMEM_KB")) return (size_t)atoi(e) * 1024;
   return (sizeof(T) == 4 && kind < 2) ? 74 * 1024 : 112 * 1024;
 }
+// y pencils (complex rows of ZC levels, at least 16-byte runs): three CTAs
+// per SM in FP32, two in FP64
+template <class T>
+size_t y2_smem_budget() {
+  return sizeof(T) == 4 ? 74 * 1024 : 112 * 1024;
+}
 
-// Dynamic shared memory of a k_fx2 (kind 0), staged k_fx2 (kind 1) or staged
-// k_ix2 (kind 2, the larger of its layouts) launch with z-chunk zc.
+// Dynamic shared memory of a k_fx2 (kinds 0 and 1: plain and staged) or k_ix2
+// (kind 2) launch with z-chunk zc.
 template <class T, class TS>
 size_t x2_smem(int kind, int zc, int nx) {
   switch (zc) {
 #define OB_X2_CASE(Z)                                                                  \
   case Z:                                                                              \
-    return kind == 0 ? fx2_layout<T, TS, Z, false>(nx).total                           \
-                     : kind == 1 ? fx2_layout<T, TS, Z, true>(nx).total                \
-                                 : ix2_layout<T, TS, Z, true>(nx).total;
+    return kind < 2 ? fx2_layout<T, TS, Z>(nx).total : ix2_layout<T, Z>(nx).total;
     OB_X2_CASE(1)
     OB_X2_CASE(2)
     OB_X2_CASE(4)
@@ -564,7 +570,7 @@ template <class T>
 int pick_y2_zc(int ny, int nz) {
   if (const char* e = getenv("ORACLE_B200_X2"))
     if (atoi(e) == 0) return 0;
-  for (size_t cap : {x2_smem_budget<T>(0), kSmemMax})
+  for (size_t cap : {y2_smem_budget<T>(), kSmemMax})
     for (int zc : {8, 4, 2, 1}) {
       if (zc > 1 && zc > nz) continue;
       if (y2_smem_zc<T>(zc, ny) <= cap) return zc;
@@ -614,7 +620,7 @@ template <class T, bool STAGE, class TS, int ZC>
 void fx2_launch(const OraclePlan* q, const TS* u, const TS* v, const TS* w, const TS* bh,
                 double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
   const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
-  k_fx2<T, STAGE, TS, ZC><<<grid, kPencilThreads, fx2_layout<T, TS, ZC, STAGE>(q->g.nx).total,
+  k_fx2<T, STAGE, TS, ZC><<<grid, kPencilThreads, fx2_layout<T, TS, ZC>(q->g.nx).total,
                             st>>>(q->g, q->px8, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx,
                                   (const cplx<T>*)q->twx, X0, X1);
 }
@@ -636,7 +642,7 @@ void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, con
                 TS* phio, cudaStream_t st) {
   const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
   k_ix2<T, MODE, TS, ZC><<<grid, kPencilThreads,
-                           ix2_layout<T, TS, ZC, MODE == IX_STAGE>(p->g.nx).total, st>>>(
+                           ix2_layout<T, ZC>(p->g.nx).total, st>>>(
       p->g, p->px8, phs, psi, p->kx, (const cplx<T>*)p->twx, u, v, w, bh, sdt, uo, vo, wo,
       phio);
 }

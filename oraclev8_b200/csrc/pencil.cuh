@@ -10,8 +10,12 @@
 //    and loop over the ZC levels of the row, so no index needs a division;
 //  * k_ix2 loads phi~ once and forms the i kx' phi~ column in its C2R
 //    pre-process instead of loading phi~ twice;
-//  * launch bounds of three CTAs per SM in FP32 and two in FP64, with the
-//    z-chunk chosen so that that many tiles fit in shared memory.
+//  * the z-chunk sets the bytes a CTA moves per global sector: a row's ZC
+//    levels are one contiguous run, so ZC = 8 in FP32 (32-byte runs) needs
+//    half the sector operations per byte of ZC = 4.  Shared memory is laid
+//    out so that ZC = 8 fits two CTAs per SM: k_ix2 stages its state tiles in
+//    the FFT buffer the last pass leaves dead, and the buoyancy rows of the
+//    staged kernels are read from L2 (prefetched when the CTA starts).
 // Layouts are those of kernels.cuh: state (x, y, z) with z contiguous, w on
 // nz + 1 levels; spectra [kx][y][z] with kx in [0, nx/2].  Element indices
 // are 32-bit: plan_create bounds nx * ny * (nz + 1) by 2^31.
@@ -26,13 +30,24 @@ constexpr int kPencilThreads = 256;
 // radix-8 butterflies need more than the 80 registers three CTAs leave.
 template <class T>
 constexpr int pencil_min_blocks() { return sizeof(T) == 8 ? 2 : 3; }
+// x pencils: two CTAs per SM at ZC = 8, where shared memory allows no more
+template <class T, int ZC>
+constexpr int x2_min_blocks() { return (sizeof(T) == 8 || ZC >= 8) ? 2 : 3; }
+
+// L2 prefetch of the lines holding the run [a, b] (inclusive) of one row
+template <class TS>
+__device__ __forceinline__ void prefetch_run(const TS* a, const TS* b) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  if ((reinterpret_cast<size_t>(a) ^ reinterpret_cast<size_t>(b)) >> 7)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(b));
+}
 
 // Shared-memory layout of k_fx2 (bytes from the dynamic base), shared by the
 // kernel and the host's launch sizing.
 struct Fx2Layout {
-  size_t tw, bufA, bufB, raw_u, raw_v, raw_w, raw_t, total;
+  size_t tw, bufA, bufB, raw_u, raw_v, raw_w, total;
 };
-template <class T, class TS, int ZC, bool STAGE>
+template <class T, class TS, int ZC>
 __host__ __device__ inline Fx2Layout fx2_layout(int nx) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   const int M = nx / 2;
@@ -46,32 +61,30 @@ __host__ __device__ inline Fx2Layout fx2_layout(int nx) {
   L.raw_u = L.bufB;
   L.raw_v = L.raw_u + al((size_t)nx * ZC * sizeof(TS));
   L.raw_w = L.raw_v + al((size_t)nx * ZC * sizeof(TS));
-  L.raw_t = L.raw_w + al((size_t)nx * (ZC + 1) * sizeof(TS));
-  const size_t raw_end = L.raw_t + (STAGE ? al((size_t)nx * (ZC + 1) * sizeof(TS)) : 0);
+  const size_t raw_end = L.raw_w + al((size_t)nx * (ZC + 1) * sizeof(TS));
   L.total = (L.bufB + buf > raw_end) ? L.bufB + buf : raw_end;
   return L;
 }
 
 // x-pencil forward kernel: rho-weighting, vertical flux divergence (STAGE:
 // of w + sdt b_half, with b_half = g theta'/theta0 on half levels given as the
-// field bh), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd), X1 = FFTx(rho v).
-// grid = (ceil(nz/ZC), ny).
+// field bh, read from L2), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd),
+// X1 = FFTx(rho v).  grid = (ceil(nz/ZC), ny).
 template <class T, bool STAGE, class TS, int ZC>
-__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
+__global__ void __launch_bounds__(kPencilThreads, x2_min_blocks<T, ZC>()) k_fx2(
     GridK g, FftPlan px, const TS* __restrict__ u, const TS* __restrict__ v,
     const TS* __restrict__ w, const TS* __restrict__ bh, double sdt,
     const double* __restrict__ rho, const double* __restrict__ rhoh,
     const double* __restrict__ kxd,
     const cplx<T>* __restrict__ twx, cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  const Fx2Layout L = fx2_layout<T, TS, ZC, STAGE>(g.nx);
+  const Fx2Layout L = fx2_layout<T, TS, ZC>(g.nx);
   cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
   cplx<T>* bufA = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufA);
   cplx<T>* bufB = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufB);
   TS* U = reinterpret_cast<TS*>(smem_dyn + L.raw_u);
   TS* V = reinterpret_cast<TS*>(smem_dyn + L.raw_v);
   TS* W = reinterpret_cast<TS*>(smem_dyn + L.raw_w);
-  TS* BH = reinterpret_cast<TS*>(smem_dyn + L.raw_t);
   const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
   constexpr int B = 3 * ZC;
   const int y = blockIdx.y;
@@ -94,9 +107,13 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
     const bool ok = z <= nz;
     const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
     copy_or_zero(&W[e], w + gi, ok);
-    if (STAGE) copy_or_zero(&BH[e], bh + gi, ok);
   }
   cp_commit();
+  if (STAGE)
+    for (int x = threadIdx.x; x < nx; x += kPencilThreads) {
+      const TS* r = bh + (x * ny + y) * (nz + 1);
+      prefetch_run(r + z0, r + min(z0 + ZC, nz));
+    }
   for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
   cp_wait<0>();
   __syncthreads();
@@ -120,9 +137,10 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
         fv[h] = (T)(r * (double)V[x * ZC + j]);
         double wl = (double)W[x * (ZC + 1) + j];
         double wu = (double)W[x * (ZC + 1) + j + 1];
-        if (STAGE) {  // provisional stage w (integrator.py:483-490)
-          wl = arn(wl, mrn(sdt, (double)BH[x * (ZC + 1) + j]));
-          wu = arn(wu, mrn(sdt, (double)BH[x * (ZC + 1) + j + 1]));
+        if (STAGE && ok) {  // provisional stage w (integrator.py:483-490)
+          const TS* r = bh + (x * ny + y) * (nz + 1) + z;
+          wl = arn(wl, mrn(sdt, (double)r[0]));
+          wu = arn(wu, mrn(sdt, (double)r[1]));
         }
         // the reference's operation order, rounded step by step (no FMA)
         fd[h] = ok ? (T)drn(srn(mrn(ru, wu), mrn(rl, wl)), dz) : (T)0;
@@ -155,13 +173,15 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_fx2(
   }
 }
 
-// Shared-memory layout of k_ix2: twiddles, the two FFT buffers, and the
-// state tiles the correction reads (u, v on ZC levels; w and, for STAGE, the
-// half-level buoyancy on ZC + 1 levels), fetched with the spectra.
+// Shared-memory layout of k_ix2: twiddles and the two FFT buffers.  The state
+// tiles the correction reads (u, v on ZC levels, w on ZC + 1) go into the
+// buffer the last FFT pass leaves dead: nx (3 ZC + 1) elements of TS, which
+// the M (3 ZC + 1) complex T of either buffer hold whenever TS is no wider
+// than T.
 struct Ix2Layout {
-  size_t tw, bufX, bufZ, su, sv, sw, sb, total;
+  size_t tw, bufX, bufZ, total;
 };
-template <class T, class TS, int ZC, bool STAGE>
+template <class T, int ZC>
 __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   const int M = nx / 2;
@@ -170,11 +190,7 @@ __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
   L.tw = 0;
   L.bufX = al((size_t)nx * sizeof(cplx<T>));
   L.bufZ = L.bufX + al((size_t)(M + 1) * B * sizeof(cplx<T>));
-  L.su = L.bufZ + al((size_t)M * B * sizeof(cplx<T>));
-  L.sv = L.su + al((size_t)nx * ZC * sizeof(TS));
-  L.sw = L.sv + al((size_t)nx * ZC * sizeof(TS));
-  L.sb = L.sw + al((size_t)nx * (ZC + 1) * sizeof(TS));
-  L.total = L.sb + (STAGE ? al((size_t)nx * (ZC + 1) * sizeof(TS)) : 0);
+  L.total = L.bufZ + al((size_t)M * B * sizeof(cplx<T>));
   return L;
 }
 
@@ -188,28 +204,27 @@ __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
 //   IX_REFINE:  as IX_CORRECT but phi_out += phi (a correction potential).
 // grid = (ceil(nz/ZC), ny).
 template <class T, int MODE, class TS, int ZC>
-__global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
+__global__ void __launch_bounds__(kPencilThreads, x2_min_blocks<T, ZC>()) k_ix2(
     GridK g, FftPlan px, const cplx<T>* __restrict__ phs, const cplx<T>* __restrict__ psi,
     const double* __restrict__ kxd, const cplx<T>* __restrict__ twx, const TS* u_in,
     const TS* v_in, const TS* w_in, const TS* __restrict__ bh, double sdt,
     TS* u_out, TS* v_out, TS* w_out, TS* phi_out) {
+  static_assert(sizeof(TS) <= sizeof(T), "the state tiles must fit a dead FFT buffer");
   constexpr bool STAGE = (MODE == IX_STAGE);
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  const Ix2Layout L = ix2_layout<T, TS, ZC, STAGE>(g.nx);
+  const Ix2Layout L = ix2_layout<T, ZC>(g.nx);
   cplx<T>* stw = reinterpret_cast<cplx<T>*>(smem_dyn + L.tw);
   cplx<T>* bufX = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufX);
   cplx<T>* bufZ = reinterpret_cast<cplx<T>*>(smem_dyn + L.bufZ);
-  TS* SU = reinterpret_cast<TS*>(smem_dyn + L.su);
-  TS* SV = reinterpret_cast<TS*>(smem_dyn + L.sv);
-  TS* SW = reinterpret_cast<TS*>(smem_dyn + L.sw);
-  TS* SB = reinterpret_cast<TS*>(smem_dyn + L.sb);
   const int nx = g.nx, ny = g.ny, nz = g.nz, M = g.M;
   constexpr int B = 3 * ZC + 1;
   const int y = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
+  const int zl = min(z0 + ZC, nz) - 1;  // last level of the chunk
 
-  // 1. phi~ (with the halo level) and psi~ rows, and the state tiles, all in
-  //    flight at once; consecutive threads on consecutive levels of a row
+  // 1. phi~ (with the halo level) and psi~ rows in flight at once;
+  //    consecutive threads on consecutive levels of a row.  The state rows
+  //    the correction reads later are prefetched into L2 meanwhile.
   constexpr int BI = 2 * ZC + 1;  // loaded spectral columns per row
   for (int e = threadIdx.x; e < (M + 1) * BI; e += kPencilThreads) {
     const int k = e / BI, b = e - k * BI;
@@ -225,23 +240,15 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
       copy_or_zero(&bufX[k * B + 2 * ZC + 1 + j], psi + ob + (ok ? z : 0), ok);
     }
   }
-  for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
-    const int x = e / ZC, j = e - x * ZC;
-    const int z = z0 + j;
-    const bool ok = z < nz;
-    const int gi = (x * ny + y) * nz + (ok ? z : 0);
-    copy_or_zero(&SU[e], u_in + gi, ok);
-    copy_or_zero(&SV[e], v_in + gi, ok);
-  }
-  for (int e = threadIdx.x; e < nx * (ZC + 1); e += kPencilThreads) {
-    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
-    const int z = z0 + j;  // half levels z0 .. z0+ZC
-    const bool ok = z <= nz;
-    const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
-    copy_or_zero(&SW[e], w_in + gi, ok);
-    if (STAGE) copy_or_zero(&SB[e], bh + gi, ok);
-  }
   cp_commit();
+  for (int x = threadIdx.x; x < nx; x += kPencilThreads) {
+    const int c = x * ny + y;
+    prefetch_run(u_in + c * nz + z0, u_in + c * nz + zl);
+    prefetch_run(v_in + c * nz + z0, v_in + c * nz + zl);
+    prefetch_run(w_in + c * (nz + 1) + z0, w_in + c * (nz + 1) + zl + 1);
+    if (STAGE) prefetch_run(bh + c * (nz + 1) + z0, bh + c * (nz + 1) + zl + 1);
+    if (MODE == IX_REFINE) prefetch_run(phi_out + c * nz + z0, phi_out + c * nz + zl);
+  }
   for (int i = threadIdx.x; i < nx; i += kPencilThreads) stw[i] = twx[i];
   cp_wait<0>();
   __syncthreads();
@@ -279,7 +286,29 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
   cplx<T>* Zr = fft_smem<T, true, 8>(bufZ, bufX, B, px, stw, 2);
   const T* rz = reinterpret_cast<const T*>(Zr);
 
-  // 4. velocity correction; consecutive threads on consecutive levels
+  // 4. the state tiles into the buffer the last pass read (dead now)
+  TS* SU = reinterpret_cast<TS*>(Zr == bufZ ? bufX : bufZ);
+  TS* SV = SU + nx * ZC;
+  TS* SW = SV + nx * ZC;
+  for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    const int gi = (x * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&SU[e], u_in + gi, ok);
+    copy_or_zero(&SV[e], v_in + gi, ok);
+  }
+  for (int e = threadIdx.x; e < nx * (ZC + 1); e += kPencilThreads) {
+    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+    const int z = z0 + j;  // half levels z0 .. z0+ZC
+    const bool ok = z <= nz;
+    copy_or_zero(&SW[e], w_in + (x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  cp_wait<0>();
+  __syncthreads();
+
+  // 5. velocity correction; consecutive threads on consecutive levels
   const T dzt = (T)g.dz;
   for (int e = threadIdx.x; e < nx * ZC; e += kPencilThreads) {
     const int x = e / ZC, j = e - x * ZC;
@@ -294,16 +323,17 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_ix2(
     const T gy = rz[rb + 2 * (2 * ZC + 1 + j)];
     const T gz = (z >= 1) ? (T)drn(srn(phi, phib), dzt) : (T)0;
     const int sw = x * (ZC + 1) + j;
+    const int wi = col * (nz + 1) + z;
     TS wcz = SW[sw], wt = (TS)0;
-    if (STAGE) wcz = (TS)arn((double)wcz, mrn(sdt, (double)SB[sw]));
+    if (STAGE) wcz = (TS)arn((double)wcz, mrn(sdt, (double)bh[wi]));
     if (z == nz - 1) {
       wt = SW[sw + 1];
-      if (STAGE) wt = (TS)arn((double)wt, mrn(sdt, (double)SB[sw + 1]));
+      if (STAGE) wt = (TS)arn((double)wt, mrn(sdt, (double)bh[wi + 1]));
     }
     u_out[idx] = (TS)((T)SU[e] - gx);
     v_out[idx] = (TS)((T)SV[e] - gy);
-    w_out[col * (nz + 1) + z] = (TS)((T)wcz - gz);
-    if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[col * (nz + 1) + nz] = wt;
+    w_out[wi] = (TS)((T)wcz - gz);
+    if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[wi + 1] = wt;
     if (MODE == IX_REFINE)
       phi_out[idx] = (TS)((T)phi_out[idx] + phi);
     else
