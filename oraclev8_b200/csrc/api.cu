@@ -300,7 +300,7 @@ size_t smem_ix(const OraclePlan* p, int B) {
 }
 // staging in the sweep type plus the zero mode's double region (k_thomas)
 size_t smem_thomas(const OraclePlan* p, size_t rsz = 8) {
-  return 3ull * kThomasCols * (p->g.nz + 1) * rsz + 3ull * (p->g.nz + 1) * 8;
+  return thomas_stage_offset(p->g.nz + 1) + 3ull * kThomasCols * (p->g.nz + 1) * rsz;
 }
 
 constexpr int kPipeThreads = 256;
@@ -941,8 +941,12 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
               const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
   dim3 blk(32, 8);
   dim3 grd((p->g.ny + 7) / 8, p->g.nx);
-  { Launch L_(p, 5, st); k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
-                                      (const T*)p->Dv, uo, vo, wo, tho); }
+  if constexpr (sizeof(T) == 4)
+    { Launch L_(p, 5, st); k_slow_f32<OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                          (const T*)p->Dv, uo, vo, wo, tho); }
+  else
+    { Launch L_(p, 5, st); k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                        (const T*)p->Dv, uo, vo, wo, tho); }
   OB_LAUNCHED();
   return OB_OK;
 }

@@ -50,6 +50,26 @@ __device__ __forceinline__ float mrn(float a, float b) { return __fmul_rn(a, b);
 __device__ __forceinline__ float arn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float srn(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float drn(float a, float b) { return __fdiv_rn(a, b); }
+// correctly rounded 1 / a: the value drn(1, a) gives, without the general
+// division's operand scaling
+__device__ __forceinline__ double rcprn(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float rcprn(float a) { return __frcp_rn(a); }
+
+// ---- cp.async (global -> shared, asynchronous, no register staging) --------
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
 
 // Grid description passed by value to every kernel.
 struct GridK {

@@ -281,6 +281,12 @@ struct ThomasK {
   double scale;        // 1 / (nx ny): inverse-FFT normalisation folded in
 };
 
+// Byte offset of a k_thomas CTA's staged columns: after the zero-mode region
+// (3 P doubles), rounded up to 16 bytes for the cp.async copies.
+__host__ __device__ inline size_t thomas_stage_offset(int P) {
+  return ((size_t)3 * P * 8 + 15) & ~size_t(15);
+}
+
 // Batched Thomas, one thread per spectral column (kx, ky).  Columns are
 // staged through shared memory (coalesced loads of TC consecutive columns);
 // the recurrence runs in double with the reference's operation order and no
@@ -308,22 +314,36 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   if (skip && skip[blk]) return;  // uniform across the block
   const int nz = g.nz;
   const int P = nz + 1;  // padded column stride (bank spread)
+  // IL: the sweep type is the data type, so the CTA's columns (one
+  // contiguous block) are staged as interleaved (re, im) pairs by cp.async,
+  // every copy in flight at once; otherwise converted on the way in.
+  constexpr bool IL = sizeof(R) == sizeof(T);
+  constexpr int S = IL ? 2 : 1;  // element stride of a staged re / im row
   double* zre = reinterpret_cast<double*>(smem_raw);  // zero mode: P real parts
   double* zim = zre + P;                                // P imag parts
   double* zcp = zim + P;                                // P source copy
-  R* sre = reinterpret_cast<R*>(zcp + P);               // TC * P real parts
-  R* sim = sre + (size_t)TC * P;                        // TC * P imag parts
-  R* scp = sim + (size_t)TC * P;                        // TC * P c' factors
+  R* sre = reinterpret_cast<R*>(smem_raw + thomas_stage_offset(P));  // TC * P real parts
+  R* sim = IL ? sre + 1 : sre + (size_t)TC * P;                      // TC * P imag parts
+  R* scp = sre + (size_t)2 * TC * P;                                 // TC * P c' factors
   const long ncols = (long)g.nxh * g.ny;
   const long c0 = blk * TC;
   const int ncl = (int)min((long)TC, ncols - c0);
   const long base = c0 * nz;
-  for (int e = threadIdx.x; e < ncl * nz; e += TC) {
-    const int cl = e / nz;
-    const int k = e - cl * nz;
-    const cplx<T> v = dh[base + e];
-    sre[cl * P + k] = (R)v.x;
-    sim[cl * P + k] = (R)v.y;
+  if constexpr (IL) {
+    cplx<R>* sc = reinterpret_cast<cplx<R>*>(sre);
+    for (int cl = 0; cl < ncl; ++cl)
+      for (int k = threadIdx.x; k < nz; k += TC)
+        cp_async(&sc[cl * P + k], dh + base + (long)cl * nz + k, (int)sizeof(cplx<T>));
+    cp_commit();
+    cp_wait<0>();
+  } else {
+    for (int e = threadIdx.x; e < ncl * nz; e += TC) {
+      const int cl = e / nz;
+      const int k = e - cl * nz;
+      const cplx<T> v = dh[base + e];
+      sre[cl * P + k] = (R)v.x;
+      sim[cl * P + k] = (R)v.y;
+    }
   }
   __syncthreads();
   const int cl = threadIdx.x;
@@ -337,8 +357,8 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
       double* im = zim;
       double* cp = zcp;
       for (int k = 0; k < nz; ++k) {
-        re[k] = (double)sre[k];
-        im[k] = (double)sim[k];
+        re[k] = (double)sre[k * S];
+        im[k] = (double)sim[k * S];
       }
       // Zero mode (poisson.py:233-236, 256, 316-325, 367-383): compatibility
       // residual, removal of the column mean, then the reduced (nz-1) system
@@ -387,55 +407,56 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
         resid = r2 - rsum * rsum / nz;
       }
       for (int k = 0; k < nz; ++k) {
-        sre[k] = (R)re[k];
-        sim[k] = (R)im[k];
+        sre[k * S] = (R)re[k];
+        sim[k * S] = (R)im[k];
       }
     } else {
-      R* re = sre + cl * P;
-      R* im = sim + cl * P;
+      R* re = sre + cl * P * S;
+      R* im = sim + cl * P * S;
       R* cp = scp + cl * P;
       const double kx = t.kx[kxi], ky = t.ky[kyi];
       const double ksq = arn(mrn(kx, kx), mrn(ky, ky));
       R b = (R)srn(t.negs[0], mrn(ksq, t.rho[0]));
-      R inv = drn((R)1, b);
+      R inv = rcprn(b);
       R cpp = mrn((R)t.c[0], inv);
       cp[0] = cpp;
       R pr = mrn(re[0], inv), pi = mrn(im[0], inv);
       re[0] = pr;
       im[0] = pi;
+#pragma unroll 4
       for (int k = 1; k < nz; ++k) {
         b = (R)srn(t.negs[k], mrn(ksq, t.rho[k]));
         const R ak = (R)t.a[k];
         const R den = srn(b, mrn(ak, cpp));
-        inv = drn((R)1, den);
+        inv = rcprn(den);
         if (k < nz - 1) {
           cpp = mrn((R)t.c[k], inv);
           cp[k] = cpp;
         }
-        pr = mrn(srn(re[k], mrn(ak, pr)), inv);
-        pi = mrn(srn(im[k], mrn(ak, pi)), inv);
-        re[k] = pr;
-        im[k] = pi;
+        pr = mrn(srn(re[k * S], mrn(ak, pr)), inv);
+        pi = mrn(srn(im[k * S], mrn(ak, pi)), inv);
+        re[k * S] = pr;
+        im[k * S] = pi;
       }
       R xr = pr, xi = pi;
       for (int k = nz - 2; k >= 0; --k) {
-        xr = srn(re[k], mrn(cp[k], xr));
-        xi = srn(im[k], mrn(cp[k], xi));
-        re[k] = xr;
-        im[k] = xi;
+        xr = srn(re[k * S], mrn(cp[k], xr));
+        xi = srn(im[k * S], mrn(cp[k], xi));
+        re[k * S] = xr;
+        im[k * S] = xi;
       }
       if (diag) {
         // r^ = L phi^ - d^, source re-read from global memory
         const double dz2 = t.dz * t.dz;
         double acc = 0;
         for (int k = 0; k < nz; ++k) {
-          const double fur = (k < nz - 1) ? t.rhoh[k + 1] * (re[k + 1] - re[k]) : 0.0;
-          const double fui = (k < nz - 1) ? t.rhoh[k + 1] * (im[k + 1] - im[k]) : 0.0;
-          const double flr = (k > 0) ? t.rhoh[k] * (re[k] - re[k - 1]) : 0.0;
-          const double fli = (k > 0) ? t.rhoh[k] * (im[k] - im[k - 1]) : 0.0;
+          const double fur = (k < nz - 1) ? t.rhoh[k + 1] * (re[(k + 1) * S] - re[k * S]) : 0.0;
+          const double fui = (k < nz - 1) ? t.rhoh[k + 1] * (im[(k + 1) * S] - im[k * S]) : 0.0;
+          const double flr = (k > 0) ? t.rhoh[k] * (re[k * S] - re[(k - 1) * S]) : 0.0;
+          const double fli = (k > 0) ? t.rhoh[k] * (im[k * S] - im[(k - 1) * S]) : 0.0;
           const cplx<T> src = dh[(size_t)col * nz + k];
-          const double rr = (fur - flr) / dz2 - ksq * t.rho[k] * re[k] - (double)src.x;
-          const double ri = (fui - fli) / dz2 - ksq * t.rho[k] * im[k] - (double)src.y;
+          const double rr = (fur - flr) / dz2 - ksq * t.rho[k] * re[k * S] - (double)src.x;
+          const double ri = (fui - fli) / dz2 - ksq * t.rho[k] * im[k * S] - (double)src.y;
           acc += rr * rr + ri * ri;
         }
         resid = ((kxi == 0 || 2 * kxi == g.nx) ? 1.0 : 2.0) * acc;
@@ -450,7 +471,8 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   for (int e = threadIdx.x; e < ncl * nz; e += TC) {
     const int c = e / nz;
     const int k = e - c * nz;
-    ph[base + e] = mk<T>((T)((double)sre[c * P + k] * t.scale), (T)((double)sim[c * P + k] * t.scale));
+    ph[base + e] = mk<T>((T)((double)sre[(c * P + k) * S] * t.scale),
+                         (T)((double)sim[(c * P + k) * S] * t.scale));
   }
 }
 
@@ -877,6 +899,157 @@ __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double
         wo[ow] = (T)(wk + dts * tw);
       else
         wo[ow] = (T)tw;
+    }
+  }
+}
+
+// WS5 upwind derivative in single precision: only the six points the upwind
+// side selects are loaded.  With s = +1 (a >= 0) or -1,
+//   d = s (-2 q[-3s] + 15 q[-2s] - 60 q[-s] + 20 q[0] + 30 q[s] - 3 q[2s]) / (60 d),
+// the two branches of ddx_ws5 with the second one's terms negated.
+__device__ __forceinline__ float ddx_ws5f(const float* __restrict__ q, int o, const int* off,
+                                          float a, float inv60d) {
+  // off[0..5] = offsets of i-3, i-2, i-1, i+1, i+2, i+3 relative to o
+  const bool up = a >= 0.0f;
+  const int m3 = up ? off[0] : off[5], m2 = up ? off[1] : off[4], m1 = up ? off[2] : off[3];
+  const int p1 = up ? off[3] : off[2], p2 = up ? off[4] : off[1];
+  const float d = -2.0f * q[o + m3] + 15.0f * q[o + m2] - 60.0f * q[o + m1] + 20.0f * q[o] +
+                  30.0f * q[o + p1] - 3.0f * q[o + p2];
+  return (up ? d : -d) * inv60d;
+}
+
+// The fused slow tendency of k_slow for single-precision state, computed in
+// single precision: the FP32 state's own rounding (2^-24 of each field) is
+// the accuracy floor of this path, and FP32 arithmetic needs no conversion
+// of the loaded values and half the registers of the double form.  Same
+// terms, summation order and boundary treatment as k_slow.
+template <int OUTMODE>
+__global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask, double dts_d,
+                                                     const float* __restrict__ u,
+                                                     const float* __restrict__ v,
+                                                     const float* __restrict__ w,
+                                                     const float* __restrict__ th,
+                                                     const float* __restrict__ dmp_u,
+                                                     const float* __restrict__ dmp_v,
+                                                     float* __restrict__ uo, float* __restrict__ vo,
+                                                     float* __restrict__ wo,
+                                                     float* __restrict__ tho) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * blockDim.y + threadIdx.y;
+  if (j >= g.ny) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nzw = nz + 1;
+  const bool adv = (mask & 1) && s.adv;
+  const bool cor = (mask & 2) && s.cor;
+  const bool dmp = (mask & 4) && s.damp;
+  const bool heat = (mask & 8) && s.heat;
+  const float dts = (float)dts_d;
+  const float inv60dx = (float)s.inv60dx, inv60dy = (float)s.inv60dy;
+  const float inv2dx = (float)s.inv2dx, inv2dy = (float)s.inv2dy;
+  const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
+  const float f = cor ? (float)((s.cor == 2) ? s.fy[j] : s.f0) : 0.0f;
+  const float u_env = (float)s.u_env, v_env = (float)s.v_env;
+  int offx[6], offy[6], offxw[6], offyw[6];
+  const int dd[6] = {-3, -2, -1, 1, 2, 3};
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    int a = i + dd[r];
+    a += (a < 0) ? nx : 0;
+    a -= (a >= nx) ? nx : 0;
+    int b = j + dd[r];
+    b += (b < 0) ? ny : 0;
+    b -= (b >= ny) ? ny : 0;
+    offx[r] = (a - i) * ny * nz;
+    offy[r] = (b - j) * nz;
+    offxw[r] = (a - i) * ny * nzw;
+    offyw[r] = (b - j) * nzw;
+  }
+  const int col = i * ny + j;
+  const float hr = heat ? (float)s.heat_r[col] : 0.0f;
+  const bool ws5 = (s.adv == 2);
+  for (int k = threadIdx.x; k <= nz; k += blockDim.x) {
+    const int o = col * nz + k;
+    const int ow = col * nzw + k;
+    if (k < nz) {
+      const float uc = u[o], vc = v[o], thc = th[o];
+      float tu = 0.0f, tv = 0.0f, tt = 0.0f;
+      if (adv) {
+        const float wc = 0.5f * (w[ow] + w[ow + 1]);
+        float czu, czv, czt;
+        if (k == 0) {
+          czu = (u[o + 1] - uc) * invdz;
+          czv = (v[o + 1] - vc) * invdz;
+          czt = (th[o + 1] - thc) * invdz;
+        } else if (k == nz - 1) {
+          czu = (uc - u[o - 1]) * invdz;
+          czv = (vc - v[o - 1]) * invdz;
+          czt = (thc - th[o - 1]) * invdz;
+        } else {
+          czu = (u[o + 1] - u[o - 1]) * inv2dz;
+          czv = (v[o + 1] - v[o - 1]) * inv2dz;
+          czt = (th[o + 1] - th[o - 1]) * inv2dz;
+        }
+        float xu, yu, xv, yv, xt, yt;
+        if (ws5) {
+          xt = ddx_ws5f(th, o, offx, uc, inv60dx);
+          yt = ddx_ws5f(th, o, offy, vc, inv60dy);
+          xu = ddx_ws5f(u, o, offx, uc, inv60dx);
+          yu = ddx_ws5f(u, o, offy, vc, inv60dy);
+          xv = ddx_ws5f(v, o, offx, uc, inv60dx);
+          yv = ddx_ws5f(v, o, offy, vc, inv60dy);
+        } else {
+          xt = (th[o + offx[3]] - th[o + offx[2]]) * inv2dx;
+          yt = (th[o + offy[3]] - th[o + offy[2]]) * inv2dy;
+          xu = (u[o + offx[3]] - u[o + offx[2]]) * inv2dx;
+          yu = (u[o + offy[3]] - u[o + offy[2]]) * inv2dy;
+          xv = (v[o + offx[3]] - v[o + offx[2]]) * inv2dx;
+          yv = (v[o + offy[3]] - v[o + offy[2]]) * inv2dy;
+        }
+        tt = -(uc * xt + vc * yt + wc * (czt + (float)s.dth0[k]));
+        tu = -(uc * xu + vc * yu + wc * czu);
+        tv = -(uc * xv + vc * yv + wc * czv);
+      }
+      if (cor) {
+        tu = tu + f * (vc - v_env);
+        tv = tv + (-f) * (uc - u_env);
+      }
+      if (dmp) {
+        tu = tu + dmp_u[o];
+        tv = tv + dmp_v[o];
+      }
+      if (heat) tt = tt + hr * (float)s.heat_z[k];
+      if (OUTMODE == 0) {
+        uo[o] = uc + dts * tu;
+        vo[o] = vc + dts * tv;
+        tho[o] = thc + dts * tt;
+      } else {
+        uo[o] = tu;
+        vo[o] = tv;
+        tho[o] = tt;
+      }
+    }
+    // w on half level k
+    {
+      const float wk = w[ow];
+      float tw = 0.0f;
+      if (adv && k > 0 && k < nz) {
+        const float uh = 0.5f * (u[o - 1] + u[o]);
+        const float vh = 0.5f * (v[o - 1] + v[o]);
+        const float czw = (w[ow + 1] - w[ow - 1]) * inv2dz;
+        float xw, yw;
+        if (ws5) {
+          xw = ddx_ws5f(w, ow, offxw, uh, inv60dx);
+          yw = ddx_ws5f(w, ow, offyw, vh, inv60dy);
+        } else {
+          xw = (w[ow + offxw[3]] - w[ow + offxw[2]]) * inv2dx;
+          yw = (w[ow + offyw[3]] - w[ow + offyw[2]]) * inv2dy;
+        }
+        tw = -(uh * xw + vh * yw + wk * czw);
+      }
+      if (OUTMODE == 0)
+        wo[ow] = wk + dts * tw;
+      else
+        wo[ow] = tw;
     }
   }
 }

@@ -18,22 +18,7 @@
 
 namespace ob {
 
-// ---- cp.async helpers (global -> shared, asynchronous) ----------------------
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  if (bytes == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-  else if (bytes == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
+// cp_async / cp_commit / cp_wait: common.cuh
 template <class T>
 __device__ __forceinline__ void copy_or_zero(T* dst, const T* src, bool ok) {
   if (ok)
