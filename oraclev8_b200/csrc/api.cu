@@ -185,6 +185,7 @@ struct OraclePlan {
   int* lw_blocks = nullptr;
   unsigned char* lw_flag = nullptr;
   int n_lw = 0;
+  float* tcoef = nullptr;  // FP32 plans: (negs, rho, a, c) per level, as float4
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // launch accounting and optional per-kernel-class event timing
@@ -659,6 +660,31 @@ void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, co
   }
 }
 
+// The single-precision short-wave launch with a compile-time level count
+// (k_thomas_f32); false when nz has no instance.
+bool thomas_f32(OraclePlan* p, int cls, cplx<float>* S3, cudaStream_t st) {
+  const long ncols = (long)p->g.nxh * p->g.ny;
+  const unsigned nb = (unsigned)((ncols + kThomasCols - 1) / kThomasCols);
+  const float scale = (float)(1.0 / ((double)p->g.nx * p->g.ny));
+  const float4* coef = reinterpret_cast<const float4*>(p->tcoef);
+  switch (p->g.nz) {
+#define OB_TF32(N)                                                                          \
+  case N: {                                                                                 \
+    const size_t sm = N * sizeof(float4) + (size_t)kThomasCols * (N + 1) * sizeof(cplx<float>); \
+    Launch L_(p, cls, st);                                                                  \
+    k_thomas_f32<N, kThomasCols><<<nb, kThomasCols, sm, st>>>(p->g, coef, p->kx, p->ky, scale, \
+                                                             S3, S3, p->lw_flag);           \
+    return true;                                                                            \
+  }
+    OB_TF32(32)
+    OB_TF32(48)
+    OB_TF32(64)
+    OB_TF32(80)
+#undef OB_TF32
+  }
+  return false;
+}
+
 // The batched Thomas solve of a projection, in place on S3: FP64 plans in one
 // double launch; FP32 plans as a double launch over the blocks holding a
 // long-wave mode and a single-precision launch over the rest (k_thomas).
@@ -680,8 +706,9 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
     { Launch L_(p, cls, p->aux); k_thomas<T, kThomasCols, double><<<(unsigned)p->n_lw, kThomasCols, smem_thomas(p, 8), p->aux>>>(
           p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, p->lw_blocks, nullptr); }
     OB_LAUNCHED();
-    { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
-          p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, nullptr, p->lw_flag); }
+    if (diag || !thomas_f32(p, cls, (cplx<float>*)S3, st))
+      { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
+            p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, nullptr, p->lw_flag); }
     OB_LAUNCHED();
     OB_CUDA(cudaEventRecord(p->ev_join, p->aux));
     OB_CUDA(cudaStreamWaitEvent(st, p->ev_join, 0));
@@ -1608,6 +1635,16 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       return bail(rc);
     OB_CUDA(cudaMemcpyAsync(p->lw_flag, flag.data(), nblk, cudaMemcpyHostToDevice, p->astream));
     OB_CUDA(cudaMemcpyAsync(p->lw_blocks, lw.data(), lw.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, p->astream));
+    std::vector<float> coef(4 * (size_t)nz);
+    for (int k = 0; k < nz; ++k) {
+      coef[4 * k + 0] = (float)negs[k];
+      coef[4 * k + 1] = (float)rf[k];
+      coef[4 * k + 2] = (float)a[k];
+      coef[4 * k + 3] = (float)c[k];
+    }
+    if ((rc = dalloc(p, &p->tcoef, coef.size() * sizeof(float)))) return bail(rc);
+    OB_CUDA(cudaMemcpyAsync(p->tcoef, coef.data(), coef.size() * sizeof(float),
                             cudaMemcpyHostToDevice, p->astream));
     // the vectors must outlive the copies: pageable copies are staged before
     // the call returns

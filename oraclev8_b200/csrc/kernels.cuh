@@ -476,6 +476,97 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   }
 }
 
+// Single-precision Thomas sweep over the short-wave column blocks, with the
+// level count NZ a compile-time constant: c' is held in registers and both
+// sweeps are unrolled, and each level's coefficients (negs, rho, a, c,
+// rounded to float on the host) are one broadcast float4 from shared memory.
+// Shared memory holds only the staged (re, im) pairs of the CTA's columns, so
+// about 1.5x the columns of k_thomas<float, TC, float> are in flight per SM,
+// each with under half its instructions per level.  The recurrence and its
+// operation order are those of k_thomas with R = float; the diagonal term
+// b = negs - k^2 rho is formed in float.  Blocks flagged in `skip` (the
+// long-wave blocks, the zero mode's among them) are left to the double
+// launch.  No residual diagnostics: the solves that record them run k_thomas.
+// dh and ph may alias (a CTA reads only its own columns before writing them).
+// CTAs per SM that the staged columns' shared memory allows (TC = 32), which
+// the register bound matches
+template <int NZ>
+constexpr int thomas_f32_blocks() { return NZ <= 64 ? 12 : 10; }
+template <int NZ, int TC>
+__global__ void __launch_bounds__(TC, thomas_f32_blocks<NZ>()) k_thomas_f32(GridK g, const float4* __restrict__ coef,
+                                                   const double* __restrict__ kxd,
+                                                   const double* __restrict__ kyd, float scale,
+                                                   const cplx<float>* dh, cplx<float>* ph,
+                                                   const unsigned char* __restrict__ skip) {
+  constexpr int P = NZ + 1;  // padded column stride (bank spread)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sco = reinterpret_cast<float4*>(smem_raw);          // NZ coefficient quadruples
+  cplx<float>* sc = reinterpret_cast<cplx<float>*>(sco + NZ);  // TC * P staged pairs
+  const long blk = blockIdx.x;
+  if (skip[blk]) return;  // uniform across the block
+  const long ncols = (long)g.nxh * g.ny;
+  const long c0 = blk * TC;
+  const int ncl = (int)min((long)TC, ncols - c0);
+  const long base = c0 * NZ;
+  for (int k = threadIdx.x; k < NZ; k += TC) cp_async(&sco[k], &coef[k], 16);
+  for (int cl = 0; cl < ncl; ++cl)
+    for (int k = threadIdx.x; k < NZ; k += TC)
+      cp_async(&sc[cl * P + k], dh + base + (long)cl * NZ + k, 8);
+  cp_commit();
+  cp_wait<0>();
+  __syncthreads();
+  const int cl = threadIdx.x;
+  if (cl < ncl) {
+    const long col = c0 + cl;
+    const int kxi = (int)(col / g.ny);
+    const int kyi = (int)(col - (long)kxi * g.ny);
+    const double kx = kxd[kxi], ky = kyd[kyi];
+    const float ksq = (float)arn(mrn(kx, kx), mrn(ky, ky));
+    cplx<float>* s = sc + cl * P;
+    float cp[NZ];
+    float4 q = sco[0];  // (negs, rho, a, c)
+    float inv = rcprn(srn(q.x, mrn(ksq, q.y)));
+    float cpp = mrn(q.w, inv);
+    cp[0] = cpp;
+    cplx<float> d = s[0];
+    float pr = mrn(d.x, inv), pi = mrn(d.y, inv);
+    s[0] = mk<float>(pr, pi);
+#pragma unroll
+    for (int k = 1; k < NZ; ++k) {
+      q = sco[k];
+      const float b = srn(q.x, mrn(ksq, q.y));
+      inv = rcprn(srn(b, mrn(q.z, cpp)));
+      if (k < NZ - 1) {
+        cpp = mrn(q.w, inv);
+        cp[k] = cpp;
+      }
+      d = s[k];
+      pr = mrn(srn(d.x, mrn(q.z, pr)), inv);
+      pi = mrn(srn(d.y, mrn(q.z, pi)), inv);
+      s[k] = mk<float>(pr, pi);
+      // loads may run ahead within a group of four levels, not further: the
+      // unrolled sweep would otherwise hoist every level's loads into
+      // registers that c' needs
+      if ((k & 3) == 3) asm volatile("" ::: "memory");
+    }
+    float xr = pr, xi = pi;
+#pragma unroll
+    for (int k = NZ - 2; k >= 0; --k) {
+      d = s[k];
+      xr = srn(d.x, mrn(cp[k], xr));
+      xi = srn(d.y, mrn(cp[k], xi));
+      s[k] = mk<float>(xr, xi);
+      if ((k & 3) == 0) asm volatile("" ::: "memory");
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < ncl; ++c)
+    for (int k = threadIdx.x; k < NZ; k += TC) {
+      const cplx<float> v = sc[c * P + k];
+      ph[base + (long)c * NZ + k] = mk<float>(v.x * scale, v.y * scale);
+    }
+}
+
 enum IyMode { IY_GRAD = 0, IY_FIELDS = 1 };
 
 // y-pencil inverse kernel.  grid = (nxh, ceil(nz/zc)).  smem 2 * ny * B cplx.

@@ -59,7 +59,9 @@ def _smooth_state(nx, ny, nz, seed):
     return u, v, w
 
 
-@pytest.mark.parametrize("shape", [(128, 96, 16), (192, 160, 24)])
+# nz = 48 and 64 run the single-precision sweep with a compile-time level
+# count (k_thomas_f32), nz = 16 and 24 the generic one
+@pytest.mark.parametrize("shape", [(128, 96, 16), (192, 160, 24), (96, 64, 48), (128, 96, 64)])
 def test_refinement_reaches_fp32_storage_floor(shape):
     nx, ny, nz = shape
     Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
