@@ -13,6 +13,7 @@
 #include "kernels.cuh"
 #include "pipe.cuh"
 #include "pencil.cuh"
+#include "xreg.cuh"
 #include "tracker.cuh"
 #include "init.cuh"
 
@@ -153,6 +154,7 @@ struct OraclePlan {
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
   FftPlan px8{}, py8{};
   int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
+  int zc3_fx = 0;  // register-resident FP32 x pencils (nx = 512): z-chunk, 0 = off
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -362,9 +364,22 @@ int x2_attrs_zc() {
   return OB_OK;
 }
 
+template <bool STAGE, int ZC>
+int xr_attr_fx3() {
+  OB_CUDA(cudaFuncSetAttribute(k_fx3<STAGE, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fx3_smem<STAGE, ZC>()));
+  return OB_OK;
+}
+
 template <class T>
 int set_x2_attrs() {
   int rc;
+  if constexpr (sizeof(T) == 4) {
+    if ((rc = xr_attr_fx3<false, 2>()) || (rc = xr_attr_fx3<true, 2>()) ||
+        (rc = xr_attr_fx3<false, 4>()) || (rc = xr_attr_fx3<true, 4>()) ||
+        (rc = xr_attr_fx3<false, 8>()) || (rc = xr_attr_fx3<true, 8>()))
+      return rc;
+  }
   if ((rc = x2_attrs_zc<T, T, 1>()) || (rc = x2_attrs_zc<T, T, 2>()) ||
       (rc = x2_attrs_zc<T, T, 4>()) || (rc = x2_attrs_zc<T, T, 8>()))
     return rc;
@@ -637,6 +652,23 @@ void fx2(const OraclePlan* q, int zc, const TS* u, const TS* v, const TS* w, con
   }
 }
 
+template <bool STAGE, int ZC>
+void fx3_launch(const OraclePlan* q, const float* u, const float* v, const float* w,
+                const float* bh, double sdt, cplx<float>* X0, cplx<float>* X1, cudaStream_t st) {
+  const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
+  k_fx3<STAGE, ZC><<<grid, 48 * ZC, fx3_smem<STAGE, ZC>(), st>>>(
+      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<float>*)q->twx, X0, X1);
+}
+template <bool STAGE>
+void fx3(const OraclePlan* q, int zc, const float* u, const float* v, const float* w,
+         const float* bh, double sdt, cplx<float>* X0, cplx<float>* X1, cudaStream_t st) {
+  switch (zc) {
+    case 2: fx3_launch<STAGE, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    case 4: fx3_launch<STAGE, 4>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    default: fx3_launch<STAGE, 8>(q, u, v, w, bh, sdt, X0, X1, st); break;
+  }
+}
+
 template <class T, int MODE, class TS, int ZC>
 void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
                 const TS* v, const TS* w, const TS* bh, double sdt, TS* uo, TS* vo, TS* wo,
@@ -782,7 +814,18 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   }
   const bool stage = stage_sdt >= 0.0;
   if (p->use_pipe) return project_pipe<T>(p, u, v, w, th, stage_sdt, uo, vo, wo, phio, diag, slot_c, slot_d, st);
-  if (stage && p->zc2_fxs && bh)
+  bool fx_done = false;
+  if constexpr (sizeof(T) == 4) {
+    if (p->zc3_fx && stage && bh) {
+      { Launch L_(p, 0, st); fx3<true>(p, p->zc3_fx, u, v, w, bh, stage_sdt, S1, S2, st); }
+      fx_done = true;
+    } else if (p->zc3_fx && !stage) {
+      { Launch L_(p, 0, st); fx3<false>(p, p->zc3_fx, u, v, w, th, 0.0, S1, S2, st); }
+      fx_done = true;
+    }
+  }
+  if (fx_done) {
+  } else if (stage && p->zc2_fxs && bh)
     { Launch L_(p, 0, st); fx2<T, true, T>(p, p->zc2_fxs, u, v, w, bh, stage_sdt, S1, S2, st); }
   else if (!stage && p->zc2_fx)
     { Launch L_(p, 0, st); fx2<T, false, T>(p, p->zc2_fx, u, v, w, th, 0.0, S1, S2, st); }
@@ -1603,6 +1646,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       p->zc2_fx = pick_x2_zc<float, float>(0, nx, nz);
       p->zc2_fxs = pick_x2_zc<float, float>(1, nx, nz);
       p->zc2_ix = pick_x2_zc<float, float>(2, nx, nz);
+      if (nx == kXrN) {
+        p->zc3_fx = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
+        if (const char* e = getenv("ORACLE_B200_FX3_ZC")) p->zc3_fx = atoi(e);
+      }
     }
   }
 

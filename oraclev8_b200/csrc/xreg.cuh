@@ -1,0 +1,204 @@
+// Register-resident x-pencil kernels for nx = 512 (M = 256), single precision.
+//
+// The M = 256 point FFT of a column is spread over a 16-lane group (two
+// groups per warp): M = 16 x 16, n = n1 + 16 n2, k = 16 k1 + k2.
+//   pass 1: lane t = n1 holds z[t + 16 n2] (n2 = 0..15), takes the 16-point
+//           DFT over n2 in registers and multiplies by W_256^(t k2);
+//   exchange: through a 16 x 17 padded shared-memory block of its own group
+//           (only __syncwarp: the group's lanes are one half of a warp);
+//   pass 2: lane t = k2 holds the n1 values and takes the 16-point DFT over
+//           n1, leaving Z[16 k1 + t] in its registers.
+// Against the shared-memory Stockham kernels (pencil.cuh) a column's data
+// crosses shared memory once in the FFT instead of three times plus a
+// pre/post-processing pass: the real-to-complex pack is fused into pass 1's
+// gather, the complex-to-real pre-process likewise, and the R2C split is
+// formed from partner lanes with warp shuffles.  Same arithmetic per element
+// as k_fx2 / k_ix2 otherwise, in single precision.
+// Layouts: state (x, y, z) with z contiguous, w on nz + 1 levels; spectra
+// [kx][y][z] with kx in [0, nx/2].  Element indices are 32-bit.
+#pragma once
+#include "pencil.cuh"
+
+namespace ob {
+
+constexpr int kXrM = 256;  // packed complex FFT length (nx = 512)
+constexpr int kXrN = 512;
+constexpr int kXrEx = 16 * 17;  // exchange block of one group (complex)
+
+// Row stride (floats) of the level-major tiles: nx plus a pad that puts the
+// rows of one warp's z-run on distinct banks.
+template <int ZC>
+__host__ __device__ constexpr int xr_stride() { return kXrN + 32 / ZC; }
+
+// Pass 1 and pass 2 of a group's 256-point FFT.  tw2[16 k2 + t] = W_256^(t k2)
+// (forward sign; conjugated for INV).  On entry a[n2] = z[t + 16 n2]; on exit
+// a[k1] = Z[16 k1 + t].  ex: the group's exchange block.  The caller makes
+// sure ex is free (a CTA barrier when it aliases other data).
+template <bool INV>
+__device__ __forceinline__ void xr_pass1(cplx<float> (&a)[16], int t,
+                                         const cplx<float>* __restrict__ tw2) {
+  dft16<float, INV>(a);
+#pragma unroll
+  for (int k2 = 1; k2 < 16; ++k2) {
+    cplx<float> w = tw2[16 * k2 + t];
+    if (INV) w.y = -w.y;
+    a[k2] = mul(a[k2], w);
+  }
+}
+template <bool INV>
+__device__ __forceinline__ void xr_pass2(cplx<float> (&a)[16], int t, cplx<float>* ex) {
+#pragma unroll
+  for (int k2 = 0; k2 < 16; ++k2) ex[k2 * 17 + t] = a[k2];
+  __syncwarp();
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) a[n1] = ex[t * 17 + n1];
+  dft16<float, INV>(a);
+}
+
+// ---- forward: k_fx3 ----------------------------------------------------------
+// Shared memory (bytes): twiddles, then one region that holds in turn the
+// level-major state tiles, the groups' exchange blocks and the spectra.
+template <bool STAGE, int ZC>
+__host__ __device__ constexpr size_t fx3_smem() {
+  constexpr int B = 3 * ZC, S = xr_stride<ZC>();
+  constexpr size_t raw = (size_t)(2 * ZC + (STAGE ? 2 : 1) * (ZC + 1)) * S * 4;
+  constexpr size_t ex = (size_t)B * kXrEx * 8;
+  constexpr size_t xs = (size_t)(kXrM + 1) * (B + 1) * 8;
+  constexpr size_t r1 = raw > ex ? raw : ex;
+  return 2 * kXrM * 8 + (r1 > xs ? r1 : xs);
+}
+template <int ZC>
+constexpr int fx3_min_blocks() { return ZC >= 8 ? 2 : 4; }
+
+// Forward x-pencil kernel (k_fx2 semantics, FP32, nx = 512): rho-weighting,
+// vertical flux divergence (STAGE: of w + sdt b_half, b_half the field bh),
+// R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd), X1 = FFTx(rho v).
+// 3 ZC columns (u, v, d at ZC levels), one 16-lane group each.
+// grid = (ceil(nz/ZC), ny), 48 ZC threads.
+template <bool STAGE, int ZC>
+__global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
+    GridK g, const float* __restrict__ u, const float* __restrict__ v,
+    const float* __restrict__ w, const float* __restrict__ bh, double sdt,
+    const double* __restrict__ rho, const double* __restrict__ rhoh,
+    const double* __restrict__ kxd, const cplx<float>* __restrict__ twx,
+    cplx<float>* __restrict__ X0, cplx<float>* __restrict__ X1) {
+  static_assert(ZC == 2 || ZC == 4 || ZC == 8, "whole warps of 16-lane groups");
+  constexpr int B = 3 * ZC, NT = 16 * B, M = kXrM, N = kXrN, S = xr_stride<ZC>(), BP = B + 1;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<float>* tw2 = reinterpret_cast<cplx<float>*>(smem_dyn);  // [16 k2 + t] = W_256^(t k2)
+  cplx<float>* twN = tw2 + M;                                   // W_512^k, k < 256
+  float* U = reinterpret_cast<float*>(twN + M);                 // [ZC][S]
+  float* V = U + ZC * S;                                        // [ZC][S]
+  float* W = V + ZC * S;                                        // [ZC + 1][S]
+  float* BH = W + (ZC + 1) * S;                                 // [ZC + 1][S] (STAGE)
+  cplx<float>* ex = reinterpret_cast<cplx<float>*>(U);          // B x 16 x 17, after the gather
+  cplx<float>* XS = reinterpret_cast<cplx<float>*>(U);          // (M + 1) x BP, after the exchange
+  const int ny = g.ny, nz = g.nz;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  const int tid = threadIdx.x;
+
+  // 1. every tile in flight at once; consecutive threads take consecutive
+  //    levels of a row (whole z-runs per warp), rows stored level-major
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    const int gi = (x * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&U[j * S + x], u + gi, ok);
+    copy_or_zero(&V[j * S + x], v + gi, ok);
+  }
+  for (int e = tid; e < N * (ZC + 1); e += NT) {
+    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+    const int z = z0 + j;  // half levels z0 .. z0+ZC
+    const bool ok = z <= nz;
+    const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
+    copy_or_zero(&W[j * S + x], w + gi, ok);
+    if (STAGE) copy_or_zero(&BH[j * S + x], bh + gi, ok);
+  }
+  cp_commit();
+  for (int i = tid; i < M; i += NT) {
+    tw2[i] = twx[2 * ((i & 15) * (i >> 4))];  // W_256^m = W_512^(2m)
+    twN[i] = twx[i];
+  }
+  cp_wait<0>();
+  __syncthreads();
+
+  // 2. gather with the pack fused: column grp = (field f, level j); lane t
+  //    takes z[t + 16 q] = f(2n) + i f(2n+1), n = t + 16 q
+  const int grp = tid >> 4, t = tid & 15;
+  const int f = grp / ZC, j = grp - f * ZC;
+  const int zj = z0 + j;
+  const bool ok = zj < nz;
+  cplx<float> a[16];
+  if (f < 2) {
+    const float r = ok ? (float)rho[zj] : 0.0f;
+    const float* R = (f == 0 ? U : V) + j * S + 2 * t;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const float2 p = *reinterpret_cast<const float2*>(R + 32 * q);
+      a[q] = mk<float>(r * p.x, r * p.y);
+    }
+  } else {
+    const float rl = ok ? (float)rhoh[zj] : 0.0f, ru = ok ? (float)rhoh[zj + 1] : 0.0f;
+    const float idz = (float)(1.0 / g.dz);
+    const float sd = (float)sdt;
+    const float* Wl = W + j * S + 2 * t;
+    const float* Bl = BH + j * S + 2 * t;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      float2 wl = *reinterpret_cast<const float2*>(Wl + 32 * q);
+      float2 wu = *reinterpret_cast<const float2*>(Wl + S + 32 * q);
+      if (STAGE) {  // provisional stage w (integrator.py:483-490)
+        const float2 bl = *reinterpret_cast<const float2*>(Bl + 32 * q);
+        const float2 bu = *reinterpret_cast<const float2*>(Bl + S + 32 * q);
+        wl.x += sd * bl.x;
+        wl.y += sd * bl.y;
+        wu.x += sd * bu.x;
+        wu.y += sd * bu.y;
+      }
+      a[q] = ok ? mk<float>((ru * wu.x - rl * wl.x) * idz, (ru * wu.y - rl * wl.y) * idz)
+                : mk<float>(0.0f, 0.0f);
+    }
+  }
+  xr_pass1<false>(a, t, tw2);
+  __syncthreads();  // every gather done: the exchange blocks reuse the tiles' space
+  xr_pass2<false>(a, t, ex + grp * kXrEx);
+
+  // 3. R2C split, a[s] = Z[k], k = 16 s + t; Z[M - k] is held by the partner
+  //    lane (16 - t) mod 16 of the group, at s' = 15 - s (t > 0), or by the
+  //    lane itself at (16 - s) mod 16 (t = 0)
+  const int plane = (tid & 16) | ((16 - t) & 15);
+  __syncthreads();  // every exchange read: the spectra reuse their space
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const float px = __shfl_sync(0xffffffffu, a[15 - s].x, plane);
+    const float py = __shfl_sync(0xffffffffu, a[15 - s].y, plane);
+    const cplx<float> zk = a[s];
+    const cplx<float> zc = conjg(t == 0 ? a[(16 - s) & 15] : mk<float>(px, py));
+    const cplx<float> E = scl(add(zk, zc), 0.5f);
+    const cplx<float> D = sub(zk, zc);
+    const cplx<float> O = mk<float>(0.5f * D.y, -0.5f * D.x);  // -i/2 * D
+    const int k = 16 * s + t;
+    const cplx<float> WO = mul(twN[k], O);
+    XS[k * BP + grp] = add(E, WO);
+    if (k == 0) XS[M * BP + grp] = conjg(sub(E, WO));
+  }
+  __syncthreads();
+
+  // 4. X0 = i kx' U + D, X1 = V (consecutive threads on consecutive levels)
+  for (int e = tid; e < (M + 1) * ZC; e += NT) {
+    const int k = e / ZC, jj = e - k * ZC;
+    const int z = z0 + jj;
+    if (z >= nz) continue;
+    const float kk = (k == M) ? 0.0f : (float)kxd[k];
+    const int o = (k * ny + y) * nz + z;
+    const cplx<float> Uk = XS[k * BP + jj];
+    const cplx<float> Vk = XS[k * BP + ZC + jj];
+    const cplx<float> Dk = XS[k * BP + 2 * ZC + jj];
+    X0[o] = add(ik(kk, Uk), Dk);
+    X1[o] = Vk;
+  }
+}
+
+}  // namespace ob

@@ -60,8 +60,10 @@ def _smooth_state(nx, ny, nz, seed):
 
 
 # nz = 48 and 64 run the single-precision sweep with a compile-time level
-# count (k_thomas_f32), nz = 16 and 24 the generic one
-@pytest.mark.parametrize("shape", [(128, 96, 16), (192, 160, 24), (96, 64, 48), (128, 96, 64)])
+# count (k_thomas_f32), nz = 16 and 24 the generic one; nx = 512 runs the
+# register-resident x pencils (xreg.cuh)
+@pytest.mark.parametrize("shape", [(128, 96, 16), (192, 160, 24), (96, 64, 48), (128, 96, 64),
+                                   (512, 48, 16)])
 def test_refinement_reaches_fp32_storage_floor(shape):
     nx, ny, nz = shape
     Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
@@ -112,13 +114,14 @@ def _vortex_case(nx, ny, nz):
                              z_peak=6e3, width_z=math.sqrt(2.0) * 2e3), noise_seed=3)
 
 
-def test_fp32_steps_track_fp64():
+@pytest.mark.parametrize("shape", [(96, 72, 16), (512, 40, 16)])
+def test_fp32_steps_track_fp64(shape):
     """Ten full steps of the vortex configuration in FP32, FP32 with one
     correction per step, and FP64: per-field error of the single-precision
     runs, relative to each field's max |.|, and the post-step divergence."""
     from oraclev8_b200.solver import RK3Integrator, State
     from tests.test_oracle_golden import oracle_initial_state
-    c = _vortex_case(96, 72, 16)
+    c = _vortex_case(*shape)
     s0, _ = oracle_initial_state(c)
     base = Base(c["nz"], c["Lz"])
     cfg = b200_config(c)
@@ -164,3 +167,45 @@ def test_refinement_controls():
     w = torch.zeros((16, 12, 9), dtype=torch.float64, device="cuda")
     with pytest.raises(ValueError):
         p64.refine(u, u.clone(), w, u.clone())
+
+
+@pytest.mark.parametrize("nz", [16, 13])
+def test_register_pencils_match_stockham(nz, monkeypatch):
+    """At nx = 512 the FP32 x pencils run the register-resident FFT
+    (xreg.cuh); with ORACLE_B200_FX3_ZC=0 the plan keeps the shared-memory
+    Stockham kernels.  Against the FP64 projection of the same input, the
+    register path is as accurate as the Stockham path, field by field; u and
+    v of the two agree to a few FP32 ulp of the wind.  nz = 13 leaves a
+    partial z-chunk.  (The staged form runs in test_fp32_steps_track_fp64 at
+    nx = 512.)"""
+    from oraclev8_b200._plan import Plan, PlanSpec
+    nx, ny = 512, 40
+    Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
+    z, rho0, th0 = O.build_base_state(nz, Lz)
+    mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
+                                    projection=True))
+    monkeypatch.setenv("ORACLE_B200_FX3_ZC", "0")
+    p_ref = mk("fp32")
+    monkeypatch.delenv("ORACLE_B200_FX3_ZC")
+    p_new = mk("fp32")
+    p64 = mk("fp64")
+    u, v, w = _smooth_state(nx, ny, nz, seed=7 + nz)
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    outs = []
+    for p, dt in ((p64, torch.float64), (p_ref, torch.float32), (p_new, torch.float32)):
+        uu, vv, ww = (dev(f32(a), dt) for a in (u, v, w))
+        phi = torch.empty_like(uu)
+        p.project(uu, vv, ww, phi)
+        outs.append([host(a).astype(np.float64) for a in (uu, vv, ww, phi)])
+    wind = max(float(np.max(np.abs(outs[0][0]))), float(np.max(np.abs(outs[0][1]))))
+    for i, name in enumerate(("u", "v", "w", "phi")):
+        r64, ref, new = outs[0][i], outs[1][i], outs[2][i]
+        scale = float(np.max(np.abs(r64)))
+        e_ref = float(np.max(np.abs(ref - r64))) / scale
+        e_new = float(np.max(np.abs(new - r64))) / scale
+        d = float(np.max(np.abs(new - ref)))
+        print(f"nz {nz} {name}: error vs FP64 stockham {e_ref:.3e} register {e_new:.3e}; "
+              f"max |register - stockham| {d:.3e}")
+        assert e_new <= 1.5 * e_ref + 1e-7, (name, e_new, e_ref)
+        if name in ("u", "v"):
+            assert d <= 1e-6 * wind, (name, d)
