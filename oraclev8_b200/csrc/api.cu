@@ -154,7 +154,7 @@ struct OraclePlan {
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
   FftPlan px8{}, py8{};
   int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
-  int zc3_fx = 0;  // register-resident FP32 x pencils (nx = 512): z-chunk, 0 = off
+  int zc3_fx = 0, zc3_ix = 0;  // register-resident FP32 x pencils (nx = 512): z-chunk, 0 = off
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -371,10 +371,27 @@ int xr_attr_fx3() {
   return OB_OK;
 }
 
+template <int MODE, int ZC>
+int xr_attr_ix3() {
+  OB_CUDA(cudaFuncSetAttribute(k_ix3<MODE, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Ix3Size<ZC>::total));
+  return OB_OK;
+}
+template <int ZC>
+int xr_attrs_ix3() {
+  int rc;
+  if ((rc = xr_attr_ix3<IX_CORRECT, ZC>()) || (rc = xr_attr_ix3<IX_STAGE, ZC>()) ||
+      (rc = xr_attr_ix3<IX_REFINE, ZC>()))
+    return rc;
+  return OB_OK;
+}
+
 template <class T>
 int set_x2_attrs() {
   int rc;
   if constexpr (sizeof(T) == 4) {
+    if ((rc = xr_attrs_ix3<2>()) || (rc = xr_attrs_ix3<4>()) || (rc = xr_attrs_ix3<8>()))
+      return rc;
     if ((rc = xr_attr_fx3<false, 2>()) || (rc = xr_attr_fx3<true, 2>()) ||
         (rc = xr_attr_fx3<false, 4>()) || (rc = xr_attr_fx3<true, 4>()) ||
         (rc = xr_attr_fx3<false, 8>()) || (rc = xr_attr_fx3<true, 8>()))
@@ -669,6 +686,25 @@ void fx3(const OraclePlan* q, int zc, const float* u, const float* v, const floa
   }
 }
 
+template <int MODE, int ZC>
+void ix3_launch(const OraclePlan* p, const cplx<float>* phs, const cplx<float>* psi,
+                const float* u, const float* v, const float* w, const float* bh, double sdt,
+                float* uo, float* vo, float* wo, float* phio, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
+  k_ix3<MODE, ZC><<<grid, 16 * (3 * ZC + 2), Ix3Size<ZC>::total, st>>>(
+      p->g, phs, psi, p->kx, (const cplx<float>*)p->twx, u, v, w, bh, sdt, uo, vo, wo, phio);
+}
+template <int MODE>
+void ix3(const OraclePlan* p, int zc, const cplx<float>* phs, const cplx<float>* psi,
+         const float* u, const float* v, const float* w, const float* bh, double sdt,
+         float* uo, float* vo, float* wo, float* phio, cudaStream_t st) {
+  switch (zc) {
+    case 2: ix3_launch<MODE, 2>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    case 4: ix3_launch<MODE, 4>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    default: ix3_launch<MODE, 8>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+  }
+}
+
 template <class T, int MODE, class TS, int ZC>
 void ix2_launch(const OraclePlan* p, const cplx<T>* phs, const cplx<T>* psi, const TS* u,
                 const TS* v, const TS* w, const TS* bh, double sdt, TS* uo, TS* vo, TS* wo,
@@ -852,7 +888,18 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
         g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
-  if (p->zc2_ix && stage && bh)
+  bool ix_done = false;
+  if constexpr (sizeof(T) == 4) {
+    if (p->zc3_ix && stage && bh) {
+      { Launch L_(p, 4, st); ix3<IX_STAGE>(p, p->zc3_ix, S1, S2, u, v, w, bh, stage_sdt, uo, vo, wo, phio, st); }
+      ix_done = true;
+    } else if (p->zc3_ix && !stage) {
+      { Launch L_(p, 4, st); ix3<IX_CORRECT>(p, p->zc3_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st); }
+      ix_done = true;
+    }
+  }
+  if (ix_done) {
+  } else if (p->zc2_ix && stage && bh)
     { Launch L_(p, 4, st); ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, bh, stage_sdt, uo, vo, wo, phio, st); }
   else if (p->zc2_ix && !stage)
     { Launch L_(p, 4, st); ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st); }
@@ -907,7 +954,9 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
     { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
         g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
-  if (p->zc2_ix)
+  if (p->zc3_ix)
+    { Launch L_(p, OB_PROF_REFINE, st); ix3<IX_REFINE>(p, p->zc3_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
+  else if (p->zc2_ix)
     { Launch L_(p, OB_PROF_REFINE, st); ix2<float, IX_REFINE, float>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
   else
     { Launch L_(p, OB_PROF_REFINE, st); k_ix<float, IX_REFINE><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 3 * p->zc_ix + 1), st>>>(
@@ -1647,8 +1696,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       p->zc2_fxs = pick_x2_zc<float, float>(1, nx, nz);
       p->zc2_ix = pick_x2_zc<float, float>(2, nx, nz);
       if (nx == kXrN) {
-        p->zc3_fx = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
+        p->zc3_fx = p->zc3_ix = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
         if (const char* e = getenv("ORACLE_B200_FX3_ZC")) p->zc3_fx = atoi(e);
+        if (const char* e = getenv("ORACLE_B200_IX3_ZC")) p->zc3_ix = atoi(e);
       }
     }
   }

@@ -201,4 +201,179 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
   }
 }
 
+// ---- inverse: k_ix3 ------------------------------------------------------------
+// Columns (groups): [0, ZC] phi at levels z0-1 .. z0+ZC-1 (one halo level),
+// [ZC+1, 2ZC] d/dx phi, [2ZC+1, 3ZC] d/dy phi (psi~), 3ZC+1 a zero column
+// that makes the group count even (whole warps).
+template <int ZC>
+struct Ix3Size {
+  static constexpr int BG = 3 * ZC + 2;  // groups
+  static constexpr int BI = 2 * ZC + 1;  // loaded spectral columns: phi (with halo), psi
+  static constexpr int SR = xr_stride<ZC>();
+  static constexpr size_t tables = 2 * kXrM * 8 + (((kXrM + 1) * 4 + 15) / 16) * 16;
+  static constexpr size_t xi = (size_t)(kXrM + 1) * BI * 8;
+  static constexpr size_t ex = (size_t)BG * kXrEx * 8;
+  static constexpr size_t zr = (size_t)BG * SR * 4;
+  static constexpr size_t regA = xi > ex ? (xi > zr ? xi : zr) : (ex > zr ? ex : zr);
+  static constexpr size_t state = (size_t)kXrN * (3 * ZC + 1) * 4;
+  static constexpr size_t total = tables + regA + state;
+};
+template <int ZC>
+constexpr int ix3_min_blocks() { return ZC >= 8 ? 2 : 3; }
+
+// Inverse x-pencil kernel with the velocity correction (k_ix2 semantics and
+// modes, FP32, nx = 512).  grid = (ceil(nz/ZC), ny), 16 (3 ZC + 2) threads.
+// Shared memory: twiddles and kx'; region A holding in turn the spectral
+// rows, the groups' exchange blocks and the real outputs (level-major rows);
+// the state tiles, requested at the start in their own cp.async group so
+// that they arrive during the FFT.
+template <int MODE, int ZC>
+__global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3(
+    GridK g, const cplx<float>* __restrict__ phs, const cplx<float>* __restrict__ psi,
+    const double* __restrict__ kxd, const cplx<float>* __restrict__ twx, const float* u_in,
+    const float* v_in, const float* w_in, const float* __restrict__ bh, double sdt,
+    float* u_out, float* v_out, float* w_out, float* phi_out) {
+  static_assert(ZC == 2 || ZC == 4 || ZC == 8, "supported z-chunks");
+  using SZ = Ix3Size<ZC>;
+  constexpr bool STAGE = (MODE == IX_STAGE);
+  constexpr int BG = SZ::BG, BI = SZ::BI, SR = SZ::SR, NT = 16 * BG, M = kXrM, N = kXrN;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<float>* tw2 = reinterpret_cast<cplx<float>*>(smem_dyn);  // [16 k2 + t] = W_256^(t k2)
+  cplx<float>* twN = tw2 + M;                                   // W_512^m, m < 256
+  float* kxs = reinterpret_cast<float*>(twN + M);               // kx'[0..M], kx'[M] = 0
+  unsigned char* regA = smem_dyn + SZ::tables;
+  cplx<float>* XI = reinterpret_cast<cplx<float>*>(regA);       // [M + 1][BI]
+  cplx<float>* ex = reinterpret_cast<cplx<float>*>(regA);       // BG x 16 x 17
+  float* ZR = reinterpret_cast<float*>(regA);                   // [BG][SR] real outputs
+  float* SU = reinterpret_cast<float*>(regA + SZ::regA);        // [x][ZC]
+  float* SV = SU + N * ZC;                                      // [x][ZC]
+  float* SW = SV + N * ZC;                                      // [x][ZC + 1]
+  const int ny = g.ny, nz = g.nz;
+  const int y = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  const int zl = min(z0 + ZC, nz) - 1;  // last level of the chunk
+  const int tid = threadIdx.x;
+
+  // 1. spectral rows (first cp.async group), then the state tiles (second);
+  //    consecutive threads on consecutive levels of a row
+  for (int e = tid; e < (M + 1) * BI; e += NT) {
+    const int k = e / BI, b = e - k * BI;
+    const int ob = (k * ny + y) * nz;
+    if (b <= ZC) {
+      const int z = z0 - 1 + b;
+      const bool ok = z >= 0 && z < nz;
+      copy_or_zero(&XI[e], phs + ob + (ok ? z : 0), ok);
+    } else {
+      const int z = z0 + b - ZC - 1;
+      const bool ok = z < nz;
+      copy_or_zero(&XI[e], psi + ob + (ok ? z : 0), ok);
+    }
+  }
+  cp_commit();
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    const int gi = (x * ny + y) * nz + (ok ? z : 0);
+    copy_or_zero(&SU[e], u_in + gi, ok);
+    copy_or_zero(&SV[e], v_in + gi, ok);
+  }
+  for (int e = tid; e < N * (ZC + 1); e += NT) {
+    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+    const int z = z0 + j;  // half levels z0 .. z0+ZC
+    const bool ok = z <= nz;
+    copy_or_zero(&SW[e], w_in + (x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  if (STAGE || MODE == IX_REFINE)
+    for (int x = tid; x < N; x += NT) {
+      const int c = x * ny + y;
+      if (STAGE) prefetch_run(bh + c * (nz + 1) + z0, bh + c * (nz + 1) + zl + 1);
+      if (MODE == IX_REFINE) prefetch_run(phi_out + c * nz + z0, phi_out + c * nz + zl);
+    }
+  for (int i = tid; i < M; i += NT) {
+    tw2[i] = twx[2 * ((i & 15) * (i >> 4))];  // W_256^m = W_512^(2m)
+    twN[i] = twx[i];
+  }
+  for (int i = tid; i <= M; i += NT) kxs[i] = (i == M) ? 0.0f : (float)kxd[i];
+  cp_wait<1>();  // the spectral rows (the state tiles may still be in flight)
+  __syncthreads();
+
+  // 2. gather with the C2R pre-process fused: a[q] = Z[t + 16 q] of column grp
+  const int grp = tid >> 4, t = tid & 15;
+  int src = 0;
+  bool dx = false;
+  if (grp <= ZC) {
+    src = grp;
+  } else if (grp <= 2 * ZC) {
+    src = grp - ZC;  // phi~ column of the same level
+    dx = true;
+  } else {
+    src = grp - ZC;  // psi~ (grp = 3 ZC + 1: the zero column)
+  }
+  const bool zero = grp == 3 * ZC + 1;
+  cplx<float> a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int m = t + 16 * q;
+    const int mc = M - m;
+    cplx<float> xm = zero ? mk<float>(0.0f, 0.0f) : XI[m * BI + src];
+    cplx<float> xc = zero ? mk<float>(0.0f, 0.0f) : XI[mc * BI + src];
+    if (dx) {
+      xm = ik(kxs[m], xm);
+      xc = ik(kxs[mc], xc);
+    }
+    if (m == 0) {
+      xm.y = 0.0f;
+      xc.y = 0.0f;
+    }
+    xc = conjg(xc);
+    const cplx<float> S = add(xm, xc);
+    const cplx<float> D = mul(sub(xm, xc), conjg(twN[m]));
+    a[q] = mk<float>(S.x - D.y, S.y + D.x);
+  }
+  xr_pass1<true>(a, t, tw2);
+  __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
+  xr_pass2<true>(a, t, ex + grp * kXrEx);
+  // a[k1] = x[2n] + i x[2n+1], n = 16 k1 + t
+  __syncthreads();  // every exchange read: the outputs reuse their space
+  float* zr = ZR + grp * SR + 2 * t;
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1)
+    *reinterpret_cast<float2*>(zr + 32 * k1) = make_float2(a[k1].x, a[k1].y);
+  cp_wait<0>();
+  __syncthreads();
+
+  // 3. velocity correction; consecutive threads on consecutive levels
+  const float dzt = (float)g.dz;
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int x = e / ZC, j = e - x * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const int col = x * ny + y;
+    const int idx = col * nz + z;
+    const float phi = ZR[(j + 1) * SR + x];
+    const float phib = ZR[j * SR + x];
+    const float gx = ZR[(ZC + 1 + j) * SR + x];
+    const float gy = ZR[(2 * ZC + 1 + j) * SR + x];
+    const float gz = (z >= 1) ? drn(srn(phi, phib), dzt) : 0.0f;
+    const int sw = x * (ZC + 1) + j;
+    const int wi = col * (nz + 1) + z;
+    float wcz = SW[sw], wt = 0.0f;
+    if (STAGE) wcz = (float)arn((double)wcz, mrn(sdt, (double)bh[wi]));
+    if (z == nz - 1) {
+      wt = SW[sw + 1];
+      if (STAGE) wt = (float)arn((double)wt, mrn(sdt, (double)bh[wi + 1]));
+    }
+    u_out[idx] = SU[e] - gx;
+    v_out[idx] = SV[e] - gy;
+    w_out[wi] = wcz - gz;
+    if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[wi + 1] = wt;
+    if (MODE == IX_REFINE)
+      phi_out[idx] = phi_out[idx] + phi;
+    else
+      phi_out[idx] = phi;
+  }
+}
+
 }  // namespace ob

@@ -172,8 +172,9 @@ def test_refinement_controls():
 @pytest.mark.parametrize("nz", [16, 13])
 def test_register_pencils_match_stockham(nz, monkeypatch):
     """At nx = 512 the FP32 x pencils run the register-resident FFT
-    (xreg.cuh); with ORACLE_B200_FX3_ZC=0 the plan keeps the shared-memory
-    Stockham kernels.  Against the FP64 projection of the same input, the
+    (xreg.cuh); with ORACLE_B200_FX3_ZC=0 and ORACLE_B200_IX3_ZC=0 the plan
+    keeps the shared-memory Stockham kernels.  Against the FP64 projection of
+    the same input, the
     register path is as accurate as the Stockham path, field by field; u and
     v of the two agree to a few FP32 ulp of the wind.  nz = 13 leaves a
     partial z-chunk.  (The staged form runs in test_fp32_steps_track_fp64 at
@@ -185,8 +186,10 @@ def test_register_pencils_match_stockham(nz, monkeypatch):
     mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
                                     projection=True))
     monkeypatch.setenv("ORACLE_B200_FX3_ZC", "0")
+    monkeypatch.setenv("ORACLE_B200_IX3_ZC", "0")
     p_ref = mk("fp32")
     monkeypatch.delenv("ORACLE_B200_FX3_ZC")
+    monkeypatch.delenv("ORACLE_B200_IX3_ZC")
     p_new = mk("fp32")
     p64 = mk("fp64")
     u, v, w = _smooth_state(nx, ny, nz, seed=7 + nz)
