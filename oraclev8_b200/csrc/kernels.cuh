@@ -1217,14 +1217,51 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
   const size_t nw = (size_t)g.nx * g.ny * (g.nz + 1);
   double mu = 0, mv = 0, mw = 0, mt = 0, sp = 0, pmin = INFINITY, pmax = -INFINITY;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += stride) {
-    mu = fmax(mu, fabs((double)u[e]));
-    mv = fmax(mv, fabs((double)v[e]));
-    mt = fmax(mt, fabs((double)th[e]));
-    sp += (double)phi[e];
+  const size_t first = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  bool done = false;
+  if constexpr (sizeof(T) == 4) {
+    // single precision: float4 loads where sizes and pointers allow; the
+    // maxima of |.| are exact in float, the phi sum stays in double
+    const size_t al = reinterpret_cast<size_t>(u) | reinterpret_cast<size_t>(v) |
+                      reinterpret_cast<size_t>(w) | reinterpret_cast<size_t>(th) |
+                      reinterpret_cast<size_t>(phi);
+    if ((n & 3) == 0 && (nw & 3) == 0 && (al & 15) == 0) {
+      float fu = 0.0f, fv = 0.0f, fw = 0.0f, ft = 0.0f;
+      const float4* u4 = reinterpret_cast<const float4*>(u);
+      const float4* v4 = reinterpret_cast<const float4*>(v);
+      const float4* t4 = reinterpret_cast<const float4*>(th);
+      const float4* p4 = reinterpret_cast<const float4*>(phi);
+      const float4* w4 = reinterpret_cast<const float4*>(w);
+      auto amax = [](float m, float4 a) {
+        return fmaxf(fmaxf(fmaxf(m, fabsf(a.x)), fmaxf(fabsf(a.y), fabsf(a.z))), fabsf(a.w));
+      };
+      for (size_t e = first; e < n / 4; e += stride) {
+        const float4 a = u4[e], b = v4[e], c = t4[e], d = p4[e];
+        fu = amax(fu, a);
+        fv = amax(fv, b);
+        ft = amax(ft, c);
+        sp += (double)d.x;
+        sp += (double)d.y;
+        sp += (double)d.z;
+        sp += (double)d.w;
+      }
+      for (size_t e = first; e < nw / 4; e += stride) fw = amax(fw, w4[e]);
+      mu = fu;
+      mv = fv;
+      mw = fw;
+      mt = ft;
+      done = true;
+    }
   }
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nw; e += stride)
-    mw = fmax(mw, fabs((double)w[e]));
+  if (!done) {
+    for (size_t e = first; e < n; e += stride) {
+      mu = fmax(mu, fabs((double)u[e]));
+      mv = fmax(mv, fabs((double)v[e]));
+      mt = fmax(mt, fabs((double)th[e]));
+      sp += (double)phi[e];
+    }
+    for (size_t e = first; e < nw; e += stride) mw = fmax(mw, fabs((double)w[e]));
+  }
   // surface level k = 0 of every column
   const size_t ncol = (size_t)g.nx * g.ny;
   for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncol; c += stride) {

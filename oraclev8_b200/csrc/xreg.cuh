@@ -341,12 +341,38 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
 #pragma unroll
   for (int k1 = 0; k1 < 16; ++k1)
     *reinterpret_cast<float2*>(zr + 32 * k1) = make_float2(a[k1].x, a[k1].y);
+  // the global values the correction reads besides the tiles (STAGE: b_half;
+  // IX_REFINE: phi) are loaded here, all at once, so that their latency
+  // overlaps the barrier instead of each correction step
+  constexpr int NE = (N * ZC + NT - 1) / NT;  // correction elements per thread
+  float gv[NE], gt[NE];
+  if (STAGE || MODE == IX_REFINE) {
+#pragma unroll
+    for (int i = 0; i < NE; ++i) {
+      const int e = tid + i * NT;
+      const int x = e / ZC, j = e - x * ZC;
+      const int z = z0 + j;
+      gv[i] = gt[i] = 0.0f;
+      if (e < N * ZC && z < nz) {
+        const int col = x * ny + y;
+        if (STAGE) {
+          gv[i] = bh[col * (nz + 1) + z];
+          if (z == nz - 1) gt[i] = bh[col * (nz + 1) + nz];
+        } else {
+          gv[i] = phi_out[col * nz + z];
+        }
+      }
+    }
+  }
   cp_wait<0>();
   __syncthreads();
 
   // 3. velocity correction; consecutive threads on consecutive levels
   const float dzt = (float)g.dz;
-  for (int e = tid; e < N * ZC; e += NT) {
+#pragma unroll
+  for (int i = 0; i < NE; ++i) {
+    const int e = tid + i * NT;
+    if (e >= N * ZC) break;
     const int x = e / ZC, j = e - x * ZC;
     const int z = z0 + j;
     if (z >= nz) continue;
@@ -360,17 +386,17 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     const int sw = x * (ZC + 1) + j;
     const int wi = col * (nz + 1) + z;
     float wcz = SW[sw], wt = 0.0f;
-    if (STAGE) wcz = (float)arn((double)wcz, mrn(sdt, (double)bh[wi]));
+    if (STAGE) wcz = (float)arn((double)wcz, mrn(sdt, (double)gv[i]));
     if (z == nz - 1) {
       wt = SW[sw + 1];
-      if (STAGE) wt = (float)arn((double)wt, mrn(sdt, (double)bh[wi + 1]));
+      if (STAGE) wt = (float)arn((double)wt, mrn(sdt, (double)gt[i]));
     }
     u_out[idx] = SU[e] - gx;
     v_out[idx] = SV[e] - gy;
     w_out[wi] = wcz - gz;
     if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[wi + 1] = wt;
     if (MODE == IX_REFINE)
-      phi_out[idx] = phi_out[idx] + phi;
+      phi_out[idx] = gv[i] + phi;
     else
       phi_out[idx] = phi;
   }
