@@ -154,7 +154,10 @@ struct OraclePlan {
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
   FftPlan px8{}, py8{};
   int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
-  int zc3_fx = 0, zc3_ix = 0;  // register-resident FP32 x pencils (nx = 512): z-chunk, 0 = off
+  // register-resident x pencils of FP32 plans at nx = 512 (z-chunk, 0 = off): the
+  // projection's forward and inverse kernels, and the FP64 residual transform
+  int zc3_fx = 0, zc3_ix = 0, zc3_fxd = 0;
+  int zc3_fy = 0;  // register-resident FP32 y pencils (ny = 512): z-chunk, 0 = off
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -364,10 +367,10 @@ int x2_attrs_zc() {
   return OB_OK;
 }
 
-template <bool STAGE, int ZC>
+template <class T, bool STAGE, int ZC>
 int xr_attr_fx3() {
-  OB_CUDA(cudaFuncSetAttribute(k_fx3<STAGE, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)fx3_smem<STAGE, ZC>()));
+  OB_CUDA(cudaFuncSetAttribute(k_fx3<T, STAGE, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fx3_smem<T, STAGE, ZC>()));
   return OB_OK;
 }
 
@@ -386,15 +389,28 @@ int xr_attrs_ix3() {
   return OB_OK;
 }
 
+template <int ZC>
+int yr_attrs() {
+  OB_CUDA(cudaFuncSetAttribute(k_fy3<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)YrSize<ZC>::total));
+  OB_CUDA(cudaFuncSetAttribute(k_iy3<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)YrSize<ZC>::total));
+  return OB_OK;
+}
+
 template <class T>
 int set_x2_attrs() {
   int rc;
   if constexpr (sizeof(T) == 4) {
+    if ((rc = yr_attrs<2>()) || (rc = yr_attrs<4>()) || (rc = yr_attrs<8>())) return rc;
+  }
+  if constexpr (sizeof(T) == 4) {
     if ((rc = xr_attrs_ix3<2>()) || (rc = xr_attrs_ix3<4>()) || (rc = xr_attrs_ix3<8>()))
       return rc;
-    if ((rc = xr_attr_fx3<false, 2>()) || (rc = xr_attr_fx3<true, 2>()) ||
-        (rc = xr_attr_fx3<false, 4>()) || (rc = xr_attr_fx3<true, 4>()) ||
-        (rc = xr_attr_fx3<false, 8>()) || (rc = xr_attr_fx3<true, 8>()))
+    if ((rc = xr_attr_fx3<float, false, 2>()) || (rc = xr_attr_fx3<float, true, 2>()) ||
+        (rc = xr_attr_fx3<float, false, 4>()) || (rc = xr_attr_fx3<float, true, 4>()) ||
+        (rc = xr_attr_fx3<float, false, 8>()) || (rc = xr_attr_fx3<float, true, 8>()) ||
+        (rc = xr_attr_fx3<double, false, 2>()) || (rc = xr_attr_fx3<double, false, 4>()))
       return rc;
   }
   if ((rc = x2_attrs_zc<T, T, 1>()) || (rc = x2_attrs_zc<T, T, 2>()) ||
@@ -630,6 +646,26 @@ void fy2(const OraclePlan* q, int zc, const cplx<T>* in0, const cplx<T>* in1, cp
   }
 }
 
+template <int ZC>
+void yr_launch(const OraclePlan* p, bool inverse, const cplx<float>* in0, const cplx<float>* in1,
+               cplx<float>* out0, cplx<float>* out1, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.nxh);
+  const cplx<float>* tw = (const cplx<float>*)p->twy;
+  if (inverse)
+    k_iy3<ZC><<<grid, 64 * ZC, YrSize<ZC>::total, st>>>(p->g, in0, p->ky, tw, out0, out1);
+  else
+    k_fy3<ZC><<<grid, 64 * ZC, YrSize<ZC>::total, st>>>(p->g, in0, in1, p->ky, tw, out0);
+}
+// register-resident FP32 y pencils (ny = 512): FY_DIV forward or the IY_GRAD inverse
+void yr(const OraclePlan* p, bool inverse, const cplx<float>* in0, const cplx<float>* in1,
+        cplx<float>* out0, cplx<float>* out1, cudaStream_t st) {
+  switch (p->zc3_fy) {
+    case 2: yr_launch<2>(p, inverse, in0, in1, out0, out1, st); break;
+    case 4: yr_launch<4>(p, inverse, in0, in1, out0, out1, st); break;
+    default: yr_launch<8>(p, inverse, in0, in1, out0, out1, st); break;
+  }
+}
+
 template <class T>
 void iy2(const OraclePlan* p, int zc, const cplx<T>* in0, cplx<T>* out0, cplx<T>* out1,
          cudaStream_t st) {
@@ -669,20 +705,26 @@ void fx2(const OraclePlan* q, int zc, const TS* u, const TS* v, const TS* w, con
   }
 }
 
-template <bool STAGE, int ZC>
+template <class T, bool STAGE, int ZC>
 void fx3_launch(const OraclePlan* q, const float* u, const float* v, const float* w,
-                const float* bh, double sdt, cplx<float>* X0, cplx<float>* X1, cudaStream_t st) {
+                const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
   const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
-  k_fx3<STAGE, ZC><<<grid, 48 * ZC, fx3_smem<STAGE, ZC>(), st>>>(
-      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<float>*)q->twx, X0, X1);
+  k_fx3<T, STAGE, ZC><<<grid, 48 * ZC, fx3_smem<T, STAGE, ZC>(), st>>>(
+      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<T>*)q->twx, X0, X1);
 }
-template <bool STAGE>
+// q's twiddles are of type T (the FP64 refiner plan for T = double)
+template <class T, bool STAGE>
 void fx3(const OraclePlan* q, int zc, const float* u, const float* v, const float* w,
-         const float* bh, double sdt, cplx<float>* X0, cplx<float>* X1, cudaStream_t st) {
-  switch (zc) {
-    case 2: fx3_launch<STAGE, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
-    case 4: fx3_launch<STAGE, 4>(q, u, v, w, bh, sdt, X0, X1, st); break;
-    default: fx3_launch<STAGE, 8>(q, u, v, w, bh, sdt, X0, X1, st); break;
+         const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    if (zc == 2) fx3_launch<T, false, 2>(q, u, v, w, bh, sdt, X0, X1, st);
+    else fx3_launch<T, false, 4>(q, u, v, w, bh, sdt, X0, X1, st);
+  } else {
+    switch (zc) {
+      case 2: fx3_launch<T, STAGE, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
+      case 4: fx3_launch<T, STAGE, 4>(q, u, v, w, bh, sdt, X0, X1, st); break;
+      default: fx3_launch<T, STAGE, 8>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    }
   }
 }
 
@@ -853,10 +895,10 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
   bool fx_done = false;
   if constexpr (sizeof(T) == 4) {
     if (p->zc3_fx && stage && bh) {
-      { Launch L_(p, 0, st); fx3<true>(p, p->zc3_fx, u, v, w, bh, stage_sdt, S1, S2, st); }
+      { Launch L_(p, 0, st); fx3<float, true>(p, p->zc3_fx, u, v, w, bh, stage_sdt, S1, S2, st); }
       fx_done = true;
     } else if (p->zc3_fx && !stage) {
-      { Launch L_(p, 0, st); fx3<false>(p, p->zc3_fx, u, v, w, th, 0.0, S1, S2, st); }
+      { Launch L_(p, 0, st); fx3<float, false>(p, p->zc3_fx, u, v, w, th, 0.0, S1, S2, st); }
       fx_done = true;
     }
   }
@@ -874,14 +916,18 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
         g, p->pxf, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
         (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
-  if (p->zc2_fy)
+  if (sizeof(T) == 4 && p->zc3_fy)
+    { Launch L_(p, 1, st); yr(p, false, (const cplx<float>*)S1, (const cplx<float>*)S2, (cplx<float>*)S3, nullptr, st); }
+  else if (p->zc2_fy)
     { Launch L_(p, 1, st); fy2<T, FY_DIV, T>(p, p->zc2_fy, S1, S2, S3, st); }
   else
     { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
         g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   RC(thomas_solve<T>(p, 2, S3, diag, slot_c, slot_d, st));
-  if (p->zc2_iy)
+  if (sizeof(T) == 4 && p->zc3_fy)
+    { Launch L_(p, 3, st); yr(p, true, (const cplx<float>*)S3, nullptr, (cplx<float>*)S1, (cplx<float>*)S2, st); }
+  else if (p->zc2_iy)
     { Launch L_(p, 3, st); iy2<T>(p, p->zc2_iy, S3, S1, S2, st); }
   else
     { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
@@ -934,7 +980,9 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
   Cf* S1 = (Cf*)p->S1;
   Cf* S2 = (Cf*)p->S2;
   Cf* S3 = (Cf*)p->S3;
-  if (q->zc2_fx)
+  if (p->zc3_fxd)
+    { Launch L_(p, OB_PROF_REFINE, st); fx3<double, false>(q, p->zc3_fxd, u, v, w, nullptr, 0.0, R1, R2, st); }
+  else if (q->zc2_fx)
     { Launch L_(p, OB_PROF_REFINE, st); fx2<double, false, float>(q, q->zc2_fx, u, v, w, nullptr, 0.0, R1, R2, st); }
   else
     { Launch L_(p, OB_PROF_REFINE, st); k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
@@ -948,7 +996,9 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
         g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
   OB_LAUNCHED();
   RC(thomas_solve<float>(p, OB_PROF_REFINE, S3, nullptr, 0, 0, st));
-  if (p->zc2_iy)
+  if (p->zc3_fy)
+    { Launch L_(p, OB_PROF_REFINE, st); yr(p, true, S3, nullptr, S1, S2, st); }
+  else if (p->zc2_iy)
     { Launch L_(p, OB_PROF_REFINE, st); iy2<float>(p, p->zc2_iy, S3, S1, S2, st); }
   else
     { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
@@ -1686,6 +1736,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     p->zc2_fy = p->prec == OB_PREC_F64 ? pick_y2_zc<double>(ny, nz) : pick_y2_zc<float>(ny, nz);
     p->zc2_iy = p->zc2_fy;
   }
+  if (p->prec == OB_PREC_F32 && ny == kYrN) {
+    p->zc3_fy = nz >= 4 ? 4 : 2;
+    if (const char* e = getenv("ORACLE_B200_FY3_ZC")) p->zc3_fy = atoi(e);
+  }
   if (factorize8(nx / 2, p->px8)) {
     if (p->prec == OB_PREC_F64) {
       p->zc2_fx = pick_x2_zc<double, double>(0, nx, nz);
@@ -1699,6 +1753,8 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
         p->zc3_fx = p->zc3_ix = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
         if (const char* e = getenv("ORACLE_B200_FX3_ZC")) p->zc3_fx = atoi(e);
         if (const char* e = getenv("ORACLE_B200_IX3_ZC")) p->zc3_ix = atoi(e);
+        p->zc3_fxd = nz >= 4 ? 4 : 2;
+        if (const char* e = getenv("ORACLE_B200_FXD3_ZC")) p->zc3_fxd = atoi(e);
       }
     }
   }

@@ -34,65 +34,69 @@ __host__ __device__ constexpr int xr_stride() { return kXrN + 32 / ZC; }
 // (forward sign; conjugated for INV).  On entry a[n2] = z[t + 16 n2]; on exit
 // a[k1] = Z[16 k1 + t].  ex: the group's exchange block.  The caller makes
 // sure ex is free (a CTA barrier when it aliases other data).
-template <bool INV>
-__device__ __forceinline__ void xr_pass1(cplx<float> (&a)[16], int t,
-                                         const cplx<float>* __restrict__ tw2) {
-  dft16<float, INV>(a);
+template <class T, bool INV>
+__device__ __forceinline__ void xr_pass1(cplx<T> (&a)[16], int t,
+                                         const cplx<T>* __restrict__ tw2) {
+  dft16<T, INV>(a);
 #pragma unroll
   for (int k2 = 1; k2 < 16; ++k2) {
-    cplx<float> w = tw2[16 * k2 + t];
+    cplx<T> w = tw2[16 * k2 + t];
     if (INV) w.y = -w.y;
     a[k2] = mul(a[k2], w);
   }
 }
-template <bool INV>
-__device__ __forceinline__ void xr_pass2(cplx<float> (&a)[16], int t, cplx<float>* ex) {
+template <class T, bool INV>
+__device__ __forceinline__ void xr_pass2(cplx<T> (&a)[16], int t, cplx<T>* ex) {
 #pragma unroll
   for (int k2 = 0; k2 < 16; ++k2) ex[k2 * 17 + t] = a[k2];
   __syncwarp();
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) a[n1] = ex[t * 17 + n1];
-  dft16<float, INV>(a);
+  dft16<T, INV>(a);
 }
 
 // ---- forward: k_fx3 ----------------------------------------------------------
 // Shared memory (bytes): twiddles, then one region that holds in turn the
-// level-major state tiles, the groups' exchange blocks and the spectra.
-template <bool STAGE, int ZC>
+// level-major state tiles (FP32), the groups' exchange blocks and the spectra
+// (arithmetic type T).
+template <class T, bool STAGE, int ZC>
 __host__ __device__ constexpr size_t fx3_smem() {
   constexpr int B = 3 * ZC, S = xr_stride<ZC>();
   constexpr size_t raw = (size_t)(2 * ZC + (STAGE ? 2 : 1) * (ZC + 1)) * S * 4;
-  constexpr size_t ex = (size_t)B * kXrEx * 8;
-  constexpr size_t xs = (size_t)(kXrM + 1) * (B + 1) * 8;
+  constexpr size_t ex = (size_t)B * kXrEx * sizeof(cplx<T>);
+  constexpr size_t xs = (size_t)(kXrM + 1) * (B + 1) * sizeof(cplx<T>);
   constexpr size_t r1 = raw > ex ? raw : ex;
-  return 2 * kXrM * 8 + (r1 > xs ? r1 : xs);
+  return 2 * kXrM * sizeof(cplx<T>) + (r1 > xs ? r1 : xs);
 }
-template <int ZC>
-constexpr int fx3_min_blocks() { return ZC >= 8 ? 2 : 4; }
+template <class T, int ZC>
+constexpr int fx3_min_blocks() { return sizeof(T) == 8 ? 2 : (ZC >= 8 ? 2 : 4); }
 
-// Forward x-pencil kernel (k_fx2 semantics, FP32, nx = 512): rho-weighting,
-// vertical flux divergence (STAGE: of w + sdt b_half, b_half the field bh),
-// R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd), X1 = FFTx(rho v).
-// 3 ZC columns (u, v, d at ZC levels), one 16-lane group each.
-// grid = (ceil(nz/ZC), ny), 48 ZC threads.
-template <bool STAGE, int ZC>
-__global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
+// Forward x-pencil kernel (k_fx2 semantics, FP32 state, nx = 512):
+// rho-weighting, vertical flux divergence (STAGE: of w + sdt b_half, b_half
+// the field bh), R2C along x; X0 = i kx' FFTx(rho u) + FFTx(vd),
+// X1 = FFTx(rho v).  T = float: the single-precision projection; T = double:
+// the FP64 residual transform of the defect correction, with k_fx2's
+// operation order in the pack.  3 ZC columns (u, v, d at ZC levels), one
+// 16-lane group each.  grid = (ceil(nz/ZC), ny), 48 ZC threads.
+template <class T, bool STAGE, int ZC>
+__global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
     GridK g, const float* __restrict__ u, const float* __restrict__ v,
     const float* __restrict__ w, const float* __restrict__ bh, double sdt,
     const double* __restrict__ rho, const double* __restrict__ rhoh,
-    const double* __restrict__ kxd, const cplx<float>* __restrict__ twx,
-    cplx<float>* __restrict__ X0, cplx<float>* __restrict__ X1) {
+    const double* __restrict__ kxd, const cplx<T>* __restrict__ twx,
+    cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
   static_assert(ZC == 2 || ZC == 4 || ZC == 8, "whole warps of 16-lane groups");
+  static_assert(sizeof(T) == 4 || !STAGE, "the FP64 form is the residual transform");
   constexpr int B = 3 * ZC, NT = 16 * B, M = kXrM, N = kXrN, S = xr_stride<ZC>(), BP = B + 1;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  cplx<float>* tw2 = reinterpret_cast<cplx<float>*>(smem_dyn);  // [16 k2 + t] = W_256^(t k2)
-  cplx<float>* twN = tw2 + M;                                   // W_512^k, k < 256
-  float* U = reinterpret_cast<float*>(twN + M);                 // [ZC][S]
+  cplx<T>* tw2 = reinterpret_cast<cplx<T>*>(smem_dyn);  // [16 k2 + t] = W_256^(t k2)
+  cplx<T>* twN = tw2 + M;                               // W_512^k, k < 256
+  float* U = reinterpret_cast<float*>(twN + M);         // [ZC][S]
   float* V = U + ZC * S;                                        // [ZC][S]
   float* W = V + ZC * S;                                        // [ZC + 1][S]
   float* BH = W + (ZC + 1) * S;                                 // [ZC + 1][S] (STAGE)
-  cplx<float>* ex = reinterpret_cast<cplx<float>*>(U);          // B x 16 x 17, after the gather
-  cplx<float>* XS = reinterpret_cast<cplx<float>*>(U);          // (M + 1) x BP, after the exchange
+  cplx<T>* ex = reinterpret_cast<cplx<T>*>(U);                  // B x 16 x 17, after the gather
+  cplx<T>* XS = reinterpret_cast<cplx<T>*>(U);                  // (M + 1) x BP, after the exchange
   const int ny = g.ny, nz = g.nz;
   const int y = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
@@ -130,14 +134,27 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
   const int f = grp / ZC, j = grp - f * ZC;
   const int zj = z0 + j;
   const bool ok = zj < nz;
-  cplx<float> a[16];
+  cplx<T> a[16];
   if (f < 2) {
-    const float r = ok ? (float)rho[zj] : 0.0f;
+    const T r = ok ? (T)rho[zj] : (T)0;
     const float* R = (f == 0 ? U : V) + j * S + 2 * t;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       const float2 p = *reinterpret_cast<const float2*>(R + 32 * q);
-      a[q] = mk<float>(r * p.x, r * p.y);
+      a[q] = mk<T>(r * (T)p.x, r * (T)p.y);
+    }
+  } else if constexpr (sizeof(T) == 8) {
+    // the reference's operation order, rounded step by step (as k_fx2)
+    const double rl = ok ? rhoh[zj] : 0.0, ru = ok ? rhoh[zj + 1] : 0.0;
+    const double dz = g.dz;
+    const float* Wl = W + j * S + 2 * t;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const float2 wl = *reinterpret_cast<const float2*>(Wl + 32 * q);
+      const float2 wu = *reinterpret_cast<const float2*>(Wl + S + 32 * q);
+      a[q] = ok ? mk<T>(drn(srn(mrn(ru, (double)wu.x), mrn(rl, (double)wl.x)), dz),
+                        drn(srn(mrn(ru, (double)wu.y), mrn(rl, (double)wl.y)), dz))
+                : mk<T>((T)0, (T)0);
     }
   } else {
     const float rl = ok ? (float)rhoh[zj] : 0.0f, ru = ok ? (float)rhoh[zj + 1] : 0.0f;
@@ -161,9 +178,9 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
                 : mk<float>(0.0f, 0.0f);
     }
   }
-  xr_pass1<false>(a, t, tw2);
+  xr_pass1<T, false>(a, t, tw2);
   __syncthreads();  // every gather done: the exchange blocks reuse the tiles' space
-  xr_pass2<false>(a, t, ex + grp * kXrEx);
+  xr_pass2<T, false>(a, t, ex + grp * kXrEx);
 
   // 3. R2C split, a[s] = Z[k], k = 16 s + t; Z[M - k] is held by the partner
   //    lane (16 - t) mod 16 of the group, at s' = 15 - s (t > 0), or by the
@@ -172,15 +189,15 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
   __syncthreads();  // every exchange read: the spectra reuse their space
 #pragma unroll
   for (int s = 0; s < 16; ++s) {
-    const float px = __shfl_sync(0xffffffffu, a[15 - s].x, plane);
-    const float py = __shfl_sync(0xffffffffu, a[15 - s].y, plane);
-    const cplx<float> zk = a[s];
-    const cplx<float> zc = conjg(t == 0 ? a[(16 - s) & 15] : mk<float>(px, py));
-    const cplx<float> E = scl(add(zk, zc), 0.5f);
-    const cplx<float> D = sub(zk, zc);
-    const cplx<float> O = mk<float>(0.5f * D.y, -0.5f * D.x);  // -i/2 * D
+    const T px = __shfl_sync(0xffffffffu, a[15 - s].x, plane);
+    const T py = __shfl_sync(0xffffffffu, a[15 - s].y, plane);
+    const cplx<T> zk = a[s];
+    const cplx<T> zc = conjg(t == 0 ? a[(16 - s) & 15] : mk<T>(px, py));
+    const cplx<T> E = scl(add(zk, zc), (T)0.5);
+    const cplx<T> D = sub(zk, zc);
+    const cplx<T> O = mk<T>((T)0.5 * D.y, (T)-0.5 * D.x);  // -i/2 * D
     const int k = 16 * s + t;
-    const cplx<float> WO = mul(twN[k], O);
+    const cplx<T> WO = mul(twN[k], O);
     XS[k * BP + grp] = add(E, WO);
     if (k == 0) XS[M * BP + grp] = conjg(sub(E, WO));
   }
@@ -191,11 +208,11 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<ZC>()) k_fx3(
     const int k = e / ZC, jj = e - k * ZC;
     const int z = z0 + jj;
     if (z >= nz) continue;
-    const float kk = (k == M) ? 0.0f : (float)kxd[k];
+    const T kk = (k == M) ? (T)0 : (T)kxd[k];
     const int o = (k * ny + y) * nz + z;
-    const cplx<float> Uk = XS[k * BP + jj];
-    const cplx<float> Vk = XS[k * BP + ZC + jj];
-    const cplx<float> Dk = XS[k * BP + 2 * ZC + jj];
+    const cplx<T> Uk = XS[k * BP + jj];
+    const cplx<T> Vk = XS[k * BP + ZC + jj];
+    const cplx<T> Dk = XS[k * BP + 2 * ZC + jj];
     X0[o] = add(ik(kk, Uk), Dk);
     X1[o] = Vk;
   }
@@ -332,9 +349,9 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     const cplx<float> D = mul(sub(xm, xc), conjg(twN[m]));
     a[q] = mk<float>(S.x - D.y, S.y + D.x);
   }
-  xr_pass1<true>(a, t, tw2);
+  xr_pass1<float, true>(a, t, tw2);
   __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
-  xr_pass2<true>(a, t, ex + grp * kXrEx);
+  xr_pass2<float, true>(a, t, ex + grp * kXrEx);
   // a[k1] = x[2n] + i x[2n+1], n = 16 k1 + t
   __syncthreads();  // every exchange read: the outputs reuse their space
   float* zr = ZR + grp * SR + 2 * t;
@@ -399,6 +416,171 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
       phi_out[idx] = gv[i] + phi;
     else
       phi_out[idx] = phi;
+  }
+}
+
+// ---- y pencils: ny = 512, one warp per column ---------------------------------
+// N = 512 = 32 x 16, n = n1 + 32 n2 (n1 < 32, n2 < 16):
+//   pass 1: lane n1 takes the 16-point DFT over n2 and multiplies by
+//           W_512^(n1 k2) (k2 < 16);
+//   exchange: through the column's 16 x 33 padded block (warp-local);
+//   pass 2: lane L = k2 + 16 p (p = 0, 1) holds Y[p + 2 m][k2] (m < 16) and
+//           takes the 16-point DFT over m: the even (p = 0) and odd (p = 1)
+//           halves of the 32-point DFT over n1;
+//   radix 2: lanes L and L ^ 16 combine them (shuffles), E + W_32^j O on
+//           p = 0 and E - W_32^j O on p = 1.
+// Lane L leaves with a[j] = X[16 (j + 16 p) + k2], j < 16.
+constexpr int kYrN = 512;
+constexpr int kYrEx = 16 * 33;  // exchange block of one column (complex)
+
+// ytw[32 k2 + n1] = W_512^(n1 k2) (forward sign), w32[j] = W_32^j.
+template <bool INV>
+__device__ __forceinline__ void yr_fft(cplx<float> (&a)[16], int lane,
+                                       const cplx<float>* __restrict__ ytw,
+                                       const cplx<float>* __restrict__ w32, cplx<float>* ex) {
+  dft16<float, INV>(a);
+#pragma unroll
+  for (int k2 = 1; k2 < 16; ++k2) {
+    cplx<float> w = ytw[32 * k2 + lane];
+    if (INV) w.y = -w.y;
+    a[k2] = mul(a[k2], w);
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < 16; ++k2) ex[k2 * 33 + lane] = a[k2];
+  __syncwarp();
+  const int k2 = lane & 15, p = lane >> 4;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) a[m] = ex[k2 * 33 + p + 2 * m];
+  dft16<float, INV>(a);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    cplx<float> w = w32[j];
+    if (INV) w.y = -w.y;
+    const float ox = __shfl_xor_sync(0xffffffffu, a[j].x, 16);
+    const float oy = __shfl_xor_sync(0xffffffffu, a[j].y, 16);
+    const cplx<float> other = mk<float>(ox, oy);
+    // p = 0 holds E, the partner O; p = 1 holds O, the partner E
+    a[j] = p == 0 ? add(a[j], mul(w, other)) : sub(other, mul(w, a[j]));
+  }
+}
+
+template <int ZC>
+constexpr int yr_min_blocks() { return ZC >= 8 ? 1 : 3; }
+
+// Shared memory of k_fy3 / k_iy3: twiddles, then one region holding in turn
+// the input rows, the columns' exchange blocks and the output rows.
+template <int ZC>
+struct YrSize {
+  static constexpr int B = 2 * ZC;   // columns (warps)
+  static constexpr int BP = B + 1;   // row stride of the row tiles (odd)
+  static constexpr size_t tables = (size_t)(kYrN + 16) * 8;
+  static constexpr size_t rows = (size_t)kYrN * BP * 8;
+  static constexpr size_t ex = (size_t)B * kYrEx * 8;
+  static constexpr size_t total = tables + (rows > ex ? rows : ex);
+};
+
+// k_fy2 FY_DIV for FP32 at ny = 512: d^ = FFTy(X0) + i ky' FFTy(X1).
+// Columns: X0 at ZC levels, X1 at ZC levels.  grid = (ceil(nz/ZC), nx/2 + 1).
+template <int ZC>
+__global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_fy3(
+    GridK g, const cplx<float>* __restrict__ in0, const cplx<float>* __restrict__ in1,
+    const double* __restrict__ kyd, const cplx<float>* __restrict__ twy,
+    cplx<float>* __restrict__ out0) {
+  using SZ = YrSize<ZC>;
+  constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kYrN;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<float>* ytw = reinterpret_cast<cplx<float>*>(smem_dyn);
+  cplx<float>* w32 = ytw + N;
+  cplx<float>* R = reinterpret_cast<cplx<float>*>(smem_dyn + SZ::tables);  // [N][BP]
+  cplx<float>* ex = R;                                                    // B x 16 x 33
+  const int ny = g.ny, nz = g.nz;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < N * B; e += NT) {
+    const int y = e / B, b = e - y * B;
+    const int f = b / ZC, j = b - f * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    copy_or_zero(&R[y * BP + b], (f == 0 ? in0 : in1) + (kx * ny + y) * nz + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  for (int i = tid; i < N; i += NT) ytw[i] = twy[(i & 31) * (i >> 5)];
+  if (tid < 16) w32[tid] = twy[16 * tid];
+  cp_wait<0>();
+  __syncthreads();
+  const int c = tid >> 5, lane = tid & 31;
+  cplx<float> a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a[q] = R[(lane + 32 * q) * BP + c];
+  __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
+  yr_fft<false>(a, lane, ytw, w32, ex + c * kYrEx);
+  __syncthreads();  // every exchange read: the output rows reuse their space
+  const int k2 = lane & 15, p = lane >> 4;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) R[(16 * (j + 16 * p) + k2) * BP + c] = a[j];
+  __syncthreads();
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int ky = e / ZC, j = e - ky * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const float kk = (ky == N / 2) ? 0.0f : (float)kyd[ky];
+    out0[(kx * ny + ky) * nz + z] = add(R[ky * BP + j], ik(kk, R[ky * BP + ZC + j]));
+  }
+}
+
+// k_iy2 for FP32 at ny = 512: phi~ = IFFTy(phi^), psi~ = IFFTy(i ky' phi^).
+// Columns: phi~ at ZC levels, then psi~ (the gather applies i ky').
+template <int ZC>
+__global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_iy3(
+    GridK g, const cplx<float>* __restrict__ in0, const double* __restrict__ kyd,
+    const cplx<float>* __restrict__ twy, cplx<float>* __restrict__ out0,
+    cplx<float>* __restrict__ out1) {
+  using SZ = YrSize<ZC>;
+  constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kYrN;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<float>* ytw = reinterpret_cast<cplx<float>*>(smem_dyn);
+  cplx<float>* w32 = ytw + N;
+  cplx<float>* R = reinterpret_cast<cplx<float>*>(smem_dyn + SZ::tables);  // [N][BP]
+  cplx<float>* ex = R;
+  const int ny = g.ny, nz = g.nz;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int y = e / ZC, j = e - y * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    copy_or_zero(&R[y * BP + j], in0 + (kx * ny + y) * nz + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  for (int i = tid; i < N; i += NT) ytw[i] = twy[(i & 31) * (i >> 5)];
+  if (tid < 16) w32[tid] = twy[16 * tid];
+  cp_wait<0>();
+  __syncthreads();
+  const int c = tid >> 5, lane = tid & 31;
+  const int src = c < ZC ? c : c - ZC;
+  cplx<float> a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int n = lane + 32 * q;
+    a[q] = R[n * BP + src];
+    if (c >= ZC) a[q] = ik(n == N / 2 ? 0.0f : (float)kyd[n], a[q]);  // ky' = 0 at Nyquist
+  }
+  __syncthreads();
+  yr_fft<true>(a, lane, ytw, w32, ex + c * kYrEx);
+  __syncthreads();
+  const int k2 = lane & 15, p = lane >> 4;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) R[(16 * (j + 16 * p) + k2) * BP + c] = a[j];
+  __syncthreads();
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int y = e / ZC, j = e - y * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const int o = (kx * ny + y) * nz + z;
+    out0[o] = R[y * BP + j];
+    out1[o] = R[y * BP + ZC + j];
   }
 }
 

@@ -114,7 +114,7 @@ def _vortex_case(nx, ny, nz):
                              z_peak=6e3, width_z=math.sqrt(2.0) * 2e3), noise_seed=3)
 
 
-@pytest.mark.parametrize("shape", [(96, 72, 16), (512, 40, 16)])
+@pytest.mark.parametrize("shape", [(96, 72, 16), (512, 40, 16), (48, 512, 16)])
 def test_fp32_steps_track_fp64(shape):
     """Ten full steps of the vortex configuration in FP32, FP32 with one
     correction per step, and FP64: per-field error of the single-precision
@@ -169,46 +169,54 @@ def test_refinement_controls():
         p64.refine(u, u.clone(), w, u.clone())
 
 
-@pytest.mark.parametrize("nz", [16, 13])
-def test_register_pencils_match_stockham(nz, monkeypatch):
+@pytest.mark.parametrize("nx, ny, nz", [(512, 40, 16), (512, 40, 13), (64, 512, 16),
+                                        (48, 512, 13)])
+def test_register_pencils_match_stockham(nx, ny, nz, monkeypatch):
     """At nx = 512 the FP32 x pencils run the register-resident FFT
-    (xreg.cuh); with ORACLE_B200_FX3_ZC=0 and ORACLE_B200_IX3_ZC=0 the plan
-    keeps the shared-memory Stockham kernels.  Against the FP64 projection of
-    the same input, the
-    register path is as accurate as the Stockham path, field by field; u and
-    v of the two agree to a few FP32 ulp of the wind.  nz = 13 leaves a
+    (xreg.cuh), the defect correction's FP64 residual transform included,
+    and at ny = 512 the y pencils; with ORACLE_B200_FX3_ZC,
+    ORACLE_B200_IX3_ZC, ORACLE_B200_FXD3_ZC and ORACLE_B200_FY3_ZC at 0 the
+    plan keeps the shared-memory Stockham kernels.  Against the FP64
+    projection of the same input, the register path is as accurate as the
+    Stockham path, field by field, before and after one correction pass; u
+    and v of the two agree to a few FP32 ulp of the wind.  nz = 13 leaves a
     partial z-chunk.  (The staged form runs in test_fp32_steps_track_fp64 at
     nx = 512.)"""
     from oraclev8_b200._plan import Plan, PlanSpec
-    nx, ny = 512, 40
     Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
     z, rho0, th0 = O.build_base_state(nz, Lz)
     mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
                                     projection=True))
-    monkeypatch.setenv("ORACLE_B200_FX3_ZC", "0")
-    monkeypatch.setenv("ORACLE_B200_IX3_ZC", "0")
+    knobs = ("ORACLE_B200_FX3_ZC", "ORACLE_B200_IX3_ZC", "ORACLE_B200_FXD3_ZC",
+             "ORACLE_B200_FY3_ZC")
+    for k in knobs:
+        monkeypatch.setenv(k, "0")
     p_ref = mk("fp32")
-    monkeypatch.delenv("ORACLE_B200_FX3_ZC")
-    monkeypatch.delenv("ORACLE_B200_IX3_ZC")
+    for k in knobs:
+        monkeypatch.delenv(k)
     p_new = mk("fp32")
     p64 = mk("fp64")
     u, v, w = _smooth_state(nx, ny, nz, seed=7 + nz)
     f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
-    outs = []
+    outs, refined = [], []
     for p, dt in ((p64, torch.float64), (p_ref, torch.float32), (p_new, torch.float32)):
         uu, vv, ww = (dev(f32(a), dt) for a in (u, v, w))
         phi = torch.empty_like(uu)
         p.project(uu, vv, ww, phi)
         outs.append([host(a).astype(np.float64) for a in (uu, vv, ww, phi)])
+        if dt == torch.float32:
+            p.refine(uu, vv, ww, phi)
+            refined.append([host(a).astype(np.float64) for a in (uu, vv, ww, phi)])
     wind = max(float(np.max(np.abs(outs[0][0]))), float(np.max(np.abs(outs[0][1]))))
-    for i, name in enumerate(("u", "v", "w", "phi")):
-        r64, ref, new = outs[0][i], outs[1][i], outs[2][i]
-        scale = float(np.max(np.abs(r64)))
-        e_ref = float(np.max(np.abs(ref - r64))) / scale
-        e_new = float(np.max(np.abs(new - r64))) / scale
-        d = float(np.max(np.abs(new - ref)))
-        print(f"nz {nz} {name}: error vs FP64 stockham {e_ref:.3e} register {e_new:.3e}; "
-              f"max |register - stockham| {d:.3e}")
-        assert e_new <= 1.5 * e_ref + 1e-7, (name, e_new, e_ref)
-        if name in ("u", "v"):
-            assert d <= 1e-6 * wind, (name, d)
+    for stage, (ref_f, new_f) in (("plain", (outs[1], outs[2])), ("refined", refined)):
+        for i, name in enumerate(("u", "v", "w", "phi")):
+            r64, ref, new = outs[0][i], ref_f[i], new_f[i]
+            scale = float(np.max(np.abs(r64)))
+            e_ref = float(np.max(np.abs(ref - r64))) / scale
+            e_new = float(np.max(np.abs(new - r64))) / scale
+            d = float(np.max(np.abs(new - ref)))
+            print(f"nz {nz} {stage} {name}: error vs FP64 stockham {e_ref:.3e} "
+                  f"register {e_new:.3e}; max |register - stockham| {d:.3e}")
+            assert e_new <= 1.5 * e_ref + 1e-7, (stage, name, e_new, e_ref)
+            if name in ("u", "v"):
+                assert d <= 1e-6 * wind, (stage, name, d)
