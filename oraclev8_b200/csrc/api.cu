@@ -590,17 +590,30 @@ size_t x2_smem(int kind, int zc, int nx) {
 
 // Largest z-chunk in {8, 4, 2, 1} (no larger than nz) whose tile fits the
 // per-CTA budget of the kernels' target occupancy, else the largest that fits
-// one CTA; 0 when none fits.
+// one CTA; 0 when none fits.  The chunk is then raised, where one CTA still
+// holds it, until a row's run of state is 16 bytes (4 FP32 / 2 FP64 levels):
+// the x pencils' time follows the sector operations per byte more than the
+// CTAs per SM.  At 1024^2 x 80 the FP64 step took 98.3 ms per step with
+// 1-level inverse chunks at two CTAs per SM and 79.5 ms with 2-level chunks at
+// one; the FP32-refined step 60.9 ms with 2-level chunks and 46.2 ms with 4.
 template <class T, class TS>
 int pick_x2_zc(int kind, int nx, int nz) {
   if (const char* e = getenv("ORACLE_B200_X2"))
     if (atoi(e) == 0) return 0;
-  for (size_t cap : {x2_smem_budget<T>(kind), kSmemMax})
-    for (int zc : {8, 4, 2, 1}) {
-      if (zc > 1 && zc > nz) continue;
-      if (x2_smem<T, TS>(kind, zc, nx) <= cap) return zc;
+  int zc = 0;
+  for (size_t cap : {x2_smem_budget<T>(kind), kSmemMax}) {
+    for (int z : {8, 4, 2, 1}) {
+      if (z > 1 && z > nz) continue;
+      if (x2_smem<T, TS>(kind, z, nx) <= cap) {
+        zc = z;
+        break;
+      }
     }
-  return 0;
+    if (zc) break;
+  }
+  const int zmin = std::min(nz, 16 / (int)sizeof(TS));
+  while (zc && zc < zmin && zc < 8 && x2_smem<T, TS>(kind, 2 * zc, nx) <= kSmemMax) zc *= 2;
+  return zc;
 }
 
 // bh: the step's half-level buoyancy field (STAGE only)
