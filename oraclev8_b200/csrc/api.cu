@@ -201,6 +201,10 @@ struct OraclePlan {
     cudaEvent_t a, b;
   };
   std::vector<Mark> marks;
+  // timing events, created when profiling is switched on and reused: a
+  // profiled launch records two of them and creates none
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_next = 0;
 };
 
 namespace {
@@ -268,10 +272,7 @@ int upload(OraclePlan* p, double** out, const double* host, size_t n) {
 // work queued on `st` before this point is done) and free the descriptor.
 void release_plan(OraclePlan* p, cudaStream_t st) {
   delete p->dbl;  // owns no allocations: its buffers are in p->allocs
-  for (auto& m : p->marks) {
-    cudaEventDestroy(m.a);
-    cudaEventDestroy(m.b);
-  }
+  for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
   for (void* q : p->allocs) cudaFreeAsync(q, st);
   if (p->astream) cudaStreamDestroy(p->astream);
   if (p->aux) cudaStreamDestroy(p->aux);
@@ -528,6 +529,17 @@ ThomasK thomas_args(const OraclePlan* p) {
 
 // Brackets one kernel launch: counts it and, when profiling is on, records a
 // pair of events on the launch stream so per-class device time can be summed.
+// Next event of the plan's timing pool (grown only when a profiled run
+// outlasts the events created up front).
+cudaEvent_t pool_event(OraclePlan* p) {
+  if (p->ev_next == p->ev_pool.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    p->ev_pool.push_back(e);
+  }
+  return p->ev_pool[p->ev_next++];
+}
+
 struct Launch {
   OraclePlan* p;
   cudaStream_t st;
@@ -536,13 +548,13 @@ struct Launch {
   Launch(OraclePlan* p_, int cls_, cudaStream_t st_) : p(p_), st(st_), cls(cls_) {
     p->launches++;
     if (p->profiling) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
+      a = pool_event(p);
+      b = pool_event(p);
       cudaEventRecord(a, st);
     }
   }
   ~Launch() {
-    if (a) {
+    if (a && b) {
       cudaEventRecord(b, st);
       p->marks.push_back({cls, a, b});
     }
@@ -2026,11 +2038,17 @@ int oracle_b200_refine(OraclePlan* p, void* u, void* v, void* w, void* phi, void
 
 int oracle_b200_profile(OraclePlan* p, int enable) {
   if (int rc = check_plan(p)) return rc;
-  for (auto& m : p->marks) {
-    cudaEventDestroy(m.a);
-    cudaEventDestroy(m.b);
-  }
+  // the previous marks' events may still be pending on the GPU
+  for (auto& m : p->marks) OB_CUDA(cudaEventSynchronize(m.b));
   p->marks.clear();
+  p->ev_next = 0;
+  // events for a few hundred steps' launches, created before any timing
+  constexpr size_t kPoolUpFront = 16384;
+  while (enable && p->ev_pool.size() < kPoolUpFront) {
+    cudaEvent_t e = nullptr;
+    OB_CUDA(cudaEventCreate(&e));
+    p->ev_pool.push_back(e);
+  }
   p->profiling = enable ? 1 : 0;
   return OB_OK;
 }

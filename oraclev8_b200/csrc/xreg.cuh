@@ -287,13 +287,27 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     }
   }
   cp_commit();
-  for (int e = tid; e < N * ZC; e += NT) {
-    const int x = e / ZC, j = e - x * ZC;
-    const int z = z0 + j;
-    const bool ok = z < nz;
-    const int gi = (x * ny + y) * nz + (ok ? z : 0);
-    copy_or_zero(&SU[e], u_in + gi, ok);
-    copy_or_zero(&SV[e], v_in + gi, ok);
+  // u, v: 16-byte copies (ZC / 4 per row) where the chunk is whole and the
+  // rows start on 16 bytes; 4-byte copies otherwise
+  const bool vec = ZC >= 4 && z0 + ZC <= nz && (nz & 3) == 0 &&
+                   ((reinterpret_cast<size_t>(u_in) | reinterpret_cast<size_t>(v_in)) & 15) == 0;
+  if (vec) {
+    constexpr int Q = ZC >= 4 ? ZC / 4 : 1;
+    for (int e = tid; e < N * Q; e += NT) {
+      const int x = e / Q, q = e - x * Q;
+      const int gi = (x * ny + y) * nz + z0 + 4 * q;
+      cp_async(&SU[x * ZC + 4 * q], u_in + gi, 16);
+      cp_async(&SV[x * ZC + 4 * q], v_in + gi, 16);
+    }
+  } else {
+    for (int e = tid; e < N * ZC; e += NT) {
+      const int x = e / ZC, j = e - x * ZC;
+      const int z = z0 + j;
+      const bool ok = z < nz;
+      const int gi = (x * ny + y) * nz + (ok ? z : 0);
+      copy_or_zero(&SU[e], u_in + gi, ok);
+      copy_or_zero(&SV[e], v_in + gi, ok);
+    }
   }
   for (int e = tid; e < N * (ZC + 1); e += NT) {
     const int x = e / (ZC + 1), j = e - x * (ZC + 1);
@@ -360,23 +374,28 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     *reinterpret_cast<float2*>(zr + 32 * k1) = make_float2(a[k1].x, a[k1].y);
   // the global values the correction reads besides the tiles (STAGE: b_half;
   // IX_REFINE: phi) are loaded here, all at once, so that their latency
-  // overlaps the barrier instead of each correction step
-  constexpr int NE = (N * ZC + NT - 1) / NT;  // correction elements per thread
-  float gv[NE], gt[NE];
+  // overlaps the barrier instead of each correction step.  The correction
+  // takes two adjacent levels (z, z + 1) of a row per thread.
+  constexpr int NPR = N * ZC / 2;             // level pairs of the tile
+  constexpr int NP = (NPR + NT - 1) / NT;     // pairs per thread
+  float g0[NP], g1[NP], gt[NP];
   if (STAGE || MODE == IX_REFINE) {
 #pragma unroll
-    for (int i = 0; i < NE; ++i) {
+    for (int i = 0; i < NP; ++i) {
       const int e = tid + i * NT;
-      const int x = e / ZC, j = e - x * ZC;
+      const int x = e / (ZC / 2), j = 2 * (e - x * (ZC / 2));
       const int z = z0 + j;
-      gv[i] = gt[i] = 0.0f;
-      if (e < N * ZC && z < nz) {
+      g0[i] = g1[i] = gt[i] = 0.0f;
+      if (e < NPR && z < nz) {
         const int col = x * ny + y;
         if (STAGE) {
-          gv[i] = bh[col * (nz + 1) + z];
-          if (z == nz - 1) gt[i] = bh[col * (nz + 1) + nz];
+          const float* r = bh + col * (nz + 1);
+          g0[i] = r[z];
+          if (z + 1 < nz) g1[i] = r[z + 1];
+          if (z + 2 >= nz) gt[i] = r[nz];  // the lid (level nz) follows this pair
         } else {
-          gv[i] = phi_out[col * nz + z];
+          g0[i] = phi_out[col * nz + z];
+          if (z + 1 < nz) g1[i] = phi_out[col * nz + z + 1];
         }
       }
     }
@@ -384,38 +403,63 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
   cp_wait<0>();
   __syncthreads();
 
-  // 3. velocity correction; consecutive threads on consecutive levels
+  // 3. velocity correction, levels (z, z + 1) of row x per thread;
+  //    consecutive threads on consecutive pairs
   const float dzt = (float)g.dz;
+  const bool st2 = (nz & 1) == 0 && ((reinterpret_cast<size_t>(u_out) |
+                                      reinterpret_cast<size_t>(v_out) |
+                                      reinterpret_cast<size_t>(phi_out)) & 7) == 0;
 #pragma unroll
-  for (int i = 0; i < NE; ++i) {
+  for (int i = 0; i < NP; ++i) {
     const int e = tid + i * NT;
-    if (e >= N * ZC) break;
-    const int x = e / ZC, j = e - x * ZC;
+    if (e >= NPR) break;
+    const int x = e / (ZC / 2), j = 2 * (e - x * (ZC / 2));
     const int z = z0 + j;
     if (z >= nz) continue;
+    const bool two = z + 1 < nz;
     const int col = x * ny + y;
     const int idx = col * nz + z;
-    const float phi = ZR[(j + 1) * SR + x];
-    const float phib = ZR[j * SR + x];
-    const float gx = ZR[(ZC + 1 + j) * SR + x];
-    const float gy = ZR[(2 * ZC + 1 + j) * SR + x];
-    const float gz = (z >= 1) ? drn(srn(phi, phib), dzt) : 0.0f;
+    const float phb = ZR[j * SR + x];  // level z - 1
+    const float ph0 = ZR[(j + 1) * SR + x];
+    const float ph1 = ZR[(j + 2) * SR + x];
+    const float gx0 = ZR[(ZC + 1 + j) * SR + x], gx1 = ZR[(ZC + 2 + j) * SR + x];
+    const float gy0 = ZR[(2 * ZC + 1 + j) * SR + x], gy1 = ZR[(2 * ZC + 2 + j) * SR + x];
+    const float gz0 = (z >= 1) ? drn(srn(ph0, phb), dzt) : 0.0f;
+    const float gz1 = drn(srn(ph1, ph0), dzt);
+    const float2 su = *reinterpret_cast<const float2*>(&SU[x * ZC + j]);
+    const float2 sv = *reinterpret_cast<const float2*>(&SV[x * ZC + j]);
     const int sw = x * (ZC + 1) + j;
-    const int wi = col * (nz + 1) + z;
-    float wcz = SW[sw], wt = 0.0f;
-    if (STAGE) wcz = (float)arn((double)wcz, mrn(sdt, (double)gv[i]));
-    if (z == nz - 1) {
-      wt = SW[sw + 1];
-      if (STAGE) wt = (float)arn((double)wt, mrn(sdt, (double)gt[i]));
+    float w0 = SW[sw], w1 = SW[sw + 1];
+    if (STAGE) {
+      w0 = (float)arn((double)w0, mrn(sdt, (double)g0[i]));
+      w1 = (float)arn((double)w1, mrn(sdt, (double)g1[i]));
     }
-    u_out[idx] = SU[e] - gx;
-    v_out[idx] = SV[e] - gy;
-    w_out[wi] = wcz - gz;
-    if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[wi + 1] = wt;
-    if (MODE == IX_REFINE)
-      phi_out[idx] = gv[i] + phi;
-    else
-      phi_out[idx] = phi;
+    const int wi = col * (nz + 1) + z;
+    const float p0 = (MODE == IX_REFINE) ? g0[i] + ph0 : ph0;
+    const float p1 = (MODE == IX_REFINE) ? g1[i] + ph1 : ph1;
+    if (two && st2) {
+      *reinterpret_cast<float2*>(&u_out[idx]) = make_float2(su.x - gx0, su.y - gx1);
+      *reinterpret_cast<float2*>(&v_out[idx]) = make_float2(sv.x - gy0, sv.y - gy1);
+      *reinterpret_cast<float2*>(&phi_out[idx]) = make_float2(p0, p1);
+    } else {
+      u_out[idx] = su.x - gx0;
+      v_out[idx] = sv.x - gy0;
+      phi_out[idx] = p0;
+      if (two) {
+        u_out[idx + 1] = su.y - gx1;
+        v_out[idx + 1] = sv.y - gy1;
+        phi_out[idx + 1] = p1;
+      }
+    }
+    w_out[wi] = w0 - gz0;
+    if (two) w_out[wi + 1] = w1 - gz1;
+    // the lid, level nz, after the top level nz - 1 of the column
+    const int zt = two ? z + 1 : z;
+    if (zt == nz - 1 && (STAGE || w_out != w_in)) {
+      float wt = SW[x * (ZC + 1) + (nz - z0)];
+      if (STAGE) wt = (float)arn((double)wt, mrn(sdt, (double)gt[i]));
+      w_out[col * (nz + 1) + nz] = wt;
+    }
   }
 }
 
