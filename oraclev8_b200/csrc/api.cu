@@ -191,6 +191,7 @@ struct OraclePlan {
   unsigned char* lw_flag = nullptr;
   int n_lw = 0;
   float* tcoef = nullptr;  // FP32 plans: (negs, rho, a, c) per level, as float4
+  float* gth = nullptr;    // FP32 plans: g / theta0 per level
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // launch accounting and optional per-kernel-class event timing
@@ -1202,7 +1203,7 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
     if (p->Bh && (p->zc2_fxs || p->zc2_ix)) {
       const long ncol = (long)p->g.nx * p->g.ny;
       { Launch L_(p, 7, st); k_bhalf<T><<<(unsigned)std::min<long>((ncol + 7) / 8, 65535), 256, 0, st>>>(
-          p->g, ath, p->theta0, (T*)p->Bh); }
+          p->g, ath, p->theta0, p->gth, (T*)p->Bh); }
       OB_LAUNCHED();
       bh = (const T*)p->Bh;
     }
@@ -1823,6 +1824,11 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     }
     if ((rc = dalloc(p, &p->tcoef, coef.size() * sizeof(float)))) return bail(rc);
     OB_CUDA(cudaMemcpyAsync(p->tcoef, coef.data(), coef.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, p->astream));
+    std::vector<float> gth(nz);
+    for (int k = 0; k < nz; ++k) gth[k] = (float)(kGravity / comp->theta0[k]);
+    if ((rc = dalloc(p, &p->gth, gth.size() * sizeof(float)))) return bail(rc);
+    OB_CUDA(cudaMemcpyAsync(p->gth, gth.data(), gth.size() * sizeof(float),
                             cudaMemcpyHostToDevice, p->astream));
     // the vectors must outlive the copies: pageable copies are staged before
     // the call returns

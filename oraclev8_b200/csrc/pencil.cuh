@@ -435,16 +435,30 @@ __global__ void __launch_bounds__(kPencilThreads, pencil_min_blocks<T>()) k_iy2(
 // of theta' (equation_set.py:255-263, staggering.py:201-208), with the
 // operation order of bhalf(): the fast stages of a step all use the buoyancy
 // of the same theta', so it is formed once per step.  One warp per column.
+// gth (single-precision plans): g / theta0 per level as float; the field is
+// then formed in float, 0.5 (gth[k-1] th[k-1] + gth[k] th[k]), without the
+// double divisions.
 template <class T>
 __global__ void __launch_bounds__(256) k_bhalf(GridK g, const T* __restrict__ th,
                                                const double* __restrict__ theta0,
+                                               const float* __restrict__ gth,
                                                T* __restrict__ bh) {
   const int lane = threadIdx.x & 31;
   const long ncol = (long)g.nx * g.ny;
   const int nz = g.nz;
   for (long c = (long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < ncol;
-       c += (long)gridDim.x * (blockDim.x / 32))
-    for (int k = lane; k <= nz; k += 32) bh[c * (nz + 1) + k] = (T)bhalf(th + c * nz, k, nz, theta0);
+       c += (long)gridDim.x * (blockDim.x / 32)) {
+    const T* thc = th + c * nz;
+    if (sizeof(T) == 4 && gth) {
+      for (int k = lane; k <= nz; k += 32)
+        bh[c * (nz + 1) + k] =
+            (k <= 0 || k >= nz)
+                ? (T)0
+                : (T)(0.5f * (gth[k - 1] * (float)thc[k - 1] + gth[k] * (float)thc[k]));
+    } else {
+      for (int k = lane; k <= nz; k += 32) bh[c * (nz + 1) + k] = (T)bhalf(thc, k, nz, theta0);
+    }
+  }
 }
 
 }  // namespace ob

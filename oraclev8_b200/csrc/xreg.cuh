@@ -203,18 +203,34 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
   }
   __syncthreads();
 
-  // 4. X0 = i kx' U + D, X1 = V (consecutive threads on consecutive levels)
-  for (int e = tid; e < (M + 1) * ZC; e += NT) {
-    const int k = e / ZC, jj = e - k * ZC;
+  // 4. X0 = i kx' U + D, X1 = V, two adjacent levels per thread
+  //    (consecutive threads on consecutive pairs; 16-byte stores of FP32
+  //    pairs where the levels start on an even index)
+  const bool st2 = sizeof(T) == 4 && (nz & 1) == 0 &&
+                   ((reinterpret_cast<size_t>(X0) | reinterpret_cast<size_t>(X1)) & 15) == 0;
+  for (int e = tid; e < (M + 1) * (ZC / 2); e += NT) {
+    const int k = e / (ZC / 2), jj = 2 * (e - k * (ZC / 2));
     const int z = z0 + jj;
     if (z >= nz) continue;
+    const bool two = z + 1 < nz;
     const T kk = (k == M) ? (T)0 : (T)kxd[k];
     const int o = (k * ny + y) * nz + z;
-    const cplx<T> Uk = XS[k * BP + jj];
-    const cplx<T> Vk = XS[k * BP + ZC + jj];
-    const cplx<T> Dk = XS[k * BP + 2 * ZC + jj];
-    X0[o] = add(ik(kk, Uk), Dk);
-    X1[o] = Vk;
+    const cplx<T> x00 = add(ik(kk, XS[k * BP + jj]), XS[k * BP + 2 * ZC + jj]);
+    const cplx<T> x01 = add(ik(kk, XS[k * BP + jj + 1]), XS[k * BP + 2 * ZC + jj + 1]);
+    const cplx<T> x10 = XS[k * BP + ZC + jj], x11 = XS[k * BP + ZC + jj + 1];
+    if constexpr (sizeof(T) == 4) {
+      if (two && st2) {
+        *reinterpret_cast<float4*>(&X0[o]) = make_float4(x00.x, x00.y, x01.x, x01.y);
+        *reinterpret_cast<float4*>(&X1[o]) = make_float4(x10.x, x10.y, x11.x, x11.y);
+        continue;
+      }
+    }
+    X0[o] = x00;
+    X1[o] = x10;
+    if (two) {
+      X0[o + 1] = x01;
+      X1[o + 1] = x11;
+    }
   }
 }
 
