@@ -158,6 +158,7 @@ struct OraclePlan {
   // projection's forward and inverse kernels, and the FP64 residual transform
   int zc3_fx = 0, zc3_ix = 0, zc3_fxd = 0;
   int zc3_fy = 0;  // register-resident FP32 y pencils (ny = 512): z-chunk, 0 = off
+  int slow_xw = 1;  // FP32 slow tendency marching along x (ORACLE_B200_SLOW_XW=0: gather form)
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -1136,9 +1137,15 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
               const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
   dim3 blk(32, 8);
   dim3 grd((p->g.ny + 7) / 8, p->g.nx);
-  if constexpr (sizeof(T) == 4)
-    { Launch L_(p, 5, st); k_slow_f32<OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
-                                          (const T*)p->Dv, uo, vo, wo, tho); }
+  if constexpr (sizeof(T) == 4) {
+    // the x-marching form where the grid tiles it; the gather form otherwise
+    if (p->slow_xw && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
+      { Launch L_(p, 5, st); k_slow_xw<OUT><<<dim3(p->g.ny / 8, p->g.nx / KXW), blk, 0, st>>>(
+            p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du, (const T*)p->Dv, uo, vo, wo, tho); }
+    else
+      { Launch L_(p, 5, st); k_slow_f32<OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                            (const T*)p->Dv, uo, vo, wo, tho); }
+  }
   else
     { Launch L_(p, 5, st); k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
                                         (const T*)p->Dv, uo, vo, wo, tho); }
@@ -1762,6 +1769,7 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     p->zc2_fy = p->prec == OB_PREC_F64 ? pick_y2_zc<double>(ny, nz) : pick_y2_zc<float>(ny, nz);
     p->zc2_iy = p->zc2_fy;
   }
+  if (const char* e = getenv("ORACLE_B200_SLOW_XW")) p->slow_xw = atoi(e) != 0;
   if (p->prec == OB_PREC_F32 && ny == kYrN) {
     p->zc3_fy = nz >= 4 ? 4 : 2;
     if (const char* e = getenv("ORACLE_B200_FY3_ZC")) p->zc3_fy = atoi(e);

@@ -1145,6 +1145,252 @@ __global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask,
   }
 }
 
+// k_slow_f32 marching along x.  A CTA covers TJ = 8 rows j, a z-chunk of 32
+// levels at a time, and KXW consecutive x cells.  Each thread keeps, for its
+// (j, k), a 7-point window of u, v, theta', w along x in registers (the x
+// stencils' points; one new column loaded per step), and the CTA shares, per
+// x step, a plane of the four fields over its rows plus three halo rows on
+// either side and one halo level above and below (the y and z neighbours),
+// double-buffered so that one barrier per step suffices.  Global loads per
+// cell: about 7, against about 48 gathered loads of k_slow_f32, whose x
+// neighbours come from the columns other CTAs own (seven L2 reads of every
+// value).  Same arithmetic, terms and order as k_slow_f32.
+// Requires ny % 8 == 0 and nx % KXW == 0.  grid = (ny / 8, nx / KXW),
+// block = (32, 8).
+constexpr int KXW = 16;
+constexpr int kXwRows = 8 + 6;   // plane rows: j0-3 .. j0+10
+constexpr int kXwCols = 32 + 2;  // plane columns: k0-1 .. k0+32
+
+__device__ __forceinline__ float ws5_win(const float (&q)[7], float a, float inv60d) {
+  // q[r] = value at offset r - 3
+  const bool up = a >= 0.0f;
+  const float m3 = up ? q[0] : q[6], m2 = up ? q[1] : q[5], m1 = up ? q[2] : q[4];
+  const float p1 = up ? q[4] : q[2], p2 = up ? q[5] : q[1];
+  const float d = -2.0f * m3 + 15.0f * m2 - 60.0f * m1 + 20.0f * q[3] + 30.0f * p1 - 3.0f * p2;
+  return (up ? d : -d) * inv60d;
+}
+// the same over plane column c: rows r0-3 .. r0+3, row stride kXwCols
+__device__ __forceinline__ float ws5_col(const float* P, int r0, int c, float a, float inv60d) {
+  const bool up = a >= 0.0f;
+  const int s = up ? kXwCols : -kXwCols;
+  const float* q = P + r0 * kXwCols + c;
+  const float d = -2.0f * q[-3 * s] + 15.0f * q[-2 * s] - 60.0f * q[-s] + 20.0f * q[0] +
+                  30.0f * q[s] - 3.0f * q[2 * s];
+  return (up ? d : -d) * inv60d;
+}
+
+template <int OUTMODE>
+__global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, double dts_d,
+                                                    const float* __restrict__ u,
+                                                    const float* __restrict__ v,
+                                                    const float* __restrict__ w,
+                                                    const float* __restrict__ th,
+                                                    const float* __restrict__ dmp_u,
+                                                    const float* __restrict__ dmp_v,
+                                                    float* __restrict__ uo, float* __restrict__ vo,
+                                                    float* __restrict__ wo,
+                                                    float* __restrict__ tho) {
+  __shared__ float plane[2][4][kXwRows * kXwCols];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nzw = nz + 1;
+  const int lane = threadIdx.x, row = threadIdx.y;
+  const int tid = row * 32 + lane;
+  const int j0 = blockIdx.x * 8, j = j0 + row;
+  const int i0 = blockIdx.y * KXW;
+  const int r0 = row + 3;  // own plane row
+  const bool adv = (mask & 1) && s.adv;
+  const bool cor = (mask & 2) && s.cor;
+  const bool dmp = (mask & 4) && s.damp;
+  const bool heat = (mask & 8) && s.heat;
+  const bool ws5 = (s.adv == 2);
+  const float dts = (float)dts_d;
+  const float inv60dx = (float)s.inv60dx, inv60dy = (float)s.inv60dy;
+  const float inv2dx = (float)s.inv2dx, inv2dy = (float)s.inv2dy;
+  const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
+  const float f = cor ? (float)((s.cor == 2) ? s.fy[j] : s.f0) : 0.0f;
+  const float u_env = (float)s.u_env, v_env = (float)s.v_env;
+  // halo row this thread loads (rows 0-2: j0-3..j0-1, rows 5-7: j0+8..j0+10)
+  const int hrow = row < 3 ? row : (row >= 5 ? row + 6 : -1);
+  int jh = j0 - 3 + (hrow < 0 ? 0 : hrow);
+  jh += (jh < 0) ? ny : 0;
+  jh -= (jh >= ny) ? ny : 0;
+  // k-halo value this thread loads: field kf, plane row kr, end ke
+  const int kf = tid / 28, krem = tid - kf * 28, kr = krem >> 1, ke = krem & 1;
+  int jk = j0 - 3 + kr;
+  jk += (jk < 0) ? ny : 0;
+  jk -= (jk >= ny) ? ny : 0;
+  // field f: 0 u, 1 v, 2 theta', 3 w (nz + 1 levels)
+  auto fptr = [&](int f_) { return f_ == 0 ? u : (f_ == 1 ? v : th); };
+
+  for (int k0 = 0; k0 < nz; k0 += 32) {
+    const int k = k0 + lane;
+    const bool kin = k < nz;
+    auto at = [&](int ii, int jj, int f_) -> float {  // cell (ii, jj, k) of field f_
+      return f_ < 3 ? fptr(f_)[(ii * ny + jj) * nz + k] : w[(ii * ny + jj) * nzw + k];
+    };
+    // the global values of step x = ii: the window's new column (x + 3), the
+    // halo row's four fields and the level-halo value at x (software
+    // pipelined: loaded one step ahead of their use)
+    float nu, nv, nt, nw, hv[4], kv;
+    auto load_step = [&](int ii) {
+      int in = ii + 3;
+      in -= (in >= nx) ? nx : 0;
+      nu = kin ? at(in, j, 0) : 0.0f;
+      nv = kin ? at(in, j, 1) : 0.0f;
+      nt = kin ? at(in, j, 2) : 0.0f;
+      nw = kin ? at(in, j, 3) : 0.0f;
+      if (hrow >= 0) {
+#pragma unroll
+        for (int f_ = 0; f_ < 4; ++f_) {
+          float val = 0.0f;
+          if (kin) val = at(ii, jh, f_);
+          else if (f_ == 3 && k == nz) val = w[(ii * ny + jh) * nzw + nz];
+          hv[f_] = val;
+        }
+      }
+      kv = 0.0f;
+      if (tid < 4 * 28) {
+        const int kk = ke ? k0 + 32 : k0 - 1;
+        const int lim = kf < 3 ? nz : nzw;
+        if (kk >= 0 && kk < lim)
+          kv = kf < 3 ? fptr(kf)[(ii * ny + jk) * nz + kk] : w[(ii * ny + jk) * nzw + kk];
+      }
+    };
+    // prefill the windows with x = i0-3 .. i0+2
+    float qu[7], qv[7], qt[7], qw[7];
+#pragma unroll
+    for (int r = 1; r < 7; ++r) {
+      int ii = i0 - 4 + r;
+      ii += (ii < 0) ? nx : 0;
+      qu[r] = kin ? at(ii, j, 0) : 0.0f;
+      qv[r] = kin ? at(ii, j, 1) : 0.0f;
+      qt[r] = kin ? at(ii, j, 2) : 0.0f;
+      qw[r] = kin ? at(ii, j, 3) : 0.0f;
+    }
+    load_step(i0);
+    for (int step = 0; step < KXW; ++step) {
+      const int i = i0 + step;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        qu[r] = qu[r + 1];
+        qv[r] = qv[r + 1];
+        qt[r] = qt[r + 1];
+        qw[r] = qw[r + 1];
+      }
+      qu[6] = nu;
+      qv[6] = nv;
+      qt[6] = nt;
+      qw[6] = nw;
+      // this step's plane: own row from the window centres, halo rows and
+      // levels from the values loaded one step ahead (the lid w at level nz
+      // included)
+      float* P = &plane[step & 1][0][0];
+      const int c = lane + 1;
+      P[0 * kXwRows * kXwCols + r0 * kXwCols + c] = qu[3];
+      P[1 * kXwRows * kXwCols + r0 * kXwCols + c] = qv[3];
+      P[2 * kXwRows * kXwCols + r0 * kXwCols + c] = qt[3];
+      P[3 * kXwRows * kXwCols + r0 * kXwCols + c] =
+          kin ? qw[3] : (k == nz ? w[(i * ny + j) * nzw + nz] : 0.0f);
+      if (hrow >= 0) {
+#pragma unroll
+        for (int f_ = 0; f_ < 4; ++f_) P[f_ * kXwRows * kXwCols + hrow * kXwCols + c] = hv[f_];
+      }
+      if (tid < 4 * 28) P[kf * kXwRows * kXwCols + kr * kXwCols + (ke ? kXwCols - 1 : 0)] = kv;
+      if (step + 1 < KXW) load_step(i + 1);
+      __syncthreads();
+      if (kin) {
+        const float* Pu = P;
+        const float* Pv = P + kXwRows * kXwCols;
+        const float* Pt = P + 2 * kXwRows * kXwCols;
+        const float* Pw = P + 3 * kXwRows * kXwCols;
+        const int pc = r0 * kXwCols + c;
+        const int col = i * ny + j;
+        const int o = col * nz + k;
+        const int ow = col * nzw + k;
+        const float uc = qu[3], vc = qv[3], thc = qt[3];
+        float tu = 0.0f, tv = 0.0f, tt = 0.0f;
+        if (adv) {
+          const float wc = 0.5f * (Pw[pc] + Pw[pc + 1]);
+          float czu, czv, czt;
+          if (k == 0) {
+            czu = (Pu[pc + 1] - uc) * invdz;
+            czv = (Pv[pc + 1] - vc) * invdz;
+            czt = (Pt[pc + 1] - thc) * invdz;
+          } else if (k == nz - 1) {
+            czu = (uc - Pu[pc - 1]) * invdz;
+            czv = (vc - Pv[pc - 1]) * invdz;
+            czt = (thc - Pt[pc - 1]) * invdz;
+          } else {
+            czu = (Pu[pc + 1] - Pu[pc - 1]) * inv2dz;
+            czv = (Pv[pc + 1] - Pv[pc - 1]) * inv2dz;
+            czt = (Pt[pc + 1] - Pt[pc - 1]) * inv2dz;
+          }
+          float xu, yu, xv, yv, xt, yt;
+          if (ws5) {
+            xt = ws5_win(qt, uc, inv60dx);
+            yt = ws5_col(Pt, r0, c, vc, inv60dy);
+            xu = ws5_win(qu, uc, inv60dx);
+            yu = ws5_col(Pu, r0, c, vc, inv60dy);
+            xv = ws5_win(qv, uc, inv60dx);
+            yv = ws5_col(Pv, r0, c, vc, inv60dy);
+          } else {
+            xt = (qt[4] - qt[2]) * inv2dx;
+            yt = (Pt[pc + kXwCols] - Pt[pc - kXwCols]) * inv2dy;
+            xu = (qu[4] - qu[2]) * inv2dx;
+            yu = (Pu[pc + kXwCols] - Pu[pc - kXwCols]) * inv2dy;
+            xv = (qv[4] - qv[2]) * inv2dx;
+            yv = (Pv[pc + kXwCols] - Pv[pc - kXwCols]) * inv2dy;
+          }
+          tt = -(uc * xt + vc * yt + wc * (czt + (float)s.dth0[k]));
+          tu = -(uc * xu + vc * yu + wc * czu);
+          tv = -(uc * xv + vc * yv + wc * czv);
+        }
+        if (cor) {
+          tu = tu + f * (vc - v_env);
+          tv = tv + (-f) * (uc - u_env);
+        }
+        if (dmp) {
+          tu = tu + dmp_u[o];
+          tv = tv + dmp_v[o];
+        }
+        if (heat) tt = tt + (float)s.heat_r[col] * (float)s.heat_z[k];
+        if (OUTMODE == 0) {
+          uo[o] = uc + dts * tu;
+          vo[o] = vc + dts * tv;
+          tho[o] = thc + dts * tt;
+        } else {
+          uo[o] = tu;
+          vo[o] = tv;
+          tho[o] = tt;
+        }
+        // w on half level k
+        const float wk = qw[3];
+        float tw = 0.0f;
+        if (adv && k > 0) {
+          const float uh = 0.5f * (Pu[pc - 1] + uc);
+          const float vh = 0.5f * (Pv[pc - 1] + vc);
+          const float czw = (Pw[pc + 1] - Pw[pc - 1]) * inv2dz;
+          float xw, yw;
+          if (ws5) {
+            xw = ws5_win(qw, uh, inv60dx);
+            yw = ws5_col(Pw, r0, c, vh, inv60dy);
+          } else {
+            xw = (qw[4] - qw[2]) * inv2dx;
+            yw = (Pw[pc + kXwCols] - Pw[pc - kXwCols]) * inv2dy;
+          }
+          tw = -(uh * xw + vh * yw + wk * czw);
+        }
+        wo[ow] = OUTMODE == 0 ? wk + dts * tw : tw;
+        if (k == nz - 1) {  // the lid, level nz: no tendency
+          const float wl = Pw[pc + 1];
+          wo[ow + 1] = OUTMODE == 0 ? wl : 0.0f;
+        }
+      }
+    }
+    __syncthreads();  // the next chunk's first step rewrites plane 0
+  }
+}
+
 // dw_dt of the buoyancy component (nz+1 levels).
 template <class T>
 __global__ void k_buoyancy(GridK g, const T* __restrict__ th, const double* __restrict__ theta0,

@@ -220,3 +220,34 @@ def test_register_pencils_match_stockham(nx, ny, nz, monkeypatch):
             assert e_new <= 1.5 * e_ref + 1e-7, (stage, name, e_new, e_ref)
             if name in ("u", "v"):
                 assert d <= 1e-6 * wind, (stage, name, d)
+
+
+@pytest.mark.parametrize("shape", [(32, 16, 16), (48, 24, 40)])
+def test_slow_tendency_forms_agree(shape, monkeypatch):
+    """For FP32 state the slow tendency runs marching along x (k_slow_xw)
+    where nx % 16 == 0 and ny % 8 == 0, else as a gather (k_slow_f32;
+    ORACLE_B200_SLOW_XW=0 forces it).  Same terms and operation order: one
+    full step of the vortex configuration from the same state agrees to FP32
+    rounding.  The shapes cover the periodic halo rows and columns (two tiles
+    in x and in y) and, at nz = 40, two z-chunks with the lid in the second."""
+    from oraclev8_b200.solver import RK3Integrator, State
+    from tests.test_oracle_golden import oracle_initial_state
+    c = _vortex_case(*shape)
+    s0, _ = oracle_initial_state(c)
+    base = Base(c["nz"], c["Lz"])
+    cfg = b200_config(c)
+    outs = []
+    for xw in ("0", "1"):
+        monkeypatch.setenv("ORACLE_B200_SLOW_XW", xw)
+        integ = RK3Integrator(cfg, base, precision="fp32")
+        d = lambda a: dev(a, torch.float32)
+        s = State(d(s0.u), d(s0.v), d(s0.w), d(s0.theta_prime), d(s0.projection_potential), 0.0)
+        for n in range(2):
+            s, _ = integ.step(s, c["dt"], n)
+        outs.append(s)
+    for f in ("u", "v", "w", "theta_prime", "projection_potential"):
+        a, r = host(getattr(outs[1], f)).astype(np.float64), host(getattr(outs[0], f)).astype(np.float64)
+        scale = float(np.max(np.abs(r)))
+        err = float(np.max(np.abs(a - r))) / scale
+        print(f"{shape} {f}: max |x-march - gather| / max|.| = {err:.3e}")
+        assert err <= 1e-5, (f, err)
