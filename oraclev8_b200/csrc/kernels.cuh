@@ -476,15 +476,16 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
   }
 }
 
-// Single-precision Thomas sweep over the short-wave column blocks, with the
-// level count NZ a compile-time constant: c' is held in registers and both
-// sweeps are unrolled, and each level's coefficients (negs, rho, a, c,
-// rounded to float on the host) are one broadcast float4 from shared memory.
+// Single-precision tridiagonal solve over the short-wave column blocks, with
+// the level count NZ a compile-time constant: a twisted factorisation (one
+// elimination from the top and one from the bottom, two independent chains
+// per column, meeting at NZ/2 - 1) with its factors held in registers and
+// every loop unrolled, and each level's coefficients (negs, rho, a, c,
+// rounded to float on the host) one broadcast float4 from shared memory.
 // Shared memory holds only the staged (re, im) pairs of the CTA's columns, so
 // about 1.5x the columns of k_thomas<float, TC, float> are in flight per SM,
-// each with under half its instructions per level.  The recurrence and its
-// operation order are those of k_thomas with R = float; the diagonal term
-// b = negs - k^2 rho is formed in float.  Blocks flagged in `skip` (the
+// each with under half its instructions per level and half its dependent
+// chain.  The diagonal term b = negs - k^2 rho is formed in float.  Blocks flagged in `skip` (the
 // long-wave blocks, the zero mode's among them) are left to the double
 // launch.  No residual diagnostics: the solves that record them run k_thomas.
 // dh and ph may alias (a CTA reads only its own columns before writing them).
@@ -523,40 +524,53 @@ __global__ void __launch_bounds__(TC, thomas_f32_blocks<NZ>()) k_thomas_f32(Grid
     const double kx = kxd[kxi], ky = kyd[kyi];
     const float ksq = (float)arn(mrn(kx, kx), mrn(ky, ky));
     cplx<float>* s = sc + cl * P;
-    float cp[NZ];
-    float4 q = sco[0];  // (negs, rho, a, c)
-    float inv = rcprn(srn(q.x, mrn(ksq, q.y)));
-    float cpp = mrn(q.w, inv);
-    cp[0] = cpp;
-    cplx<float> d = s[0];
-    float pr = mrn(d.x, inv), pi = mrn(d.y, inv);
-    s[0] = mk<float>(pr, pi);
+    // twisted factorisation: elimination from the top over levels 0 .. MT
+    // and from the bottom over NZ-1 .. MT+1, two independent chains; x_MT
+    // from the 2 x 2 system where they meet, then substitution both ways.
+    //   top:    cp_k = c_k / (b_k - a_k cp_{k-1}),  x_k = dp_k - cp_k x_{k+1}
+    //   bottom: ap_k = a_k / (b_k - c_k ap_{k+1}),  x_k = dq_k - ap_k x_{k-1}
+    constexpr int MT = NZ / 2 - 1;
+    float f[NZ];  // cp (k <= MT) and ap (k > MT)
+    float tr = 0.0f, ti = 0.0f, br = 0.0f, bi = 0.0f;
 #pragma unroll
-    for (int k = 1; k < NZ; ++k) {
-      q = sco[k];
-      const float b = srn(q.x, mrn(ksq, q.y));
-      inv = rcprn(srn(b, mrn(q.z, cpp)));
-      if (k < NZ - 1) {
-        cpp = mrn(q.w, inv);
-        cp[k] = cpp;
-      }
-      d = s[k];
-      pr = mrn(srn(d.x, mrn(q.z, pr)), inv);
-      pi = mrn(srn(d.y, mrn(q.z, pi)), inv);
-      s[k] = mk<float>(pr, pi);
+    for (int t = 0; t <= MT; ++t) {
+      const int kt = t, kb = NZ - 1 - t;
+      const float4 qt = sco[kt], qb = sco[kb];  // (negs, rho, a, c)
+      const float btt = srn(qt.x, mrn(ksq, qt.y)), bbb = srn(qb.x, mrn(ksq, qb.y));
+      const float it = rcprn(t == 0 ? btt : srn(btt, mrn(qt.z, f[kt - (t > 0)])));
+      const float ib = rcprn(t == 0 ? bbb : srn(bbb, mrn(qb.w, f[kb + (t > 0)])));
+      f[kt] = mrn(qt.w, it);
+      f[kb] = mrn(qb.z, ib);
+      const cplx<float> dt = s[kt], db = s[kb];
+      tr = mrn(t == 0 ? dt.x : srn(dt.x, mrn(qt.z, tr)), it);
+      ti = mrn(t == 0 ? dt.y : srn(dt.y, mrn(qt.z, ti)), it);
+      br = mrn(t == 0 ? db.x : srn(db.x, mrn(qb.w, br)), ib);
+      bi = mrn(t == 0 ? db.y : srn(db.y, mrn(qb.w, bi)), ib);
+      s[kt] = mk<float>(tr, ti);
+      s[kb] = mk<float>(br, bi);
       // loads may run ahead within a group of four levels, not further: the
       // unrolled sweep would otherwise hoist every level's loads into
-      // registers that c' needs
-      if ((k & 3) == 3) asm volatile("" ::: "memory");
+      // registers that the factors need
+      if ((t & 3) == 3) asm volatile("" ::: "memory");
     }
-    float xr = pr, xi = pi;
+    // meeting point: x_MT = dp_MT - cp_MT x_{MT+1},  x_{MT+1} = dq_{MT+1} - ap_{MT+1} x_MT
+    const float den = rcprn(srn(1.0f, mrn(f[MT], f[MT + 1])));
+    float xr = mrn(srn(tr, mrn(f[MT], br)), den);
+    float xi = mrn(srn(ti, mrn(f[MT], bi)), den);
+    float yr = srn(br, mrn(f[MT + 1], xr)), yi = srn(bi, mrn(f[MT + 1], xi));
+    s[MT] = mk<float>(xr, xi);
+    s[MT + 1] = mk<float>(yr, yi);
 #pragma unroll
-    for (int k = NZ - 2; k >= 0; --k) {
-      d = s[k];
-      xr = srn(d.x, mrn(cp[k], xr));
-      xi = srn(d.y, mrn(cp[k], xi));
-      s[k] = mk<float>(xr, xi);
-      if ((k & 3) == 0) asm volatile("" ::: "memory");
+    for (int t = 1; t <= MT; ++t) {
+      const int kt = MT - t, kb = MT + 1 + t;
+      const cplx<float> dt = s[kt], db = s[kb];
+      xr = srn(dt.x, mrn(f[kt], xr));
+      xi = srn(dt.y, mrn(f[kt], xi));
+      yr = srn(db.x, mrn(f[kb], yr));
+      yi = srn(db.y, mrn(f[kb], yi));
+      s[kt] = mk<float>(xr, xi);
+      s[kb] = mk<float>(yr, yi);
+      if ((t & 3) == 0) asm volatile("" ::: "memory");
     }
   }
   __syncthreads();
