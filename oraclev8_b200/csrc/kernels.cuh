@@ -336,6 +336,24 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
         cp_async(&sc[cl * P + k], dh + base + (long)cl * nz + k, (int)sizeof(cplx<T>));
     cp_commit();
     cp_wait<0>();
+  } else if constexpr (sizeof(cplx<T>) <= sizeof(R)) {
+    // a wider sweep type (FP32 data, FP64 sweep): the pairs are staged by
+    // cp.async in the c' area (unused until the sweep, and exactly their
+    // size), then widened into the sweep's rows
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(scp);
+    for (int cl = 0; cl < ncl; ++cl)
+      for (int k = threadIdx.x; k < nz; k += TC)
+        cp_async(&stg[cl * P + k], dh + base + (long)cl * nz + k, (int)sizeof(cplx<T>));
+    cp_commit();
+    cp_wait<0>();
+    __syncthreads();
+    for (int e = threadIdx.x; e < ncl * nz; e += TC) {
+      const int cl = e / nz;
+      const int k = e - cl * nz;
+      const cplx<T> v = stg[cl * P + k];
+      sre[cl * P + k] = (R)v.x;
+      sim[cl * P + k] = (R)v.y;
+    }
   } else {
     for (int e = threadIdx.x; e < ncl * nz; e += TC) {
       const int cl = e / nz;
