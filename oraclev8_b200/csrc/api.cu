@@ -406,6 +406,10 @@ int set_x2_attrs() {
   int rc;
   if constexpr (sizeof(T) == 4) {
     if ((rc = yr_attrs<2>()) || (rc = yr_attrs<4>()) || (rc = yr_attrs<8>())) return rc;
+  } else {  // the defect correction's FP64 residual y transform
+    OB_CUDA(cudaFuncSetAttribute(k_fy3<2, double, FY_RESID, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)YrSize<2, double>::total));
   }
   if constexpr (sizeof(T) == 4) {
     if ((rc = xr_attrs_ix3<2>()) || (rc = xr_attrs_ix3<4>()) || (rc = xr_attrs_ix3<8>()))
@@ -1016,7 +1020,10 @@ int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStr
         g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
         (const Cd*)q->twx, R1, R2, nullptr); }
   OB_LAUNCHED();
-  if (q->zc2_fy)
+  if (p->zc3_fy)
+    { Launch L_(p, OB_PROF_REFINE, st); k_fy3<2, double, FY_RESID, float><<<dim3((g.nz + 1) / 2, g.nxh), 128,
+          YrSize<2, double>::total, st>>>(g, R1, R2, q->ky, (const Cd*)q->twy, S3); }
+  else if (q->zc2_fy)
     { Launch L_(p, OB_PROF_REFINE, st); fy2<double, FY_RESID, float>(q, q->zc2_fy, R1, R2, S3, st); }
   else
     { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(

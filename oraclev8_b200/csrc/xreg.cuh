@@ -494,14 +494,14 @@ constexpr int kYrN = 512;
 constexpr int kYrEx = 16 * 33;  // exchange block of one column (complex)
 
 // ytw[32 k2 + n1] = W_512^(n1 k2) (forward sign), w32[j] = W_32^j.
-template <bool INV>
-__device__ __forceinline__ void yr_fft(cplx<float> (&a)[16], int lane,
-                                       const cplx<float>* __restrict__ ytw,
-                                       const cplx<float>* __restrict__ w32, cplx<float>* ex) {
-  dft16<float, INV>(a);
+template <class T, bool INV>
+__device__ __forceinline__ void yr_fft(cplx<T> (&a)[16], int lane,
+                                       const cplx<T>* __restrict__ ytw,
+                                       const cplx<T>* __restrict__ w32, cplx<T>* ex) {
+  dft16<T, INV>(a);
 #pragma unroll
   for (int k2 = 1; k2 < 16; ++k2) {
-    cplx<float> w = ytw[32 * k2 + lane];
+    cplx<T> w = ytw[32 * k2 + lane];
     if (INV) w.y = -w.y;
     a[k2] = mul(a[k2], w);
   }
@@ -511,14 +511,14 @@ __device__ __forceinline__ void yr_fft(cplx<float> (&a)[16], int lane,
   const int k2 = lane & 15, p = lane >> 4;
 #pragma unroll
   for (int m = 0; m < 16; ++m) a[m] = ex[k2 * 33 + p + 2 * m];
-  dft16<float, INV>(a);
+  dft16<T, INV>(a);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    cplx<float> w = w32[j];
+    cplx<T> w = w32[j];
     if (INV) w.y = -w.y;
-    const float ox = __shfl_xor_sync(0xffffffffu, a[j].x, 16);
-    const float oy = __shfl_xor_sync(0xffffffffu, a[j].y, 16);
-    const cplx<float> other = mk<float>(ox, oy);
+    const T ox = __shfl_xor_sync(0xffffffffu, a[j].x, 16);
+    const T oy = __shfl_xor_sync(0xffffffffu, a[j].y, 16);
+    const cplx<T> other = mk<T>(ox, oy);
     // p = 0 holds E, the partner O; p = 1 holds O, the partner E
     a[j] = p == 0 ? add(a[j], mul(w, other)) : sub(other, mul(w, a[j]));
   }
@@ -528,31 +528,35 @@ template <int ZC>
 constexpr int yr_min_blocks() { return ZC >= 8 ? 1 : 3; }
 
 // Shared memory of k_fy3 / k_iy3: twiddles, then one region holding in turn
-// the input rows, the columns' exchange blocks and the output rows.
-template <int ZC>
+// the input rows, the columns' exchange blocks and the output rows (complex
+// values of type T).
+template <int ZC, class T = float>
 struct YrSize {
   static constexpr int B = 2 * ZC;   // columns (warps)
   static constexpr int BP = B + 1;   // row stride of the row tiles (odd)
-  static constexpr size_t tables = (size_t)(kYrN + 16) * 8;
-  static constexpr size_t rows = (size_t)kYrN * BP * 8;
-  static constexpr size_t ex = (size_t)B * kYrEx * 8;
+  static constexpr size_t tables = (size_t)(kYrN + 16) * sizeof(cplx<T>);
+  static constexpr size_t rows = (size_t)kYrN * BP * sizeof(cplx<T>);
+  static constexpr size_t ex = (size_t)B * kYrEx * sizeof(cplx<T>);
   static constexpr size_t total = tables + (rows > ex ? rows : ex);
 };
 
-// k_fy2 FY_DIV for FP32 at ny = 512: d^ = FFTy(X0) + i ky' FFTy(X1).
-// Columns: X0 at ZC levels, X1 at ZC levels.  grid = (ceil(nz/ZC), nx/2 + 1).
-template <int ZC>
-__global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_fy3(
-    GridK g, const cplx<float>* __restrict__ in0, const cplx<float>* __restrict__ in1,
-    const double* __restrict__ kyd, const cplx<float>* __restrict__ twy,
-    cplx<float>* __restrict__ out0) {
-  using SZ = YrSize<ZC>;
+// k_fy2 at ny = 512: d^ = FFTy(X0) + i ky' FFTy(X1) in arithmetic type T,
+// stored as TO.  FY_DIV: the projection (T = TO = float); FY_RESID: the
+// defect correction's FP64 residual (T = double, TO = float), its Nyquist
+// rows (ky = ny/2 or kx = nx/2) zeroed.  Columns: X0 at ZC levels, X1 at ZC
+// levels.  grid = (ceil(nz/ZC), nx/2 + 1).
+template <int ZC, class T = float, int MODE = FY_DIV, class TO = float>
+__global__ void __launch_bounds__(64 * ZC, sizeof(T) == 8 ? 4 : yr_min_blocks<ZC>()) k_fy3(
+    GridK g, const cplx<T>* __restrict__ in0, const cplx<T>* __restrict__ in1,
+    const double* __restrict__ kyd, const cplx<T>* __restrict__ twy,
+    cplx<TO>* __restrict__ out0) {
+  using SZ = YrSize<ZC, T>;
   constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kYrN;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  cplx<float>* ytw = reinterpret_cast<cplx<float>*>(smem_dyn);
-  cplx<float>* w32 = ytw + N;
-  cplx<float>* R = reinterpret_cast<cplx<float>*>(smem_dyn + SZ::tables);  // [N][BP]
-  cplx<float>* ex = R;                                                    // B x 16 x 33
+  cplx<T>* ytw = reinterpret_cast<cplx<T>*>(smem_dyn);
+  cplx<T>* w32 = ytw + N;
+  cplx<T>* R = reinterpret_cast<cplx<T>*>(smem_dyn + SZ::tables);  // [N][BP]
+  cplx<T>* ex = R;                                                // B x 16 x 33
   const int ny = g.ny, nz = g.nz;
   const int kx = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
@@ -570,11 +574,11 @@ __global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_fy3(
   cp_wait<0>();
   __syncthreads();
   const int c = tid >> 5, lane = tid & 31;
-  cplx<float> a[16];
+  cplx<T> a[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) a[q] = R[(lane + 32 * q) * BP + c];
   __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
-  yr_fft<false>(a, lane, ytw, w32, ex + c * kYrEx);
+  yr_fft<T, false>(a, lane, ytw, w32, ex + c * kYrEx);
   __syncthreads();  // every exchange read: the output rows reuse their space
   const int k2 = lane & 15, p = lane >> 4;
 #pragma unroll
@@ -584,8 +588,10 @@ __global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_fy3(
     const int ky = e / ZC, j = e - ky * ZC;
     const int z = z0 + j;
     if (z >= nz) continue;
-    const float kk = (ky == N / 2) ? 0.0f : (float)kyd[ky];
-    out0[(kx * ny + ky) * nz + z] = add(R[ky * BP + j], ik(kk, R[ky * BP + ZC + j]));
+    const T kk = (ky == N / 2) ? (T)0 : (T)kyd[ky];
+    cplx<T> d = add(R[ky * BP + j], ik(kk, R[ky * BP + ZC + j]));
+    if (MODE == FY_RESID && (ky == N / 2 || kx == g.nx / 2)) d = mk<T>((T)0, (T)0);
+    out0[(kx * ny + ky) * nz + z] = mk<TO>((TO)d.x, (TO)d.y);
   }
 }
 
@@ -628,7 +634,7 @@ __global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_iy3(
     if (c >= ZC) a[q] = ik(n == N / 2 ? 0.0f : (float)kyd[n], a[q]);  // ky' = 0 at Nyquist
   }
   __syncthreads();
-  yr_fft<true>(a, lane, ytw, w32, ex + c * kYrEx);
+  yr_fft<float, true>(a, lane, ytw, w32, ex + c * kYrEx);
   __syncthreads();
   const int k2 = lane & 15, p = lane >> 4;
 #pragma unroll
