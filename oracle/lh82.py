@@ -251,6 +251,83 @@ def helmholtz_tendency(u, v, epsilon, dt, Lx, Ly):
 # Shared operators (tendency.py:393-500)
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# Production slow components (tendency.py:1259-1668) and the intensity cap
+# ---------------------------------------------------------------------------
+
+def surface_drag_tendency(u, v, z, Cd=1.5e-3, H_bl=1000.0, u_env=0.0, v_env=0.0):
+    """SurfaceDragComponent — tendency.py:1318-1338: bulk drag on the
+    perturbation wind, rate Cd |V'(k=0)| / dz tapered linearly to 0 at H_bl."""
+    dz = float(z[1] - z[0]) if len(z) > 1 else float(z[0])
+    u_p = u - u_env
+    v_p = v - v_env
+    V_sfc = np.sqrt(u_p[:, :, 0] ** 2 + v_p[:, :, 0] ** 2)
+    alpha_sfc = Cd * V_sfc / dz
+    weight = np.maximum(0.0, 1.0 - z / H_bl)
+    alpha = alpha_sfc[:, :, None] * weight[None, None, :]
+    return -alpha * u_p, -alpha * v_p
+
+
+def sponge_profiles(z, Lz=10_000.0, alpha_max=0.01, sponge_fraction=0.3):
+    """SpongeDampingComponent._alpha_full and the half-level profile —
+    tendency.py:1478-1498."""
+    z_sp = Lz * (1.0 - sponge_fraction)
+    alpha = np.zeros_like(z)
+    above = z > z_sp
+    if np.any(above):
+        alpha[above] = alpha_max * ((z[above] - z_sp) / (Lz - z_sp)) ** 2
+    nz = len(z)
+    ah = np.zeros(nz + 1)
+    ah[1:-1] = 0.5 * (alpha[:-1] + alpha[1:])
+    ah[0] = alpha[0]
+    ah[-1] = alpha[-1]
+    return alpha, ah
+
+
+def sponge_tendency(u, v, w, th, z, Lz=10_000.0, alpha_max=0.01, sponge_fraction=0.3,
+                    u_env=0.0, v_env=0.0):
+    """SpongeDampingComponent.compute_tendency — tendency.py:1489-1508."""
+    alpha, ah = sponge_profiles(z, Lz, alpha_max, sponge_fraction)
+    return (-alpha[None, None, :] * (u - u_env), -alpha[None, None, :] * (v - v_env),
+            -ah[None, None, :] * w, -alpha[None, None, :] * th)
+
+
+def laplacian_h(f, dx2, dy2):
+    """Periodic 5-point horizontal Laplacian — tendency.py:1551-1558 and
+    HyperDiffusionComponent._laplacian (tendency.py:1608-1613)."""
+    return ((np.roll(f, -1, axis=0) - 2.0 * f + np.roll(f, +1, axis=0)) / dx2
+            + (np.roll(f, -1, axis=1) - 2.0 * f + np.roll(f, +1, axis=1)) / dy2)
+
+
+def horizontal_diffusion_tendency(u, v, nu_H, Lx, Ly, nx, ny):
+    """HorizontalDiffusionComponent — tendency.py:1548-1562."""
+    dx2, dy2 = (Lx / nx) ** 2, (Ly / ny) ** 2
+    return nu_H * laplacian_h(u, dx2, dy2), nu_H * laplacian_h(v, dx2, dy2)
+
+
+def hyper_diffusion_tendency(u, v, nu4, Lx, Ly, nx, ny):
+    """HyperDiffusionComponent — tendency.py:1615-1621 (two Laplacians)."""
+    dx2, dy2 = (Lx / nx) ** 2, (Ly / ny) ** 2
+    bu = laplacian_h(laplacian_h(u, dx2, dy2), dx2, dy2)
+    bv = laplacian_h(laplacian_h(v, dx2, dy2), dx2, dy2)
+    return -float(nu4) * bu, -float(nu4) * bv
+
+
+def newtonian_cooling_tendency(th, tau=3600.0):
+    """NewtonianCoolingComponent — tendency.py:1658-1662."""
+    return -(1.0 / float(tau)) * th
+
+
+def intensity_cap_tendency(u, v, v_cap=70.0, tau=300.0, u_env=0.0, v_env=0.0):
+    """IntensityCapComponent.compute_tendency — tendency.py:1396-1403."""
+    u_p = u - u_env
+    v_p = v - v_env
+    spd = np.sqrt(u_p ** 2 + v_p ** 2)
+    excess = np.maximum(0.0, spd - v_cap)
+    alpha = excess / (tau * np.maximum(spd, 1e-6))
+    return -alpha * u_p, -alpha * v_p
+
+
 def anelastic_divergence(u, v, w, rho_full, rho_half, kx, ky, dz):
     """d = div(rho u) — tendency.py:393-437."""
     rho_u = rho_full[None, None, :] * u
@@ -447,7 +524,8 @@ class Projection:
 class StepConfig:
     """Which components are active, in OperatorConfig slot order
     (operator_config.py:147-160): buoyancy | projection | advection |
-    coriolis | divergence_damping | diabatic_heating."""
+    coriolis | surface_drag | sponge_damping | horiz_diffusion |
+    newtonian_cooling | divergence_damping | diabatic_heating."""
     nx: int
     ny: int
     nz: int
@@ -460,6 +538,11 @@ class StepConfig:
     coriolis: Optional[dict] = None            # kwargs of CoriolisComponent
     damping_epsilon: Optional[float] = None    # HelmholtzDivergenceDamping
     heating: Optional[dict] = None             # kwargs of DiabaticHeatingComponent (no grid)
+    drag: Optional[dict] = None                # kwargs of SurfaceDragComponent
+    sponge: Optional[dict] = None              # kwargs of SpongeDampingComponent (Lz = grid's)
+    laplacian: Optional[float] = None          # HorizontalDiffusionComponent nu_H
+    hyper: Optional[float] = None              # HyperDiffusionComponent nu4
+    cooling: Optional[float] = None            # NewtonianCoolingComponent tau
     poisson_diag_every: int = 60
 
 
@@ -507,11 +590,16 @@ class Integrator:
     def slow_active(self):
         c = self.cfg
         return bool(c.advection or c.coriolis is not None
-                    or c.damping_epsilon is not None or c.heating is not None)
+                    or c.damping_epsilon is not None or c.heating is not None
+                    or c.drag is not None or c.sponge is not None
+                    or c.laplacian is not None or c.hyper is not None
+                    or c.cooling is not None)
 
     def slow_writes_momentum(self):
         c = self.cfg
-        return bool(c.advection or c.coriolis is not None or c.damping_epsilon is not None)
+        return bool(c.advection or c.coriolis is not None or c.damping_epsilon is not None
+                    or c.drag is not None or c.sponge is not None
+                    or c.laplacian is not None or c.hyper is not None)
 
     def slow_tendency(self, st: State, dt_slow: float):
         """Summed slow tendency in slot order — integrator.py:346-357."""
@@ -525,6 +613,22 @@ class Integrator:
         if c.coriolis is not None:
             cu, cv = coriolis_tendency(st.u, st.v, self.f0, self.f_y, self.u_env, self.v_env)
             du += cu; dv += cv
+        if c.drag is not None:
+            gu, gv = surface_drag_tendency(st.u, st.v, self.z, **c.drag)
+            du += gu; dv += gv
+        if c.sponge is not None:
+            su, sv, sw, sth = sponge_tendency(st.u, st.v, st.w, st.theta_prime, self.z,
+                                              Lz=c.Lz, **c.sponge)
+            du += su; dv += sv; dw += sw; dth += sth
+        if c.laplacian is not None:
+            lu, lv = horizontal_diffusion_tendency(st.u, st.v, c.laplacian, c.Lx, c.Ly,
+                                                   c.nx, c.ny)
+            du += lu; dv += lv
+        if c.hyper is not None:
+            bu, bv = hyper_diffusion_tendency(st.u, st.v, c.hyper, c.Lx, c.Ly, c.nx, c.ny)
+            du += bu; dv += bv
+        if c.cooling is not None:
+            dth += newtonian_cooling_tendency(st.theta_prime, c.cooling)
         if c.damping_epsilon is not None:
             hu, hv = helmholtz_tendency(st.u, st.v, c.damping_epsilon, dt_slow, c.Lx, c.Ly)
             du += hu; dv += hv

@@ -32,6 +32,10 @@ from oracle_v8.solver import (  # noqa: E402
     AdvectionComponent, CoriolisComponent, DiabaticHeatingComponent,
     HelmholtzDivergenceDampingComponent, OperatorConfig, RK3Integrator, State,
 )
+from oracle_v8.solver.tendency import (  # noqa: E402
+    SurfaceDragComponent, SpongeDampingComponent, HorizontalDiffusionComponent,
+    HyperDiffusionComponent, NewtonianCoolingComponent, IntensityCapComponent,
+)
 from oracle_v8.grid.staggering import LorenzStaggering  # noqa: E402
 from oracle_v8.solver.tendency import anelastic_divergence, _phi_gradient  # noqa: E402
 from oracle_v8.solver.poisson import VariableCoefficientPoissonSolver  # noqa: E402
@@ -147,6 +151,36 @@ def gen_components():
     np.savez_compressed(OUT / "components.npz", **out)
 
 
+def gen_production():
+    """Production slow components (tendency.py:1259-1668) and the intensity
+    cap, on the components fixture's random state."""
+    nx, ny, nz = 16, 12, 8
+    Lx, Ly, Lz = 320e3, 300e3, 4000.0
+    rng = np.random.default_rng(1234)
+    base = Base(nz, Lz)
+    s = random_state(rng, nx, ny, nz)
+    eq, stg = LH82AnelasticEquationSet(), LorenzStaggering()
+    out = dict(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, Lz=Lz)
+    out.update(st_dict("in_", s))
+    comps = {
+        "drag": SurfaceDragComponent(Cd=1.5e-3, H_bl=1500.0, u_env=2.0, v_env=-1.0),
+        "drag0": SurfaceDragComponent(),
+        "sponge": SpongeDampingComponent(Lz=Lz, alpha_max=0.01, sponge_fraction=0.4,
+                                         u_env=-1.5, v_env=0.5),
+        "lap": HorizontalDiffusionComponent(nu_H=2.0e5, Lx=Lx, Ly=Ly, nx=nx, ny=ny),
+        "hyper": HyperDiffusionComponent(nu4=3.0e12, Lx=Lx, Ly=Ly, nx=nx, ny=ny),
+        "cool": NewtonianCoolingComponent(tau=1800.0),
+        "cap": IntensityCapComponent(v_cap=15.0, tau=300.0, u_env=1.0, v_env=-2.0),
+    }
+    for k, c in comps.items():
+        t = c.compute_tendency(s, eq, stg, base, 30.0)
+        for f in ("du_dt", "dv_dt", "dw_dt", "dtheta_prime_dt"):
+            val = getattr(t, f)
+            if val is not None:
+                out[f"{k}_{f}"] = val
+    np.savez_compressed(OUT / "production.npz", **out)
+
+
 # ---------------------------------------------------------------------------
 # Integrator fixtures (a few full RK3 steps per component set)
 # ---------------------------------------------------------------------------
@@ -182,6 +216,31 @@ STEP_CASES = {
                                                 u_env=2.0, v_env=-1.0),
                           coriolis=dict(f=5e-5, mode="f_plane", u_env=2.0, v_env=-1.0),
                           advection="centered2", buoyancy=True, damping=0.5),
+    # production slow components: drag, sponge, biharmonic diffusion, Newtonian
+    # cooling (production_config.py:128-150) on the beta plane, with heating
+    "prod_beta": dict(nx=32, ny=24, nz=10, Lx=640e3, Ly=480e3, Lz=16e3, dt=30.0, nsteps=3,
+                      vortex=dict(Vmax=45.0, Rmax=40e3, B=1.6, f=4.99e-5, u_env=-2.0,
+                                  v_env=1.0),
+                      coriolis=dict(f=4.99e-5, mode="beta_plane", beta=2.15e-11,
+                                    periodic_taper=True, u_env=-2.0, v_env=1.0),
+                      advection="upwind5h", buoyancy=True,
+                      heating=dict(Q_max=3.0 / 3600.0, r_eyewall=40e3,
+                                   width_r=math.sqrt(2.0) * 15e3, z_peak=6e3,
+                                   width_z=math.sqrt(2.0) * 2e3),
+                      drag=dict(Cd=1.5e-3, H_bl=1000.0, u_env=-2.0, v_env=1.0),
+                      sponge=dict(alpha_max=0.01, sponge_fraction=0.3, u_env=-2.0, v_env=1.0),
+                      hyper=3.0e12, cooling=3600.0),
+    # Laplacian diffusion, drag and sponge with a background flow, f plane,
+    # centred advection and the divergence damper
+    "prod_lap_fplane": dict(nx=16, ny=16, nz=8, Lx=320e3, Ly=320e3, Lz=10e3, dt=30.0,
+                            nsteps=2, vortex=dict(Vmax=35.0, Rmax=40e3, B=1.5, f=5e-5,
+                                                  u_env=2.0, v_env=-1.0),
+                            coriolis=dict(f=5e-5, mode="f_plane", u_env=2.0, v_env=-1.0),
+                            advection="centered2", buoyancy=True, damping=0.5,
+                            drag=dict(Cd=2.0e-3, H_bl=1500.0, u_env=2.0, v_env=-1.0),
+                            sponge=dict(alpha_max=0.02, sponge_fraction=0.4, u_env=2.0,
+                                        v_env=-1.0),
+                            laplacian=2.0e5, cooling=1800.0),
     # projection only (the pre-balance else-branch)
     "projection_only": dict(nx=16, ny=16, nz=8, Lx=320e3, Ly=320e3, Lz=10e3, dt=1.0,
                             nsteps=2, vortex=dict(Vmax=30.0, Rmax=40e3, B=1.5, f=5e-5),
@@ -208,6 +267,18 @@ def build_ref_config(c):
     if c.get("heating"):
         kw["diabatic_heating"] = DiabaticHeatingComponent(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly,
                                                           Lz=Lz, **c["heating"])
+    if c.get("drag"):
+        kw["surface_drag"] = SurfaceDragComponent(**c["drag"])
+    if c.get("sponge"):
+        kw["sponge_damping"] = SpongeDampingComponent(Lz=Lz, **c["sponge"])
+    if c.get("laplacian") is not None:
+        kw["horiz_diffusion"] = HorizontalDiffusionComponent(nu_H=c["laplacian"], Lx=Lx, Ly=Ly,
+                                                             nx=nx, ny=ny)
+    if c.get("hyper") is not None:
+        kw["horiz_diffusion"] = HyperDiffusionComponent(nu4=c["hyper"], Lx=Lx, Ly=Ly,
+                                                        nx=nx, ny=ny)
+    if c.get("cooling") is not None:
+        kw["newtonian_cooling"] = NewtonianCoolingComponent(tau=c["cooling"])
     return OperatorConfig(**kw)
 
 
@@ -393,7 +464,7 @@ if __name__ == "__main__":
     ap.add_argument("--long", action="store_true")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
-    jobs = dict(components=gen_components, steps=gen_steps,
+    jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
                 vortex_tracker=gen_vortex_tracker, pins=gen_pins)
     for k, f in jobs.items():
         if a.only and k != a.only:

@@ -92,7 +92,8 @@ def test_operators_and_solve(comp):
         assert np.array_equal(getattr(s2, f), g["proj_" + k]), f
 
 
-STEP_CASES = ["beta_ws5", "beta_ws5_heat", "beta_env", "damper_fplane", "projection_only"]
+STEP_CASES = ["beta_ws5", "beta_ws5_heat", "beta_env", "damper_fplane", "projection_only",
+              "prod_beta", "prod_lap_fplane"]
 
 
 def oracle_config(c):
@@ -104,7 +105,10 @@ def oracle_config(c):
     return O.StepConfig(nx=c["nx"], ny=c["ny"], nz=c["nz"], Lx=c["Lx"], Ly=c["Ly"],
                         Lz=c["Lz"], buoyancy=bool(c.get("buoyancy")),
                         advection=c.get("advection"), coriolis=cor,
-                        damping_epsilon=c.get("damping"), heating=c.get("heating"))
+                        damping_epsilon=c.get("damping"), heating=c.get("heating"),
+                        drag=c.get("drag"), sponge=c.get("sponge"),
+                        laplacian=c.get("laplacian"), hyper=c.get("hyper"),
+                        cooling=c.get("cooling"))
 
 
 def oracle_initial_state(c):
@@ -215,3 +219,33 @@ def test_warm_bubble_first_step(golden_dir):
     s1, dg = O.Integrator(cfg, z, rho0, th0).step(s, 1.0)
     assert dg.surface_phi_min == pytest.approx(pins["1.0"]["surface_phi_min"], rel=1e-12)
     assert dg.max_w == pytest.approx(pins["1.0"]["max_w"], rel=1e-12)
+
+
+def test_production_component_tendencies(golden_dir):
+    """Surface drag, sponge, Laplacian and biharmonic diffusion, Newtonian
+    cooling and the intensity cap (tendency.py:1259-1668) against the
+    reference's own outputs on a random state, bit for bit."""
+    g = np.load(golden_dir / "production.npz")
+    nx, ny, nz = int(g["nx"]), int(g["ny"]), int(g["nz"])
+    Lx, Ly, Lz = float(g["Lx"]), float(g["Ly"]), float(g["Lz"])
+    z, _, _ = O.build_base_state(nz, Lz)
+    u, v, w, th = g["in_u"], g["in_v"], g["in_w"], g["in_th"]
+    got = {
+        "drag": O.surface_drag_tendency(u, v, z, Cd=1.5e-3, H_bl=1500.0, u_env=2.0, v_env=-1.0),
+        "drag0": O.surface_drag_tendency(u, v, z),
+        "sponge": O.sponge_tendency(u, v, w, th, z, Lz=Lz, alpha_max=0.01,
+                                    sponge_fraction=0.4, u_env=-1.5, v_env=0.5),
+        "lap": O.horizontal_diffusion_tendency(u, v, 2.0e5, Lx, Ly, nx, ny),
+        "hyper": O.hyper_diffusion_tendency(u, v, 3.0e12, Lx, Ly, nx, ny),
+        "cool": (O.newtonian_cooling_tendency(th, 1800.0),),
+        "cap": O.intensity_cap_tendency(u, v, v_cap=15.0, tau=300.0, u_env=1.0, v_env=-2.0),
+    }
+    fields = {"drag": ("du_dt", "dv_dt"), "drag0": ("du_dt", "dv_dt"),
+              "sponge": ("du_dt", "dv_dt", "dw_dt", "dtheta_prime_dt"),
+              "lap": ("du_dt", "dv_dt"), "hyper": ("du_dt", "dv_dt"),
+              "cool": ("dtheta_prime_dt",), "cap": ("du_dt", "dv_dt")}
+    for k, names in fields.items():
+        for a, f in zip(got[k], names):
+            assert np.array_equal(a, g[f"{k}_{f}"]), (k, f)
+    # the cap acts only above v_cap
+    assert 0 < np.count_nonzero(g["cap_du_dt"]) < g["cap_du_dt"].size
