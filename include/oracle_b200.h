@@ -56,6 +56,15 @@ extern "C" {
 #define OB_TEND_CORIOLIS 2
 #define OB_TEND_DAMPING 4
 #define OB_TEND_HEATING 8
+#define OB_TEND_DRAG 16       /* SurfaceDragComponent */
+#define OB_TEND_SPONGE 32     /* SpongeDampingComponent */
+#define OB_TEND_DIFFUSION 64  /* HorizontalDiffusion / HyperDiffusionComponent */
+#define OB_TEND_COOLING 128   /* NewtonianCoolingComponent */
+
+/* horizontal diffusion kinds (OperatorConfig.horiz_diffusion) */
+#define OB_DIFF_NONE 0
+#define OB_DIFF_LAPLACIAN 1   /* HorizontalDiffusionComponent (tendency.py:1517-1566) */
+#define OB_DIFF_BIHARMONIC 2  /* HyperDiffusionComponent (tendency.py:1569-1627) */
 
 /* Layout of the diagnostics block read by oracle_b200_read_diag
  * (StepDiagnostics, oracle_v8/solver/integrator.py:83-132). */
@@ -95,6 +104,22 @@ typedef struct OracleComponentDesc {
     const double *rho0;         /* (nz) base-state density, full levels */
     const double *theta0;       /* (nz) base-state potential temperature */
     int poisson_diag_every;     /* ORACLE_POISSON_DIAG_EVERY (tendency.py:769-774) */
+    /* production slow components (operator_config.py:100-103), summed in slot
+     * order after Coriolis and before the divergence damper */
+    int drag;                   /* SurfaceDragComponent (tendency.py:1259-1357) */
+    double drag_cd;             /* Cd */
+    double drag_dz;             /* z[1] - z[0] of the base state */
+    double drag_u_env, drag_v_env;
+    const double *drag_weight;  /* (nz) max(0, 1 - z / H_bl) */
+    int sponge;                 /* SpongeDampingComponent (tendency.py:1417-1514) */
+    double sponge_u_env, sponge_v_env;
+    const double *sponge_alpha;   /* (nz) damping rate on full levels */
+    const double *sponge_alpha_h; /* (nz+1) on half levels */
+    int diffusion;              /* OB_DIFF_* */
+    double diff_nu;             /* nu_H (Laplacian) or nu4 (biharmonic) */
+    double diff_dx2, diff_dy2;  /* (Lx/nx)^2, (Ly/ny)^2 */
+    int cooling;                /* NewtonianCoolingComponent (tendency.py:1630-1668) */
+    double cool_alpha;          /* 1 / tau */
 } OracleComponentDesc;
 
 typedef struct OracleStatePtrs {
@@ -175,6 +200,15 @@ int oracle_b200_buoyancy(OraclePlan *plan, const void *theta_prime, void *dw_dt,
 int oracle_b200_tendency(OraclePlan *plan, int mask, const OracleStatePtrs *state,
                          void *du, void *dv, void *dw, void *dth, double dt_slow,
                          void *stream);
+
+/* IntensityCapComponent.compute_tendency (tendency.py:1396-1403) on n cells:
+ * du = -alpha (u - u_env), dv = -alpha (v - v_env), alpha = max(0, |V'| - v_cap)
+ * / (tau max(|V'|, 1e-6)).  The reference's run loop adds dt times it to the
+ * state after every step (run_storm.py:168-172).  precision: OB_PREC_*; the
+ * outputs may alias nothing. */
+int oracle_b200_intensity_cap(const void *u, const void *v, int precision, long n,
+                              double v_cap, double tau, double u_env, double v_env,
+                              void *du, void *dv, void *stream);
 
 /* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
 int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);

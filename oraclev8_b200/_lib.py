@@ -16,6 +16,8 @@ OB_PREC_F64, OB_PREC_F32 = 0, 1
 OB_ADV_NONE, OB_ADV_CENTERED2, OB_ADV_UPWIND5H = 0, 1, 2
 OB_COR_NONE, OB_COR_FPLANE, OB_COR_BETA = 0, 1, 2
 OB_TEND_ADVECTION, OB_TEND_CORIOLIS, OB_TEND_DAMPING, OB_TEND_HEATING = 1, 2, 4, 8
+OB_TEND_DRAG, OB_TEND_SPONGE, OB_TEND_DIFFUSION, OB_TEND_COOLING = 16, 32, 64, 128
+OB_DIFF_NONE, OB_DIFF_LAPLACIAN, OB_DIFF_BIHARMONIC = 0, 1, 2
 DIAG = dict(max_u=0, max_v=1, max_w=2, max_th=3, phi_min=4, phi_max=5, compat0=6, disc0=9,
             last_compat=12, last_disc=13)
 DIAG_COUNT = 16
@@ -34,6 +36,7 @@ EXPORTS = (
     "oracle_b200_track_vorticity", "oracle_b200_step_graph_create",
     "oracle_b200_step_graph_launch", "oracle_b200_step_graph_kernels",
     "oracle_b200_step_graph_destroy", "oracle_b200_vortex_fill", "oracle_b200_plan_release",
+    "oracle_b200_intensity_cap",
 )
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
@@ -49,7 +52,14 @@ class ComponentDesc(ctypes.Structure):
                 ("v_env", c_double), ("f_y", POINTER(c_double)), ("damping", c_int),
                 ("epsilon", c_double), ("heating", c_int), ("heat_r", POINTER(c_double)),
                 ("heat_z", POINTER(c_double)), ("rho0", POINTER(c_double)),
-                ("theta0", POINTER(c_double)), ("poisson_diag_every", c_int)]
+                ("theta0", POINTER(c_double)), ("poisson_diag_every", c_int),
+                ("drag", c_int), ("drag_cd", c_double), ("drag_dz", c_double),
+                ("drag_u_env", c_double), ("drag_v_env", c_double),
+                ("drag_weight", POINTER(c_double)), ("sponge", c_int),
+                ("sponge_u_env", c_double), ("sponge_v_env", c_double),
+                ("sponge_alpha", POINTER(c_double)), ("sponge_alpha_h", POINTER(c_double)),
+                ("diffusion", c_int), ("diff_nu", c_double), ("diff_dx2", c_double),
+                ("diff_dy2", c_double), ("cooling", c_int), ("cool_alpha", c_double)]
 
 
 class StatePtrs(ctypes.Structure):
@@ -92,6 +102,8 @@ def load(path: Path | None = None):
         "oracle_b200_apply_operator": ([vp, vp, vp, vp], c_int),
         "oracle_b200_buoyancy": ([vp, vp, vp, vp], c_int),
         "oracle_b200_tendency": ([vp, c_int, POINTER(StatePtrs), vp, vp, vp, vp, c_double, vp], c_int),
+        "oracle_b200_intensity_cap": ([vp, vp, c_int, ctypes.c_long, c_double, c_double, c_double,
+                                       c_double, vp, vp, vp], c_int),
         "oracle_b200_read_diag": ([vp, POINTER(c_double), c_int, vp], c_int),
         "oracle_b200_last_error": ([], ctypes.c_char_p),
         "oracle_b200_version": ([], c_int),

@@ -47,6 +47,24 @@ class PlanSpec:
     heat_r: Optional[np.ndarray] = None
     heat_z: Optional[np.ndarray] = None
     poisson_diag_every: int = 60
+    # production slow components (tendency.py:1259-1668)
+    drag: bool = False
+    drag_cd: float = 0.0
+    drag_dz: float = 1.0
+    drag_u_env: float = 0.0
+    drag_v_env: float = 0.0
+    drag_weight: Optional[np.ndarray] = None
+    sponge: bool = False
+    sponge_u_env: float = 0.0
+    sponge_v_env: float = 0.0
+    sponge_alpha: Optional[np.ndarray] = None
+    sponge_alpha_h: Optional[np.ndarray] = None
+    diffusion: int = L.OB_DIFF_NONE
+    diff_nu: float = 0.0
+    diff_dx2: float = 1.0
+    diff_dy2: float = 1.0
+    cooling: bool = False
+    cool_alpha: float = 0.0
 
 
 def _f64(a):
@@ -64,8 +82,10 @@ class Plan:
         self.device = torch.device("cuda", torch.cuda.current_device())
         g = L.GridDesc(spec.nx, spec.ny, spec.nz, spec.Lx, spec.Ly, spec.Lz, self.prec)
         keep = [_f64(spec.rho0), _f64(spec.theta0), _f64(spec.f_y), _f64(spec.heat_r),
-                _f64(spec.heat_z)]
-        rho0, theta0, f_y, heat_r, heat_z = keep
+                _f64(spec.heat_z), _f64(spec.drag_weight), _f64(spec.sponge_alpha),
+                _f64(spec.sponge_alpha_h)]
+        rho0, theta0, f_y, heat_r, heat_z, drag_w, sp_a, sp_ah = keep
+        self._keep = keep
         if rho0.shape != (spec.nz,) or theta0.shape != (spec.nz,):
             raise ValueError(f"rho0/theta0 must have shape ({spec.nz},)")
         c = L.ComponentDesc(int(spec.buoyancy), int(spec.projection), int(spec.advection),
@@ -73,7 +93,13 @@ class Plan:
                             float(spec.v_env), L.dptr(f_y), int(spec.damping),
                             float(spec.epsilon), int(spec.heating), L.dptr(heat_r),
                             L.dptr(heat_z), L.dptr(rho0), L.dptr(theta0),
-                            int(spec.poisson_diag_every))
+                            int(spec.poisson_diag_every), int(spec.drag),
+                            float(spec.drag_cd), float(spec.drag_dz), float(spec.drag_u_env),
+                            float(spec.drag_v_env), L.dptr(drag_w), int(spec.sponge),
+                            float(spec.sponge_u_env), float(spec.sponge_v_env), L.dptr(sp_a),
+                            L.dptr(sp_ah), int(spec.diffusion), float(spec.diff_nu),
+                            float(spec.diff_dx2), float(spec.diff_dy2), int(spec.cooling),
+                            float(spec.cool_alpha))
         h = ctypes.c_void_p()
         L.check(self.lib.oracle_b200_plan_create(ctypes.byref(g), ctypes.byref(c), ctypes.byref(h)))
         self.handle = h
@@ -263,7 +289,12 @@ def _key(spec: PlanSpec) -> tuple:
             spec.precision, b(spec.rho0), b(spec.theta0), spec.buoyancy, spec.projection,
             spec.advection, spec.coriolis, float(spec.f0), float(spec.u_env),
             float(spec.v_env), b(spec.f_y), spec.damping, float(spec.epsilon), spec.heating,
-            b(spec.heat_r), b(spec.heat_z), spec.poisson_diag_every)
+            b(spec.heat_r), b(spec.heat_z), spec.poisson_diag_every, spec.drag,
+            float(spec.drag_cd), float(spec.drag_dz), float(spec.drag_u_env),
+            float(spec.drag_v_env), b(spec.drag_weight), spec.sponge, float(spec.sponge_u_env),
+            float(spec.sponge_v_env), b(spec.sponge_alpha), b(spec.sponge_alpha_h),
+            spec.diffusion, float(spec.diff_nu), float(spec.diff_dx2), float(spec.diff_dy2),
+            spec.cooling, float(spec.cool_alpha))
 
 
 def cached_plan(spec: PlanSpec) -> Plan:

@@ -142,6 +142,13 @@ struct OraclePlan {
   GridK g{};
   int buoyancy = 0, projection = 0, advection = 0, coriolis = 0, damping = 0, heating = 0;
   double f0 = 0, u_env = 0, v_env = 0, epsilon = 0;
+  // production slow components (OracleComponentDesc)
+  int drag = 0, sponge = 0, diffusion = 0, cooling = 0;
+  double drag_cd = 0, drag_dz = 1, drag_u_env = 0, drag_v_env = 0;
+  double sponge_u_env = 0, sponge_v_env = 0;
+  double diff_nu = 0, diff_dx2 = 1, diff_dy2 = 1, cool_alpha = 0;
+  double *drag_w = nullptr, *sp_a = nullptr, *sp_ah = nullptr;
+  void *Lu = nullptr, *Lv = nullptr;  // biharmonic: the inner Laplacians
   int diag_every = 60;
   long solve_count = 0;
   FftPlan px{}, py{};    // radix-16-first plans (inverse kernels)
@@ -1136,6 +1143,25 @@ SlowK slow_args(const OraclePlan* p) {
   s.inv60dy = 1.0 / (60.0 * p->g.dy);
   s.inv2dz = 1.0 / (2.0 * p->g.dz);
   s.invdz = 1.0 / p->g.dz;
+  s.drag = p->drag;
+  s.sponge = p->sponge;
+  s.diff = p->diffusion;
+  s.cool = p->cooling;
+  s.drag_cd = p->drag_cd;
+  s.drag_dz = p->drag_dz;
+  s.drag_u_env = p->drag_u_env;
+  s.drag_v_env = p->drag_v_env;
+  s.drag_w = p->drag_w;
+  s.sp_u_env = p->sponge_u_env;
+  s.sp_v_env = p->sponge_v_env;
+  s.sp_a = p->sp_a;
+  s.sp_ah = p->sp_ah;
+  s.diff_nu = p->diff_nu;
+  s.diff_dx2 = p->diff_dx2;
+  s.diff_dy2 = p->diff_dy2;
+  s.lap_u = p->Lu;
+  s.lap_v = p->Lv;
+  s.cool_alpha = p->cool_alpha;
   return s;
 }
 
@@ -1144,18 +1170,34 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
               const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
   dim3 blk(32, 8);
   dim3 grd((p->g.ny + 7) / 8, p->g.nx);
+  // the biharmonic diffusion's inner Laplacians of this slow half's u, v
+  if ((mask & OB_TEND_DIFFUSION) && p->diffusion == OB_DIFF_BIHARMONIC) {
+    const long n = (long)p->g.nx * p->g.ny * p->g.nz;
+    { Launch L_(p, 5, st); k_lap2<T><<<(unsigned)std::min<long>((n + 255) / 256, 148L * 64), 256, 0, st>>>(
+          p->g, u, v, p->diff_dx2, p->diff_dy2, (T*)p->Lu, (T*)p->Lv); }
+    OB_LAUNCHED();
+  }
+  // production components run in the gather kernels
+  const bool extra = (mask & (OB_TEND_DRAG | OB_TEND_SPONGE | OB_TEND_DIFFUSION | OB_TEND_COOLING)) &&
+                     (p->drag || p->sponge || p->diffusion || p->cooling);
   if constexpr (sizeof(T) == 4) {
     // the x-marching form where the grid tiles it; the gather form otherwise
-    if (p->slow_xw && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
+    if (p->slow_xw && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
       { Launch L_(p, 5, st); k_slow_xw<OUT><<<dim3(p->g.ny / 8, p->g.nx / KXW), blk, 0, st>>>(
             p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du, (const T*)p->Dv, uo, vo, wo, tho); }
+    else if (extra)
+      { Launch L_(p, 5, st); k_slow_f32<OUT, true><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                                  (const T*)p->Dv, uo, vo, wo, tho); }
     else
       { Launch L_(p, 5, st); k_slow_f32<OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
                                             (const T*)p->Dv, uo, vo, wo, tho); }
-  }
-  else
+  } else if (extra) {
+    { Launch L_(p, 5, st); k_slow<T, OUT, true><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
+                                              (const T*)p->Dv, uo, vo, wo, tho); }
+  } else {
     { Launch L_(p, 5, st); k_slow<T, OUT><<<grd, blk, 0, st>>>(p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du,
                                         (const T*)p->Dv, uo, vo, wo, tho); }
+  }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -1185,9 +1227,12 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
   const size_t n = (size_t)p->g.nx * p->g.ny * p->g.nz;
   const size_t nw = (size_t)p->g.nx * p->g.ny * (p->g.nz + 1);
   const double dts = dt * 0.5;
-  const bool slow = p->advection || p->coriolis || p->damping || p->heating;
-  const bool mom = p->advection || p->coriolis || p->damping;
-  const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_DAMPING | OB_TEND_HEATING;
+  const bool slow = p->advection || p->coriolis || p->damping || p->heating || p->drag ||
+                    p->sponge || p->diffusion || p->cooling;
+  const bool mom = p->advection || p->coriolis || p->damping || p->drag || p->sponge ||
+                   p->diffusion;
+  const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_DAMPING | OB_TEND_HEATING |
+                  OB_TEND_DRAG | OB_TEND_SPONGE | OB_TEND_DIFFUSION | OB_TEND_COOLING;
   // anchor state y^n after the first slow half step
   const T *au = (const T*)in->u, *av = (const T*)in->v, *aw = (const T*)in->w,
           *ath = (const T*)in->theta_prime, *aphi = (const T*)in->phi;
@@ -1623,6 +1668,14 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     return fail(OB_ERR_ARG, "beta-plane Coriolis needs f_y");
   if (comp->heating && (!comp->heat_r || !comp->heat_z))
     return fail(OB_ERR_ARG, "heating needs heat_r and heat_z");
+  if (comp->drag && (!comp->drag_weight || !(comp->drag_dz > 0)))
+    return fail(OB_ERR_ARG, "surface drag needs drag_weight and a positive drag_dz");
+  if (comp->sponge && (!comp->sponge_alpha || !comp->sponge_alpha_h))
+    return fail(OB_ERR_ARG, "sponge damping needs sponge_alpha and sponge_alpha_h");
+  if (comp->diffusion < OB_DIFF_NONE || comp->diffusion > OB_DIFF_BIHARMONIC)
+    return fail(OB_ERR_ARG, "unknown horizontal diffusion %d", comp->diffusion);
+  if (comp->diffusion && !(comp->diff_dx2 > 0 && comp->diff_dy2 > 0))
+    return fail(OB_ERR_ARG, "horizontal diffusion needs positive diff_dx2 and diff_dy2");
   if ((long)nx * ny * (nz + 1) > (1L << 31))
     return fail(OB_ERR_ARG, "grid too large for 32-bit launch geometry");
 
@@ -1653,6 +1706,20 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
   p->coriolis = comp->coriolis;
   p->damping = comp->damping != 0;
   p->heating = comp->heating != 0;
+  p->drag = comp->drag != 0;
+  p->sponge = comp->sponge != 0;
+  p->diffusion = comp->diffusion;
+  p->cooling = comp->cooling != 0;
+  p->drag_cd = comp->drag_cd;
+  p->drag_dz = comp->drag_dz > 0 ? comp->drag_dz : 1.0;
+  p->drag_u_env = comp->drag_u_env;
+  p->drag_v_env = comp->drag_v_env;
+  p->sponge_u_env = comp->sponge_u_env;
+  p->sponge_v_env = comp->sponge_v_env;
+  p->diff_nu = comp->diff_nu;
+  p->diff_dx2 = comp->diffusion ? comp->diff_dx2 : 1.0;
+  p->diff_dy2 = comp->diffusion ? comp->diff_dy2 : 1.0;
+  p->cool_alpha = comp->cool_alpha;
   p->f0 = comp->f0;
   p->u_env = comp->u_env;
   p->v_env = comp->v_env;
@@ -1730,6 +1797,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     if ((rc = upload(p, &p->heat_r, comp->heat_r, (size_t)nx * ny))) return bail(rc);
     if ((rc = upload(p, &p->heat_z, comp->heat_z, nz))) return bail(rc);
   }
+  if (p->drag && (rc = upload(p, &p->drag_w, comp->drag_weight, nz))) return bail(rc);
+  if (p->sponge && ((rc = upload(p, &p->sp_a, comp->sponge_alpha, nz)) ||
+                    (rc = upload(p, &p->sp_ah, comp->sponge_alpha_h, nz + 1))))
+    return bail(rc);
   if (p->prec == OB_PREC_F64) {
     auto tx = twiddles<double>(nx), ty = twiddles<double>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<double>)))) return bail(rc);
@@ -1811,6 +1882,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       (rc = dalloc(p, &p->Sw, nw * e)) || (rc = dalloc(p, &p->Sphi, n * e)) ||
       (rc = dalloc(p, &p->Du, n * e)) || (rc = dalloc(p, &p->Dv, n * e)))
     return bail(rc);
+  if (p->diffusion == OB_DIFF_BIHARMONIC &&
+      ((rc = dalloc(p, &p->Lu, n * e)) || (rc = dalloc(p, &p->Lv, n * e))))
+    return bail(rc);
   if (p->buoyancy && p->projection && (rc = dalloc(p, &p->Bh, nw * e))) return bail(rc);
   if (p->prec == OB_PREC_F32) {
     const long ncols = (long)p->g.nxh * ny;
@@ -1818,9 +1892,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     std::vector<unsigned char> flag(nblk, 0);
     std::vector<int> lw;
     const double Lz = grid->Lz;
-    for (long c = 0; c < ncols; ++c) {
-      const int ix = (int)(c / ny), iy = (int)(c - (long)ix * ny);
-      if ((kx[ix] * kx[ix] + ky[iy] * ky[iy]) * (Lz * Lz) < 1.0) flag[c / kThomasCols] = 1;
+    for (long col = 0; col < ncols; ++col) {
+      const int ix = (int)(col / ny), iy = (int)(col - (long)ix * ny);
+      if ((kx[ix] * kx[ix] + ky[iy] * ky[iy]) * (Lz * Lz) < 1.0) flag[col / kThomasCols] = 1;
     }
     for (long b = 0; b < nblk; ++b)
       if (flag[b]) lw.push_back((int)b);
@@ -2034,6 +2108,27 @@ int oracle_b200_tendency(OraclePlan* p, int mask, const OracleStatePtrs* s, void
                                         (double*)dth, dt_slow, st),
                   tendency_impl<float>(p, mask, s, (float*)du, (float*)dv, (float*)dw,
                                        (float*)dth, dt_slow, st));
+}
+
+int oracle_b200_intensity_cap(const void* u, const void* v, int precision, long n,
+                              double v_cap, double tau, double u_env, double v_env, void* du,
+                              void* dv, void* stream) {
+  if (!u || !v || !du || !dv) return fail(OB_ERR_ARG, "intensity_cap: NULL pointer");
+  if (n < 0) return fail(OB_ERR_ARG, "intensity_cap: negative size");
+  if (!(tau > 0)) return fail(OB_ERR_ARG, "intensity_cap: tau must be positive");
+  if (n == 0) return OB_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned nb = (unsigned)std::min<long>((n + 255) / 256, 148L * 32);
+  if (precision == OB_PREC_F64)
+    k_intensity_cap<double><<<nb, 256, 0, st>>>((const double*)u, (const double*)v, n, v_cap,
+                                                tau, u_env, v_env, (double*)du, (double*)dv);
+  else if (precision == OB_PREC_F32)
+    k_intensity_cap<float><<<nb, 256, 0, st>>>((const float*)u, (const float*)v, n, v_cap, tau,
+                                               u_env, v_env, (float*)du, (float*)dv);
+  else
+    return fail(OB_ERR_ARG, "intensity_cap: unknown precision %d", precision);
+  OB_CUDA(cudaGetLastError());
+  return OB_OK;
 }
 
 long oracle_b200_launch_count(const OraclePlan* p) { return p ? p->launches : -1; }

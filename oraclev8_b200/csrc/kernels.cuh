@@ -869,7 +869,32 @@ struct SlowK {
   const double* heat_r; // (nx*ny)
   const double* heat_z; // (nz)
   double inv2dx, inv2dy, inv60dx, inv60dy, inv2dz, invdz;
+  // production components, in slot order after Coriolis (operator_config.py:147-160)
+  int drag, sponge, diff, cool;
+  double drag_cd, drag_dz, drag_u_env, drag_v_env;
+  const double* drag_w;  // (nz) max(0, 1 - z / H_bl)
+  double sp_u_env, sp_v_env;
+  const double* sp_a;    // (nz) full levels
+  const double* sp_ah;   // (nz+1) half levels
+  double diff_nu, diff_dx2, diff_dy2;
+  const void* lap_u;     // biharmonic: lap(u), lap(v) of this slow half (element type T)
+  const void* lap_v;
+  double cool_alpha;
 };
+
+// mask bits of the production components (OB_TEND_*)
+constexpr int kTendDrag = 16, kTendSponge = 32, kTendDiffusion = 64, kTendCooling = 128;
+
+// Periodic 5-point horizontal Laplacian of q at o, in the reference's order
+// ((q[i+1] - 2 q) + q[i-1]) / dx2 + ((q[j+1] - 2 q) + q[j-1]) / dy2
+// (tendency.py:1551-1558, 1608-1613).  off[2], off[3]: offsets of i-1, i+1.
+template <class T, class A>
+__device__ __forceinline__ A lap5(const T* __restrict__ q, int o, const int* offx,
+                                  const int* offy, A dx2, A dy2) {
+  const A c = (A)q[o];
+  return ((A)q[o + offx[3]] - (A)2 * c + (A)q[o + offx[2]]) / dx2 +
+         ((A)q[o + offy[3]] - (A)2 * c + (A)q[o + offy[2]]) / dy2;
+}
 
 // WS5 upwind derivative along one horizontal axis.  cols[r] are the linear
 // column indices of the neighbours i-3, i-2, i-1, i+1, i+2, i+3 (periodic);
@@ -895,7 +920,9 @@ __device__ __forceinline__ double ddx_c2(const T* __restrict__ q, int o, const i
 // One thread per (i, j, k), k in [0, nz] (k = nz only updates w).
 // grid = (ceil(ny / blockDim.y), nx); blockDim.x strides k.
 // OUTMODE 0: out = in + dts * tendency (state update); 1: out = tendency.
-template <class T, int OUTMODE>
+// PROD: with the production components (surface drag, sponge, horizontal
+// diffusion, Newtonian cooling); without them the kernel compiles as before.
+template <class T, int OUTMODE, bool PROD = false>
 __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double dts,
                                               const T* __restrict__ u, const T* __restrict__ v,
                                               const T* __restrict__ w,
@@ -913,6 +940,10 @@ __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double
   const bool cor = (mask & 2) && s.cor;
   const bool dmp = (mask & 4) && s.damp;
   const bool heat = (mask & 8) && s.heat;
+  const bool drg = PROD && (mask & kTendDrag) && s.drag;
+  const bool spg = PROD && (mask & kTendSponge) && s.sponge;
+  const int dif = (PROD && (mask & kTendDiffusion)) ? s.diff : 0;
+  const bool col_ = PROD && (mask & kTendCooling) && s.cool;
   // periodic neighbour columns
   int ix[6], jy[6];
   const int dd[6] = {-3, -2, -1, 1, 2, 3};
@@ -985,6 +1016,29 @@ __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double
         tu = tu + f * (vc - s.v_env);
         tv = tv + (-f) * (uc - s.u_env);
       }
+      if (drg) {  // SurfaceDragComponent (tendency.py:1318-1338)
+        const double up0 = (double)u[col * nz] - s.drag_u_env;
+        const double vp0 = (double)v[col * nz] - s.drag_v_env;
+        const double al = s.drag_cd * sqrt(up0 * up0 + vp0 * vp0) / s.drag_dz * s.drag_w[k];
+        tu = tu + (-al) * (uc - s.drag_u_env);
+        tv = tv + (-al) * (vc - s.drag_v_env);
+      }
+      if (spg) {  // SpongeDampingComponent (tendency.py:1489-1508)
+        const double a = s.sp_a[k];
+        tu = tu + (-a) * (uc - s.sp_u_env);
+        tv = tv + (-a) * (vc - s.sp_v_env);
+        tt = tt + (-a) * thc;
+      }
+      if (dif == 1) {  // HorizontalDiffusionComponent (tendency.py:1548-1562)
+        tu = tu + s.diff_nu * lap5<T, double>(u, o, offx, offy, s.diff_dx2, s.diff_dy2);
+        tv = tv + s.diff_nu * lap5<T, double>(v, o, offx, offy, s.diff_dx2, s.diff_dy2);
+      } else if (dif == 2) {  // HyperDiffusionComponent (tendency.py:1615-1621)
+        const T* lu = static_cast<const T*>(s.lap_u);
+        const T* lv = static_cast<const T*>(s.lap_v);
+        tu = tu + (-s.diff_nu) * lap5<T, double>(lu, o, offx, offy, s.diff_dx2, s.diff_dy2);
+        tv = tv + (-s.diff_nu) * lap5<T, double>(lv, o, offx, offy, s.diff_dx2, s.diff_dy2);
+      }
+      if (col_) tt = tt + (-s.cool_alpha) * thc;  // NewtonianCooling (tendency.py:1661-1662)
       if (dmp) {
         tu = tu + (double)dmp_u[o];
         tv = tv + (double)dmp_v[o];
@@ -1018,6 +1072,7 @@ __global__ void __launch_bounds__(256) k_slow(GridK g, SlowK s, int mask, double
         }
         tw = -(uh * xw + vh * yw + wk * czw);
       }
+      if (spg) tw = tw + (-s.sp_ah[k]) * wk;  // sponge on half levels (tendency.py:1506)
       if (OUTMODE == 0)
         wo[ow] = (T)(wk + dts * tw);
       else
@@ -1046,7 +1101,7 @@ __device__ __forceinline__ float ddx_ws5f(const float* __restrict__ q, int o, co
 // the accuracy floor of this path, and FP32 arithmetic needs no conversion
 // of the loaded values and half the registers of the double form.  Same
 // terms, summation order and boundary treatment as k_slow.
-template <int OUTMODE>
+template <int OUTMODE, bool PROD = false>
 __global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask, double dts_d,
                                                      const float* __restrict__ u,
                                                      const float* __restrict__ v,
@@ -1072,6 +1127,11 @@ __global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask,
   const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
   const float f = cor ? (float)((s.cor == 2) ? s.fy[j] : s.f0) : 0.0f;
   const float u_env = (float)s.u_env, v_env = (float)s.v_env;
+  const bool drg = PROD && (mask & kTendDrag) && s.drag;
+  const bool spg = PROD && (mask & kTendSponge) && s.sponge;
+  const int dif = (PROD && (mask & kTendDiffusion)) ? s.diff : 0;
+  const bool col_ = PROD && (mask & kTendCooling) && s.cool;
+  const float dnu = (float)s.diff_nu, ddx2 = (float)s.diff_dx2, ddy2 = (float)s.diff_dy2;
   int offx[6], offy[6], offxw[6], offyw[6];
   const int dd[6] = {-3, -2, -1, 1, 2, 3};
 #pragma unroll
@@ -1136,6 +1196,30 @@ __global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask,
         tu = tu + f * (vc - v_env);
         tv = tv + (-f) * (uc - u_env);
       }
+      if (drg) {
+        const float du_env = (float)s.drag_u_env, dv_env = (float)s.drag_v_env;
+        const float up0 = u[col * nz] - du_env, vp0 = v[col * nz] - dv_env;
+        const float al = (float)s.drag_cd * sqrtf(up0 * up0 + vp0 * vp0) / (float)s.drag_dz *
+                         (float)s.drag_w[k];
+        tu = tu + (-al) * (uc - du_env);
+        tv = tv + (-al) * (vc - dv_env);
+      }
+      if (spg) {
+        const float a = (float)s.sp_a[k];
+        tu = tu + (-a) * (uc - (float)s.sp_u_env);
+        tv = tv + (-a) * (vc - (float)s.sp_v_env);
+        tt = tt + (-a) * thc;
+      }
+      if (dif == 1) {
+        tu = tu + dnu * lap5<float, float>(u, o, offx, offy, ddx2, ddy2);
+        tv = tv + dnu * lap5<float, float>(v, o, offx, offy, ddx2, ddy2);
+      } else if (dif == 2) {
+        const float* lu = static_cast<const float*>(s.lap_u);
+        const float* lv = static_cast<const float*>(s.lap_v);
+        tu = tu + (-dnu) * lap5<float, float>(lu, o, offx, offy, ddx2, ddy2);
+        tv = tv + (-dnu) * lap5<float, float>(lv, o, offx, offy, ddx2, ddy2);
+      }
+      if (col_) tt = tt + (-(float)s.cool_alpha) * thc;
       if (dmp) {
         tu = tu + dmp_u[o];
         tv = tv + dmp_v[o];
@@ -1169,6 +1253,7 @@ __global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask,
         }
         tw = -(uh * xw + vh * yw + wk * czw);
       }
+      if (spg) tw = tw + (-(float)s.sp_ah[k]) * wk;
       if (OUTMODE == 0)
         wo[ow] = wk + dts * tw;
       else
@@ -1420,6 +1505,54 @@ __global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, 
       }
     }
     __syncthreads();  // the next chunk's first step rewrites plane 0
+  }
+}
+
+// lap(u), lap(v) of one slow half for the biharmonic diffusion: the
+// reference applies its 5-point Laplacian twice and rounds the inner one to a
+// field (tendency.py:1608-1621), so it is formed as one.  One thread per cell.
+template <class T>
+__global__ void __launch_bounds__(256) k_lap2(GridK g, const T* __restrict__ u,
+                                              const T* __restrict__ v, double dx2, double dy2,
+                                              T* __restrict__ lu, T* __restrict__ lv) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long n = (long)nx * ny * nz;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n;
+       e += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % nz);
+    const long col = e / nz;
+    const int i = (int)(col / ny), j = (int)(col - (long)i * ny);
+    const int ip = i + 1 == nx ? 0 : i + 1, im = i == 0 ? nx - 1 : i - 1;
+    const int jp = j + 1 == ny ? 0 : j + 1, jm = j == 0 ? ny - 1 : j - 1;
+    const int o = (int)e;
+    const int offx[6] = {0, 0, (im - i) * ny * nz, (ip - i) * ny * nz, 0, 0};
+    const int offy[6] = {0, 0, (jm - j) * nz, (jp - j) * nz, 0, 0};
+    (void)k;
+    if (sizeof(T) == 8) {
+      lu[o] = (T)lap5<T, double>(u, o, offx, offy, dx2, dy2);
+      lv[o] = (T)lap5<T, double>(v, o, offx, offy, dx2, dy2);
+    } else {
+      lu[o] = (T)lap5<T, float>(u, o, offx, offy, (float)dx2, (float)dy2);
+      lv[o] = (T)lap5<T, float>(v, o, offx, offy, (float)dx2, (float)dy2);
+    }
+  }
+}
+
+// IntensityCapComponent.compute_tendency (tendency.py:1396-1403), elementwise.
+template <class T>
+__global__ void __launch_bounds__(256) k_intensity_cap(const T* __restrict__ u,
+                                                       const T* __restrict__ v, long n,
+                                                       double v_cap, double tau, double u_env,
+                                                       double v_env, T* __restrict__ du,
+                                                       T* __restrict__ dv) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n;
+       e += (long)gridDim.x * blockDim.x) {
+    const double up = (double)u[e] - u_env, vp = (double)v[e] - v_env;
+    const double spd = sqrt(up * up + vp * vp);
+    const double excess = fmax(0.0, spd - v_cap);
+    const double alpha = excess / (tau * fmax(spd, 1e-6));
+    du[e] = (T)(-alpha * up);
+    dv[e] = (T)(-alpha * vp);
   }
 }
 

@@ -21,7 +21,8 @@ from .. import _lib as L
 from .._plan import Plan, PlanSpec
 from .. import backend
 from ..backend import asarray, to_numpy, wrap_base
-from .tendency import State
+from .tendency import (State, cooling_fields, diffusion_fields, drag_fields,
+                       sponge_fields)
 
 _DIAG_EVERY = max(1, int(os.environ.get("ORACLE_DIAG_EVERY", "1")))
 
@@ -42,8 +43,7 @@ class StepDiagnostics:
     surface_phi_max: float = 0.0
 
 
-_UNSUPPORTED_SLOTS = ("pressure_gradient", "surface_drag", "sponge_damping", "horiz_diffusion",
-                      "newtonian_cooling")
+_UNSUPPORTED_SLOTS = ("pressure_gradient",)
 
 
 def compile_config(config, base, precision: str, poisson_diag_every: int | None = None,
@@ -105,7 +105,27 @@ def compile_config(config, base, precision: str, poisson_diag_every: int | None 
                                       "DiabaticHeatingComponent (separable factors)")
         spec.heating = True
         spec.heat_r, spec.heat_z = heat.heat_factors
+    # production components (operator_config.py:100-103); their attribute
+    # names are the reference's, so either side's objects compile alike
+    z = None
+    if config.surface_drag is not None or config.sponge_damping is not None:
+        z = np.asarray(to_numpy(base.z), dtype=np.float64).reshape(-1)
+        if z.shape != (int(nz),):
+            raise ValueError(f"base.z has shape {z.shape}, expected ({nz},)")
+    if config.surface_drag is not None:
+        _set(spec, drag_fields(config.surface_drag, z))
+    if config.sponge_damping is not None:
+        _set(spec, sponge_fields(config.sponge_damping, z))
+    if config.horiz_diffusion is not None:
+        _set(spec, diffusion_fields(config.horiz_diffusion))
+    if config.newtonian_cooling is not None:
+        _set(spec, cooling_fields(config.newtonian_cooling))
     return spec
+
+
+def _set(spec: PlanSpec, fields: dict) -> None:
+    for k, v in fields.items():
+        setattr(spec, k, v)
 
 
 class RK3Integrator:

@@ -10,6 +10,7 @@ plan (see integrator.py).
 from __future__ import annotations
 
 import abc
+import ctypes
 from dataclasses import dataclass
 from enum import Enum
 from typing import Optional
@@ -494,45 +495,235 @@ class HelmholtzDivergenceDampingComponent(TendencyComponent):
         return (StateVar.U, StateVar.V)
 
 
-class _NotOnB200(TendencyComponent):
-    """Production slow components that are not part of the B200 step yet
-    (tendency.py:1259-1668).  Constructing one raises, so a run never silently
-    drops a term."""
-    name = "not_implemented"
+# ---------------------------------------------------------------------------
+# Production slow components (tendency.py:1259-1668) and the intensity cap.
+# Each stores the reference's constructor arguments under the reference's
+# attribute names, so that compile_config reads a reference object and one of
+# these alike (the *_fields helpers below).
+# ---------------------------------------------------------------------------
 
-    def __init__(self, *a, **k):
-        raise NotImplementedError(
-            f"{type(self).__name__} is not implemented on the oraclev8_b200 backend")
+def _base_z(base, nz):
+    if base is None or getattr(base, "z", None) is None:
+        raise ValueError("this component needs the base state's z levels")
+    z = np.asarray(to_numpy(base.z), dtype=np.float64).reshape(-1)
+    if z.shape != (nz,):
+        raise ValueError(f"base.z has shape {z.shape}, expected ({nz},)")
+    return z
 
-    def compute_tendency(self, *a, **k):
-        raise NotImplementedError
+
+def drag_fields(comp, z) -> dict:
+    """PlanSpec fields of a SurfaceDragComponent (tendency.py:1318-1338): the
+    level spacing and the vertical weight exactly as the reference forms them."""
+    dz = float(z[1] - z[0]) if len(z) > 1 else float(z[0])
+    weight = np.maximum(0.0, 1.0 - z / float(comp._H_bl))
+    return dict(drag=True, drag_cd=float(comp._Cd), drag_dz=dz, drag_u_env=float(comp._u_env),
+                drag_v_env=float(comp._v_env), drag_weight=weight)
+
+
+def sponge_fields(comp, z) -> dict:
+    """PlanSpec fields of a SpongeDampingComponent: its full- and half-level
+    damping rates (tendency.py:1478-1498)."""
+    z_sp, Lz, amax = float(comp._z_sponge), float(comp._Lz), float(comp._alpha_max)
+    alpha = np.zeros_like(z)
+    above = z > z_sp
+    if np.any(above):
+        alpha[above] = amax * ((z[above] - z_sp) / (Lz - z_sp)) ** 2
+    nz = len(z)
+    ah = np.zeros(nz + 1)
+    ah[1:-1] = 0.5 * (alpha[:-1] + alpha[1:])
+    ah[0] = alpha[0]
+    ah[-1] = alpha[-1]
+    return dict(sponge=True, sponge_u_env=float(comp._u_env), sponge_v_env=float(comp._v_env),
+                sponge_alpha=alpha, sponge_alpha_h=ah)
+
+
+def diffusion_fields(comp) -> dict:
+    """PlanSpec fields of a HorizontalDiffusionComponent (nu_H, Laplacian) or
+    a HyperDiffusionComponent (nu4, biharmonic)."""
+    if hasattr(comp, "_nu4"):
+        return dict(diffusion=L.OB_DIFF_BIHARMONIC, diff_nu=float(comp._nu4),
+                    diff_dx2=float(comp._dx2), diff_dy2=float(comp._dy2))
+    return dict(diffusion=L.OB_DIFF_LAPLACIAN, diff_nu=float(comp._nu_H),
+                diff_dx2=float(comp._dx2), diff_dy2=float(comp._dy2))
+
+
+def cooling_fields(comp) -> dict:
+    return dict(cooling=True, cool_alpha=float(comp._alpha))
+
+
+class SurfaceDragComponent(TendencyComponent):
+    """Bulk aerodynamic drag on the perturbation wind (u - u_env, v - v_env)
+    with the rate Cd |V'(k=0)| / dz tapered linearly to zero at H_bl
+    (tendency.py:1259-1357)."""
+    name = "surface_drag"
+    stage = StepStage.SLOW
+
+    def __init__(self, Cd: float = 1.5e-3, H_bl: float = 1000.0, u_env: float = 0.0,
+                 v_env: float = 0.0) -> None:
+        self._Cd = float(Cd)
+        self._H_bl = float(H_bl)
+        self._u_env = float(u_env)
+        self._v_env = float(v_env)
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        z = _base_z(base, int(state.u.shape[2]))
+        p = _plan_for(state.u, base, **drag_fields(self, z))
+        du, dv, _, _ = p.tendency(L.OB_TEND_DRAG, state.u, state.v, state.w,
+                                  state.theta_prime, float(dt))
+        return Tendency(du_dt=du, dv_dt=dv)
+
+    def set_env(self, u_env: float, v_env: float) -> None:
+        """tendency.py:1340-1351."""
+        self._u_env = float(u_env)
+        self._v_env = float(v_env)
 
     def reads(self):
-        return ()
+        return (StateVar.U, StateVar.V)
 
     def writes(self):
-        return ()
+        return (StateVar.U, StateVar.V)
 
 
-class SurfaceDragComponent(_NotOnB200):
-    name = "surface_drag"
-
-
-class IntensityCapComponent(_NotOnB200):
-    name = "intensity_cap"
-
-
-class SpongeDampingComponent(_NotOnB200):
+class SpongeDampingComponent(TendencyComponent):
+    """Rayleigh damping of the perturbations toward the environment near the
+    lid, quadratic in height above z_sp = Lz (1 - sponge_fraction)
+    (tendency.py:1417-1514)."""
     name = "sponge_damping"
+    stage = StepStage.SLOW
+
+    def __init__(self, Lz: float = 10_000.0, alpha_max: float = 0.01,
+                 sponge_fraction: float = 0.3, u_env: float = 0.0, v_env: float = 0.0) -> None:
+        self._Lz = Lz
+        self._alpha_max = alpha_max
+        self._z_sponge = Lz * (1.0 - sponge_fraction)
+        self._u_env = u_env
+        self._v_env = v_env
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        z = _base_z(base, int(state.u.shape[2]))
+        p = _plan_for(state.u, base, **sponge_fields(self, z))
+        du, dv, dw, dth = p.tendency(L.OB_TEND_SPONGE, state.u, state.v, state.w,
+                                     state.theta_prime, float(dt))
+        return Tendency(du_dt=du, dv_dt=dv, dw_dt=dw, dtheta_prime_dt=dth)
+
+    def reads(self):
+        return (StateVar.U, StateVar.V, StateVar.W, StateVar.THETA_PRIME)
+
+    def writes(self):
+        return (StateVar.U, StateVar.V, StateVar.W, StateVar.THETA_PRIME)
 
 
-class HorizontalDiffusionComponent(_NotOnB200):
+class HorizontalDiffusionComponent(TendencyComponent):
+    """Second-order horizontal Laplacian diffusion of u, v, periodic
+    5-point stencil (tendency.py:1517-1566)."""
     name = "horizontal_diffusion"
+    stage = StepStage.SLOW
+
+    def __init__(self, nu_H: float, Lx: float, Ly: float, nx: int, ny: int) -> None:
+        self._nu_H = float(nu_H)
+        self._dx2 = (Lx / nx) ** 2
+        self._dy2 = (Ly / ny) ** 2
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        p = _plan_for(state.u, base, **diffusion_fields(self))
+        du, dv, _, _ = p.tendency(L.OB_TEND_DIFFUSION, state.u, state.v, state.w,
+                                  state.theta_prime, float(dt))
+        return Tendency(du_dt=du, dv_dt=dv)
+
+    def reads(self):
+        return (StateVar.U, StateVar.V)
+
+    def writes(self):
+        return (StateVar.U, StateVar.V)
 
 
-class HyperDiffusionComponent(_NotOnB200):
+class HyperDiffusionComponent(TendencyComponent):
+    """Fourth-order (biharmonic) horizontal diffusion of u, v as two
+    applications of the 5-point Laplacian (tendency.py:1569-1627)."""
     name = "hyper_diffusion"
+    stage = StepStage.SLOW
+
+    def __init__(self, nu4: float, Lx: float, Ly: float, nx: int, ny: int) -> None:
+        self._nu4 = float(nu4)
+        self._dx2 = (Lx / nx) ** 2
+        self._dy2 = (Ly / ny) ** 2
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        p = _plan_for(state.u, base, **diffusion_fields(self))
+        du, dv, _, _ = p.tendency(L.OB_TEND_DIFFUSION, state.u, state.v, state.w,
+                                  state.theta_prime, float(dt))
+        return Tendency(du_dt=du, dv_dt=dv)
+
+    def reads(self):
+        return (StateVar.U, StateVar.V)
+
+    def writes(self):
+        return (StateVar.U, StateVar.V)
 
 
-class NewtonianCoolingComponent(_NotOnB200):
+class NewtonianCoolingComponent(TendencyComponent):
+    """Relaxation of theta' toward zero on the time scale tau
+    (tendency.py:1630-1668)."""
     name = "newtonian_cooling"
+    stage = StepStage.SLOW
+
+    def __init__(self, tau: float = 3600.0) -> None:
+        self._alpha = 1.0 / float(tau)
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        p = _plan_for(state.u, base, **cooling_fields(self))
+        _, _, _, dth = p.tendency(L.OB_TEND_COOLING, state.u, state.v, state.w,
+                                  state.theta_prime, float(dt))
+        return Tendency(dtheta_prime_dt=dth)
+
+    def reads(self):
+        return (StateVar.THETA_PRIME,)
+
+    def writes(self):
+        return (StateVar.THETA_PRIME,)
+
+
+class IntensityCapComponent(TendencyComponent):
+    """Perturbation-wind speed limiter (tendency.py:1360-1414): relaxes
+    |V'| toward v_cap where it exceeds it, preserving direction.  Not an
+    OperatorConfig slot: the reference's run loop adds dt times this
+    tendency to the state after each step (run_storm.py:168-172)."""
+    name = "intensity_cap"
+    stage = StepStage.SLOW
+
+    def __init__(self, v_cap: float = 70.0, tau: float = 300.0, u_env: float = 0.0,
+                 v_env: float = 0.0) -> None:
+        self._v_cap = float(v_cap)
+        self._tau = float(tau)
+        self._u_env = float(u_env)
+        self._v_env = float(v_env)
+
+    def compute_tendency(self, state, equation_set, staggering, base, dt):
+        u, v = state.u, state.v
+        if not (isinstance(u, torch.Tensor) and u.is_cuda):
+            raise TypeError("IntensityCapComponent reads device fields (CUDA torch tensors)")
+        if u.dtype not in (torch.float64, torch.float32) or v.dtype != u.dtype:
+            raise ValueError("u and v must share a float64 or float32 dtype")
+        if tuple(v.shape) != tuple(u.shape):
+            raise ValueError("u and v must have the same shape")
+        u, v = u.contiguous(), v.contiguous()
+        du, dv = torch.empty_like(u), torch.empty_like(v)
+        lib = L.load()
+        prec = L.OB_PREC_F64 if u.dtype == torch.float64 else L.OB_PREC_F32
+        stream = torch.cuda.current_stream(u.device).cuda_stream
+        L.check(lib.oracle_b200_intensity_cap(
+            ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(v.data_ptr()), prec, u.numel(),
+            self._v_cap, self._tau, self._u_env, self._v_env, ctypes.c_void_p(du.data_ptr()),
+            ctypes.c_void_p(dv.data_ptr()), ctypes.c_void_p(stream)))
+        return Tendency(du_dt=du, dv_dt=dv)
+
+    def set_env(self, u_env: float, v_env: float) -> None:
+        """tendency.py:1405-1408."""
+        self._u_env = float(u_env)
+        self._v_env = float(v_env)
+
+    def reads(self):
+        return (StateVar.U, StateVar.V)
+
+    def writes(self):
+        return (StateVar.U, StateVar.V)

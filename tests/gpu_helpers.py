@@ -37,7 +37,10 @@ def b200_config(c, nx=None):
                                       BuoyancyComponent, CoriolisComponent,
                                       DiabaticHeatingComponent,
                                       HelmholtzDivergenceDampingComponent,
-                                      LH82AnelasticEquationSet, OperatorConfig)
+                                      HorizontalDiffusionComponent, HyperDiffusionComponent,
+                                      LH82AnelasticEquationSet, NewtonianCoolingComponent,
+                                      OperatorConfig, SpongeDampingComponent,
+                                      SurfaceDragComponent)
     from oraclev8_b200.grid import LorenzStaggering
     nx, ny, nz, Lx, Ly, Lz = c["nx"], c["ny"], c["nz"], c["Lx"], c["Ly"], c["Lz"]
     kw = dict(equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
@@ -57,6 +60,16 @@ def b200_config(c, nx=None):
     if c.get("heating"):
         kw["diabatic_heating"] = DiabaticHeatingComponent(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly,
                                                           Lz=Lz, **c["heating"])
+    if c.get("drag"):
+        kw["surface_drag"] = SurfaceDragComponent(**c["drag"])
+    if c.get("sponge"):
+        kw["sponge_damping"] = SpongeDampingComponent(Lz=Lz, **c["sponge"])
+    if c.get("laplacian") is not None:
+        kw["horiz_diffusion"] = HorizontalDiffusionComponent(c["laplacian"], Lx, Ly, nx, ny)
+    if c.get("hyper") is not None:
+        kw["horiz_diffusion"] = HyperDiffusionComponent(c["hyper"], Lx, Ly, nx, ny)
+    if c.get("cooling") is not None:
+        kw["newtonian_cooling"] = NewtonianCoolingComponent(tau=c["cooling"])
     return OperatorConfig(**kw)
 
 

@@ -67,15 +67,46 @@ def test_compile_config_maps_every_slot():
     assert spec.buoyancy and spec.projection and spec.damping and spec.heating
     assert spec.advection == L.OB_ADV_UPWIND5H and spec.coriolis == L.OB_COR_BETA
     assert spec.epsilon == 0.5 and spec.f_y.shape == (24,) and spec.precision == "fp32"
+    assert not (spec.drag or spec.sponge or spec.cooling) and spec.diffusion == L.OB_DIFF_NONE
+
+
+@pytest.mark.parametrize("hyper", [False, True])
+def test_compile_config_maps_production_slots(hyper):
+    """The drag weight and level spacing, the sponge's full and half level
+    rates, the diffusion kind and 1/tau reach the plan as the reference forms
+    them (tendency.py:1318-1338, 1478-1498, 1544-1546, 1604-1606, 1659)."""
+    from oraclev8_b200 import _lib as L
+    from oraclev8_b200.solver.integrator import compile_config
+    from oraclev8_b200.solver import (SurfaceDragComponent, SpongeDampingComponent,
+                                      HorizontalDiffusionComponent, HyperDiffusionComponent,
+                                      NewtonianCoolingComponent)
+    from oraclev8_b200.production_config import BaseState
+    base = BaseState(8, 16e3)
+    diff = (HyperDiffusionComponent(1e12, 640e3, 480e3, 32, 24) if hyper
+            else HorizontalDiffusionComponent(500.0, 640e3, 480e3, 32, 24))
+    cfg = _cfg(surface_drag=SurfaceDragComponent(2e-3, 3000.0, -4.0, 1.5),
+               sponge_damping=SpongeDampingComponent(16e3, 0.02, 0.25, -4.0, 1.5),
+               horiz_diffusion=diff, newtonian_cooling=NewtonianCoolingComponent(1800.0))
+    spec = compile_config(cfg, base, "fp64")
+    z = np.asarray(base.z, dtype=np.float64)
+    assert spec.drag and spec.drag_cd == 2e-3 and spec.drag_dz == z[1] - z[0]
+    assert np.array_equal(spec.drag_weight, np.maximum(0.0, 1.0 - z / 3000.0))
+    assert (spec.drag_u_env, spec.drag_v_env) == (-4.0, 1.5)
+    zs = 16e3 * 0.75
+    a = np.where(z > zs, 0.02 * ((z - zs) / (16e3 - zs)) ** 2, 0.0)
+    assert spec.sponge and np.array_equal(spec.sponge_alpha, a)
+    assert np.array_equal(spec.sponge_alpha_h, np.r_[a[0], 0.5 * (a[:-1] + a[1:]), a[-1]])
+    assert (spec.sponge_u_env, spec.sponge_v_env) == (-4.0, 1.5)
+    assert spec.diffusion == (L.OB_DIFF_BIHARMONIC if hyper else L.OB_DIFF_LAPLACIAN)
+    assert spec.diff_nu == (1e12 if hyper else 500.0)
+    assert (spec.diff_dx2, spec.diff_dy2) == ((640e3 / 32) ** 2, (480e3 / 24) ** 2)
+    assert spec.cooling and spec.cool_alpha == 1.0 / 1800.0
 
 
 def test_unsupported_components_raise_and_guards():
-    from oraclev8_b200.solver import (NewtonianCoolingComponent, PressureGradientComponent,
-                                      AdvectionComponent)
+    from oraclev8_b200.solver import PressureGradientComponent, AdvectionComponent
     from oraclev8_b200.solver.integrator import compile_config
     from oraclev8_b200.production_config import BaseState
-    with pytest.raises(NotImplementedError):
-        NewtonianCoolingComponent(tau=1800.0)
     with pytest.raises(ValueError):
         _cfg(pressure_gradient=PressureGradientComponent(32, 24, 8, 1, 1, 1))
     cfg = _cfg(pressure_gradient=PressureGradientComponent(32, 24, 8, 1, 1, 1),
