@@ -33,6 +33,13 @@ stream with HBM admission and reports p50/p95/p99 time-to-completion.  Sizes
 are set by ``--ensemble-runs/--ensemble-hours`` and
 ``--serving-requests/--serving-scale``; ``--no-ensemble`` skips both.
 
+Production physics (``production``; ``--no-production`` skips it): the
+reference's build_production_config (centred advection, beta-plane,
+biharmonic diffusion, divergence damping, Newtonian cooling, surface drag,
+projection, no buoyancy) on the same grid and initial state, with the
+intensity cap added after each step as the reference's run loop does; timed
+in the bench's precision and in plain FP64, with the slow class's roofline.
+
 N > 1: N independent replicas, one per GPU (the path partitions into
 independent runs; no collective on the data path).
 
@@ -439,6 +446,9 @@ def run_b200(args):
         ms64, _, _ = _timed_steps(integ64, st64, dt, args.steps, args.warmup, barrier)
         companion = (ms64, _precision_report(st, st64, integ64.plan))
         del st64, integ64
+    production = None
+    if not args.no_production:
+        production = production_report(args, w, hs, barrier, dev, load_peaks()[0])
     clk = clocks.stop()
     red = max_over_ranks([ms] + ([companion[0]] if companion else []), dev)
     ms = red[0]
@@ -550,6 +560,8 @@ def run_b200(args):
         line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
                                 note="this run vs the FP64 run from the same initial state; "
                                      "divergence = anelastic divergence evaluated in FP64")
+    if production is not None:
+        line["production"] = production
     if not args.no_ensemble:
         ens = ensemble_report(args, load_peaks()[0])
         if rank == 0:
@@ -566,6 +578,100 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def production_report(args, w, hs, barrier, dev, peak_gbs):
+    """The reference's production physics on the bench grid.
+
+    build_production_config (centred advection, beta-plane Coriolis,
+    biharmonic diffusion, Helmholtz divergence damping, Newtonian cooling,
+    surface drag, projection; no buoyancy) stepped on the workload's grid and
+    initial state, with the intensity cap added after every step as the
+    reference's run loop does (run_storm.py:168-172).  A step here is
+    ``RK3Integrator.step_`` + the cap's tendency + the two in-place updates.
+    Timed in the bench's precision and in plain FP64, W warm-up + K steps
+    each, with CUDA events on the launching stream."""
+    import torch
+    from oraclev8_b200.production_config import (TAU_CAP, VMAX_CAP_MS, BaseState,
+                                                 build_production_config)
+    from oraclev8_b200.solver import IntensityCapComponent, RK3Integrator, State
+    nx, ny, nz, Lx, Ly, Lz = grid_of(w)
+    f0 = w["coriolis"]["f"]
+    u_env, v_env = w["coriolis"].get("u_env", 0.0), w["coriolis"].get("v_env", 0.0)
+    base = BaseState(nz, Lz)
+    cfg = build_production_config(nx, ny, nz, Lx, Ly, Lz, f0, u_env, v_env)
+    cap = IntensityCapComponent(v_cap=VMAX_CAP_MS, tau=TAU_CAP, u_env=u_env, v_env=v_env)
+    dt = w["dt"]
+    runs = {}
+    precs = [args.precision] + (["fp64"] if args.precision != "fp64" else [])
+    for prec in precs:
+        integ = RK3Integrator(cfg, base, precision=prec)
+        ty = integ.dtype
+        st = State(*(torch.as_tensor(a, dtype=ty).to(dev) for a in
+                     (hs.u, hs.v, hs.w, hs.theta_prime, hs.projection_potential)), 0.0)
+
+        def one():
+            integ.step_(st, dt, want_diag=True)
+            ct = cap.compute_tendency(st, None, None, base, dt)
+            st.u.add_(ct.du_dt, alpha=dt)
+            st.v.add_(ct.dv_dt, alpha=dt)
+
+        for _ in range(args.warmup):
+            one()
+        torch.cuda.synchronize()
+        plan = integ.plan
+        plan.profile(True)
+        l0 = plan.launches
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            one()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks([e0.elapsed_time(e1)], dev)[0]
+        prof = plan.profile_read()
+        plan.profile(False)
+        if not bool(torch.isfinite(st.u).all()):
+            raise RuntimeError("non-finite state after the production steps")
+        # the library's launches plus one intensity-cap kernel per step
+        runs[prec] = (ms, plan.launches - l0 + args.steps, prof, st, integ)
+    ms, launches, prof, st, _ = runs[args.precision]
+    S = 8 if args.precision == "fp64" else 4
+    n = nx * ny * nz
+    nw = nx * ny * (nz + 1)
+    # per slow half: the inner Laplacians (read u, v; write Lu, Lv) and the
+    # fused slow kernel (read u, v, w, theta', the damper's Du, Dv and Lu, Lv;
+    # write u, v, w, theta')
+    slow_bytes = 2 * ((2 * (3 * n + nw) + 4 * n) * S + 4 * n * S)
+    slow_ms = prof["slow"][0] / args.steps
+    cells = n * args.steps
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rep = {
+        "workload": f"production physics (build_production_config: centred advection, "
+                    f"beta-plane, nu4 3e11 biharmonic, Helmholtz damping 0.5, cooling 1800 s, "
+                    f"drag Cd 1.5e-3 / 1 km, projection, no buoyancy) on the {nx}x{ny}x{nz} "
+                    f"grid and initial state, intensity cap 70 m/s / 300 s after each step, "
+                    f"dt={dt}s",
+        "precision": args.precision,
+        "value": world * cells / (ms / 1e3), "unit": "cell-updates/s",
+        "ms_per_step": ms / args.steps,
+        "gpu_launches": launches,
+        "kernels_ms_per_step": {c: prof[c][0] / args.steps for c in prof if prof[c][1]},
+        "slow_roofline": {"bound": "hbm", "bytes_per_step": slow_bytes,
+                          "achieved": slow_bytes / (slow_ms / 1e3) / 1e9, "peak": peak_gbs,
+                          "unit": "GB/s", "frac": slow_bytes / (slow_ms / 1e3) / 1e9 / peak_gbs},
+    }
+    if "fp64" in runs and args.precision != "fp64":
+        ms64, _, _, st64, integ64 = runs["fp64"]
+        rep["fp64_plain"] = {"value": world * cells / (ms64 / 1e3), "unit": "cell-updates/s",
+                             "ms_per_step": ms64 / args.steps, "ratio": ms64 / ms}
+        rep["accuracy"] = dict(_precision_report(st, st64, integ64.plan),
+                               after_steps=args.warmup + args.steps)
+    return rep
 
 
 def ensemble_report(args, peak_gbs):
@@ -674,6 +780,8 @@ def main():
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-production", action="store_true",
+                    help="skip the production-physics leg")
     ap.add_argument("--no-fp64-companion", action="store_true",
                     help="skip the plain-FP64 timing and accuracy report (profiling runs)")
     ap.add_argument("--ensemble-runs", type=int, default=64)

@@ -40,6 +40,7 @@ from oracle_v8.grid.staggering import LorenzStaggering  # noqa: E402
 from oracle_v8.solver.tendency import anelastic_divergence, _phi_gradient  # noqa: E402
 from oracle_v8.solver.poisson import VariableCoefficientPoissonSolver  # noqa: E402
 from oracle_v8.production_config import build_base_state  # noqa: E402
+from oracle_v8 import production_config as PC  # noqa: E402
 from oracle_v8.vortex_init import HollandVortexInit  # noqa: E402
 from oracle_v8.storm_tracker import find_storm_centre  # noqa: E402
 from oracle_v8.validation import analytical_solutions as ana  # noqa: E402
@@ -310,6 +311,53 @@ def gen_steps():
 
 
 # ---------------------------------------------------------------------------
+# The production run loop (run_storm.py:120-172) on a small grid: the vortex
+# with wind taper, theta' zeroed, the projection-only pre-balance, then the
+# reference's build_production_config steps with the intensity cap added after
+# each step.  Vmax is above the cap so the cap acts.
+# ---------------------------------------------------------------------------
+
+STORM = dict(nx=32, ny=32, nz=8, dx=PC.DX, Lz=PC.LZ, f=6.0e-5, u_env=-4.0, v_env=1.5,
+             vortex=dict(Vmax=78.0, Rmax=60e3, B=1.6, R_env=220e3, wind_taper=True,
+                         taper_start_frac=0.4),
+             n_prebal=PC.N_PREBAL, nsteps=4, dt=PC.DT, v_cap=PC.VMAX_CAP_MS,
+             tau_cap=PC.TAU_CAP)
+
+
+def gen_production_storm():
+    from dataclasses import replace as dc_replace
+    c = STORM
+    nx, ny, nz = c["nx"], c["ny"], c["nz"]
+    Lx, Ly, Lz = nx * c["dx"], ny * c["dx"], c["Lz"]
+    base = Base(nz, Lz)
+    init = HollandVortexInit(f=c["f"], u_env=c["u_env"], v_env=c["v_env"], **c["vortex"])
+    s = init.build_state(nx, ny, nz, Lx, Ly, base)
+    s = dc_replace(s, theta_prime=np.zeros_like(s.theta_prime))
+    out = {"config_json": np.array(json.dumps(c))}
+    out.update(st_dict("s0_", s))
+    pre = RK3Integrator(config=PC.build_prebal_config(nx, ny, nz, Lx, Ly, Lz), base=base)
+    for i in range(c["n_prebal"]):
+        s, _ = pre.step(s, dt=1.0, step_number=i)
+    out.update(st_dict("pb_", s))
+    integ = RK3Integrator(config=PC.build_production_config(nx, ny, nz, Lx, Ly, Lz, c["f"],
+                                                            c["u_env"], c["v_env"]),
+                          base=base)
+    cap = IntensityCapComponent(v_cap=c["v_cap"], tau=c["tau_cap"], u_env=c["u_env"],
+                                v_env=c["v_env"])
+    capped = []
+    for n in range(c["nsteps"]):
+        s, dg = integ.step(s, dt=c["dt"], step_number=n)
+        ct = cap.compute_tendency(s, None, None, base, c["dt"])
+        capped.append(int(np.count_nonzero(ct.du_dt)))
+        s = dc_replace(s, u=s.u + c["dt"] * ct.du_dt, v=s.v + c["dt"] * ct.dv_dt)
+        out.update(st_dict(f"s{n + 1}_", s))
+        out[f"d{n + 1}"] = np.array([dg.max_u, dg.max_v, dg.max_w, dg.max_theta_prime,
+                                     dg.surface_phi_min, dg.surface_phi_max])
+    out["capped_cells"] = np.array(capped)
+    np.savez_compressed(OUT / "production_storm.npz", **out)
+
+
+# ---------------------------------------------------------------------------
 # Vortex init and tracker fixtures
 # ---------------------------------------------------------------------------
 
@@ -465,6 +513,7 @@ if __name__ == "__main__":
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
+                production_storm=gen_production_storm,
                 vortex_tracker=gen_vortex_tracker, pins=gen_pins)
     for k, f in jobs.items():
         if a.only and k != a.only:

@@ -142,6 +142,51 @@ def test_rk3_steps_match_reference(golden_dir, case):
         np.testing.assert_allclose(d, g[f"d{n + 1}"], rtol=1e-13, atol=0)
 
 
+def test_production_run_loop(golden_dir):
+    """The reference's production run loop (run_storm.py:120-172): tapered
+    vortex with theta' zeroed, projection-only pre-balance, then
+    build_production_config steps (production_config.py:128-150) with the
+    intensity cap added after each step."""
+    g = np.load(golden_dir / "production_storm.npz")
+    c = json.loads(str(g["config_json"]))
+    nx, ny, nz = c["nx"], c["ny"], c["nz"]
+    Lx, Ly, Lz = nx * c["dx"], ny * c["dx"], c["Lz"]
+    z, rho0, th0 = O.build_base_state(nz, Lz)
+    s = O.Holland(f=c["f"], u_env=c["u_env"], v_env=c["v_env"], **c["vortex"]).build_state(
+        nx, ny, nz, Lx, Ly, z, rho0, th0)
+    s.theta_prime = np.zeros_like(s.theta_prime)
+    ref = _state(g, "s0_")
+    for f in ("u", "v", "w", "theta_prime"):
+        assert rel(getattr(s, f), getattr(ref, f)) <= TIGHT, f
+    pre = O.Integrator(O.StepConfig(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, Lz=Lz, buoyancy=False,
+                                    advection=None), z, rho0, th0)
+    for i in range(c["n_prebal"]):
+        s, _ = pre.step(s, 1.0, step_number=i)
+    ref = _state(g, "pb_")
+    for f in ("u", "v", "w", "theta_prime", "projection_potential"):
+        assert rel(getattr(s, f), getattr(ref, f)) <= TIGHT, ("prebal", f)
+    cfg = O.StepConfig(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, Lz=Lz, buoyancy=False,
+                       advection="centered2",
+                       coriolis=dict(f=c["f"], mode="beta_plane", Ly=Ly, ny=ny,
+                                     u_env=c["u_env"], v_env=c["v_env"], periodic_taper=True),
+                       damping_epsilon=0.5, hyper=3.0e11, cooling=1800.0,
+                       drag=dict(Cd=1.5e-3, H_bl=1000.0, u_env=c["u_env"], v_env=c["v_env"]))
+    integ = O.Integrator(cfg, z, rho0, th0)
+    for n in range(c["nsteps"]):
+        s, dg = integ.step(s, c["dt"], step_number=n)
+        du, dv = O.intensity_cap_tendency(s.u, s.v, c["v_cap"], c["tau_cap"], c["u_env"],
+                                          c["v_env"])
+        assert np.count_nonzero(du) == g["capped_cells"][n]
+        s.u = s.u + c["dt"] * du
+        s.v = s.v + c["dt"] * dv
+        ref = _state(g, f"s{n + 1}_")
+        for f in ("u", "v", "w", "theta_prime", "projection_potential"):
+            assert rel(getattr(s, f), getattr(ref, f)) <= TIGHT, (n, f)
+        d = np.array([dg.max_u, dg.max_v, dg.max_w, dg.max_theta_prime,
+                      dg.surface_phi_min, dg.surface_phi_max])
+        np.testing.assert_allclose(d, g[f"d{n + 1}"], rtol=1e-13, atol=0)
+
+
 def test_vortex_init_and_tracker(golden_dir):
     g = np.load(golden_dir / "vortex_tracker.npz")
     nx, ny, nz, Lx, Ly, Lz = 32, 24, 8, 640e3, 480e3, 16e3
