@@ -562,6 +562,8 @@ def run_b200(args):
                                      "divergence = anelastic divergence evaluated in FP64")
     if production is not None:
         line["production"] = production
+    if rank == 0 and world == 1 and not args.no_diagnostics:
+        line["diagnostics"] = diagnostics_report(w, st, base)
     if not args.no_ensemble:
         ens = ensemble_report(args, load_peaks()[0])
         if rank == 0:
@@ -674,6 +676,54 @@ def production_report(args, w, hs, barrier, dev, peak_gbs):
     return rep
 
 
+def diagnostics_report(w, st, base, reps=20, cpu_reps=3):
+    """The vortex diagnostics read-outs on the bench state (device fields of
+    the timed run): ``compute_diagnostics`` and the sub-cell refinement,
+    each a synchronous API call (kernels + the host's scalar logic + the
+    copies of the scalars), median wall time of ``reps`` calls after two
+    warm-up calls; beside them the oracle (NumPy, one core) on the same
+    state, median of ``cpu_reps`` calls."""
+    import torch
+    from oracle import vortex_diag as VD
+    from oraclev8_b200 import diagnostics as D
+    nx, ny, nz, Lx, Ly, Lz = grid_of(w)
+    dx = Lx / nx
+    cx, cy = 0.5 * Lx, 0.5 * Ly
+    u_env, v_env = w["coriolis"].get("u_env", 0.0), w["coriolis"].get("v_env", 0.0)
+
+    def dev_call():
+        d = D.compute_diagnostics(st, base, cx, cy, dx, dx, u_env, v_env, theta_xy_m=(cx, cy))
+        return d, D.subcell_refine(st, d["xv_m"], d["yv_m"], dx)
+
+    def med(fn, n):
+        ts = []
+        for _ in range(n):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts) * 1e3, out
+
+    for _ in range(2):
+        dev_call()
+    ms, (d, xy) = med(dev_call, reps)
+    u = st.u.double().cpu().numpy()
+    v = st.v.double().cpu().numpy()
+    z = np.asarray(base.z)
+
+    def cpu_call():
+        dd = VD.compute_diagnostics(u, v, z, cx, cy, dx, dx, u_env, v_env, theta_xy_m=(cx, cy))
+        return dd, VD.subcell_refine(u, v, dd["xv_m"], dd["yv_m"], dx)
+
+    cms, (dref, xyref) = med(cpu_call, cpu_reps)
+    return {"calls": "compute_diagnostics + subcell_refine (one diagnostics read-out)",
+            "ms_per_readout": ms, "cpu_oracle_ms_per_readout": cms, "cpu_cores": 1,
+            "speedup_vs_cpu_oracle": cms / ms,
+            "centre_equal_to_oracle": (d["xv_m"], d["yv_m"]) == (dref["xv_m"], dref["yv_m"]),
+            "subcell_max_abs_diff_m": float(max(abs(a - b) for a, b in zip(xy, xyref)))}
+
+
 def ensemble_report(args, peak_gbs):
     """Ensemble and serving measurements through ``oraclev8_b200.serving``.
 
@@ -782,6 +832,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-production", action="store_true",
                     help="skip the production-physics leg")
+    ap.add_argument("--no-diagnostics", action="store_true",
+                    help="skip the vortex-diagnostics read-out timing")
     ap.add_argument("--no-fp64-companion", action="store_true",
                     help="skip the plain-FP64 timing and accuracy report (profiling runs)")
     ap.add_argument("--ensemble-runs", type=int, default=64)

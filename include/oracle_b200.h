@@ -302,6 +302,65 @@ int oracle_b200_track_theta(OracleTracker *tracker, const void *theta_prime, int
 int oracle_b200_track_vorticity(OracleTracker *tracker, const void *u, const void *v,
                                 int precision, double dx, double *zcol_host, void *stream);
 
+/* ---- vortex diagnostics read-outs (oracle_v8/diagnostics.py) ------------ */
+/* Device reductions behind diagnostics.low_level_vmax, vmax_3d,
+ * ventilation_flow, vorticity_center, perturbation_ke and enstrophy
+ * (diagnostics.py:65-220) and the sub-cell centre refinement
+ * (run_translation_test.py:115-161).  u, v: device (nx, ny, nz) fields of
+ * `precision`; arithmetic in double.  levels: HOST array of nlev ascending
+ * level indices (the level band).  Every call blocks until its host outputs
+ * hold the result. */
+typedef struct OracleVortexDiag OracleVortexDiag;
+
+/* numpy.argmax result: value and C-order flat index. */
+typedef struct OracleVdMax {
+  double value;
+  long long index;
+} OracleVdMax;
+
+int oracle_b200_vdiag_create(int nx, int ny, int nz, OracleVortexDiag **out);
+int oracle_b200_vdiag_destroy(OracleVortexDiag *diag);
+
+/* argmax over the listed levels of |(u - u_env, v - v_env)|; index
+ * (ix * ny + iy) * nz + iz (low_level_vmax :65-98 with its band, vmax_3d
+ * :101-112 with every level). */
+int oracle_b200_vdiag_speed_max(OracleVortexDiag *diag, const void *u, const void *v,
+                                int precision, const int *levels, int nlev, double u_env,
+                                double v_env, OracleVdMax *out, void *stream);
+
+/* Band-mean winds, their periodic centred vorticity, its argmax inside
+ * r < window_m about (cx_m, cy_m) (index ix * ny + iy; 0 when the window holds
+ * no cell) and the sum of zeta^2 over the plane (vorticity_center :172-191,
+ * enstrophy :210-220). */
+int oracle_b200_vdiag_vorticity(OracleVortexDiag *diag, const void *u, const void *v,
+                                int precision, const int *levels, int nlev, double dx,
+                                double dy, double cx_m, double cy_m, double window_m,
+                                OracleVdMax *center, double *zeta_sq_sum, void *stream);
+
+/* Sum over every cell of (u - u_env)^2 + (v - v_env)^2 (perturbation_ke :203-207). */
+int oracle_b200_vdiag_ke(OracleVortexDiag *diag, const void *u, const void *v, int precision,
+                         double u_env, double v_env, double *sum, void *stream);
+
+/* Band-mean winds summed over the rings edges[b] <= r < edges[b+1]
+ * (b < n_bins, 1 <= n_bins <= 64) and over the disk r < r_vent_m:
+ * out[3 b + 0..2] = (cells, sum u, sum v), the disk at b = n_bins
+ * (ventilation_flow :150-166). */
+int oracle_b200_vdiag_rings(OracleVortexDiag *diag, const void *u, const void *v,
+                            int precision, const int *levels, int nlev, double dx, double dy,
+                            double cx_m, double cy_m, const double *edges, int n_bins,
+                            double r_vent_m, double *out, void *stream);
+
+/* The refinement's field: positive vorticity mean over levels [0, nz/2)
+ * (nz/2 <= 128), spacing dx on both axes, [1,2,1] smoothed in x then y; kept
+ * in the workspace for oracle_b200_vdiag_centroid. */
+int oracle_b200_vdiag_zpos(OracleVortexDiag *diag, const void *u, const void *v, int precision,
+                           double dx, void *stream);
+
+/* (sum w, sum ix w, sum iy w), w = field^2, over [i0, i1) x [j0, j1) of the
+ * last oracle_b200_vdiag_zpos field: one centroid iteration. */
+int oracle_b200_vdiag_centroid(OracleVortexDiag *diag, int i0, int i1, int j0, int j1,
+                               double *out, void *stream);
+
 /* Poisson solve that allocates no device memory.  No counterpart in the
  * reference: it is an extra entry point for callers that cannot call
  * cudaMalloc when they need a solve (a process whose own allocator already

@@ -36,7 +36,9 @@ EXPORTS = (
     "oracle_b200_track_vorticity", "oracle_b200_step_graph_create",
     "oracle_b200_step_graph_launch", "oracle_b200_step_graph_kernels",
     "oracle_b200_step_graph_destroy", "oracle_b200_vortex_fill", "oracle_b200_plan_release",
-    "oracle_b200_intensity_cap",
+    "oracle_b200_intensity_cap", "oracle_b200_vdiag_create", "oracle_b200_vdiag_destroy",
+    "oracle_b200_vdiag_speed_max", "oracle_b200_vdiag_vorticity", "oracle_b200_vdiag_ke",
+    "oracle_b200_vdiag_rings", "oracle_b200_vdiag_zpos", "oracle_b200_vdiag_centroid",
 )
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
@@ -72,6 +74,10 @@ class TrackFix(ctypes.Structure):
                 ("raw_idx", ctypes.c_longlong), ("raw_nb", c_double * 5),
                 ("win_min", c_double), ("win_max", c_double),
                 ("win_idx", ctypes.c_longlong), ("win_nb", c_double * 5)]
+
+
+class VdMax(ctypes.Structure):
+    _fields_ = [("value", c_double), ("index", ctypes.c_longlong)]
 
 
 _lib = None
@@ -125,6 +131,21 @@ def load(path: Path | None = None):
         "oracle_b200_step_graph_destroy": ([vp], c_int),
         "oracle_b200_vortex_fill": ([c_int, c_int, c_int, c_int, vp, vp, vp, vp, c_int, c_double,
                                      c_double, POINTER(StatePtrs), vp], c_int),
+        "oracle_b200_vdiag_create": ([c_int, c_int, c_int, POINTER(vp)], c_int),
+        "oracle_b200_vdiag_destroy": ([vp], c_int),
+        "oracle_b200_vdiag_speed_max": ([vp, vp, vp, c_int, POINTER(c_int), c_int, c_double,
+                                         c_double, POINTER(VdMax), vp], c_int),
+        "oracle_b200_vdiag_vorticity": ([vp, vp, vp, c_int, POINTER(c_int), c_int, c_double,
+                                         c_double, c_double, c_double, c_double, POINTER(VdMax),
+                                         POINTER(c_double), vp], c_int),
+        "oracle_b200_vdiag_ke": ([vp, vp, vp, c_int, c_double, c_double, POINTER(c_double), vp],
+                                 c_int),
+        "oracle_b200_vdiag_rings": ([vp, vp, vp, c_int, POINTER(c_int), c_int, c_double, c_double,
+                                     c_double, c_double, POINTER(c_double), c_int, c_double,
+                                     POINTER(c_double), vp], c_int),
+        "oracle_b200_vdiag_zpos": ([vp, vp, vp, c_int, c_double, vp], c_int),
+        "oracle_b200_vdiag_centroid": ([vp, c_int, c_int, c_int, c_int, POINTER(c_double), vp],
+                                       c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

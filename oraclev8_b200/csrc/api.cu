@@ -15,6 +15,7 @@
 #include "pencil.cuh"
 #include "xreg.cuh"
 #include "tracker.cuh"
+#include "vdiag.cuh"
 #include "init.cuh"
 
 using namespace ob;
@@ -1622,6 +1623,241 @@ int oracle_b200_track_vorticity(OracleTracker* t, const void* u, const void* v, 
   OB_LAUNCHED();
   OB_CUDA(cudaMemcpyAsync(zcol_host, t->zcol, (size_t)t->nx * t->ny * sizeof(double),
                           cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+/* ---- vortex diagnostics ------------------------------------------------- */
+
+struct OracleVortexDiag {
+  int nx = 0, ny = 0, nz = 0;
+  int nblk = 1;  // CTAs of the grid-wide reductions
+  int* lev = nullptr;
+  double *um = nullptr, *vm = nullptr, *zeta = nullptr, *zp = nullptr, *zs = nullptr;
+  double *sq = nullptr, *dsum = nullptr, *ring = nullptr, *edges = nullptr, *cen = nullptr;
+  VdMax *part = nullptr, *best = nullptr;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+constexpr int kVdMaxBins = 64;
+
+void vdiag_free(OracleVortexDiag* d) {
+  for (void* q : d->allocs) cudaFree(q);
+  delete d;
+}
+
+int vdiag_call(const OracleVortexDiag* d, int precision, const void* u, const void* v) {
+  if (!d) return fail(OB_ERR_ARG, "vdiag: workspace is NULL");
+  if (!u || !v) return fail(OB_ERR_ARG, "vdiag: NULL field");
+  if (precision != OB_PREC_F64 && precision != OB_PREC_F32)
+    return fail(OB_ERR_ARG, "vdiag: precision must be OB_PREC_F64 or OB_PREC_F32");
+  return OB_OK;
+}
+
+// Uploads the level list after checking it is ascending inside [0, nz).
+int vdiag_levels(OracleVortexDiag* d, const int* lev, int nlev, cudaStream_t st) {
+  if (!lev || nlev < 1 || nlev > d->nz) return fail(OB_ERR_ARG, "vdiag: bad level list");
+  for (int l = 0; l < nlev; ++l)
+    if (lev[l] < 0 || lev[l] >= d->nz || (l > 0 && lev[l] <= lev[l - 1]))
+      return fail(OB_ERR_ARG, "vdiag: levels must ascend inside [0, nz)");
+  OB_CUDA(cudaMemcpyAsync(d->lev, lev, nlev * sizeof(int), cudaMemcpyHostToDevice, st));
+  return OB_OK;
+}
+
+int vdiag_mean_winds(OracleVortexDiag* d, const void* u, const void* v, int precision, int nlev,
+                     cudaStream_t st) {
+  const long long ncol = (long long)d->nx * d->ny;
+  if (precision == OB_PREC_F64)
+    k_vd_band_mean<double><<<d->nblk, kVdThreads, 0, st>>>(
+        (const double*)u, (const double*)v, ncol, d->nz, d->lev, nlev, d->um, d->vm);
+  else
+    k_vd_band_mean<float><<<d->nblk, kVdThreads, 0, st>>>(
+        (const float*)u, (const float*)v, ncol, d->nz, d->lev, nlev, d->um, d->vm);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+}  // namespace
+
+int oracle_b200_vdiag_create(int nx, int ny, int nz, OracleVortexDiag** out) {
+  if (!out) return fail(OB_ERR_ARG, "vdiag_create: out is NULL");
+  *out = nullptr;
+  if (nx < 3 || ny < 3 || nz < 1 || (long long)nx * ny > (1LL << 30) ||
+      (long long)nx * ny * nz > (1LL << 40))
+    return fail(OB_ERR_ARG, "vdiag_create: need nx, ny >= 3 and nz >= 1 (got %d, %d, %d)", nx,
+                ny, nz);
+  int dev = 0, nsm = 148;
+  OB_CUDA(cudaGetDevice(&dev));
+  OB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  OracleVortexDiag* d = new OracleVortexDiag();
+  d->nx = nx;
+  d->ny = ny;
+  d->nz = nz;
+  const long long ncol = (long long)nx * ny;
+  d->nblk = (int)std::min<long long>((ncol + kVdThreads - 1) / kVdThreads, 2LL * nsm);
+  auto A = [&](void** q, size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return fail(OB_ERR_CUDA, "vdiag_create: cudaMalloc");
+    d->allocs.push_back(p);
+    *q = p;
+    return (int)OB_OK;
+  };
+  int rc;
+  if ((rc = A((void**)&d->lev, nz * sizeof(int))) || (rc = A((void**)&d->um, ncol * 8)) ||
+      (rc = A((void**)&d->vm, ncol * 8)) || (rc = A((void**)&d->zeta, ncol * 8)) ||
+      (rc = A((void**)&d->zp, ncol * 8)) || (rc = A((void**)&d->zs, ncol * 8)) ||
+      (rc = A((void**)&d->sq, d->nblk * 8)) || (rc = A((void**)&d->dsum, 8)) ||
+      (rc = A((void**)&d->ring, 3 * (kVdMaxBins + 1) * 8)) ||
+      (rc = A((void**)&d->edges, (kVdMaxBins + 1) * 8)) || (rc = A((void**)&d->cen, 3 * 8)) ||
+      (rc = A((void**)&d->part, d->nblk * sizeof(VdMax))) ||
+      (rc = A((void**)&d->best, sizeof(VdMax)))) {
+    vdiag_free(d);
+    return rc;
+  }
+  *out = d;
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_destroy(OracleVortexDiag* d) {
+  if (d) vdiag_free(d);
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_speed_max(OracleVortexDiag* d, const void* u, const void* v,
+                                int precision, const int* levels, int nlev, double u_env,
+                                double v_env, OracleVdMax* out, void* stream) {
+  if (int rc = vdiag_call(d, precision, u, v)) return rc;
+  if (!out) return fail(OB_ERR_ARG, "vdiag_speed_max: out is NULL");
+  static_assert(sizeof(VdMax) == sizeof(OracleVdMax), "VdMax layout");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (int rc = vdiag_levels(d, levels, nlev, st)) return rc;
+  const long long ncol = (long long)d->nx * d->ny;
+  if (precision == OB_PREC_F64)
+    k_vd_speed_max<double><<<d->nblk, kVdThreads, 0, st>>>(
+        (const double*)u, (const double*)v, ncol, d->nz, d->lev, nlev, u_env, v_env, d->part);
+  else
+    k_vd_speed_max<float><<<d->nblk, kVdThreads, 0, st>>>(
+        (const float*)u, (const float*)v, ncol, d->nz, d->lev, nlev, u_env, v_env, d->part);
+  OB_LAUNCHED();
+  k_vd_max_final<<<1, kVdThreads, 0, st>>>(d->part, d->nblk, d->best);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(out, d->best, sizeof(VdMax), cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_vorticity(OracleVortexDiag* d, const void* u, const void* v,
+                                int precision, const int* levels, int nlev, double dx,
+                                double dy, double cx_m, double cy_m, double window_m,
+                                OracleVdMax* center, double* zeta_sq_sum, void* stream) {
+  if (int rc = vdiag_call(d, precision, u, v)) return rc;
+  if (!center || !zeta_sq_sum || !(dx > 0.0) || !(dy > 0.0))
+    return fail(OB_ERR_ARG, "vdiag_vorticity: bad output or spacing");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (int rc = vdiag_levels(d, levels, nlev, st)) return rc;
+  if (int rc = vdiag_mean_winds(d, u, v, precision, nlev, st)) return rc;
+  k_vd_zeta<<<d->nblk, kVdThreads, 0, st>>>(d->um, d->vm, d->nx, d->ny, dx, dy, cx_m, cy_m,
+                                            window_m, d->zeta, d->part, d->sq);
+  OB_LAUNCHED();
+  k_vd_max_final<<<1, kVdThreads, 0, st>>>(d->part, d->nblk, d->best);
+  OB_LAUNCHED();
+  k_vd_sum_final<<<1, kVdThreads, 0, st>>>(d->sq, d->nblk, d->dsum);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(center, d->best, sizeof(VdMax), cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaMemcpyAsync(zeta_sq_sum, d->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_ke(OracleVortexDiag* d, const void* u, const void* v, int precision,
+                         double u_env, double v_env, double* sum, void* stream) {
+  if (int rc = vdiag_call(d, precision, u, v)) return rc;
+  if (!sum) return fail(OB_ERR_ARG, "vdiag_ke: out is NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)d->nx * d->ny * d->nz;
+  if (precision == OB_PREC_F64)
+    k_vd_ke<double><<<d->nblk, kVdThreads, 0, st>>>((const double*)u, (const double*)v, n,
+                                                    u_env, v_env, d->sq);
+  else
+    k_vd_ke<float><<<d->nblk, kVdThreads, 0, st>>>((const float*)u, (const float*)v, n, u_env,
+                                                   v_env, d->sq);
+  OB_LAUNCHED();
+  k_vd_sum_final<<<1, kVdThreads, 0, st>>>(d->sq, d->nblk, d->dsum);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(sum, d->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_rings(OracleVortexDiag* d, const void* u, const void* v,
+                            int precision, const int* levels, int nlev, double dx, double dy,
+                            double cx_m, double cy_m, const double* edges, int n_bins,
+                            double r_vent_m, double* out, void* stream) {
+  if (int rc = vdiag_call(d, precision, u, v)) return rc;
+  if (!out || !edges || n_bins < 1 || n_bins > kVdMaxBins || !(dx > 0.0) || !(dy > 0.0))
+    return fail(OB_ERR_ARG, "vdiag_rings: bad output, edges, bin count (1..%d) or spacing",
+                kVdMaxBins);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (int rc = vdiag_levels(d, levels, nlev, st)) return rc;
+  if (int rc = vdiag_mean_winds(d, u, v, precision, nlev, st)) return rc;
+  // bounding box of the disk, one cell of margin each side (every cell with
+  // r < r_vent lies inside it); empty for a non-finite centre or radius
+  double rmax = r_vent_m;
+  for (int b = 0; b <= n_bins; ++b) rmax = std::fmax(rmax, edges[b]);
+  int i0 = 0, i1 = 0, j0 = 0, j1 = 0;
+  if (std::isfinite(cx_m) && std::isfinite(cy_m) && std::isfinite(rmax)) {
+    auto clampi = [](double a, int n) { return (int)std::fmin(std::fmax(a, 0.0), (double)n); };
+    i0 = clampi(std::floor((cx_m - rmax) / dx - 0.5) - 1.0, d->nx);
+    i1 = clampi(std::ceil((cx_m + rmax) / dx - 0.5) + 2.0, d->nx);
+    j0 = clampi(std::floor((cy_m - rmax) / dy - 0.5) - 1.0, d->ny);
+    j1 = clampi(std::ceil((cy_m + rmax) / dy - 0.5) + 2.0, d->ny);
+  }
+  if (i1 <= i0 || j1 <= j0) {
+    i0 = i1 = 0;
+    j0 = j1 = 0;
+  }
+  OB_CUDA(cudaMemcpyAsync(d->edges, edges, (n_bins + 1) * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  k_vd_rings<<<1, kVdThreads, 0, st>>>(d->um, d->vm, d->ny, i0, i1, j0, j1, dx, dy, cx_m, cy_m,
+                                       d->edges, n_bins, r_vent_m, d->ring);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(out, d->ring, 3 * (n_bins + 1) * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_zpos(OracleVortexDiag* d, const void* u, const void* v, int precision,
+                           double dx, void* stream) {
+  if (int rc = vdiag_call(d, precision, u, v)) return rc;
+  if (!(dx > 0.0)) return fail(OB_ERR_ARG, "vdiag_zpos: dx must be > 0");
+  if (d->nz < 2 || d->nz / 2 > kVdMaxPairwise)
+    return fail(OB_ERR_ARG, "vdiag_zpos: need 2 <= nz and nz / 2 <= %d", kVdMaxPairwise);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == OB_PREC_F64)
+    k_vd_zpos<double><<<d->nblk, kVdThreads, 0, st>>>((const double*)u, (const double*)v,
+                                                      d->nx, d->ny, d->nz, dx, d->zp);
+  else
+    k_vd_zpos<float><<<d->nblk, kVdThreads, 0, st>>>((const float*)u, (const float*)v, d->nx,
+                                                     d->ny, d->nz, dx, d->zp);
+  OB_LAUNCHED();
+  k_vd_smooth<<<d->nblk, kVdThreads, 0, st>>>(d->zp, d->nx, d->ny, d->zs);
+  OB_LAUNCHED();
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+int oracle_b200_vdiag_centroid(OracleVortexDiag* d, int i0, int i1, int j0, int j1,
+                               double* out, void* stream) {
+  if (!d || !out) return fail(OB_ERR_ARG, "vdiag_centroid: NULL argument");
+  if (i0 < 0 || j0 < 0 || i1 > d->nx || j1 > d->ny || i1 < i0 || j1 < j0)
+    return fail(OB_ERR_ARG, "vdiag_centroid: patch outside the grid");
+  cudaStream_t st = (cudaStream_t)stream;
+  k_vd_centroid<<<1, kVdThreads, 0, st>>>(d->zs, d->ny, i0, i1, j0, j1, d->cen);
+  OB_LAUNCHED();
+  OB_CUDA(cudaMemcpyAsync(out, d->cen, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
   OB_CUDA(cudaStreamSynchronize(st));
   return OB_OK;
 }

@@ -358,6 +358,103 @@ def gen_production_storm():
 
 
 # ---------------------------------------------------------------------------
+# Vortex diagnostics read-outs (diagnostics.py) and the sub-cell centre
+# refinement of run_translation_test.py.  That module exits on import without
+# CuPy, so its _subcell_refine is taken from the file with ast and run as is,
+# with NumPy as its array module.
+# ---------------------------------------------------------------------------
+
+def _reference_subcell_refine():
+    import ast
+    path = Path(REF) / "oracle_v8" / "run_translation_test.py"
+    tree = ast.parse(path.read_text())
+    fn = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == "_subcell_refine"]
+    ns = {"xp": np, "np": np}
+    exec(compile(ast.Module(body=fn, type_ignores=[]), str(path), "exec"), ns)
+    return ns["_subcell_refine"]
+
+
+def gen_diagnostics():
+    import types
+    import warnings
+    from oracle_v8 import diagnostics as dg
+    refine = _reference_subcell_refine()
+    ps = np.load(OUT / "production_storm.npz")
+    vt = np.load(OUT / "vortex_tracker.npz")
+    # a deeper state: 40 levels, off-centre vortex in a background flow, noise
+    nx, ny, nz, Lx, Ly, Lz = 24, 20, 40, 480e3, 400e3, 10e3
+    base_c = Base(nz, Lz)
+    sc = HollandVortexInit(Vmax=60.0, Rmax=30e3, B=1.7, f=5.5e-5, u_env=2.0, v_env=-1.5
+                           ).build_state(nx, ny, nz, Lx, Ly, base_c, x_c=210e3, y_c=230e3)
+    rng = np.random.default_rng(4242)
+    cu = sc.u + 0.5 * rng.standard_normal(sc.u.shape)
+    cv = sc.v + 0.5 * rng.standard_normal(sc.v.shape)
+    out = {"c_u": cu, "c_v": cv}
+    cases = {
+        "storm": (ps["s4_u"], ps["s4_v"], 32, 32, 8, 15_625.0, 20e3, -4.0, 1.5),
+        "tracker": (vt["exp_u"], vt["exp_v"], 32, 24, 8, 20e3, 16e3, -3.0, 1.0),
+        "deep": (cu, cv, nx, ny, nz, 20e3, Lz, 2.0, -1.5),
+    }
+    res = {}
+    for name, (u, v, nx_, ny_, nz_, dx, Lz_, ue, ve) in cases.items():
+        st = types.SimpleNamespace(u=u, v=v, theta_prime=np.zeros_like(u))
+        base = Base(nz_, Lz_)
+        Lx_, Ly_ = nx_ * dx, ny_ * dx
+        cx, cy = 0.47 * Lx_, 0.52 * Ly_
+        calls = []
+
+        def rec(fn, kw, val):
+            calls.append(dict(fn=fn, kw=kw, out=val))
+
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            kw = dict(cx_m=cx, cy_m=cy, u_env=ue, v_env=ve, theta_xy_m=[cx + 7e3, cy - 4e3],
+                      r_vent_m=120e3)
+            d = dg.compute_diagnostics(st, base, kw["cx_m"], kw["cy_m"], dx, dx, ue, ve,
+                                       theta_xy_m=tuple(kw["theta_xy_m"]), r_vent_m=120e3)
+            rec("compute_diagnostics", kw, d)
+            rec("format_diag_line", kw, dg.format_diag_line(d))
+            for w, zt in ((200e3, 3000.0), (100e3, 1500.0), (250e3, 6000.0), (1.0, 3000.0)):
+                rec("vorticity_center", dict(cx_m=cx, cy_m=cy, window_m=w, z_top_m=zt),
+                    dg.vorticity_center(st, cx, cy, dx, dx, base=base, window_m=w,
+                                        z_top_m=zt))
+            rec("vorticity_center", dict(cx_m=cx, cy_m=cy, window_m=200e3, z_top_m=3000.0,
+                                         no_base=True),
+                dg.vorticity_center(st, cx, cy, dx, dx, base=None))
+            for zt in (3000.0, 500.0, 1e5):
+                rec("low_level_vmax", dict(cx_m=cx, cy_m=cy, u_env=ue, v_env=ve, z_top_m=zt),
+                    dg.low_level_vmax(st, base, cx, cy, dx, dx, u_env=ue, v_env=ve,
+                                      z_top_m=zt))
+            rec("vmax_3d", dict(u_env=ue, v_env=ve), dg.vmax_3d(st, base, u_env=ue, v_env=ve))
+            for r_v, nb, c in ((150e3, 12, (cx, cy)), (80e3, 5, (cx, cy)),
+                               (120e3, 12, (-1e7, -1e7)), (90e3, 7, (0.1 * Lx_, 0.9 * Ly_))):
+                rec("ventilation_flow", dict(cx_m=c[0], cy_m=c[1], r_vent_m=r_v, n_bins=nb,
+                                             u_env=ue, v_env=ve),
+                    dg.ventilation_flow(st, c[0], c[1], dx, dx, base=base, r_vent_m=r_v,
+                                        n_bins=nb, u_env=ue, v_env=ve))
+            rec("ventilation_flow", dict(cx_m=cx, cy_m=cy, r_vent_m=150e3, n_bins=12,
+                                         no_base=True, z_lo_m=0.0, z_hi_m=12000.0),
+                dg.ventilation_flow(st, cx, cy, dx, dx, base=None))
+            rec("ventilation_flow", dict(cx_m=cx, cy_m=cy, r_vent_m=150e3, n_bins=12,
+                                         z_lo_m=2000.0, z_hi_m=5000.0),
+                dg.ventilation_flow(st, cx, cy, dx, dx, base=base, z_lo_m=2000.0,
+                                    z_hi_m=5000.0))
+            rec("perturbation_ke", dict(u_env=ue, v_env=ve),
+                dg.perturbation_ke(st, u_env=ue, v_env=ve))
+            for zt in (3000.0, 8000.0):
+                rec("enstrophy", dict(z_top_m=zt), dg.enstrophy(st, dx, dx, base=base,
+                                                               z_top_m=zt))
+            for (x0, y0, patch) in ((cx, cy, 9), (0.3 * dx, 0.2 * dx, 9), (cx, cy, 3),
+                                    (Lx_ - 0.4 * dx, 0.5 * Ly_, 5), (float("nan"), cy, 9),
+                                    (-60 * dx, cy, 9)):
+                xr, yr = refine(st, x0, y0, dx, patch=patch)
+                rec("subcell_refine", dict(x_m=x0, y_m=y0, patch=patch), [xr, yr])
+        res[name] = dict(dx=dx, Lz=Lz_, nz=nz_, calls=calls)
+    out["results_json"] = np.array(json.dumps(res))
+    np.savez_compressed(OUT / "diagnostics.npz", **out)
+
+
+# ---------------------------------------------------------------------------
 # Vortex init and tracker fixtures
 # ---------------------------------------------------------------------------
 
@@ -513,7 +610,7 @@ if __name__ == "__main__":
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
-                production_storm=gen_production_storm,
+                production_storm=gen_production_storm, diagnostics=gen_diagnostics,
                 vortex_tracker=gen_vortex_tracker, pins=gen_pins)
     for k, f in jobs.items():
         if a.only and k != a.only:

@@ -180,3 +180,14 @@ def test_tracker_host_logic_matches_oracle():
     for last in (None, (80e3, 70e3), (150e3, 20e3)):
         assert T._vorticity_centre(zcol, nx, ny, dx, last) == \
             O.vorticity_centre(u, v, nx, ny, dx, last_pos=last)
+
+
+def test_diagnostics_refuse_host_fields():
+    """The diagnostics read device fields only (no CPU fallback)."""
+    import types
+    from oraclev8_b200 import diagnostics as D
+    st = types.SimpleNamespace(u=np.zeros((4, 4, 4)), v=np.zeros((4, 4, 4)))
+    with pytest.raises(TypeError):
+        D.vmax_3d(st, None)
+    with pytest.raises(TypeError):
+        D.subcell_refine(st, 1.0, 1.0, 1.0)

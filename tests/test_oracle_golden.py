@@ -294,3 +294,23 @@ def test_production_component_tendencies(golden_dir):
             assert np.array_equal(a, g[f"{k}_{f}"]), (k, f)
     # the cap acts only above v_cap
     assert 0 < np.count_nonzero(g["cap_du_dt"]) < g["cap_du_dt"].size
+
+
+def test_vortex_diagnostics_match_reference(golden_dir):
+    """Every recorded call of diagnostics.py (vorticity centre with and without
+    a base state and with an empty window, low-level Vmax with an empty band,
+    ventilation flow with an off-grid centre, budgets, the one-call wrapper and
+    its log line) and run_translation_test._subcell_refine (clipped and empty
+    patches, a NaN seed), bit for bit."""
+    import warnings
+    from oracle import vortex_diag as VD
+    from tests.diag_cases import diag_states, replay, same
+    n = 0
+    for name, (u, v, z, dx, calls) in diag_states(golden_dir).items():
+        for c in calls:
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore", RuntimeWarning)
+                got = replay(c, VD, u, v, z, dx)
+            assert same(got, c["out"]), (name, c["fn"], c["kw"], got, c["out"])
+            n += 1
+    assert n == 78
