@@ -855,9 +855,21 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
     { Launch L_(p, cls, p->aux); k_thomas<T, kThomasCols, double><<<(unsigned)p->n_lw, kThomasCols, smem_thomas(p, 8), p->aux>>>(
           p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, p->lw_blocks, nullptr); }
     OB_LAUNCHED();
-    if (diag || !thomas_f32(p, cls, (cplx<float>*)S3, st))
+    // A solve that logs its residuals (every diag_every-th solve, counted
+    // from the plan's first) takes them from the generic sweep, writing into
+    // S1: no caller holds data there between the forward y transform and the
+    // inverse one.  Its solution comes from the same kernel as every other
+    // solve, so no result depends on the logging cadence or on how many
+    // solves the plan has run before (a run resumed on a new plan continues
+    // bit for bit).
+    if (diag) {
       { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
-            p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, nullptr, p->lw_flag); }
+            p->g, thomas_args(p), S3, (cplx<T>*)p->S1, diag, slot_c, slot_d, nullptr, p->lw_flag); }
+      OB_LAUNCHED();
+    }
+    if (!thomas_f32(p, cls, (cplx<float>*)S3, st))
+      { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
+            p->g, thomas_args(p), S3, S3, nullptr, slot_c, slot_d, nullptr, p->lw_flag); }
     OB_LAUNCHED();
     OB_CUDA(cudaEventRecord(p->ev_join, p->aux));
     OB_CUDA(cudaStreamWaitEvent(st, p->ev_join, 0));

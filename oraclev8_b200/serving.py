@@ -52,6 +52,11 @@ class RunRequest:
     arrival_s: float = 0.0
     dx: float = 10e3
     lz: float = 16e3
+    resume: Optional[dict] = None  # snapshot (oraclev8_b200.snapshot) to continue from
+
+    @property
+    def start_step(self) -> int:
+        return int(self.resume.get("step", 0)) if self.resume is not None else 0
 
     @property
     def f0(self) -> float:
@@ -124,8 +129,15 @@ def build_run(req: RunRequest, device_dtype=None):
         coriolis=CoriolisComponent(f=req.f0, mode="beta_plane", beta=req.beta, Ly=L, ny=n,
                                    periodic_taper=True))
     integ = RK3Integrator(cfg, base, precision=req.precision)
-    state = HollandVortexInit(req.vmax, req.rmax, req.b, f=req.f0, wind_decay_top=12e3
-                              ).build_state(n, n, nz, L, L, base, dtype=integ.dtype)
+    if req.resume is not None:
+        from .snapshot import state_from_snapshot
+        state = state_from_snapshot(req.resume, dtype=integ.dtype)
+        if tuple(state.u.shape) != (n, n, nz):
+            raise ValueError(f"resume snapshot has shape {tuple(state.u.shape)}, the "
+                             f"request {(n, n, nz)}")
+    else:
+        state = HollandVortexInit(req.vmax, req.rmax, req.b, f=req.f0, wind_decay_top=12e3
+                                  ).build_state(n, n, nz, L, L, base, dtype=integ.dtype)
     return integ, state, base
 
 
@@ -176,6 +188,8 @@ class _Active:
     left: int
     events: list = field(default_factory=list)
     bytes: int = 0
+    t: float = 0.0           # model time after the launched steps
+    snaps: list = field(default_factory=list)  # snapshot copies in flight
 
 
 class ServingEngine:
@@ -187,11 +201,22 @@ class ServingEngine:
     keep_final: copy each run's final state to the host when it retires.
     prepare_ahead: admitted runs being set up at once on the preparation
     thread.  inflight_cells: cells of the runs allowed work on the device at
-    once; runs are fed shortest remaining work first."""
+    once; runs are fed shortest remaining work first.
+    snapshot_every / snapshot_sink: every ``snapshot_every`` steps (at the
+    first graph boundary at or past each multiple) the run's state is copied
+    to pinned host memory on the run's own stream, and ``snapshot_sink(rid,
+    snapshot)`` receives it once the copy has landed (on the serving thread;
+    ``oraclev8_b200.snapshot.save_snapshot`` persists one).  A request whose
+    ``resume`` holds such a snapshot continues from it."""
 
     def __init__(self, hbm_budget: float = 150e9, chunk: int = 16, depth: int = 2,
                  realtime: bool = True, keep_final: bool = False, max_active: int = 256,
-                 prepare_ahead: int = 32, inflight_cells: float = 64e6):
+                 prepare_ahead: int = 32, inflight_cells: float = 64e6,
+                 snapshot_every: int = 0, snapshot_sink=None):
+        self.snapshot_every = int(snapshot_every)
+        self.snapshot_sink = snapshot_sink
+        if self.snapshot_every < 0 or (self.snapshot_every and snapshot_sink is None):
+            raise ValueError("snapshot_every needs a snapshot_sink (and must be >= 0)")
         self.budget = float(hbm_budget)
         self.inflight_cells = float(inflight_cells)
         self.prepare_ahead = int(prepare_ahead)
@@ -204,29 +229,48 @@ class ServingEngine:
         """Set a run up (plan, device initial state, step graphs): host work,
         done on the preparation thread while the main loop feeds the GPU."""
         stream = torch.cuda.Stream()
+        left = req.nsteps - req.start_step
+        if left < 1:
+            raise ValueError(f"request {req.rid}: nothing left to run after step "
+                             f"{req.start_step} of {req.nsteps}")
         with torch.cuda.stream(stream):
             integ, state, _ = build_run(req)
             graphs = {}
-            full = min(self.chunk, req.nsteps)
+            full = min(self.chunk, left)
             graphs[full] = integ.capture(state, req.dt, full)
-            tail = req.nsteps % full
+            tail = left % full
             if tail:
                 graphs[tail] = integ.capture(state, req.dt, tail)
         rec = RunRecord(req.rid, req.n, req.nz, req.precision, req.nsteps, req.cells,
                         req.arrival_s)
-        return _Active(req, rec, integ, state, stream, graphs, req.nsteps,
-                       bytes=footprint_bytes(req))
+        return _Active(req, rec, integ, state, stream, graphs, left,
+                       bytes=footprint_bytes(req), t=float(state.t))
 
     def _launch(self, a: _Active) -> None:
+        from .snapshot import SnapshotCopy
         k = min(self.chunk, a.left)
+        before = a.req.nsteps - a.left
         a.graphs[k].launch(a.stream)
+        if a.integ._fast:  # t advances once per step, as the step loop adds it
+            for _ in range(k):
+                a.t = a.t + a.req.dt
         ev = torch.cuda.Event()
         ev.record(a.stream)
         a.events.append(ev)
         a.left -= k
+        n = self.snapshot_every
+        if n and (a.req.nsteps - a.left) // n > before // n:
+            with torch.cuda.stream(a.stream):
+                a.snaps.append(SnapshotCopy(a.state, t=a.t, step=a.req.nsteps - a.left,
+                                            stream=a.stream))
+
+    def _drain_snapshots(self, a: _Active, wait: bool = False) -> None:
+        while a.snaps and (wait or a.snaps[0].ready()):
+            self.snapshot_sink(a.req.rid, a.snaps.pop(0).result())
 
     def _retire(self, a: _Active, now: float) -> RunRecord:
         a.rec.done_s = now
+        self._drain_snapshots(a, wait=True)
         if self.keep_final:
             with torch.cuda.stream(a.stream):
                 s = a.state
@@ -309,6 +353,8 @@ class ServingEngine:
                 for a in active:
                     if a.events:
                         a.events = [e for e in a.events if not e.query()]
+                    if a.snaps:
+                        self._drain_snapshots(a)
                 busy = sum(a.req.cells for a in active if a.events)
                 for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
                     if a.left > 0 and (a.events or busy < self.inflight_cells):

@@ -191,3 +191,37 @@ def test_diagnostics_refuse_host_fields():
         D.vmax_3d(st, None)
     with pytest.raises(TypeError):
         D.subcell_refine(st, 1.0, 1.0, 1.0)
+
+
+def test_snapshot_file_round_trip(tmp_path):
+    """The snapshot record of run_translation_test.py:291-295 through .npz and
+    back, keys and values unchanged; a file without the fields is refused."""
+    from oraclev8_b200 import snapshot as S
+    rng = np.random.default_rng(5)
+    snap = {f: rng.standard_normal((6, 5, 4 + (f == "w"))) for f in S.FIELDS}
+    snap.update(t=1234.5, cx=3.5e5, cy=None, step=17)
+    back = S.load_snapshot(S.save_snapshot(tmp_path / "s", snap))
+    assert set(back) == set(snap)
+    for k, val in snap.items():
+        if isinstance(val, np.ndarray):
+            assert np.array_equal(back[k], val) and back[k].dtype == val.dtype
+        else:
+            assert back[k] == val
+    np.savez(tmp_path / "bad.npz", u=snap["u"])
+    with pytest.raises(ValueError):
+        S.load_snapshot(tmp_path / "bad.npz")
+
+
+def test_gyre_snapshot_record(tmp_path):
+    """run_translation_test.py:2104-2125: column means, centred vorticity with
+    dx on both axes, centre and dx."""
+    from oraclev8_b200 import snapshot as S
+    rng = np.random.default_rng(6)
+    u, v = rng.standard_normal((8, 6, 5)), rng.standard_normal((8, 6, 5))
+    p = S.save_gyre_snapshot(tmp_path / "g", dict(u=u, v=v, cx=1.0, cy=2.0), 5e3)
+    d = np.load(p)
+    u2, v2 = u.mean(axis=2), v.mean(axis=2)
+    zeta = ((np.roll(v2, -1, 0) - np.roll(v2, 1, 0)) / (2 * 5e3)
+            - (np.roll(u2, -1, 1) - np.roll(u2, 1, 1)) / (2 * 5e3))
+    assert np.array_equal(d["zeta"], zeta) and np.array_equal(d["u"], u2)
+    assert float(d["cx"]) == 1.0 and float(d["cy"]) == 2.0 and float(d["dx"]) == 5e3
