@@ -564,6 +564,7 @@ def run_b200(args):
         line["production"] = production
     if rank == 0 and world == 1 and not args.no_diagnostics:
         line["diagnostics"] = diagnostics_report(w, st, base)
+        line["snapshot"] = snapshot_report(integ, st, dt)
     if not args.no_ensemble:
         ens = ensemble_report(args, load_peaks()[0])
         if rank == 0:
@@ -722,6 +723,57 @@ def diagnostics_report(w, st, base, reps=20, cpu_reps=3):
             "speedup_vs_cpu_oracle": cms / ms,
             "centre_equal_to_oracle": (d["xv_m"], d["yv_m"]) == (dref["xv_m"], dref["yv_m"]),
             "subcell_max_abs_diff_m": float(max(abs(a - b) for a, b in zip(xy, xyref)))}
+
+
+def snapshot_report(integ, st, dt, steps=12, every=4):
+    """Checkpoint cost on the bench state: one synchronous snapshot (device
+    to pinned host, median of 5), and ``steps`` public steps with an
+    asynchronous snapshot of every ``every``-th state on a side stream
+    (each step writes a new state, so the copy overlaps the next steps)
+    against the same steps without snapshots; device time with CUDA events."""
+    import torch
+    from oraclev8_b200 import snapshot as S
+    nbytes = sum(getattr(st, f).numel() * getattr(st, f).element_size() for f in S.FIELDS)
+    ts = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.take_snapshot(st)
+        ts.append(time.perf_counter() - t0)
+    sync_ms = statistics.median(ts) * 1e3
+    side = torch.cuda.Stream()
+    pinned = {}
+
+    def run(with_snaps):
+        s = st
+        copies = []
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for n in range(steps):
+            s, _ = integ.step(s, dt, n)
+            if with_snaps and (n + 1) % every == 0:
+                if copies:
+                    copies[-1].result()  # the pinned buffers are reused
+                copies.append(S.SnapshotCopy(s, step=n + 1, stream=side, pinned=pinned))
+                if not pinned:
+                    pinned.update(copies[-1].host)
+        e1.record(stream)
+        for c in copies:
+            c.result()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    run(False)
+    base_ms = run(False)
+    snap_ms = run(True)
+    return {"state_bytes": nbytes, "sync_snapshot_ms": sync_ms,
+            "sync_snapshot_gbs": nbytes / (sync_ms / 1e3) / 1e9,
+            "steps": steps, "snapshot_every": every,
+            "ms_per_step_without": base_ms / steps, "ms_per_step_with_async": snap_ms / steps,
+            "note": "async snapshots copy on a side stream into reused pinned buffers while "
+                    "the next steps run"}
 
 
 def ensemble_report(args, peak_gbs):
