@@ -406,6 +406,8 @@ int yr_attrs() {
                                (int)YrSize<ZC>::total));
   OB_CUDA(cudaFuncSetAttribute(k_iy3<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)YrSize<ZC>::total));
+  OB_CUDA(cudaFuncSetAttribute(k_hy3<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)HySize<ZC>::total));
   return OB_OK;
 }
 
@@ -695,6 +697,22 @@ void yr_launch(const OraclePlan* p, bool inverse, const cplx<float>* in0, const 
   else
     k_fy3<ZC><<<grid, 64 * ZC, YrSize<ZC>::total, st>>>(p->g, in0, in1, p->ky, tw, out0);
 }
+// the damper's fused y stage (FP32, ny = 512), in place on (S1, S2)
+template <int ZC>
+void hy_launch(const OraclePlan* p, double scale, cplx<float>* s1, cplx<float>* s2,
+               cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.nxh);
+  k_hy3<ZC><<<grid, 64 * ZC, HySize<ZC>::total, st>>>(
+      p->g, s1, s2, p->kx, p->ky, (const cplx<float>*)p->twy, scale, s1, s2);
+}
+void hy(const OraclePlan* p, double scale, cplx<float>* s1, cplx<float>* s2, cudaStream_t st) {
+  switch (p->zc3_fy) {
+    case 2: hy_launch<2>(p, scale, s1, s2, st); break;
+    case 4: hy_launch<4>(p, scale, s1, s2, st); break;
+    default: hy_launch<8>(p, scale, s1, s2, st); break;
+  }
+}
+
 // register-resident FP32 y pencils (ny = 512): FY_DIV forward or the IY_GRAD inverse
 void yr(const OraclePlan* p, bool inverse, const cplx<float>* in0, const cplx<float>* in1,
         cplx<float>* out0, cplx<float>* out1, cudaStream_t st) {
@@ -1124,12 +1142,18 @@ int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStrea
       (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   const double scale = -(p->epsilon / dt_slow) / ((double)g.nx * (double)g.ny);
+  if (sizeof(T) == 4 && p->zc3_fy) {
+    // forward y, multipliers and inverse y in one register-resident pass
+    { Launch L_(p, 1, st); hy(p, scale, (cplx<float>*)S1, (cplx<float>*)S2, st); }
+    OB_LAUNCHED();
+  } else {
   { Launch L_(p, 1, st); k_fy<T, FY_HELM><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
       g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, scale, S1, S2); }
   OB_LAUNCHED();
   { Launch L_(p, 3, st); k_iy<T, IY_FIELDS><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
       g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
+  }
   { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
       g, p->px, p->zc_ix, 2, S1, S2, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
       nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr); }
@@ -1185,8 +1209,8 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
   dim3 grd((p->g.ny + 7) / 8, p->g.nx);
   // the biharmonic diffusion's inner Laplacians of this slow half's u, v
   if ((mask & OB_TEND_DIFFUSION) && p->diffusion == OB_DIFF_BIHARMONIC) {
-    const long n = (long)p->g.nx * p->g.ny * p->g.nz;
-    { Launch L_(p, 5, st); k_lap2<T><<<(unsigned)std::min<long>((n + 255) / 256, 148L * 64), 256, 0, st>>>(
+    const dim3 lg((unsigned)((p->g.ny * p->g.nz + 255) / 256), (unsigned)p->g.nx);
+    { Launch L_(p, 5, st); k_lap2<T><<<lg, 256, 0, st>>>(
           p->g, u, v, p->diff_dx2, p->diff_dy2, (T*)p->Lu, (T*)p->Lv); }
     OB_LAUNCHED();
   }

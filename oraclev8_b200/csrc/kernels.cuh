@@ -1102,7 +1102,7 @@ __device__ __forceinline__ float ddx_ws5f(const float* __restrict__ q, int o, co
 // of the loaded values and half the registers of the double form.  Same
 // terms, summation order and boundary treatment as k_slow.
 template <int OUTMODE, bool PROD = false>
-__global__ void __launch_bounds__(256, 4) k_slow_f32(GridK g, SlowK s, int mask, double dts_d,
+__global__ void __launch_bounds__(256, PROD ? 5 : 4) k_slow_f32(GridK g, SlowK s, int mask, double dts_d,
                                                      const float* __restrict__ u,
                                                      const float* __restrict__ v,
                                                      const float* __restrict__ w,
@@ -1510,24 +1510,25 @@ __global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, 
 
 // lap(u), lap(v) of one slow half for the biharmonic diffusion: the
 // reference applies its 5-point Laplacian twice and rounds the inner one to a
-// field (tendency.py:1608-1621), so it is formed as one.  One thread per cell.
+// field (tendency.py:1608-1621), so it is formed as one.  One thread per cell;
+// grid = (ceil(ny nz / 256), nx), so that an x plane is one grid row and the
+// only division is r / nz (32-bit: nx ny (nz + 1) < 2^31, plan_create).
 template <class T>
 __global__ void __launch_bounds__(256) k_lap2(GridK g, const T* __restrict__ u,
                                               const T* __restrict__ v, double dx2, double dy2,
                                               T* __restrict__ lu, T* __restrict__ lv) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const long n = (long)nx * ny * nz;
-  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n;
-       e += (long)gridDim.x * blockDim.x) {
-    const int k = (int)(e % nz);
-    const long col = e / nz;
-    const int i = (int)(col / ny), j = (int)(col - (long)i * ny);
+  const int pl = ny * nz;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= pl) return;
+  const int i = blockIdx.y;
+  const int j = r / nz;
+  {
     const int ip = i + 1 == nx ? 0 : i + 1, im = i == 0 ? nx - 1 : i - 1;
     const int jp = j + 1 == ny ? 0 : j + 1, jm = j == 0 ? ny - 1 : j - 1;
-    const int o = (int)e;
-    const int offx[6] = {0, 0, (im - i) * ny * nz, (ip - i) * ny * nz, 0, 0};
+    const int o = i * pl + r;
+    const int offx[6] = {0, 0, (im - i) * pl, (ip - i) * pl, 0, 0};
     const int offy[6] = {0, 0, (jm - j) * nz, (jp - j) * nz, 0, 0};
-    (void)k;
     if (sizeof(T) == 8) {
       lu[o] = (T)lap5<T, double>(u, o, offx, offy, dx2, dy2);
       lv[o] = (T)lap5<T, double>(v, o, offx, offy, dx2, dy2);

@@ -650,4 +650,98 @@ __global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_iy3(
   }
 }
 
+// The Helmholtz damper's y stage for FP32 at ny = 512 in one pass (what k_fy
+// FY_HELM followed by k_iy IY_FIELDS compute): forward y transforms of the U
+// and V columns, the divergent-part multipliers
+//   out0 = s (Kx^2/K^2 U + (KxKy/K^2)' V),  out1 = s ((KxKy/K^2)' U + Ky^2/K^2 V)
+// (the primed cross term zero where exactly one of kx, ky is the Nyquist
+// index; s = scale), then inverse y transforms.  The multipliers are formed in
+// double as k_fy forms them, once per ky, into a table in shared memory.  In
+// place is allowed: each CTA rewrites exactly the columns it read.
+// grid = (ceil(nz/ZC), nx/2 + 1), 64 ZC threads.
+template <int ZC>
+struct HySize {
+  static constexpr size_t mult = (size_t)kYrN * 3 * sizeof(float);
+  static constexpr size_t total = YrSize<ZC>::total + mult;
+};
+
+template <int ZC>
+__global__ void __launch_bounds__(64 * ZC, yr_min_blocks<ZC>()) k_hy3(
+    GridK g, const cplx<float>* in0, const cplx<float>* in1, const double* __restrict__ kxd,
+    const double* __restrict__ kyd, const cplx<float>* __restrict__ twy, double scale,
+    cplx<float>* out0, cplx<float>* out1) {
+  using SZ = YrSize<ZC>;
+  constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kYrN;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<float>* ytw = reinterpret_cast<cplx<float>*>(smem_dyn);
+  cplx<float>* w32 = ytw + N;
+  cplx<float>* R = reinterpret_cast<cplx<float>*>(smem_dyn + SZ::tables);  // [N][BP]
+  cplx<float>* ex = R;
+  float* m3 = reinterpret_cast<float*>(smem_dyn + SZ::total);  // [ky][sxx, syy, sxy]
+  const int ny = g.ny, nz = g.nz;
+  const int kx = blockIdx.y;
+  const int z0 = blockIdx.x * ZC;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < N * B; e += NT) {
+    const int y = e / B, b = e - y * B;
+    const int f = b / ZC, j = b - f * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    copy_or_zero(&R[y * BP + b], (f == 0 ? in0 : in1) + (kx * ny + y) * nz + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  for (int i = tid; i < N; i += NT) ytw[i] = twy[(i & 31) * (i >> 5)];
+  if (tid < 16) w32[tid] = twy[16 * tid];
+  for (int ky = tid; ky < N; ky += NT) {
+    const double Kx = kxd[kx], Ky = kyd[ky];
+    const double K2 = Kx * Kx + Ky * Ky;
+    double mxx = 0, myy = 0, mxy = 0;
+    if (K2 > 0) {
+      mxx = Kx * Kx / K2;
+      myy = Ky * Ky / K2;
+      const bool nyqx = (kx == g.nx / 2), nyqy = (ky == N / 2);
+      mxy = (nyqx != nyqy) ? 0.0 : Kx * Ky / K2;
+    }
+    m3[3 * ky + 0] = (float)(scale * mxx);
+    m3[3 * ky + 1] = (float)(scale * myy);
+    m3[3 * ky + 2] = (float)(scale * mxy);
+  }
+  cp_wait<0>();
+  __syncthreads();
+  const int c = tid >> 5, lane = tid & 31;
+  const int k2 = lane & 15, p = lane >> 4;
+  cplx<float> a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a[q] = R[(lane + 32 * q) * BP + c];
+  __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
+  yr_fft<float, false>(a, lane, ytw, w32, ex + c * kYrEx);
+  __syncthreads();  // every exchange read: the rows come back in natural order
+#pragma unroll
+  for (int j = 0; j < 16; ++j) R[(16 * (j + 16 * p) + k2) * BP + c] = a[j];
+  __syncthreads();
+  for (int e = tid; e < N * ZC; e += NT) {
+    const int ky = e / ZC, j = e - ky * ZC;
+    const float sxx = m3[3 * ky], syy = m3[3 * ky + 1], sxy = m3[3 * ky + 2];
+    const cplx<float> U = R[ky * BP + j], V = R[ky * BP + ZC + j];
+    R[ky * BP + j] = mk<float>(sxx * U.x + sxy * V.x, sxx * U.y + sxy * V.y);
+    R[ky * BP + ZC + j] = mk<float>(sxy * U.x + syy * V.x, sxy * U.y + syy * V.y);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a[q] = R[(lane + 32 * q) * BP + c];
+  __syncthreads();
+  yr_fft<float, true>(a, lane, ytw, w32, ex + c * kYrEx);
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 16; ++j) R[(16 * (j + 16 * p) + k2) * BP + c] = a[j];
+  __syncthreads();
+  for (int e = tid; e < N * B; e += NT) {
+    const int y = e / B, b = e - y * B;
+    const int f = b / ZC, j = b - f * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    (f == 0 ? out0 : out1)[(kx * ny + y) * nz + z] = R[y * BP + b];
+  }
+}
+
 }  // namespace ob

@@ -251,3 +251,44 @@ def test_slow_tendency_forms_agree(shape, monkeypatch):
         err = float(np.max(np.abs(a - r))) / scale
         print(f"{shape} {f}: max |x-march - gather| / max|.| = {err:.3e}")
         assert err <= 1e-5, (f, err)
+
+
+@pytest.mark.parametrize("nx, nz", [(64, 16), (48, 13)])
+def test_register_damper_y_stage(nx, nz, monkeypatch):
+    """At ny = 512 an FP32 plan runs the Helmholtz damper's y stage (forward
+    y transforms, the divergent-part multipliers, inverse y transforms) as
+    one register-resident pass; with ORACLE_B200_FY3_ZC=0 it keeps the
+    separate shared-memory kernels.  Against the FP64 damper tendency of the
+    same input, the fused pass is as accurate as the separate kernels, and
+    the two FP32 forms agree to FP32 rounding.  nz = 13 leaves a partial
+    z-chunk."""
+    from oraclev8_b200 import _lib as L
+    from oraclev8_b200._plan import Plan, PlanSpec
+    ny = 512
+    Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
+    z, rho0, th0 = O.build_base_state(nz, Lz)
+    mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
+                                    projection=True, damping=True, epsilon=0.5))
+    monkeypatch.setenv("ORACLE_B200_FY3_ZC", "0")
+    p_ref = mk("fp32")
+    monkeypatch.delenv("ORACLE_B200_FY3_ZC")
+    p_new = mk("fp32")
+    p64 = mk("fp64")
+    u, v, w = _smooth_state(nx, ny, nz, seed=31 + nz)
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    th = np.zeros((nx, ny, nz))
+    outs = []
+    for p, dt in ((p64, torch.float64), (p_ref, torch.float32), (p_new, torch.float32)):
+        du, dv, _, _ = p.tendency(L.OB_TEND_DAMPING, dev(f32(u), dt), dev(f32(v), dt),
+                                  dev(f32(w), dt), dev(th, dt), 30.0)
+        outs.append([host(du).astype(np.float64), host(dv).astype(np.float64)])
+    for i, name in enumerate(("du", "dv")):
+        r64, ref, new = outs[0][i], outs[1][i], outs[2][i]
+        scale = float(np.max(np.abs(r64)))
+        assert scale > 0.0
+        e_ref = float(np.max(np.abs(ref - r64))) / scale
+        e_new = float(np.max(np.abs(new - r64))) / scale
+        e_two = float(np.max(np.abs(new - ref))) / scale
+        print(name, f"separate {e_ref:.2e} fused {e_new:.2e} between {e_two:.2e}")
+        assert e_new <= 1.5 * e_ref + 1e-7, (name, e_new, e_ref)
+        assert e_two <= 2e-6, (name, e_two)
