@@ -896,6 +896,16 @@ __device__ __forceinline__ A lap5(const T* __restrict__ q, int o, const int* off
          ((A)q[o + offy[3]] - (A)2 * c + (A)q[o + offy[2]]) / dy2;
 }
 
+// The same Laplacian with the spacings' reciprocals, for single-precision
+// state: two multiplies where lap5 takes two IEEE divisions (the FP32 path is
+// held to its rounding, not to the reference's operation order).
+__device__ __forceinline__ float lap5r(const float* __restrict__ q, int o, const int* offx,
+                                       const int* offy, float rdx2, float rdy2) {
+  const float c = q[o];
+  return (q[o + offx[3]] - 2.0f * c + q[o + offx[2]]) * rdx2 +
+         (q[o + offy[3]] - 2.0f * c + q[o + offy[2]]) * rdy2;
+}
+
 // WS5 upwind derivative along one horizontal axis.  cols[r] are the linear
 // column indices of the neighbours i-3, i-2, i-1, i+1, i+2, i+3 (periodic);
 // the value at neighbour r, level k is q[cols[r] * nzk + k].  Only the six
@@ -1131,7 +1141,8 @@ __global__ void __launch_bounds__(256, PROD ? 5 : 4) k_slow_f32(GridK g, SlowK s
   const bool spg = PROD && (mask & kTendSponge) && s.sponge;
   const int dif = (PROD && (mask & kTendDiffusion)) ? s.diff : 0;
   const bool col_ = PROD && (mask & kTendCooling) && s.cool;
-  const float dnu = (float)s.diff_nu, ddx2 = (float)s.diff_dx2, ddy2 = (float)s.diff_dy2;
+  const float dnu = (float)s.diff_nu, rdx2 = (float)(1.0 / s.diff_dx2),
+              rdy2 = (float)(1.0 / s.diff_dy2);
   int offx[6], offy[6], offxw[6], offyw[6];
   const int dd[6] = {-3, -2, -1, 1, 2, 3};
 #pragma unroll
@@ -1211,13 +1222,13 @@ __global__ void __launch_bounds__(256, PROD ? 5 : 4) k_slow_f32(GridK g, SlowK s
         tt = tt + (-a) * thc;
       }
       if (dif == 1) {
-        tu = tu + dnu * lap5<float, float>(u, o, offx, offy, ddx2, ddy2);
-        tv = tv + dnu * lap5<float, float>(v, o, offx, offy, ddx2, ddy2);
+        tu = tu + dnu * lap5r(u, o, offx, offy, rdx2, rdy2);
+        tv = tv + dnu * lap5r(v, o, offx, offy, rdx2, rdy2);
       } else if (dif == 2) {
         const float* lu = static_cast<const float*>(s.lap_u);
         const float* lv = static_cast<const float*>(s.lap_v);
-        tu = tu + (-dnu) * lap5<float, float>(lu, o, offx, offy, ddx2, ddy2);
-        tv = tv + (-dnu) * lap5<float, float>(lv, o, offx, offy, ddx2, ddy2);
+        tu = tu + (-dnu) * lap5r(lu, o, offx, offy, rdx2, rdy2);
+        tv = tv + (-dnu) * lap5r(lv, o, offx, offy, rdx2, rdy2);
       }
       if (col_) tt = tt + (-(float)s.cool_alpha) * thc;
       if (dmp) {
@@ -1533,8 +1544,9 @@ __global__ void __launch_bounds__(256) k_lap2(GridK g, const T* __restrict__ u,
       lu[o] = (T)lap5<T, double>(u, o, offx, offy, dx2, dy2);
       lv[o] = (T)lap5<T, double>(v, o, offx, offy, dx2, dy2);
     } else {
-      lu[o] = (T)lap5<T, float>(u, o, offx, offy, (float)dx2, (float)dy2);
-      lv[o] = (T)lap5<T, float>(v, o, offx, offy, (float)dx2, (float)dy2);
+      const float rdx2 = (float)(1.0 / dx2), rdy2 = (float)(1.0 / dy2);
+      lu[o] = (T)lap5r((const float*)u, o, offx, offy, rdx2, rdy2);
+      lv[o] = (T)lap5r((const float*)v, o, offx, offy, rdx2, rdy2);
     }
   }
 }
@@ -1548,12 +1560,23 @@ __global__ void __launch_bounds__(256) k_intensity_cap(const T* __restrict__ u,
                                                        T* __restrict__ dv) {
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n;
        e += (long)gridDim.x * blockDim.x) {
-    const double up = (double)u[e] - u_env, vp = (double)v[e] - v_env;
-    const double spd = sqrt(up * up + vp * vp);
-    const double excess = fmax(0.0, spd - v_cap);
-    const double alpha = excess / (tau * fmax(spd, 1e-6));
-    du[e] = (T)(-alpha * up);
-    dv[e] = (T)(-alpha * vp);
+    if constexpr (sizeof(T) == 8) {
+      const double up = (double)u[e] - u_env, vp = (double)v[e] - v_env;
+      const double spd = sqrt(up * up + vp * vp);
+      const double excess = fmax(0.0, spd - v_cap);
+      const double alpha = excess / (tau * fmax(spd, 1e-6));
+      du[e] = (T)(-alpha * up);
+      dv[e] = (T)(-alpha * vp);
+    } else {
+      // single-precision fields: single-precision arithmetic (the tendency
+      // is held to the FP32 rounding of the state)
+      const float up = (float)u[e] - (float)u_env, vp = (float)v[e] - (float)v_env;
+      const float spd = sqrtf(up * up + vp * vp);
+      const float excess = fmaxf(0.0f, spd - (float)v_cap);
+      const float alpha = excess / ((float)tau * fmaxf(spd, 1e-6f));
+      du[e] = (T)(-alpha * up);
+      dv[e] = (T)(-alpha * vp);
+    }
   }
 }
 
