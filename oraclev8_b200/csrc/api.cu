@@ -395,8 +395,11 @@ template <int ZC>
 int xr_attrs_ix3() {
   int rc;
   if ((rc = xr_attr_ix3<IX_CORRECT, ZC>()) || (rc = xr_attr_ix3<IX_STAGE, ZC>()) ||
-      (rc = xr_attr_ix3<IX_REFINE, ZC>()))
+      (rc = xr_attr_ix3<IX_REFINE, ZC>()) || (rc = xr_attr_ix3<IX_FIELDS, ZC>()))
     return rc;
+  OB_CUDA(cudaFuncSetAttribute(k_fx3<float, false, ZC, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fx3_smem<float, false, ZC>()));
   return OB_OK;
 }
 
@@ -785,6 +788,24 @@ void fx3(const OraclePlan* q, int zc, const float* u, const float* v, const floa
   }
 }
 
+// the Helmholtz damper's forward x transform (FP32, nx = 512): FFTx(u), FFTx(v)
+template <int ZC>
+void fx3f_launch(const OraclePlan* p, const float* u, const float* v, cplx<float>* X0,
+                 cplx<float>* X1, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
+  k_fx3<float, false, ZC, true><<<grid, 48 * ZC, fx3_smem<float, false, ZC>(), st>>>(
+      p->g, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->kx, (const cplx<float>*)p->twx,
+      X0, X1);
+}
+void fx3f(const OraclePlan* p, int zc, const float* u, const float* v, cplx<float>* X0,
+          cplx<float>* X1, cudaStream_t st) {
+  switch (zc) {
+    case 2: fx3f_launch<2>(p, u, v, X0, X1, st); break;
+    case 4: fx3f_launch<4>(p, u, v, X0, X1, st); break;
+    default: fx3f_launch<8>(p, u, v, X0, X1, st); break;
+  }
+}
+
 template <int MODE, int ZC>
 void ix3_launch(const OraclePlan* p, const cplx<float>* phs, const cplx<float>* psi,
                 const float* u, const float* v, const float* w, const float* bh, double sdt,
@@ -1137,9 +1158,13 @@ int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStrea
   const GridK g = p->g;
   C* S1 = (C*)p->S1;
   C* S2 = (C*)p->S2;
-  { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
-      g, p->pxf, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-      (const C*)p->twx, S1, S2, nullptr); }
+  if (sizeof(T) == 4 && p->zc3_fx)
+    { Launch L_(p, 0, st); fx3f(p, p->zc3_fx, (const float*)u, (const float*)v, (cplx<float>*)S1,
+                               (cplx<float>*)S2, st); }
+  else
+    { Launch L_(p, 0, st); k_fx<T, FX_FIELDS><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 2), st>>>(
+        g, p->pxf, p->zc_fx, 2, u, v, nullptr, nullptr, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2, nullptr); }
   OB_LAUNCHED();
   const double scale = -(p->epsilon / dt_slow) / ((double)g.nx * (double)g.ny);
   if (sizeof(T) == 4 && p->zc3_fy) {
@@ -1154,9 +1179,15 @@ int damper_impl(OraclePlan* p, const T* u, const T* v, double dt_slow, cudaStrea
       g, p->py, p->zc_iy, 2, S1, S2, p->ky, (const C*)p->twy, 1.0, S1, S2); }
   OB_LAUNCHED();
   }
-  { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
-      g, p->px, p->zc_ix, 2, S1, S2, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
-      nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr); }
+  if (sizeof(T) == 4 && p->zc3_ix)
+    { Launch L_(p, 4, st); ix3<IX_FIELDS>(p, p->zc3_ix, (const cplx<float>*)S1,
+                                          (const cplx<float>*)S2, nullptr, nullptr, nullptr,
+                                          nullptr, 0.0, (float*)p->Du, (float*)p->Dv, nullptr,
+                                          nullptr, st); }
+  else
+    { Launch L_(p, 4, st); k_ix<T, IX_FIELDS><<<grid_x(p, p->zc_ix), kFftThreads, smem_ix(p, 2 * p->zc_ix), st>>>(
+        g, p->px, p->zc_ix, 2, S1, S2, nullptr, p->kx, (const C*)p->twx, nullptr, nullptr,
+        nullptr, nullptr, 0.0, p->theta0, (T*)p->Du, (T*)p->Dv, nullptr, nullptr); }
   OB_LAUNCHED();
   return OB_OK;
 }

@@ -78,7 +78,10 @@ constexpr int fx3_min_blocks() { return sizeof(T) == 8 ? 2 : (ZC >= 8 ? 2 : 4); 
 // the FP64 residual transform of the defect correction, with k_fx2's
 // operation order in the pack.  3 ZC columns (u, v, d at ZC levels), one
 // 16-lane group each.  grid = (ceil(nz/ZC), ny), 48 ZC threads.
-template <class T, bool STAGE, int ZC>
+// FIELDS (FP32, no stage): the plain half-spectra X0 = FFTx(u), X1 = FFTx(v),
+// the Nyquist bin included (what k_fx FX_FIELDS writes; the Helmholtz
+// damper's forward x transform); w is not read and the d columns stay zero.
+template <class T, bool STAGE, int ZC, bool FIELDS = false>
 __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
     GridK g, const float* __restrict__ u, const float* __restrict__ v,
     const float* __restrict__ w, const float* __restrict__ bh, double sdt,
@@ -87,6 +90,7 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
     cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
   static_assert(ZC == 2 || ZC == 4 || ZC == 8, "whole warps of 16-lane groups");
   static_assert(sizeof(T) == 4 || !STAGE, "the FP64 form is the residual transform");
+  static_assert(!FIELDS || (sizeof(T) == 4 && !STAGE), "the field form is FP32 without a stage");
   constexpr int B = 3 * ZC, NT = 16 * B, M = kXrM, N = kXrN, S = xr_stride<ZC>(), BP = B + 1;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   cplx<T>* tw2 = reinterpret_cast<cplx<T>*>(smem_dyn);  // [16 k2 + t] = W_256^(t k2)
@@ -112,14 +116,15 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
     copy_or_zero(&U[j * S + x], u + gi, ok);
     copy_or_zero(&V[j * S + x], v + gi, ok);
   }
-  for (int e = tid; e < N * (ZC + 1); e += NT) {
-    const int x = e / (ZC + 1), j = e - x * (ZC + 1);
-    const int z = z0 + j;  // half levels z0 .. z0+ZC
-    const bool ok = z <= nz;
-    const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
-    copy_or_zero(&W[j * S + x], w + gi, ok);
-    if (STAGE) copy_or_zero(&BH[j * S + x], bh + gi, ok);
-  }
+  if constexpr (!FIELDS)
+    for (int e = tid; e < N * (ZC + 1); e += NT) {
+      const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+      const int z = z0 + j;  // half levels z0 .. z0+ZC
+      const bool ok = z <= nz;
+      const int gi = (x * ny + y) * (nz + 1) + (ok ? z : 0);
+      copy_or_zero(&W[j * S + x], w + gi, ok);
+      if (STAGE) copy_or_zero(&BH[j * S + x], bh + gi, ok);
+    }
   cp_commit();
   for (int i = tid; i < M; i += NT) {
     tw2[i] = twx[2 * ((i & 15) * (i >> 4))];  // W_256^m = W_512^(2m)
@@ -136,7 +141,7 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
   const bool ok = zj < nz;
   cplx<T> a[16];
   if (f < 2) {
-    const T r = ok ? (T)rho[zj] : (T)0;
+    const T r = FIELDS ? (T)1 : (ok ? (T)rho[zj] : (T)0);
     const float* R = (f == 0 ? U : V) + j * S + 2 * t;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
@@ -156,6 +161,9 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
                         drn(srn(mrn(ru, (double)wu.y), mrn(rl, (double)wl.y)), dz))
                 : mk<T>((T)0, (T)0);
     }
+  } else if constexpr (FIELDS) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) a[q] = mk<T>((T)0, (T)0);
   } else {
     const float rl = ok ? (float)rhoh[zj] : 0.0f, ru = ok ? (float)rhoh[zj + 1] : 0.0f;
     const float idz = (float)(1.0 / g.dz);
@@ -215,8 +223,10 @@ __global__ void __launch_bounds__(48 * ZC, fx3_min_blocks<T, ZC>()) k_fx3(
     const bool two = z + 1 < nz;
     const T kk = (k == M) ? (T)0 : (T)kxd[k];
     const int o = (k * ny + y) * nz + z;
-    const cplx<T> x00 = add(ik(kk, XS[k * BP + jj]), XS[k * BP + 2 * ZC + jj]);
-    const cplx<T> x01 = add(ik(kk, XS[k * BP + jj + 1]), XS[k * BP + 2 * ZC + jj + 1]);
+    const cplx<T> x00 = FIELDS ? XS[k * BP + jj]
+                               : add(ik(kk, XS[k * BP + jj]), XS[k * BP + 2 * ZC + jj]);
+    const cplx<T> x01 = FIELDS ? XS[k * BP + jj + 1]
+                               : add(ik(kk, XS[k * BP + jj + 1]), XS[k * BP + 2 * ZC + jj + 1]);
     const cplx<T> x10 = XS[k * BP + ZC + jj], x11 = XS[k * BP + ZC + jj + 1];
     if constexpr (sizeof(T) == 4) {
       if (two && st2) {
@@ -256,6 +266,9 @@ constexpr int ix3_min_blocks() { return ZC >= 8 ? 2 : 3; }
 
 // Inverse x-pencil kernel with the velocity correction (k_ix2 semantics and
 // modes, FP32, nx = 512).  grid = (ceil(nz/ZC), ny), 16 (3 ZC + 2) threads.
+// IX_FIELDS: the real C2R outputs of two spectra, u_out = C2R(phs) and
+// v_out = C2R(psi) (what k_ix IX_FIELDS writes: the Helmholtz damper's inverse
+// x transform); no state is read and nothing else is written.
 // Shared memory: twiddles and kx'; region A holding in turn the spectral
 // rows, the groups' exchange blocks and the real outputs (level-major rows);
 // the state tiles, requested at the start in their own cp.async group so
@@ -305,6 +318,7 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
   cp_commit();
   // u, v: 16-byte copies (ZC / 4 per row) where the chunk is whole and the
   // rows start on 16 bytes; 4-byte copies otherwise
+  if constexpr (MODE != IX_FIELDS) {
   const bool vec = ZC >= 4 && z0 + ZC <= nz && (nz & 3) == 0 &&
                    ((reinterpret_cast<size_t>(u_in) | reinterpret_cast<size_t>(v_in)) & 15) == 0;
   if (vec) {
@@ -330,6 +344,7 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     const int z = z0 + j;  // half levels z0 .. z0+ZC
     const bool ok = z <= nz;
     copy_or_zero(&SW[e], w_in + (x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
+  }
   }
   cp_commit();
   if (STAGE || MODE == IX_REFINE)
@@ -435,6 +450,23 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     const bool two = z + 1 < nz;
     const int col = x * ny + y;
     const int idx = col * nz + z;
+    if constexpr (MODE == IX_FIELDS) {
+      // phi group j + 1 and psi group 2 ZC + 1 + j hold level z
+      const float a0 = ZR[(j + 1) * SR + x], a1 = ZR[(j + 2) * SR + x];
+      const float b0 = ZR[(2 * ZC + 1 + j) * SR + x], b1 = ZR[(2 * ZC + 2 + j) * SR + x];
+      if (two && st2) {
+        *reinterpret_cast<float2*>(&u_out[idx]) = make_float2(a0, a1);
+        *reinterpret_cast<float2*>(&v_out[idx]) = make_float2(b0, b1);
+      } else {
+        u_out[idx] = a0;
+        v_out[idx] = b0;
+        if (two) {
+          u_out[idx + 1] = a1;
+          v_out[idx + 1] = b1;
+        }
+      }
+      continue;
+    }
     const float phb = ZR[j * SR + x];  // level z - 1
     const float ph0 = ZR[(j + 1) * SR + x];
     const float ph1 = ZR[(j + 2) * SR + x];

@@ -253,25 +253,32 @@ def test_slow_tendency_forms_agree(shape, monkeypatch):
         assert err <= 1e-5, (f, err)
 
 
-@pytest.mark.parametrize("nx, nz", [(64, 16), (48, 13)])
-def test_register_damper_y_stage(nx, nz, monkeypatch):
-    """At ny = 512 an FP32 plan runs the Helmholtz damper's y stage (forward
-    y transforms, the divergent-part multipliers, inverse y transforms) as
-    one register-resident pass; with ORACLE_B200_FY3_ZC=0 it keeps the
-    separate shared-memory kernels.  Against the FP64 damper tendency of the
-    same input, the fused pass is as accurate as the separate kernels, and
+@pytest.mark.parametrize("nx, ny, nz", [(64, 512, 16), (48, 512, 13), (512, 40, 16),
+                                        (512, 48, 13), (512, 512, 8)])
+def test_register_damper_matches_stockham(nx, ny, nz, monkeypatch):
+    """An FP32 plan runs the Helmholtz damper in the register-resident
+    kernels where the grid allows: the x transforms at nx = 512 (the field
+    forms of the forward and inverse x pencils) and the y stage at ny = 512
+    (forward y transforms, the divergent-part multipliers and inverse y
+    transforms in one pass).  With ORACLE_B200_FX3_ZC, ORACLE_B200_IX3_ZC,
+    ORACLE_B200_FXD3_ZC and ORACLE_B200_FY3_ZC at 0 it keeps the
+    shared-memory kernels.  Against the FP64 damper tendency of the same
+    input, the register forms are as accurate as the shared-memory ones, and
     the two FP32 forms agree to FP32 rounding.  nz = 13 leaves a partial
     z-chunk."""
     from oraclev8_b200 import _lib as L
     from oraclev8_b200._plan import Plan, PlanSpec
-    ny = 512
     Lx, Ly, Lz = nx * 5e3, ny * 5e3, 16e3
     z, rho0, th0 = O.build_base_state(nz, Lz)
     mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
                                     projection=True, damping=True, epsilon=0.5))
-    monkeypatch.setenv("ORACLE_B200_FY3_ZC", "0")
+    knobs = ("ORACLE_B200_FX3_ZC", "ORACLE_B200_IX3_ZC", "ORACLE_B200_FXD3_ZC",
+             "ORACLE_B200_FY3_ZC")
+    for k in knobs:
+        monkeypatch.setenv(k, "0")
     p_ref = mk("fp32")
-    monkeypatch.delenv("ORACLE_B200_FY3_ZC")
+    for k in knobs:
+        monkeypatch.delenv(k)
     p_new = mk("fp32")
     p64 = mk("fp64")
     u, v, w = _smooth_state(nx, ny, nz, seed=31 + nz)
@@ -289,6 +296,6 @@ def test_register_damper_y_stage(nx, nz, monkeypatch):
         e_ref = float(np.max(np.abs(ref - r64))) / scale
         e_new = float(np.max(np.abs(new - r64))) / scale
         e_two = float(np.max(np.abs(new - ref))) / scale
-        print(name, f"separate {e_ref:.2e} fused {e_new:.2e} between {e_two:.2e}")
+        print(name, f"shared-memory {e_ref:.2e} register {e_new:.2e} between {e_two:.2e}")
         assert e_new <= 1.5 * e_ref + 1e-7, (name, e_new, e_ref)
         assert e_two <= 2e-6, (name, e_two)
