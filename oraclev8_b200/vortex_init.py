@@ -41,6 +41,38 @@ class HollandVortexInit:
             Vt = Vt * 0.5 * (1.0 + np.cos(np.pi * frac))
         return Vt
 
+    def vertical_structure(self, z):
+        """The warm core's Gaussian S(z) = exp(-(z - z_peak)^2 / (2 sigma_z^2))
+        (vortex_init.py:191-204)."""
+        return np.exp(-0.5 * ((np.asarray(z) - self.z_peak) / self.sigma_z) ** 2)
+
+    def surface_pressure_deficit(self, rho_bar_surface):
+        """P'(r = 0) at the surface in Pa, negative for a cyclone
+        (vortex_init.py:376-382)."""
+        return float(self._pressure_deficit_1d(rho_bar_surface, 1.0)[0])
+
+    def peak_wind_check(self):
+        """(radius, speed) of the largest tangential wind on the radial grid
+        (vortex_init.py:384-391)."""
+        vt = self.tangential_wind(self._r1d)
+        i = int(np.argmax(vt))
+        return float(self._r1d[i]), float(vt[i])
+
+    def summary(self):
+        """The reference's one-line log of the vortex (vortex_init.py:393-411)."""
+        _, _ = self.peak_wind_check()
+        p_min = self.surface_pressure_deficit(rho_bar_surface=1.15)
+        if self.wind_taper:
+            taper = (f"wind_taper=ON start={self.taper_start_frac * self.R_env / 1000:.0f} km "
+                     f"(frac={self.taper_start_frac:.2f})  ")
+        else:
+            taper = "wind_taper=OFF  "
+        return (f"HollandVortex: Vmax={self.Vmax:.0f} m/s  Rmax={self.Rmax / 1000:.0f} km  "
+                f"B={self.B:.2f}  f={self.f:.2e}  R_env={self.R_env / 1000:.0f} km  {taper}"
+                f"P_min~{p_min:.0f} Pa  z_peak={self.z_peak / 1000:.0f} km  "
+                f"sz={self.sigma_z / 1000:.0f} km  u_env={self.u_env:.1f}  "
+                f"v_env={self.v_env:.1f} m/s")
+
     def wind_vertical_structure(self, z):
         if self.wind_decay_top is not None:
             return np.maximum(0.0, 1.0 - z / self.wind_decay_top)

@@ -491,6 +491,22 @@ def gen_vortex_tracker():
     np.savez_compressed(OUT / "vortex_tracker.npz", **out)
 
 
+def gen_vortex_helpers():
+    """The vortex initialiser's host helpers (vortex_init.py:191-411): the
+    warm-core profile, the central surface pressure deficit, the peak-wind
+    check and the one-line summary, for two vortices."""
+    out = []
+    z = np.linspace(0.0, 20e3, 9)
+    for kw in (dict(Vmax=60.0, Rmax=40e3, B=1.6, f=5e-5),
+               dict(Vmax=78.0, Rmax=75e3, B=1.4, f=6e-5, R_env=500e3, wind_taper=True,
+                    taper_start_frac=0.4, u_env=-3.0, v_env=1.5)):
+        v = HollandVortexInit(**kw)
+        out.append(dict(kw=kw, summary=v.summary(), peak=list(v.peak_wind_check()),
+                        p_sfc=v.surface_pressure_deficit(1.15),
+                        s_z=[float(x) for x in v.vertical_structure(z)]))
+    (OUT / "vortex_helpers.json").write_text(json.dumps(out, indent=1))
+
+
 # ---------------------------------------------------------------------------
 # Scalar known answers of the reference's own tests
 # ---------------------------------------------------------------------------
@@ -611,6 +627,7 @@ if __name__ == "__main__":
     a = ap.parse_args()
     jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
                 production_storm=gen_production_storm, diagnostics=gen_diagnostics,
+                vortex_helpers=gen_vortex_helpers,
                 vortex_tracker=gen_vortex_tracker, pins=gen_pins)
     for k, f in jobs.items():
         if a.only and k != a.only:

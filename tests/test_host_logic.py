@@ -225,3 +225,17 @@ def test_gyre_snapshot_record(tmp_path):
             - (np.roll(u2, -1, 1) - np.roll(u2, 1, 1)) / (2 * 5e3))
     assert np.array_equal(d["zeta"], zeta) and np.array_equal(d["u"], u2)
     assert float(d["cx"]) == 1.0 and float(d["cy"]) == 2.0 and float(d["dx"]) == 5e3
+
+
+def test_vortex_init_host_helpers(golden_dir):
+    """vertical_structure, surface_pressure_deficit, peak_wind_check and the
+    summary line equal the reference's (vortex_init.py:191-411)."""
+    import json
+    from oraclev8_b200.vortex_init import HollandVortexInit
+    z = np.linspace(0.0, 20e3, 9)
+    for rec in json.loads((golden_dir / "vortex_helpers.json").read_text()):
+        v = HollandVortexInit(**rec["kw"])
+        assert v.summary() == rec["summary"]
+        assert list(v.peak_wind_check()) == rec["peak"]
+        assert v.surface_pressure_deficit(1.15) == rec["p_sfc"]
+        assert [float(x) for x in v.vertical_structure(z)] == rec["s_z"]
