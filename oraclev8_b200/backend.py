@@ -11,24 +11,64 @@ from __future__ import annotations
 import os as _os
 
 import numpy as _np
-import torch as xp  # device arrays are torch tensors
+import torch as _torch  # device arrays are torch tensors
 
-GPU_AVAILABLE: bool = bool(xp.cuda.is_available())
+
+class _DeviceArrays:
+    """The ``xp`` of this backend: torch, under the NumPy spellings that the
+    reference's drivers and harnesses use on device fields (``axis=`` for
+    ``roll``, Python scalars as operands of ``maximum``, ``minimum`` and
+    ``clip``; run_storm.py:128-137, run_translation_test.py:132-160).  Every
+    other name is torch's own."""
+
+    __name__ = "torch"
+
+    def __getattr__(self, name):
+        return getattr(_torch, name)
+
+    @staticmethod
+    def roll(a, shift, axis=None):
+        return _torch.roll(a, shift, dims=axis)
+
+    @staticmethod
+    def _pair(a, b):
+        if not isinstance(a, _torch.Tensor):
+            a = _torch.as_tensor(a, dtype=b.dtype, device=b.device)
+        if not isinstance(b, _torch.Tensor):
+            b = _torch.as_tensor(b, dtype=a.dtype, device=a.device)
+        return a, b
+
+    @classmethod
+    def maximum(cls, a, b):
+        return _torch.maximum(*cls._pair(a, b))
+
+    @classmethod
+    def minimum(cls, a, b):
+        return _torch.minimum(*cls._pair(a, b))
+
+    @classmethod
+    def clip(cls, a, lo, hi):
+        return cls.minimum(cls.maximum(a, lo), hi)
+
+
+xp = _DeviceArrays()
+
+GPU_AVAILABLE: bool = bool(_torch.cuda.is_available())
 PRECISION: str = _os.environ.get("ORACLE_B200_PRECISION", "fp64")
 if PRECISION not in ("fp64", "fp32", "fp32r"):
     raise ValueError(f"ORACLE_B200_PRECISION must be fp64, fp32 or fp32r, got {PRECISION!r}")
-DTYPE = xp.float64 if PRECISION == "fp64" else xp.float32
+DTYPE = _torch.float64 if PRECISION == "fp64" else _torch.float32
 
 
 def _device():
     if not GPU_AVAILABLE:
         raise RuntimeError("the oraclev8_b200 backend needs a CUDA device (no CPU fallback)")
-    return xp.device("cuda", xp.cuda.current_device())
+    return _torch.device("cuda", _torch.cuda.current_device())
 
 
 def to_numpy(arr):
     """Host NumPy copy of a device tensor (backend.py:61-77); other inputs pass through."""
-    if isinstance(arr, xp.Tensor):
+    if isinstance(arr, _torch.Tensor):
         return arr.detach().to("cpu").numpy()
     return arr
 
@@ -37,10 +77,10 @@ def asarray(arr, dtype=None):
     """Move ``arr`` to the CUDA device as a contiguous tensor (backend.py:80-89)."""
     dt = DTYPE if dtype is None else dtype
     if isinstance(dt, _np.dtype) or dt in (float, _np.float64, _np.float32):
-        dt = xp.float64 if _np.dtype(dt) == _np.float64 else xp.float32
-    if isinstance(arr, xp.Tensor):
+        dt = _torch.float64 if _np.dtype(dt) == _np.float64 else _torch.float32
+    if isinstance(arr, _torch.Tensor):
         return arr.to(device=_device(), dtype=dt).contiguous()
-    return xp.as_tensor(_np.ascontiguousarray(arr), dtype=dt, device=_device())
+    return _torch.as_tensor(_np.ascontiguousarray(arr), dtype=dt, device=_device())
 
 
 def wrap_base(base):

@@ -239,3 +239,33 @@ def test_vortex_init_host_helpers(golden_dir):
         assert list(v.peak_wind_check()) == rec["peak"]
         assert v.surface_pressure_deficit(1.15) == rec["p_sfc"]
         assert [float(x) for x in v.vertical_structure(z)] == rec["s_z"]
+
+
+def test_backend_xp_takes_the_harness_spellings():
+    """The drivers and harnesses call the backend's ``xp`` with NumPy
+    spellings (run_storm.py:128-137, run_translation_test.py:132-160):
+    roll with axis=, maximum with a Python scalar, mean with axis=, arange
+    with dtype, sum.  On torch tensors they give NumPy's values."""
+    import torch
+    from oraclev8_b200.backend import xp
+    rng = np.random.default_rng(12)
+    a = rng.standard_normal((6, 5, 4))
+    t = torch.as_tensor(a)
+    dx = 5e3
+    got = xp.mean(xp.maximum((xp.roll(t, -1, axis=0) - xp.roll(t, 1, axis=0)) / (2.0 * dx)
+                             - (xp.roll(t, -1, axis=1) - xp.roll(t, 1, axis=1)) / (2.0 * dx),
+                             0.0), axis=2)
+    want = np.mean(np.maximum((np.roll(a, -1, axis=0) - np.roll(a, 1, axis=0)) / (2.0 * dx)
+                              - (np.roll(a, -1, axis=1) - np.roll(a, 1, axis=1)) / (2.0 * dx),
+                              0.0), axis=2)
+    assert np.allclose(got.numpy(), want, rtol=1e-15, atol=0.0)
+    w = got ** 2
+    ix = xp.arange(1, 5, dtype=xp.float64)[:, None]
+    assert float(xp.sum(ix * w[1:5])) == pytest.approx(float(np.sum(np.arange(1, 5.0)[:, None]
+                                                                     * (want ** 2)[1:5])),
+                                                       rel=1e-14)
+    assert np.array_equal(xp.minimum(t, 0.5).numpy(), np.minimum(a, 0.5))
+    assert np.array_equal(xp.clip(t, -0.5, 0.5).numpy(), np.clip(a, -0.5, 0.5))
+    assert float(xp.sqrt(xp.mean(t ** 2))) == pytest.approx(float(np.sqrt(np.mean(a ** 2))),
+                                                            rel=1e-14)
+    assert xp.zeros_like(t).shape == t.shape and isinstance(t, xp.Tensor)
