@@ -32,6 +32,8 @@ from typing import Optional
 import numpy as np
 import torch
 
+from .snapshot import SnapshotCopy
+
 OMEGA = 7.2921e-5
 R_EARTH = 6.371e6
 SIZES = (96, 128, 192, 256, 384)
@@ -247,7 +249,6 @@ class ServingEngine:
                        bytes=footprint_bytes(req), t=float(state.t))
 
     def _launch(self, a: _Active) -> None:
-        from .snapshot import SnapshotCopy
         k = min(self.chunk, a.left)
         before = a.req.nsteps - a.left
         a.graphs[k].launch(a.stream)

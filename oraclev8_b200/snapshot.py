@@ -37,7 +37,9 @@ class SnapshotCopy:
     waits for the producing stream and then overlaps the work queued after
     it; the caller must then not overwrite the fields before ``ready()``
     (step a second state, or wait).  ``result()`` waits for the copy and
-    returns the snapshot dict."""
+    returns the snapshot dict, whose arrays are views of the pinned buffers:
+    a ``pinned`` dict passed again to a later copy overwrites them, so keep
+    (or copy) a result before its buffers are reused."""
 
     def __init__(self, state, t=None, cx=None, cy=None, step: Optional[int] = None,
                  stream: Optional[torch.cuda.Stream] = None, pinned: Optional[dict] = None):
