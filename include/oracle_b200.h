@@ -213,7 +213,7 @@ int oracle_b200_intensity_cap(const void *u, const void *v, int precision, long 
 /* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
 int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);
 
-/* FP64 defect correction of single-precision plans (BASELINE precision
+/* FP64 defect correction of single-precision plans (the FP32-refined
  * scheme; no counterpart in the reference, which is FP64 throughout).  After
  * the final projection of every `every`-th step, `passes` correction passes
  * run: the divergence of the stored FP32 velocity is formed in FP64, the

@@ -3,7 +3,7 @@ against the plain FP64 GPU step (itself held to the reference at 1e-12 by
 test_gpu_parity.py).
 
 The FP32 state cannot be more accurate than its own rounding, so the
-correction is judged against that floor: the non-Nyquist anelastic
+correction is measured against that floor: the non-Nyquist anelastic
 divergence (evaluated in FP64) of the FP64 projection rounded to FP32.
 """
 import math

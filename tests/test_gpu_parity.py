@@ -1,8 +1,8 @@
 """FP64 parity of the sm_100a kernels with the reference (golden fixtures made by
 the unmodified reference) and with the oracle on fresh seeded inputs.
 
-Bar: each tendency, the projected velocity and every
-state field within 1e-12 of the reference, relative to the field's max |.|.
+Bar: each tendency, the projected velocity and every state field within
+1e-12 of the reference, relative to the field's max |.|.
 """
 import json
 import math
