@@ -41,3 +41,33 @@ def test_version_and_error_string_without_gpu():
     assert b"even" in lib.oracle_b200_last_error()
     rc = lib.oracle_b200_step(None, None, None, 1.0, 0, None)
     assert rc == _lib.OB_ERR_ARG
+
+
+def test_new_entry_points_validate_before_cuda():
+    """The intensity cap and the diagnostics workspace reject bad arguments
+    with OB_ERR_ARG and a message, before any CUDA call."""
+    from oraclev8_b200 import _lib
+    lib = _lib.load()
+    vp = ctypes.c_void_p
+    one = vp(1)
+    rc = lib.oracle_b200_intensity_cap(None, one, _lib.OB_PREC_F64, 10, 70.0, 300.0, 0.0, 0.0,
+                                       one, one, None)
+    assert rc == _lib.OB_ERR_ARG and b"NULL" in lib.oracle_b200_last_error()
+    rc = lib.oracle_b200_intensity_cap(one, one, _lib.OB_PREC_F64, 10, 70.0, 0.0, 0.0, 0.0,
+                                       one, one, None)
+    assert rc == _lib.OB_ERR_ARG and b"tau" in lib.oracle_b200_last_error()
+    rc = lib.oracle_b200_intensity_cap(one, one, 7, 10, 70.0, 300.0, 0.0, 0.0, one, one, None)
+    assert rc == _lib.OB_ERR_ARG and b"precision" in lib.oracle_b200_last_error()
+    assert lib.oracle_b200_intensity_cap(one, one, _lib.OB_PREC_F32, 0, 70.0, 300.0, 0.0, 0.0,
+                                         one, one, None) == _lib.OB_OK  # nothing to do
+    h = vp()
+    assert lib.oracle_b200_vdiag_create(2, 8, 4, ctypes.byref(h)) == _lib.OB_ERR_ARG
+    assert not h.value
+    assert lib.oracle_b200_vdiag_create(8, 8, 4, None) == _lib.OB_ERR_ARG
+    out = _lib.VdMax()
+    lev = (ctypes.c_int * 1)(0)
+    rc = lib.oracle_b200_vdiag_speed_max(None, one, one, _lib.OB_PREC_F64, lev, 1, 0.0, 0.0,
+                                         ctypes.byref(out), None)
+    assert rc == _lib.OB_ERR_ARG and b"workspace" in lib.oracle_b200_last_error()
+    assert lib.oracle_b200_vdiag_centroid(None, 0, 1, 0, 1, None, None) == _lib.OB_ERR_ARG
+    assert lib.oracle_b200_vdiag_destroy(None) == _lib.OB_OK
