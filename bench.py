@@ -1,21 +1,24 @@
 """Benchmark of the LH82 anelastic RK3 step (cell-updates/s) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32r|fp64|fp32]
-                    [--workload config1|config0|config2] [--impl b200|reference]
+                    [--workload config2|config1|config0] [--impl b200|reference]
+                    [--track-hours H]
 
-Default workload: the mid-size single run — 512 x 512 x 64 cells, dx = 5 km,
-0-16 km (dz = 250 m), beta-plane at 20N (f0 = 4.99e-5, beta = 2.15e-11,
-periodic taper), Holland vortex Vmax 50 m/s / Rmax 40 km / B 1.6 with wind
-decaying linearly to zero at 12 km, eyewall heating ring (3 K/h, r0 40 km,
-sigma_r 15 km, z0 6 km, sigma_z 2 km), seeded +-0.05 K theta' noise,
-WS5 advection, buoyancy, projection, dt = 20 s.  Synthetic inputs (the
-reference has no dataset); every field is > L2-sized (64-134 MB per field),
-so consecutive steps stream from HBM.
+Default workload: the production-size single run, the one the FP32-refined
+versus plain-FP64 target is quoted on -- 1024 x 1024 x 80 cells, dx = 4 km,
+0-20 km (dz = 250 m), beta-plane at 25N (f0 = 2 Omega sin 25, beta =
+2 Omega cos 25 / R, periodic taper), Holland vortex Vmax 55 m/s / Rmax 30 km /
+B 1.8 with wind decaying linearly to zero at 12 km and a uniform 3 m/s
+easterly background flow (vortex and Coriolis), WS5 advection, buoyancy,
+projection, dt = 15 s.  Synthetic inputs (the reference has no dataset);
+every field is larger than L2 (336-671 MB per field), so consecutive steps
+stream from HBM.  ``--workload config1`` is the mid-size run (512 x 512 x 64,
+dx 5 km, eyewall heating, seeded theta' noise, dt 20 s).
 
 One "step" = one full RK3Integrator.step: two Strang slow half steps (fused
-WS5 + Coriolis + heating tendency and forward Euler), three fast stages, five
-anelastic projections (FFT x/y + Thomas z + correction) and the device-side
-step diagnostics.
+WS5 + Coriolis (+ heating) tendency and forward Euler), three fast stages,
+five anelastic projections (FFT x/y + Thomas z + correction) and the
+device-side step diagnostics.
 
 Precision (the metric is FP32-refined against plain FP64): the default
 ``fp32r`` runs the step on an FP32 state and, after its final projection, one
@@ -23,7 +26,13 @@ defect correction whose residual divergence is formed in FP64.  The same line
 then carries ``fp64_plain`` (the plain FP64 step timed the same way on the
 same workload, and the ratio) and ``accuracy`` (per-field error of the FP32
 run against the FP64 run after the same steps, and the FP64-evaluated
-divergence of both).  ``--precision fp64`` times the plain FP64 step alone.
+divergence of both); these two come last in the line.  ``--precision fp64``
+times the plain FP64 step alone.
+
+``cufft``: the transforms of one projection (three real-to-complex x
+transforms, two complex y transforms and their inverses) done by cuFFT
+through torch.fft on the same fields, timed beside this library's pencil
+kernels, which also do the projection's arithmetic.  A comparison only.
 
 Ensemble and serving (the metric's latency half, at N = 1): ``ensemble``
 serves a sample of the mixed 256-run ensemble through the serving loop
@@ -40,13 +49,20 @@ projection, no buoyancy) on the same grid and initial state, with the
 intensity cap added after each step as the reference's run loop does; timed
 in the bench's precision and in plain FP64, with the slow class's roofline.
 
+``--track-hours H`` (not part of the default run): the workload run for H
+hours in FP32-refined and in plain FP64 on the device, with the storm centre
+found every hour (find_storm_centre chained through last_pos /
+last_raw_pos as run_storm.py:180-190 does); prints one JSON line with the
+hourly centre differences, max|w| differences and the final per-field errors.
+
 N > 1: N independent replicas, one per GPU (the path partitions into
 independent runs; no collective on the data path).
 
 --impl reference times the reference algorithm on the host CPU (the NumPy
 oracle; the reference is pure Python and cannot be installed on the GPU host)
-on a bounded sample of the same workload: the same 512 x 512 horizontal grid
-with 8 levels, one independent sample run per host core.
+on a bounded sample of the same workload: the workload's full column (same
+nz, Lz and physics) on a 128 x 128 horizontal tile at the workload's dx, one
+independent sample run per host core.
 """
 from __future__ import annotations
 
@@ -93,7 +109,7 @@ WORKLOADS = {
 # as 1): slow halves 2 x 8, fast stages 3 x 1, projections 5 x 14 = 89, plus
 # 2 (heating factors read per slow half) when heating is on.
 PASSES_BASE, PASSES_HEAT = 89, 2
-SAMPLE_NZ = 8  # levels of the bounded CPU sample
+SAMPLE_N = 128  # horizontal size of the bounded CPU sample (full column depth)
 
 
 def grid_of(w):
@@ -105,7 +121,7 @@ def grid_of(w):
 # configuration builders
 # ---------------------------------------------------------------------------
 
-def b200_integrator(w, precision):
+def b200_integrator(w, precision, blowup_u_max=0.0):
     from oraclev8_b200.grid import LorenzStaggering
     from oraclev8_b200.production_config import BaseState
     from oraclev8_b200.solver import (AdvectionComponent, AnelasticProjection,
@@ -122,7 +138,8 @@ def b200_integrator(w, precision):
     if w["heating"]:
         kw["diabatic_heating"] = DiabaticHeatingComponent(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly,
                                                           Lz=Lz, **w["heating"])
-    return RK3Integrator(OperatorConfig(**kw), base, precision=precision), base
+    return RK3Integrator(OperatorConfig(**kw), base, precision=precision,
+                         blowup_u_max=blowup_u_max), base
 
 
 def host_initial_state(w, base):
@@ -193,14 +210,13 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle on a bounded sample (same nx, ny; SAMPLE_NZ levels)
+# CPU baseline: the oracle on a bounded sample (full column, 128 x 128 tile)
 # ---------------------------------------------------------------------------
 
 def _sample_integrator(w):
     from oracle import lh82 as O
-    nx, ny = w["nx"], w["ny"]
-    nz = SAMPLE_NZ
-    Lz = nz * (w["Lz"] / w["nz"])
+    nx = ny = min(SAMPLE_N, w["nx"])
+    nz, Lz = w["nz"], w["Lz"]
     Lx, Ly = nx * w["dx"], ny * w["dx"]
     z, rho0, th0 = O.build_base_state(nz, Lz)
     cor = dict(w["coriolis"], Ly=Ly, ny=ny)
@@ -238,7 +254,7 @@ def cpu_sample_rate(wname, procs, steps, warmup):
         p.start()
         pipes.append(a)
         ps.append(p)
-    cells = WORKLOADS[wname]["nx"] * WORKLOADS[wname]["ny"] * SAMPLE_NZ
+    cells = sample_cells(WORKLOADS[wname])
     rates = []
     try:
         for i in range(warmup + steps):
@@ -259,6 +275,16 @@ def cpu_sample_rate(wname, procs, steps, warmup):
         for p in ps:
             p.join(timeout=10)
     return rates, cells
+
+
+def sample_cells(w):
+    n = min(SAMPLE_N, w["nx"])
+    return n * n * w["nz"]
+
+
+def sample_name(w):
+    n = min(SAMPLE_N, w["nx"])
+    return f"{n}x{n}x{w['nz']}"
 
 
 def host_cores():
@@ -316,18 +342,34 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# dominant kernel class from one ncu capture of this workload
-# (profiles/ncu_pencil_kernels_config1_fp32r.md): k_ix3 moves 0.558 GB in
-# correction mode and 0.642 GB in stage mode, weighted 2:3 as the five
-# projections of a step use them.
-NCU_TRAFFIC = {
-    ("config1", "fp32r"): {"ix": (2 * 0.558e9 + 3 * 0.642e9) / 5},
-}
+TRAFFIC_FILE = ROOT / "profiles" / "dram_traffic_per_launch.txt"
 
 
 def load_traffic(wname, precision):
-    return NCU_TRAFFIC.get((wname, precision), {})
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    kernel classes, captured by ncu outside this run and committed as text:
+    one ``workload precision class bytes`` row per capture (``#`` comments
+    give the command).  {} where the file has no row for this workload."""
+    out = {}
+    if not TRAFFIC_FILE.exists():
+        return out
+    for ln in TRAFFIC_FILE.read_text().splitlines():
+        ln = ln.split("#", 1)[0].split()
+        if len(ln) >= 4 and ln[0] == wname and ln[1] == precision:
+            out[ln[2]] = float(ln[3])
+    return out
+
+
+def bench_config(args, w, world):
+    """The ``config`` object of both arms' lines (identical, so that the
+    reference arm times the same named workload)."""
+    return {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step, "
+                        f"WS5 + beta-plane + buoyancy + projection"
+                        + (" + heating" if w["heating"] else "")
+                        + (f", u_env={w['coriolis']['u_env']} m/s" if w["coriolis"].get("u_env")
+                           else "") + f", dt={w['dt']}s",
+            "precision": args.precision, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (every state field > 126 MB)"}
 
 
 def max_over_ranks(vals, device):
@@ -514,6 +556,9 @@ def run_b200(args):
     dms, dn = prof[dom]
     ach = kb[dom] / (dms / dn / 1e3) / 1e9
     traffic = load_traffic(args.workload, args.precision).get(dom)
+    cufft = None
+    if not args.no_cufft and rank == 0:
+        cufft = cufft_report(w, args.precision, dev, {c: prof[c][0] for c in prof}, args.steps)
     passes = PASSES_BASE + (PASSES_HEAT if w["heating"] else 0)
     step_gbs = passes * S * cells * args.steps / (ms / 1e3) / 1e9
     line = {
@@ -530,15 +575,14 @@ def run_b200(args):
         "dtype": "f64" if args.precision == "fp64" else "f32 (f64 residual)" if
         args.precision == "fp32r" else "f32",
         "data": "synthetic (seeded Holland vortex + theta' noise; no dataset in the reference)",
-        "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step, "
-                               f"WS5 + beta-plane + buoyancy + projection"
-                               + (" + heating" if w["heating"] else "") + f", dt={dt}s",
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (>= 67 MB per field, 5 fields)"},
+        "config": bench_config(args, w, world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak,
                      "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "bytes_per_launch": kb[dom],
-                     "avg_launch_ms": dms / dn},
+                     "traffic": traffic,
+                     "traffic_source": ("ncu capture outside this run "
+                                        "(profiles/dram_traffic_per_launch.txt)"
+                                        if traffic is not None else None),
+                     "bytes_per_launch": kb[dom], "avg_launch_ms": dms / dn},
         "step_roofline": {"passes_per_cell": passes, "achieved": step_gbs, "peak": peak,
                           "unit": "GB/s", "frac": step_gbs / peak},
         "kernels_ms_per_step": {c: prof[c][0] / args.steps for c in prof if prof[c][1]},
@@ -550,16 +594,8 @@ def run_b200(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if companion:
-        v64 = world * cells * args.steps / (companion[0] / 1e3)
-        line["fp64_plain"] = {"value": v64, "unit": "cell-updates/s",
-                              "ms_per_step": companion[0] / args.steps,
-                              "ratio": value / v64,
-                              "note": "plain FP64 step on the same workload and GPU, timed "
-                                      "the same way (W warm-up + K timed steps)"}
-        line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
-                                note="this run vs the FP64 run from the same initial state; "
-                                     "divergence = anelastic divergence evaluated in FP64")
+    if cufft is not None:
+        line["cufft"] = cufft
     if production is not None:
         line["production"] = production
     if rank == 0 and world == 1 and not args.no_diagnostics:
@@ -575,8 +611,20 @@ def run_b200(args):
             "value": statistics.median(rates), "unit": "cell-updates/s", "cores": 1,
             "kind": "port",
             "sample": f"oracle (NumPy restatement of the reference, FP64) on "
-                      f"{w['nx']}x{w['ny']}x{SAMPLE_NZ} with the same physics, 1 warm-up + "
+                      f"{sample_name(w)} (the workload's column depth and physics on a "
+                      f"smaller horizontal tile at the same dx), 1 warm-up + "
                       f"1 timed step, 1 process"}
+    # the FP32-refined / FP64 comparison last, where a truncated log keeps it
+    if companion:
+        v64 = world * cells * args.steps / (companion[0] / 1e3)
+        line["accuracy"] = dict(companion[1], after_steps=args.warmup + args.steps,
+                                note="this run vs the FP64 run from the same initial state; "
+                                     "divergence = anelastic divergence evaluated in FP64")
+        line["fp64_plain"] = {"value": v64, "unit": "cell-updates/s",
+                              "ms_per_step": companion[0] / args.steps,
+                              "ratio": value / v64,
+                              "note": "plain FP64 step on the same workload and GPU, timed "
+                                      "the same way (W warm-up + K timed steps)"}
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -836,6 +884,127 @@ def ensemble_report(args, peak_gbs):
     return ens, serving
 
 
+def cufft_report(w, precision, dev, kernels_ms, steps, projections=5, reps=5):
+    """cuFFT through torch.fft doing the transforms of one projection on the
+    workload's grid: R2C along x of three real fields, C2C along y of two of
+    the results, the two inverse y transforms and three C2R along x (the
+    transform count of this library's pencils), in the step's arithmetic
+    precision, timed with CUDA events on the current stream (median of
+    ``reps`` after a warm-up).  Beside it, this library's pencil classes per
+    projection (fx + fy + iy + ix from the timed steps), which also do the
+    projection's arithmetic and its state reads and writes."""
+    import torch
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    g = torch.Generator(device=dev).manual_seed(5)
+    f = [torch.randn(nx, ny, nz, dtype=dt, device=dev, generator=g) for _ in range(3)]
+
+    def once():
+        X = [torch.fft.rfft(a, dim=0) for a in f]
+        Y = [torch.fft.fft(X[0], dim=1), torch.fft.fft(X[1], dim=1)]
+        Z = [torch.fft.ifft(Y[0], dim=1), torch.fft.ifft(Y[1], dim=1)]
+        return [torch.fft.irfft(Z[0], n=nx, dim=0), torch.fft.irfft(Z[1], n=nx, dim=0),
+                torch.fft.irfft(X[2], n=nx, dim=0)]
+
+    once()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        out = once()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+        del out
+    del f
+    torch.cuda.empty_cache()
+    ours = sum(kernels_ms.get(c, 0.0) for c in ("fx", "fy", "iy", "ix")) / steps / projections
+    cu = statistics.median(ts)
+    return {"what": "3 R2C x + 2 C2C y + 2 inverse C2C y + 3 C2R x (one projection's "
+                    "transforms), torch.fft (cuFFT) on (nx, ny, nz) z-contiguous fields",
+            "precision": "fp64" if precision == "fp64" else "fp32",
+            "cufft_ms_per_projection": cu,
+            "pencils_ms_per_projection": ours,
+            "pencils_note": "fx + fy + iy + ix kernel classes of the timed steps / projections; "
+                            "they also form the divergence, read and correct the state",
+            "ratio_cufft_over_pencils": cu / ours if ours > 0 else None}
+
+
+def _hour_chunk(steps_per_hour, cap=24):
+    return max(c for c in range(1, cap + 1) if steps_per_hour % c == 0)
+
+
+def track_report(args):
+    """The workload run for ``--track-hours`` hours in FP32-refined and in
+    plain FP64 on this GPU, with the hourly storm centre of each
+    (find_storm_centre chained through last_pos / last_raw_pos, with the
+    background flow, as run_storm.py:180-190 does), the hourly max|w| and, at
+    the end, the per-field error of the FP32-refined run against the FP64 run
+    and the FP64-evaluated non-Nyquist divergence of both.  The steps run as
+    captured step graphs of a whole number of steps per hour."""
+    import torch
+    from oraclev8_b200.solver import State
+    from oraclev8_b200.storm_tracker import find_storm_centre
+    torch.cuda.set_device(0)
+    w = WORKLOADS[args.workload]
+    nx, ny, nz, Lx, Ly, Lz = grid_of(w)
+    dx = Lx / nx
+    dt = w["dt"]
+    sph = int(round(3600.0 / dt))
+    chunk = _hour_chunk(sph)
+    u_env = w["coriolis"].get("u_env", 0.0)
+    v_env = w["coriolis"].get("v_env", 0.0)
+    runs = {}
+    hs = None
+    for prec in ("fp64", "fp32r"):
+        integ, base = b200_integrator(w, prec, blowup_u_max=400.0)
+        if hs is None:
+            hs = host_initial_state(w, base)
+        ty = integ.dtype
+        st = State(*(torch.as_tensor(a, dtype=ty).cuda() for a in
+                     (hs.u, hs.v, hs.w, hs.theta_prime, hs.projection_potential)), 0.0)
+        runs[prec] = dict(integ=integ, base=base, st=st, graph=integ.capture(st, dt, chunk),
+                          last=None, last_raw=None, fixes=[])
+    hours = int(args.track_hours)
+    t0 = time.perf_counter()
+    for h in range(hours + 1):
+        for prec, r in runs.items():
+            if h > 0:
+                for _ in range(sph // chunk):
+                    r["graph"].launch()
+            (x, y), m, d = find_storm_centre(r["st"], r["base"], nx, ny, dx,
+                                             last_pos=r["last"], u_env_ms=u_env,
+                                             v_env_ms=v_env, dt_output_s=3600.0,
+                                             return_diag=True, last_raw_pos=r["last_raw"])
+            r["last"], r["last_raw"] = (x, y), d["theta_raw_m"]
+            r["fixes"].append(dict(x=x, y=y, method=m, max_w=float(r["st"].w.abs().max()),
+                                   max_u=float(r["st"].u.abs().max())))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    f64, f32 = runs["fp64"]["fixes"], runs["fp32r"]["fixes"]
+    rows = []
+    for h, (a, b) in enumerate(zip(f32, f64)):
+        rows.append(dict(h=h, dist_m=float(math.hypot(a["x"] - b["x"], a["y"] - b["y"])),
+                         max_w_rel=abs(a["max_w"] - b["max_w"]) / max(b["max_w"], 1e-30),
+                         method_fp32r=a["method"], method_fp64=b["method"],
+                         x_fp64_km=b["x"] / 1e3, y_fp64_km=b["y"] / 1e3))
+    st32, st64 = runs["fp32r"]["st"], runs["fp64"]["st"]
+    rep = _precision_report(st32, st64, runs["fp64"]["integ"].plan)
+    line = {"track": {
+        "workload": f"{args.workload}: {nx}x{ny}x{nz}, dt={dt}s, {hours} h = {hours * sph} steps "
+                    f"in each precision, step graphs of {chunk} steps",
+        "hours": rows,
+        "max_centre_diff_m": max(r["dist_m"] for r in rows),
+        "max_w_rel_diff_max": max(r["max_w_rel"] for r in rows),
+        "fp64_track_km": [(round(r["x_fp64_km"], 3), round(r["y_fp64_km"], 3)) for r in rows],
+        "final": rep,
+        "blowup": {p: runs[p]["integ"].plan.blown_up() for p in runs},
+        "wall_s": wall}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -859,11 +1028,11 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} LH82 RK3 step",
-                   "parallelism": f"{procs} host processes"},
+        "config": bench_config(args, w, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "port",
                          "sample": f"{procs} independent oracle runs (NumPy restatement of the "
-                                   f"reference, FP64), each {w['nx']}x{w['ny']}x{SAMPLE_NZ} "
+                                   f"reference, FP64), each {sample_name(w)} (the "
+                                   f"workload's column depth on a smaller horizontal tile) "
                                    f"with the workload's physics; one step per process per "
                                    f"bench step"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
@@ -879,7 +1048,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp32r", choices=["fp64", "fp32", "fp32r"])
-    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-production", action="store_true",
@@ -892,7 +1061,13 @@ def main():
     ap.add_argument("--ensemble-hours", type=float, default=6.0)
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--serving-scale", type=float, default=4.0)
+    ap.add_argument("--track-hours", type=float, default=0.0,
+                    help="run the FP32-refined vs FP64 hourly track comparison instead")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
     args = ap.parse_args()
+    if args.track_hours > 0:
+        track_report(args)
+        return
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":

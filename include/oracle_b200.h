@@ -78,6 +78,11 @@ extern "C" {
 #define OB_DIAG_DISC0 9        /* discrete-operator residual of the 3 stages */
 #define OB_DIAG_LAST_COMPAT 12 /* last solve's compat residual */
 #define OB_DIAG_LAST_DISC 13   /* last solve's discrete residual */
+/* Blow-up flag, sticky over the plan's life: 1 once a diagnosed state held a
+ * non-finite value, 2 once max|u| exceeded the plan's blowup_u_max (the
+ * blow-up test of oracle_v8/measure_lh82_phase3.py:129-130).  The maxima in
+ * slots 0-3 propagate NaN as NumPy's max does. */
+#define OB_DIAG_BLOWUP 14
 #define OB_DIAG_COUNT 16
 
 typedef struct OracleGridDesc {
@@ -120,6 +125,10 @@ typedef struct OracleComponentDesc {
     double diff_dx2, diff_dy2;  /* (Lx/nx)^2, (Ly/ny)^2 */
     int cooling;                /* NewtonianCoolingComponent (tendency.py:1630-1668) */
     double cool_alpha;          /* 1 / tau */
+    /* blow-up limit of max|u| in m/s for OB_DIAG_BLOWUP (0: non-finite values
+     * only); no OperatorConfig slot, the reference's harnesses test it after
+     * each step (measure_lh82_phase3.py:129-130) */
+    double blowup_u_max;
 } OracleComponentDesc;
 
 typedef struct OracleStatePtrs {
@@ -210,7 +219,9 @@ int oracle_b200_intensity_cap(const void *u, const void *v, int precision, long 
                               double v_cap, double tau, double u_env, double v_env,
                               void *du, void *dv, void *stream);
 
-/* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`). */
+/* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`).
+ * Returns OB_ERR_NONFINITE, with host_out filled all the same, when the plan's
+ * blow-up flag (OB_DIAG_BLOWUP) is set. */
 int oracle_b200_read_diag(OraclePlan *plan, double *host_out, int n, void *stream);
 
 /* FP64 defect correction of single-precision plans (the FP32-refined
@@ -368,18 +379,27 @@ int oracle_b200_vdiag_centroid(OracleVortexDiag *diag, int i0, int i1, int j0, i
  * device memory, or a latency-critical caller that cannot afford cudaMalloc's
  * device synchronisation).  Same result as oracle_b200_poisson_solve on a plan
  * of the same grid and rho0 (host array, nz values), without a plan.
- *  - Working memory is one fixed 32 MiB array per device, reserved by the CUDA
- *    module on every GPU that loads this library until the process exits.
- *    Grids whose tables plus two half-spectrum buffers exceed it, or with
- *    nx, ny > 2048 or nz > 512, are rejected with OB_ERR_ARG (e.g. 128x128x32
- *    FP64 uses about 8.5 MB; 256x256x32 FP64 does not fit).
- *  - The first call on each device looks up the array's address and sets
- *    kernel attributes; make that first call before any stream capture.
+ *  - Working memory is one fixed 32 MiB array per device.  It needs the
+ *    tables (under 0.2 MiB) plus 2 (nx/2 + 1) ny nz 2 sizeof(T) bytes for two
+ *    half-spectrum buffers; grids beyond that, or with nx, ny > 2048 or
+ *    nz > 512, are rejected with OB_ERR_ARG.  FP64: 192x192x32 fits (19 MB),
+ *    256x256x32 does not (33.8 MB).  FP32: 256x256x48 fits (25 MB),
+ *    256x256x64 does not.
+ *  - The array is part of this library's CUDA module and is reserved on a
+ *    device when the module loads there: under CUDA's lazy module loading, at
+ *    the first call of this function or the first plan created on that
+ *    device.  It stays reserved until the process exits.  A host that gives
+ *    the GPU's free memory to its own allocator makes that first call before
+ *    doing so; later calls allocate nothing.
+ *  - The first call on each device also looks up the array's address and
+ *    sets kernel attributes.
+ *  - It cannot be captured into a CUDA graph: on a capturing stream it returns
+ *    OB_ERR_ARG before enqueuing anything, and the capture stays valid.  The
+ *    tables are copied from a shared host staging buffer, so the call returns
+ *    after they are staged; the solve itself is enqueued on `stream`.
  *  - Every call shares the array and overwrites all of it that it reads, so
  *    nothing carries over between calls; calls whose GPU work overlaps (other
- *    streams, other host threads on the same device) race on it.
- *  - The tables are copied from pageable host memory, so the call returns
- *    after they are staged; the solve itself is enqueued on `stream`. */
+ *    streams, other host threads on the same device) race on it. */
 int oracle_b200_poisson_solve_noalloc(const OracleGridDesc *grid, const double *rho0,
                                       const void *d, void *phi, void *stream);
 

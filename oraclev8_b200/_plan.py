@@ -65,6 +65,9 @@ class PlanSpec:
     diff_dy2: float = 1.0
     cooling: bool = False
     cool_alpha: float = 0.0
+    # max|u| (m/s) above which the device's blow-up flag is raised; 0: only
+    # non-finite values raise it (measure_lh82_phase3.py:129-130)
+    blowup_u_max: float = 0.0
 
 
 def _f64(a):
@@ -99,7 +102,7 @@ class Plan:
                             float(spec.sponge_u_env), float(spec.sponge_v_env), L.dptr(sp_a),
                             L.dptr(sp_ah), int(spec.diffusion), float(spec.diff_nu),
                             float(spec.diff_dx2), float(spec.diff_dy2), int(spec.cooling),
-                            float(spec.cool_alpha))
+                            float(spec.cool_alpha), float(spec.blowup_u_max))
         h = ctypes.c_void_p()
         L.check(self.lib.oracle_b200_plan_create(ctypes.byref(g), ctypes.byref(c), ctypes.byref(h)))
         self.handle = h
@@ -187,9 +190,20 @@ class Plan:
         return StepGraph(self, ptrs, dt, nsteps)
 
     def read_diag(self) -> np.ndarray:
+        """The diagnostics block (synchronises the current stream).  A raised
+        blow-up flag is not an error here: it is slot ``DIAG["blowup"]``, and
+        the values are returned as computed (NaN maxima propagate as NumPy's
+        max does)."""
         buf = (ctypes.c_double * L.DIAG_COUNT)()
-        L.check(self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream()))
+        rc = self.lib.oracle_b200_read_diag(self.handle, buf, L.DIAG_COUNT, self._stream())
+        if rc != L.OB_ERR_NONFINITE:
+            L.check(rc)
         return np.frombuffer(buf, dtype=np.float64).copy()
+
+    def blown_up(self) -> int:
+        """The plan's sticky blow-up flag as of its last diagnosed step: 0 none,
+        1 a non-finite value, 2 max|u| above ``blowup_u_max``."""
+        return int(self.read_diag()[L.DIAG["blowup"]])
 
     def project(self, u, v, w, phi, log_diag=False):
         s = self.shape
@@ -294,7 +308,7 @@ def _key(spec: PlanSpec) -> tuple:
             float(spec.drag_v_env), b(spec.drag_weight), spec.sponge, float(spec.sponge_u_env),
             float(spec.sponge_v_env), b(spec.sponge_alpha), b(spec.sponge_alpha_h),
             spec.diffusion, float(spec.diff_nu), float(spec.diff_dx2), float(spec.diff_dy2),
-            spec.cooling, float(spec.cool_alpha))
+            spec.cooling, float(spec.cool_alpha), float(spec.blowup_u_max))
 
 
 def cached_plan(spec: PlanSpec) -> Plan:

@@ -11,7 +11,6 @@
 
 #include "../../include/oracle_b200.h"
 #include "kernels.cuh"
-#include "pipe.cuh"
 #include "pencil.cuh"
 #include "xreg.cuh"
 #include "tracker.cuh"
@@ -111,29 +110,83 @@ bool factorize8(int M, FftPlan& p) {
   return m == 1;
 }
 
-// 2 pi fftfreq(n, d=L/n), with NumPy's operation order (numpy/fft/_helper.py).
-std::vector<double> wavenumbers(int n, double L) {
+// 2 pi fftfreq(n, d=L/n), with NumPy's operation order (numpy/fft/_helper.py),
+// into k[0..n).
+void fill_wavenumbers(double* k, int n, double L) {
   const double d = L / n;
   const double val = 1.0 / ((double)n * d);
   const int N = (n - 1) / 2 + 1;
-  std::vector<double> k(n);
   for (int i = 0; i < n; ++i) {
     const long si = (i < N) ? i : (long)i - n;
     k[i] = (2.0 * M_PI) * ((double)si * val);
   }
+}
+std::vector<double> wavenumbers(int n, double L) {
+  std::vector<double> k(n);
+  fill_wavenumbers(k.data(), n, L);
   return k;
 }
 
+// W_N^t = exp(-2 pi i t / N), t < N, evaluated in long double, into tw[0..N).
 template <class T>
-std::vector<cplx<T>> twiddles(int N) {
-  std::vector<cplx<T>> tw(N);
+void fill_twiddles(cplx<T>* tw, int N) {
   for (int t = 0; t < N; ++t) {
     const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)t /
                           (long double)N;
     tw[t].x = (T)cosl(a);
     tw[t].y = (T)sinl(a);
   }
+}
+template <class T>
+std::vector<cplx<T>> twiddles(int N) {
+  std::vector<cplx<T>> tw(N);
+  fill_twiddles<T>(tw.data(), N);
   return tw;
+}
+
+// Host tables of the anelastic Poisson solver, written into caller-provided
+// arrays, shared by oracle_b200_plan_create and the allocation-free solve so
+// that the two cannot drift apart:
+//   rh[nz + 1]   rho on half levels: interior means, boundary copies
+//                (tendency.py:748-754);
+//   a, c, negs[nz]  the vertical operator's sub / super diagonals and the
+//                negated sum of the flux weights, Neumann edge rows
+//                (poisson.py:286-315);
+//   a0, cp0, inv0[nz - 1]  forward-elimination factors of the zero mode's
+//                reduced system with phi(0, 0, 0) pinned (poisson.py:316-325).
+struct SolverTables {
+  double *rh, *a, *c, *negs, *a0, *cp0, *inv0;
+};
+void fill_solver_tables(int nz, double dz, const double* rf, const SolverTables& t) {
+  double* rh = t.rh;
+  for (int k = 1; k < nz; ++k) rh[k] = 0.5 * (rf[k - 1] + rf[k]);
+  rh[0] = rf[0];
+  rh[nz] = rf[nz - 1];
+  const double dz2 = dz * dz;
+  auto rl = [&](int k) { return rh[k] / dz2; };
+  auto ru = [&](int k) { return rh[k + 1] / dz2; };
+  for (int k = 0; k < nz; ++k) {
+    t.a[k] = rl(k);
+    t.c[k] = ru(k);
+    t.negs[k] = -(rl(k) + ru(k));
+  }
+  t.a[0] = 0.0;
+  t.c[nz - 1] = 0.0;
+  t.negs[0] = -ru(0);
+  t.negs[nz - 1] = -rl(nz - 1);
+  // the reduced system's rows j = 0 .. n0 - 1 are levels 1 .. nz - 1
+  const int n0 = nz - 1;
+  auto a0 = [&](int j) { return j == 0 ? 0.0 : (j == n0 - 1 ? rl(nz - 1) : rl(j + 1)); };
+  auto b0 = [&](int j) { return j == n0 - 1 ? -rl(nz - 1) : -(rl(j + 1) + ru(j + 1)); };
+  auto c0 = [&](int j) { return j == n0 - 1 ? 0.0 : ru(j + 1); };
+  for (int j = 0; j < n0; ++j) t.a0[j] = a0(j);
+  t.inv0[0] = 1.0 / b0(0);
+  t.cp0[0] = c0(0) * t.inv0[0];
+  for (int j = 1; j < n0; ++j) {
+    const double den = b0(j) - t.a0[j] * t.cp0[j - 1];
+    t.inv0[j] = 1.0 / den;
+    t.cp0[j] = (j < n0 - 1) ? c0(j) * t.inv0[j] : 0.0;
+  }
 }
 
 }  // namespace
@@ -148,6 +201,7 @@ struct OraclePlan {
   double drag_cd = 0, drag_dz = 1, drag_u_env = 0, drag_v_env = 0;
   double sponge_u_env = 0, sponge_v_env = 0;
   double diff_nu = 0, diff_dx2 = 1, diff_dy2 = 1, cool_alpha = 0;
+  double blowup_u = 0;  // max|u| limit of the blow-up flag (0: non-finite values only)
   double *drag_w = nullptr, *sp_a = nullptr, *sp_ah = nullptr;
   void *Lu = nullptr, *Lv = nullptr;  // biharmonic: the inner Laplacians
   int diag_every = 60;
@@ -155,10 +209,6 @@ struct OraclePlan {
   FftPlan px{}, py{};    // radix-16-first plans (inverse kernels)
   FftPlan pxf{}, pyf{};  // radix-4-first plans (forward kernels: lower register pressure)
   int zc_fx = 1, zc_fy = 1, zc_iy = 1, zc_ix = 1;
-  // pipelined projection kernels: z-chunk and persistent grid size
-  int zc_fxp = 1, zc_fyp = 1, zc_iyp = 1, zc_ixp = 1;
-  int grid_fxp = 1, grid_fyp = 1, grid_iyp = 1, grid_ixp = 1;
-  int use_pipe = 0;  // projection through the persistent pipelined kernels
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
   FftPlan px8{}, py8{};
   int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
@@ -320,43 +370,6 @@ size_t smem_thomas(const OraclePlan* p, size_t rsz = 8) {
   return thomas_stage_offset(p->g.nz + 1) + 3ull * kThomasCols * (p->g.nz + 1) * rsz;
 }
 
-constexpr int kPipeThreads = 256;
-
-size_t smem_fxp(const OraclePlan* p, int zc) {
-  const size_t raw = (fxp_raw_elems<double>(p->g.nx, zc, true) * p->esz + 15) & ~size_t(15);
-  return tw_bytes(p, p->g.nx) + 2 * raw + 2ull * (p->g.M + 1) * ((3 * zc) | 1) * 2 * p->esz;
-}
-size_t smem_fyp(const OraclePlan* p, int zc) {
-  return tw_bytes(p, p->g.ny) + 3ull * p->g.ny * ((2 * zc) | 1) * 2 * p->esz;
-}
-size_t smem_iyp(const OraclePlan* p, int zc) {
-  return tw_bytes(p, p->g.ny) + 2ull * p->g.ny * zc * 2 * p->esz +
-         2ull * p->g.ny * ((2 * zc) | 1) * 2 * p->esz;
-}
-size_t smem_ixp(const OraclePlan* p, int zc) {
-  const size_t raw = p->esz == 8 ? ixp_raw_bytes<double>(p->g.nx, zc, true)
-                                 : ixp_raw_bytes<float>(p->g.nx, zc, true);
-  return tw_bytes(p, p->g.nx) + 2 * raw + (size_t)(2 * p->g.M + 1) * ((3 * zc + 1) | 1) * 2 * p->esz;
-}
-
-// Largest z-chunk whose footprint lets `occ` CTAs share an SM (occ = 2 by
-// default; ORACLE_B200_PIPE_OCC=1 prefers one CTA with a deeper chunk);
-// falls back to one CTA per SM.
-template <class F>
-int pick_pipe_zc(int nz, F&& smem) {
-  int occ = 2;
-  if (const char* e = getenv("ORACLE_B200_PIPE_OCC")) occ = atoi(e) == 1 ? 1 : 2;
-  const size_t budget = occ == 2 ? (kSmemMax - 1024) / 2 : kSmemMax;
-  for (size_t lim : {budget, kSmemMax})
-    for (int zc : {8, 4, 2, 1}) {
-      if (zc > nz && zc > 1) continue;
-      if (smem(zc) <= lim) return zc;
-    }
-  return 0;
-}
-
-// x2 pencil kernels: allow the full shared-memory carve-out so that the
-// target number of CTAs fits on an SM.
 template <class K>
 int x2_attr(K kernel) {
   OB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
@@ -463,12 +476,6 @@ int set_smem_attrs() {
   OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ix<T, IX_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_thomas<T, kThomasCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_fxp<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_fxp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_fyp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_iyp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_ixp<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  OB_CUDA(cudaFuncSetAttribute(k_ixp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_fx<double, FX_DIV, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_fy<double, FY_RESID, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_ix<float, IX_REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -487,45 +494,6 @@ int set_smem_attrs_once() {
   if (known && done[dev]) return OB_OK;
   if (int rc = set_smem_attrs<T>()) return rc;
   if (known) done[dev] = true;
-  return OB_OK;
-}
-
-// Persistent grid: resident CTAs per SM (occupancy API) x SMs, capped by items.
-template <class K>
-int persistent_grid(K kernel, size_t smem, int items, int* out) {
-  int dev = 0, nsm = 148, per = 1;
-  OB_CUDA(cudaGetDevice(&dev));
-  OB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  OB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPipeThreads, smem));
-  if (per < 1) return fail(OB_ERR_ARG, "pipelined kernel does not fit on an SM (smem %zu)", smem);
-  *out = std::max(1, std::min(items, per * nsm));
-  return OB_OK;
-}
-
-template <class T>
-int setup_pipes(OraclePlan* p) {
-  const int nz = p->g.nz;
-  p->zc_fxp = pick_pipe_zc(nz, [&](int zc) { return smem_fxp(p, zc); });
-  p->zc_fyp = pick_pipe_zc(nz, [&](int zc) { return smem_fyp(p, zc); });
-  p->zc_iyp = pick_pipe_zc(nz, [&](int zc) { return smem_iyp(p, zc); });
-  p->zc_ixp = pick_pipe_zc(nz, [&](int zc) { return smem_ixp(p, zc); });
-  if (!p->zc_fxp || !p->zc_fyp || !p->zc_iyp || !p->zc_ixp)
-    return fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds the pipelined kernels' shared memory",
-                p->g.nx, p->g.ny, nz);
-  auto nzc = [&](int zc) { return (nz + zc - 1) / zc; };
-  int rc;
-  if ((rc = persistent_grid(k_fxp<T, true>, smem_fxp(p, p->zc_fxp), p->g.ny * nzc(p->zc_fxp),
-                            &p->grid_fxp)))
-    return rc;
-  if ((rc = persistent_grid(k_fyp<T>, smem_fyp(p, p->zc_fyp), p->g.nxh * nzc(p->zc_fyp),
-                            &p->grid_fyp)))
-    return rc;
-  if ((rc = persistent_grid(k_iyp<T>, smem_iyp(p, p->zc_iyp), p->g.nxh * nzc(p->zc_iyp),
-                            &p->grid_iyp)))
-    return rc;
-  if ((rc = persistent_grid(k_ixp<T, true>, smem_ixp(p, p->zc_ixp), p->g.ny * nzc(p->zc_ixp),
-                            &p->grid_ixp)))
-    return rc;
   return OB_OK;
 }
 
@@ -916,45 +884,6 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
   return OB_OK;
 }
 
-// projection through the persistent pipelined kernels (pipe.cuh)
-template <class T>
-int project_pipe(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
-                 double stage_sdt, T* uo, T* vo, T* wo, T* phio, double* diag, int slot_c,
-                 int slot_d, cudaStream_t st) {
-  using C = cplx<T>;
-  const GridK g = p->g;
-  C* S1 = (C*)p->S1;
-  C* S2 = (C*)p->S2;
-  C* S3 = (C*)p->S3;
-  const bool stage = stage_sdt >= 0.0;
-  if (stage)
-    { Launch L_(p, 0, st); k_fxp<T, true><<<p->grid_fxp, kPipeThreads, smem_fxp(p, p->zc_fxp), st>>>(
-        g, p->pxf, p->zc_fxp, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2); }
-  else
-    { Launch L_(p, 0, st); k_fxp<T, false><<<p->grid_fxp, kPipeThreads, smem_fxp(p, p->zc_fxp), st>>>(
-        g, p->pxf, p->zc_fxp, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2); }
-  OB_LAUNCHED();
-  { Launch L_(p, 1, st); k_fyp<T><<<p->grid_fyp, kPipeThreads, smem_fyp(p, p->zc_fyp), st>>>(
-      g, p->pyf, p->zc_fyp, S1, S2, p->ky, (const C*)p->twy, S3); }
-  OB_LAUNCHED();
-  RC(thomas_solve<T>(p, 2, S3, diag, slot_c, slot_d, st));
-  { Launch L_(p, 3, st); k_iyp<T><<<p->grid_iyp, kPipeThreads, smem_iyp(p, p->zc_iyp), st>>>(
-      g, p->py, p->zc_iyp, S3, p->ky, (const C*)p->twy, 1.0, S1, S2); }
-  OB_LAUNCHED();
-  if (stage)
-    { Launch L_(p, 4, st); k_ixp<T, true><<<p->grid_ixp, kPipeThreads, smem_ixp(p, p->zc_ixp), st>>>(
-        g, p->px, p->zc_ixp, S1, S2, p->kx, (const C*)p->twx, u, v, w, th, stage_sdt,
-        p->theta0, uo, vo, wo, phio); }
-  else
-    { Launch L_(p, 4, st); k_ixp<T, false><<<p->grid_ixp, kPipeThreads, smem_ixp(p, p->zc_ixp), st>>>(
-        g, p->px, p->zc_ixp, S1, S2, p->kx, (const C*)p->twx, u, v, w, th, 0.0, p->theta0,
-        uo, vo, wo, phio); }
-  OB_LAUNCHED();
-  return OB_OK;
-}
-
 // ---- projection pipeline -------------------------------------------------
 // stage_sdt < 0: in-place projection of (u, v, w) with phi output.
 // stage_sdt >= 0: inputs are the anchor state (u, v, w, th); the provisional
@@ -981,7 +910,6 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
     OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
   }
   const bool stage = stage_sdt >= 0.0;
-  if (p->use_pipe) return project_pipe<T>(p, u, v, w, th, stage_sdt, uo, vo, wo, phio, diag, slot_c, slot_d, st);
   bool fx_done = false;
   if constexpr (sizeof(T) == 4) {
     if (p->zc3_fx && stage && bh) {
@@ -1283,7 +1211,7 @@ int diag_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th, co
   { Launch L_(p, 6, st); k_diag_partial<T><<<p->nparts, 256, 0, st>>>(p->g, u, v, w, th, phi, p->parts); }
   OB_LAUNCHED();
   { Launch L_(p, 6, st); k_diag_final<<<1, 32, 0, st>>>(p->parts, p->nparts,
-                                 (double)p->g.nx * p->g.ny * p->g.nz, p->diag); }
+                                 (double)p->g.nx * p->g.ny * p->g.nz, p->blowup_u, p->diag); }
   OB_LAUNCHED();
   return OB_OK;
 }
@@ -2023,6 +1951,9 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
   p->diff_dx2 = comp->diffusion ? comp->diff_dx2 : 1.0;
   p->diff_dy2 = comp->diffusion ? comp->diff_dy2 : 1.0;
   p->cool_alpha = comp->cool_alpha;
+  if (!(comp->blowup_u_max >= 0.0))
+    return bail(fail(OB_ERR_ARG, "blowup_u_max must be >= 0 (got %g)", comp->blowup_u_max));
+  p->blowup_u = comp->blowup_u_max;
   p->f0 = comp->f0;
   p->u_env = comp->u_env;
   p->v_env = comp->v_env;
@@ -2034,45 +1965,12 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
 
   const double dz = p->g.dz;
   const double* rf = comp->rho0;
-  // rho on half levels (tendency.py:748-754)
-  std::vector<double> rh(nz + 1);
-  for (int k = 1; k < nz; ++k) rh[k] = 0.5 * (rf[k - 1] + rf[k]);
-  rh[0] = rf[0];
-  rh[nz] = rf[nz - 1];
-  // Thomas tables (poisson.py:286-325)
-  const double dz2 = dz * dz;
-  std::vector<double> rl(nz), ru(nz), a(nz), c(nz), negs(nz);
-  for (int k = 0; k < nz; ++k) {
-    rl[k] = rh[k] / dz2;
-    ru[k] = rh[k + 1] / dz2;
-  }
-  for (int k = 0; k < nz; ++k) {
-    a[k] = rl[k];
-    c[k] = ru[k];
-    negs[k] = -(rl[k] + ru[k]);
-  }
-  a[0] = 0.0;
-  c[nz - 1] = 0.0;
-  negs[0] = -ru[0];
-  negs[nz - 1] = -rl[nz - 1];
+  // rho on half levels and the Thomas tables
   const int n0 = nz - 1;
-  std::vector<double> a0(n0), b0(n0), c0(n0), inv0(n0), cp0(n0);
-  for (int j = 0; j < n0; ++j) {
-    a0[j] = rl[j + 1];
-    b0[j] = -(rl[j + 1] + ru[j + 1]);
-    c0[j] = ru[j + 1];
-  }
-  a0[0] = 0.0;
-  a0[n0 - 1] = rl[nz - 1];
-  c0[n0 - 1] = 0.0;
-  b0[n0 - 1] = -rl[nz - 1];
-  inv0[0] = 1.0 / b0[0];
-  cp0[0] = c0[0] * inv0[0];
-  for (int j = 1; j < n0; ++j) {
-    const double den = b0[j] - a0[j] * cp0[j - 1];
-    inv0[j] = 1.0 / den;
-    cp0[j] = (j < n0 - 1) ? c0[j] * inv0[j] : 0.0;
-  }
+  std::vector<double> rh(nz + 1), a(nz), c(nz), negs(nz), a0(n0), inv0(n0), cp0(n0);
+  fill_solver_tables(nz, dz, rf,
+                     SolverTables{rh.data(), a.data(), c.data(), negs.data(), a0.data(),
+                                  cp0.data(), inv0.data()});
   // d theta0 / dz (tendency.py:1013-1016)
   const double* t0 = comp->theta0;
   std::vector<double> dth0(nz);
@@ -2114,10 +2012,6 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
                         p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs_once<double>())) return bail(rc);
-    // the persistent pipelined projection is optional (ORACLE_B200_PIPE=1):
-    // sized only when asked for, and left off where its tiles do not fit
-    if (const char* e = getenv("ORACLE_B200_PIPE"))
-      if (atoi(e) != 0) p->use_pipe = setup_pipes<double>(p) == OB_OK;
   } else {
     auto tx = twiddles<float>(nx), ty = twiddles<float>(ny);
     if ((rc = dalloc(p, &p->twx, nx * sizeof(cplx<float>)))) return bail(rc);
@@ -2128,10 +2022,6 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
                         p->astream))
       return bail(fail(OB_ERR_CUDA, "twiddle upload failed"));
     if ((rc = set_smem_attrs_once<float>())) return bail(rc);
-    // the persistent pipelined projection is optional (ORACLE_B200_PIPE=1):
-    // sized only when asked for, and left off where its tiles do not fit
-    if (const char* e = getenv("ORACLE_B200_PIPE"))
-      if (atoi(e) != 0) p->use_pipe = setup_pipes<float>(p) == OB_OK;
   }
 
   // chunk sizes: largest z-chunk whose shared-memory footprint allows two CTAs/SM
@@ -2285,9 +2175,13 @@ int oracle_b200_step_graph_create(OraclePlan* p, const OracleStatePtrs* state, d
   const long l0 = p->launches;
   p->capturing = 1;
   int rc = OB_OK;
-  for (int s = 0; s < nsteps && rc == OB_OK; ++s)
-    rc = DISPATCH(p, step_impl<double>(p, state, state, dt, 0, cs),
-                  step_impl<float>(p, state, state, dt, 0, cs));
+  // the last step of the graph also runs the diagnostics reductions, so the
+  // plan's blow-up flag is updated once per graph launch
+  for (int s = 0; s < nsteps && rc == OB_OK; ++s) {
+    const int dg = s == nsteps - 1;
+    rc = DISPATCH(p, step_impl<double>(p, state, state, dt, dg, cs),
+                  step_impl<float>(p, state, state, dt, dg, cs));
+  }
   p->capturing = 0;
   cudaGraph_t graph = nullptr;
   e = cudaStreamEndCapture(cs, &graph);
@@ -2503,6 +2397,11 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
   for (int s : {OB_DIAG_DISC0, OB_DIAG_DISC0 + 1, OB_DIAG_DISC0 + 2, OB_DIAG_LAST_DISC})
     buf[s] = std::sqrt(std::fmax(buf[s], 0.0) / norm);
   std::memcpy(host_out, buf, n * sizeof(double));
+  if (buf[OB_DIAG_BLOWUP] >= 2.0)
+    return fail(OB_ERR_NONFINITE, "blow-up: max|u| exceeded %g m/s in a diagnosed step",
+                p->blowup_u);
+  if (buf[OB_DIAG_BLOWUP] >= 1.0)
+    return fail(OB_ERR_NONFINITE, "blow-up: a diagnosed state held a non-finite value");
   return OB_OK;
 }
 
@@ -2520,8 +2419,11 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
 // serves them: it performs the same FFT + Thomas solve as
 // oracle_b200_poisson_solve, but every byte of working memory (spectral
 // buffers, wavenumber / twiddle / Thomas tables) lives in the fixed array
-// below.  The CUDA module reserves that array on every device that loads this
-// library, and it stays reserved until the process exits.
+// below.  The array belongs to this library's CUDA module: it is reserved on a
+// device when the module is loaded there (with CUDA's lazy module loading, at
+// the first call of this entry point or the first plan created on that
+// device) and stays reserved until the process exits.  Hosts that hand the
+// GPU's memory to their own allocator make that first call beforehand.
 
 namespace {
 
@@ -2635,62 +2537,12 @@ int noalloc_solve(const OracleGridDesc* grid, const double* rho0, const T* d, T*
   double* a0 = (double*)(h + o_a0);
   double* cp0 = (double*)(h + o_cp0);
   double* inv0 = (double*)(h + o_inv0);
-  {
-    const double dxk = grid->Lx / nx, dyk = grid->Ly / ny;
-    const double vx = 1.0 / ((double)nx * dxk), vy = 1.0 / ((double)ny * dyk);
-    for (int i = 0; i < nx; ++i) {
-      const long si = (i < (nx - 1) / 2 + 1) ? i : (long)i - nx;
-      kx[i] = (2.0 * M_PI) * ((double)si * vx);
-    }
-    for (int i = 0; i < ny; ++i) {
-      const long si = (i < (ny - 1) / 2 + 1) ? i : (long)i - ny;
-      ky[i] = (2.0 * M_PI) * ((double)si * vy);
-    }
-  }
+  fill_wavenumbers(kx, nx, grid->Lx);
+  fill_wavenumbers(ky, ny, grid->Ly);
   for (int k = 0; k < nz; ++k) rf[k] = rho0[k];
-  for (int k = 1; k < nz; ++k) rh[k] = 0.5 * (rf[k - 1] + rf[k]);
-  rh[0] = rf[0];
-  rh[nz] = rf[nz - 1];
-  const double dz2 = p.g.dz * p.g.dz;
-  for (int k = 0; k < nz; ++k) {
-    const double rl = rh[k] / dz2, ru = rh[k + 1] / dz2;
-    a[k] = rl;
-    c[k] = ru;
-    negs[k] = -(rl + ru);
-  }
-  a[0] = 0.0;
-  c[nz - 1] = 0.0;
-  negs[0] = -(rh[1] / dz2);
-  negs[nz - 1] = -(rh[nz - 1] / dz2);
-  {
-    const int n0 = nz - 1;
-    double b0[kNoAllocMaxNz], c0[kNoAllocMaxNz];
-    for (int j = 0; j < n0; ++j) {
-      const double rl = rh[j + 1] / dz2, ru = rh[j + 2] / dz2;
-      a0[j] = rl;
-      b0[j] = -(rl + ru);
-      c0[j] = ru;
-    }
-    a0[0] = 0.0;
-    a0[n0 - 1] = rh[nz - 1] / dz2;
-    c0[n0 - 1] = 0.0;
-    b0[n0 - 1] = -(rh[nz - 1] / dz2);
-    inv0[0] = 1.0 / b0[0];
-    cp0[0] = c0[0] * inv0[0];
-    for (int j = 1; j < n0; ++j) {
-      const double den = b0[j] - a0[j] * cp0[j - 1];
-      inv0[j] = 1.0 / den;
-      cp0[j] = (j < n0 - 1) ? c0[j] * inv0[j] : 0.0;
-    }
-  }
-  for (int t = 0; t < nx; ++t) {
-    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * t / nx;
-    ((cplx<T>*)(h + o_twx))[t] = cplx<T>{(T)cosl(ang), (T)sinl(ang)};
-  }
-  for (int t = 0; t < ny; ++t) {
-    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * t / ny;
-    ((cplx<T>*)(h + o_twy))[t] = cplx<T>{(T)cosl(ang), (T)sinl(ang)};
-  }
+  fill_solver_tables(nz, p.g.dz, rf, SolverTables{rh, a, c, negs, a0, cp0, inv0});
+  fill_twiddles<T>((cplx<T>*)(h + o_twx), nx);
+  fill_twiddles<T>((cplx<T>*)(h + o_twy), ny);
   // pageable source: the call returns once the bytes are staged, so the host
   // buffer may be rewritten by the next call
   OB_CUDA(cudaMemcpyAsync(base, h, table_bytes, cudaMemcpyHostToDevice, st));
@@ -2728,6 +2580,19 @@ extern "C" int oracle_b200_poisson_solve_noalloc(const OracleGridDesc* grid, con
   if (!(grid->Lx > 0 && grid->Ly > 0 && grid->Lz > 0))
     return fail(OB_ERR_ARG, "poisson_solve_noalloc: domain lengths must be positive");
   cudaStream_t st = (cudaStream_t)stream;
+  // Never inside a stream capture: the tables are copied from the shared host
+  // staging buffer, and a captured copy would read that buffer when the graph
+  // is replayed, after later calls may have rewritten it with another grid's
+  // tables.  The check comes before anything is enqueued, so a refused call
+  // leaves the caller's capture valid.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const cudaError_t ce = cudaStreamIsCapturing(st, &cap);
+  if (ce != cudaSuccess)
+    return fail(OB_ERR_CUDA, "poisson_solve_noalloc: cudaStreamIsCapturing failed: %s",
+                cudaGetErrorString(ce));
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(OB_ERR_ARG, "poisson_solve_noalloc cannot be captured into a CUDA graph: the "
+                "stream is capturing; call it outside the capture");
   if (grid->precision == OB_PREC_F64)
     return noalloc_solve<double>(grid, rho0, (const double*)d, (double*)phi, st);
   if (grid->precision == OB_PREC_F32)

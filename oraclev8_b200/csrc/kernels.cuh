@@ -1642,6 +1642,12 @@ struct DiagPart {
   double mu, mv, mw, mt, sp, pmin, pmax, pad;
 };
 
+// Maximum and minimum that propagate NaN as NumPy's max / min do (fmax and
+// fmin would drop it): once either operand is NaN the result stays NaN.
+__device__ __forceinline__ double nan_max(double m, double x) { return (x > m || x != x) ? x : m; }
+__device__ __forceinline__ double nan_min(double m, double x) { return (x < m || x != x) ? x : m; }
+__device__ __forceinline__ float nan_maxf(float m, float x) { return (x > m || x != x) ? x : m; }
+
 template <class T>
 __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restrict__ u,
                                                       const T* __restrict__ v,
@@ -1668,7 +1674,8 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
       const float4* p4 = reinterpret_cast<const float4*>(phi);
       const float4* w4 = reinterpret_cast<const float4*>(w);
       auto amax = [](float m, float4 a) {
-        return fmaxf(fmaxf(fmaxf(m, fabsf(a.x)), fmaxf(fabsf(a.y), fabsf(a.z))), fabsf(a.w));
+        return nan_maxf(nan_maxf(nan_maxf(m, fabsf(a.x)), nan_maxf(fabsf(a.y), fabsf(a.z))),
+                        fabsf(a.w));
       };
       for (size_t e = first; e < n / 4; e += stride) {
         const float4 a = u4[e], b = v4[e], c = t4[e], d = p4[e];
@@ -1690,19 +1697,19 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
   }
   if (!done) {
     for (size_t e = first; e < n; e += stride) {
-      mu = fmax(mu, fabs((double)u[e]));
-      mv = fmax(mv, fabs((double)v[e]));
-      mt = fmax(mt, fabs((double)th[e]));
+      mu = nan_max(mu, fabs((double)u[e]));
+      mv = nan_max(mv, fabs((double)v[e]));
+      mt = nan_max(mt, fabs((double)th[e]));
       sp += (double)phi[e];
     }
-    for (size_t e = first; e < nw; e += stride) mw = fmax(mw, fabs((double)w[e]));
+    for (size_t e = first; e < nw; e += stride) mw = nan_max(mw, fabs((double)w[e]));
   }
   // surface level k = 0 of every column
   const size_t ncol = (size_t)g.nx * g.ny;
   for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncol; c += stride) {
     const double p = phi[c * g.nz];
-    pmin = fmin(pmin, p);
-    pmax = fmax(pmax, p);
+    pmin = nan_min(pmin, p);
+    pmax = nan_max(pmax, p);
   }
   __shared__ double red[8][8];
   double vals[7] = {mu, mv, mw, mt, sp, pmin, pmax};
@@ -1711,7 +1718,7 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
     double x = vals[q];
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_xor_sync(0xffffffffu, x, o);
-      x = (q == 4) ? x + y : (q == 5 ? fmin(x, y) : fmax(x, y));
+      x = (q == 4) ? x + y : (q == 5 ? nan_min(x, y) : nan_max(x, y));
     }
     vals[q] = x;
   }
@@ -1726,7 +1733,7 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
     for (int ww = 1; ww < nw_; ++ww)
       for (int q = 0; q < 7; ++q)
         r[q] = (q == 4) ? r[q] + red[ww][q]
-                        : (q == 5 ? fmin(r[q], red[ww][q]) : fmax(r[q], red[ww][q]));
+                        : (q == 5 ? nan_min(r[q], red[ww][q]) : nan_max(r[q], red[ww][q]));
     DiagPart p;
     p.mu = r[0];
     p.mv = r[1];
@@ -1741,28 +1748,32 @@ __global__ void __launch_bounds__(256) k_diag_partial(GridK g, const T* __restri
 }
 
 // One warp combines the per-CTA partials (fixed order: lane-strided, then a
-// butterfly), so the result does not depend on timing.
-__global__ void k_diag_final(const DiagPart* part, int np, double ncell, double* diag) {
+// butterfly), so the result does not depend on timing.  It also raises the
+// plan's sticky blow-up flag diag[14] (OB_DIAG_BLOWUP): 1 for a non-finite
+// value in any field, 2 for max|u| above umax_limit (> 0), the blow-up test
+// of the reference's harness (measure_lh82_phase3.py:129-130).
+__global__ void k_diag_final(const DiagPart* part, int np, double ncell, double umax_limit,
+                             double* diag) {
   if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   double mu = 0, mv = 0, mw = 0, mt = 0, sp = 0, pmin = INFINITY, pmax = -INFINITY;
   for (int b = threadIdx.x; b < np; b += 32) {
     const DiagPart q = part[b];
-    mu = fmax(mu, q.mu);
-    mv = fmax(mv, q.mv);
-    mw = fmax(mw, q.mw);
-    mt = fmax(mt, q.mt);
+    mu = nan_max(mu, q.mu);
+    mv = nan_max(mv, q.mv);
+    mw = nan_max(mw, q.mw);
+    mt = nan_max(mt, q.mt);
     sp += q.sp;
-    pmin = fmin(pmin, q.pmin);
-    pmax = fmax(pmax, q.pmax);
+    pmin = nan_min(pmin, q.pmin);
+    pmax = nan_max(pmax, q.pmax);
   }
   for (int o = 16; o > 0; o >>= 1) {
-    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
-    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
-    mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
-    mt = fmax(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+    mu = nan_max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = nan_max(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    mw = nan_max(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+    mt = nan_max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
     sp += __shfl_xor_sync(0xffffffffu, sp, o);
-    pmin = fmin(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
-    pmax = fmax(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+    pmin = nan_min(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
+    pmax = nan_max(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
   }
   if (threadIdx.x != 0) return;
   const double mean = sp / ncell;
@@ -1772,6 +1783,12 @@ __global__ void k_diag_final(const DiagPart* part, int np, double ncell, double*
   diag[3] = mt;
   diag[4] = pmin - mean;
   diag[5] = pmax - mean;
+  const bool finite = isfinite(mu) && isfinite(mv) && isfinite(mw) && isfinite(mt) &&
+                      isfinite(sp) && isfinite(pmin) && isfinite(pmax);
+  double flag = diag[14];
+  if (!finite) flag = fmax(flag, 1.0);
+  else if (umax_limit > 0.0 && mu > umax_limit) flag = fmax(flag, 2.0);
+  diag[14] = flag;
 }
 
 }  // namespace ob

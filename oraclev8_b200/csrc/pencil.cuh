@@ -21,9 +21,25 @@
 // are 32-bit: plan_create bounds nx * ny * (nz + 1) by 2^31.
 #pragma once
 #include "kernels.cuh"
-#include "pipe.cuh"
 
 namespace ob {
+
+// One element global -> shared with cp.async (cp_async / cp_commit / cp_wait:
+// common.cuh), or a zero where the source is out of range.
+template <class T>
+__device__ __forceinline__ void copy_or_zero(T* dst, const T* src, bool ok) {
+  if (ok)
+    cp_async(dst, src, (int)sizeof(T));
+  else
+    *dst = (T)0;
+}
+template <class T>
+__device__ __forceinline__ void copy_or_zero(cplx<T>* dst, const cplx<T>* src, bool ok) {
+  if (ok)
+    cp_async(dst, src, (int)sizeof(cplx<T>));
+  else
+    *dst = mk<T>((T)0, (T)0);
+}
 
 constexpr int kPencilThreads = 256;
 // CTAs per SM the launch bounds target: three in FP32; two in FP64, whose

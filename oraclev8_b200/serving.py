@@ -110,11 +110,17 @@ def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: fl
     return out
 
 
-def build_run(req: RunRequest, device_dtype=None):
+# max|u| in m/s above which a run counts as blown up (measure_lh82_phase3.py:
+# 129-130 tests the same after each step); non-finite values always do
+BLOWUP_U_MAX = 400.0
+
+
+def build_run(req: RunRequest, device_dtype=None, blowup_u_max: float = BLOWUP_U_MAX):
     """Integrator and device initial state of a request: WS5 advection,
     beta-plane Coriolis (periodic taper), buoyancy and the anelastic
     projection; Holland vortex at the domain centre with the 12-km linear
-    wind decay."""
+    wind decay.  The plan raises its blow-up flag on non-finite values or
+    max|u| > ``blowup_u_max``."""
     from .grid import LorenzStaggering
     from .production_config import BaseState
     from .solver import (AdvectionComponent, AnelasticProjection, BuoyancyComponent,
@@ -130,7 +136,7 @@ def build_run(req: RunRequest, device_dtype=None):
         advection=AdvectionComponent(n, n, nz, L, L, req.lz, scheme="upwind5h"),
         coriolis=CoriolisComponent(f=req.f0, mode="beta_plane", beta=req.beta, Ly=L, ny=n,
                                    periodic_taper=True))
-    integ = RK3Integrator(cfg, base, precision=req.precision)
+    integ = RK3Integrator(cfg, base, precision=req.precision, blowup_u_max=blowup_u_max)
     if req.resume is not None:
         from .snapshot import state_from_snapshot
         state = state_from_snapshot(req.resume, dtype=integ.dtype)
@@ -169,6 +175,9 @@ class RunRecord:
     admit_s: float = math.nan
     done_s: float = math.nan
     final: Optional[dict] = None
+    # set when the run's final diagnostics show a blow-up (non-finite state or
+    # max|u| above the limit): the run is retired and its slot backfilled
+    error: Optional[str] = None
 
     @property
     def latency_s(self) -> float:
@@ -272,6 +281,14 @@ class ServingEngine:
     def _retire(self, a: _Active, now: float) -> RunRecord:
         a.rec.done_s = now
         self._drain_snapshots(a, wait=True)
+        # the last step of every step graph runs the diagnostics reductions,
+        # which keep the plan's sticky blow-up flag (the run's work is done,
+        # so this read does not wait on the GPU)
+        with torch.cuda.stream(a.stream):
+            flag = a.integ.plan.blown_up()
+        if flag:
+            a.rec.error = ("non-finite state" if flag == 1 else
+                           f"max|u| above {a.integ.spec.blowup_u_max:g} m/s")
         if self.keep_final:
             with torch.cuda.stream(a.stream):
                 s = a.state
@@ -422,7 +439,8 @@ def summarize(records: "list[RunRecord]", makespan_s: Optional[float] = None) ->
     cu = float(sum(r.cells * r.steps for r in records))
     span = makespan_s if makespan_s is not None else float(max(r.done_s for r in records))
     pct = lambda a, p: float(np.percentile(a, p))
-    return {"runs": len(records), "cell_updates": cu, "makespan_s": span,
+    return {"runs": len(records), "blown_up": sum(1 for r in records if r.error),
+            "cell_updates": cu, "makespan_s": span,
             "cell_updates_per_s": cu / span,
             "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99),
                           "max": float(lat.max())},
@@ -447,7 +465,11 @@ def serve_serial_plain(requests: "list[RunRequest]", realtime: bool = True
         for n in range(r64.nsteps):
             state, _ = integ.step(state, r64.dt, n)
         torch.cuda.synchronize()
-        recs.append(RunRecord(req.rid, req.n, req.nz, "fp64", r64.nsteps, r64.cells,
-                              req.arrival_s, admit_s=admit, done_s=time.perf_counter() - t0))
+        rec = RunRecord(req.rid, req.n, req.nz, "fp64", r64.nsteps, r64.cells,
+                        req.arrival_s, admit_s=admit, done_s=time.perf_counter() - t0)
+        flag = integ.plan.blown_up()
+        if flag:
+            rec.error = "non-finite state" if flag == 1 else "max|u| above the limit"
+        recs.append(rec)
         del integ, state
     return recs

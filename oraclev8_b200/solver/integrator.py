@@ -41,6 +41,10 @@ class StepDiagnostics:
     max_theta_prime: float = 0.0
     surface_phi_min: float = 0.0
     surface_phi_max: float = 0.0
+    # not in the reference's dataclass: the device's sticky blow-up flag
+    # (0 none, 1 a non-finite value, 2 max|u| above the integrator's
+    # blowup_u_max) as of this step
+    blowup: int = 0
 
 
 _UNSUPPORTED_SLOTS = ("pressure_gradient",)
@@ -133,11 +137,15 @@ class RK3Integrator:
     _STAGE_ALPHAS = (1.0 / 3.0, 1.0 / 2.0, 1.0)
 
     def __init__(self, config, base, precision: str | None = None,
-                 refine_passes: int | None = None, refine_every: int = 1) -> None:
+                 refine_passes: int | None = None, refine_every: int = 1,
+                 blowup_u_max: float = 0.0) -> None:
         """precision: "fp64", "fp32" or "fp32r".  "fp32r" is the FP32 step
         followed, every ``refine_every`` steps, by ``refine_passes`` (default 1)
         defect corrections of the final projection whose residual divergence
-        is formed in FP64."""
+        is formed in FP64.  blowup_u_max > 0 also raises the device's blow-up
+        flag (``StepDiagnostics.blowup``) when max|u| exceeds it; non-finite
+        values always do.  Steps never raise on it, as the reference's step
+        does not: a harness tests the flag (measure_lh82_phase3.py:129-130)."""
         self.config = config
         self.base = wrap_base(base)
         self.precision = precision or backend.PRECISION
@@ -147,6 +155,7 @@ class RK3Integrator:
         if refine_passes is None:
             refine_passes = 1 if self.precision == "fp32r" else 0
         self.spec = compile_config(config, self.base, plan_prec)
+        self.spec.blowup_u_max = float(blowup_u_max)
         self.plan = Plan(self.spec)
         self.refine_passes, self.refine_every = int(refine_passes), int(refine_every)
         if self.refine_passes:
@@ -178,6 +187,7 @@ class RK3Integrator:
         dg.max_u, dg.max_v = float(d[D["max_u"]]), float(d[D["max_v"]])
         dg.max_w, dg.max_theta_prime = float(d[D["max_w"]]), float(d[D["max_th"]])
         dg.surface_phi_min, dg.surface_phi_max = float(d[D["phi_min"]]), float(d[D["phi_max"]])
+        dg.blowup = int(d[D["blowup"]])
         if self._fast:
             dg.stage_compat_residuals = [float(d[D["compat0"] + s]) for s in range(3)]
             dg.stage_disc_op_residuals = [float(d[D["disc0"] + s]) for s in range(3)]

@@ -1,9 +1,10 @@
 """Generate golden fixtures by running the UNMODIFIED reference (Oracle V8).
 
-Run in a container where the reference tree is mounted at /root/reference:
+Give the root of the reference tree (the directory holding ``oracle_v8``) with
+``--reference PATH`` or the ``ORACLE_V8_REF`` environment variable:
 
-    python tests/golden/make_golden.py            # small fixtures (seconds)
-    python tests/golden/make_golden.py --long     # + config-0 6 h run (~8 min)
+    python tests/golden/make_golden.py --reference PATH          # small fixtures (seconds)
+    python tests/golden/make_golden.py --reference PATH --long   # + config-0 6 h run (~8 min)
 
 It imports ``oracle_v8`` from the reference with ``ORACLE_GPU=0`` (NumPy path),
 builds seeded inputs with the reference's own public constructors, and stores
@@ -22,7 +23,23 @@ from pathlib import Path
 os.environ["ORACLE_GPU"] = "0"
 os.environ.setdefault("ORACLE_DIAG_EVERY", "1")
 sys.dont_write_bytecode = True
-REF = "/root/reference"
+
+
+def _reference_root() -> str:
+    """The reference tree's root: ``--reference PATH`` or ``ORACLE_V8_REF``."""
+    argv = sys.argv[1:]
+    for i, a in enumerate(argv):
+        if a == "--reference" and i + 1 < len(argv):
+            return argv[i + 1]
+        if a.startswith("--reference="):
+            return a.split("=", 1)[1]
+    ref = os.environ.get("ORACLE_V8_REF")
+    if not ref:
+        sys.exit("make_golden.py: give the reference tree with --reference PATH or ORACLE_V8_REF")
+    return ref
+
+
+REF = _reference_root()
 sys.path.insert(0, REF)
 
 import numpy as np  # noqa: E402
@@ -623,6 +640,7 @@ def gen_config0_long():
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--long", action="store_true")
+    ap.add_argument("--reference", default=None, help="root of the reference tree (read above)")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
