@@ -104,6 +104,10 @@ WORKLOADS = {
                                   periodic_taper=True, u_env=-3.0),
                     heating=None, noise_seed=None),
 }
+# a 1024 x 256 x 80 slab of the production grid (same dx, column and physics):
+# the case kernel-level ncu captures of the 1024-point pencils run on, its
+# fields (84 MB each) still larger than L2 together
+WORKLOADS["config2s"] = dict(WORKLOADS["config2"], ny=256)
 # Algorithmic field passes per cell-update of one step (one read or write of
 # an nx*ny*nz field = 1 pass; w counts as nz; a half-spectrum complex field
 # as 1): slow halves 2 x 8, fast stages 3 x 1, projections 5 x 14 = 89, plus
@@ -592,6 +596,7 @@ def run_b200(args):
                         "step, StepDiagnostics, full state D2H to pinned host; copies of "
                         "neighbouring steps overlap the step (copy-in/copy-out streams)"},
         "gpu_launches": launches,
+        "kernel_variants": {k: v for k, v in integ.plan.variants().items() if v},
         "clocks": clk,
     }
     if cufft is not None:
@@ -835,11 +840,18 @@ def ensemble_report(args, peak_gbs):
     80% FP32-refined / 20% FP64, 150 GB HBM budget; against the same stream
     served serially in plain FP64."""
     import torch.distributed as dist
-    from oraclev8_b200.serving import (ServingEngine, draw_requests, gather_records,
-                                       serve_serial_plain, shard_requests, summarize)
+    from oraclev8_b200.serving import (RunRequest, ServingEngine, draw_requests,
+                                       gather_records, serve_serial_plain, shard_requests,
+                                       summarize)
     rank = dist.get_rank() if dist.is_available() and dist.is_initialized() else 0
     world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
-    # library, kernels and the plan pool warm before timing
+    # library, kernels, kernel-form tuning of every grid and the plan pool
+    # warm before timing
+    every = (draw_requests(args.ensemble_runs, 3, hours=args.ensemble_hours)
+             + draw_requests(args.serving_requests, 4, rate=2.0, fp32r_frac=0.8))
+    ServingEngine.prepare_kernels(every)
+    ServingEngine.prepare_kernels([RunRequest(**{**r.__dict__, "precision": "fp64"})
+                                   for r in every])
     ServingEngine(realtime=False).run(draw_requests(6, 99, hours=0.2, fp32r_frac=0.5))
     serve_serial_plain(draw_requests(2, 98, hours=0.1), realtime=False)
     # N > 1: whole runs are dealt to the GPUs (no exchange between runs)

@@ -85,6 +85,39 @@ extern "C" {
 #define OB_DIAG_BLOWUP 14
 #define OB_DIAG_COUNT 16
 
+/* Kernel-variant choices of a plan, in this order (oracle_b200_plan_get_variants,
+ * oracle_b200_plan_set_variants, oracle_b200_plan_tune).  Each pencil entry is
+ * the z-chunk (levels per CTA) of one kernel form, 0 = that form off; a class
+ * runs the first form that is on, in the order register-resident 1024-point
+ * (ZC4), register-resident 512-point (ZC3), compile-time-chunk Stockham (ZC2),
+ * and otherwise the runtime-chunk Stockham kernels.  _FXS: the stage forward
+ * x transform; _FX: the correction one; _FXD / _FYD and RZC2_*: the FP64
+ * residual transforms of the defect correction. */
+#define OB_VAR_ZC2_FX 0
+#define OB_VAR_ZC2_FXS 1
+#define OB_VAR_ZC2_IX 2
+#define OB_VAR_ZC2_FY 3
+#define OB_VAR_ZC2_IY 4
+#define OB_VAR_ZC3_FX 5
+#define OB_VAR_ZC3_FXS 6
+#define OB_VAR_ZC3_IX 7
+#define OB_VAR_ZC3_FXD 8
+#define OB_VAR_ZC3_FY 9     /* forward and inverse y at ny = 512 */
+#define OB_VAR_ZC3_FYD 10
+#define OB_VAR_ZC4_FX 11
+#define OB_VAR_ZC4_FXS 12
+#define OB_VAR_ZC4_IX 13
+#define OB_VAR_ZC4_FXD 14
+#define OB_VAR_ZC4_FY 15
+#define OB_VAR_ZC4_IY 16
+#define OB_VAR_SLOW_XW 17   /* FP32 slow tendency marching along x (1) or gathering (0) */
+#define OB_VAR_THOMAS_FAST 18 /* FP32 sweep with a compile-time level count (1) */
+#define OB_VAR_RZC2_FX 19
+#define OB_VAR_RZC2_FY 20
+#define OB_VAR_COUNT 21
+
+#define OB_TUNE_FORCE 1  /* time the candidates even when a choice is cached */
+
 typedef struct OracleGridDesc {
     int nx, ny, nz;      /* even nx, ny; nz >= 3 */
     double Lx, Ly, Lz;   /* metres */
@@ -218,6 +251,23 @@ int oracle_b200_tendency(OraclePlan *plan, int mask, const OracleStatePtrs *stat
 int oracle_b200_intensity_cap(const void *u, const void *v, int precision, long n,
                               double v_cap, double tau, double u_env, double v_env,
                               void *du, void *dv, void *stream);
+
+/* Kernel variants (OB_VAR_*).  No counterpart in the reference, which leaves
+ * its transforms to the array library: these choose among this library's
+ * kernel forms for the same operations.  get: the n first choices of the plan.
+ * set: validates every value against the forms the plan's grid and precision
+ * allow (OB_ERR_ARG otherwise, nothing changed).  tune: for each kernel
+ * class, times every allowed form on the plan's own buffers (a warm-up launch
+ * and the best of three, CUDA events, after the work queued on `stream`) and
+ * keeps the fastest; the choice is cached per grid, precision, component set
+ * and device for the life of the process, and also in the file named by
+ * ORACLE_B200_TUNE_CACHE when that variable is set.  A later plan of the same
+ * key takes the cached choice without timing (unless flags has
+ * OB_TUNE_FORCE).  Tuning overwrites the plan's scratch and stage buffers:
+ * call it before the plan holds state.  Synchronises. */
+int oracle_b200_plan_get_variants(const OraclePlan *plan, int *out, int n);
+int oracle_b200_plan_set_variants(OraclePlan *plan, const int *values, int n);
+int oracle_b200_plan_tune(OraclePlan *plan, int flags, void *stream);
 
 /* Copy the OB_DIAG_COUNT diagnostics doubles to host (synchronises `stream`).
  * Returns OB_ERR_NONFINITE, with host_out filled all the same, when the plan's

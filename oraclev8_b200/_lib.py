@@ -39,7 +39,13 @@ EXPORTS = (
     "oracle_b200_intensity_cap", "oracle_b200_vdiag_create", "oracle_b200_vdiag_destroy",
     "oracle_b200_vdiag_speed_max", "oracle_b200_vdiag_vorticity", "oracle_b200_vdiag_ke",
     "oracle_b200_vdiag_rings", "oracle_b200_vdiag_zpos", "oracle_b200_vdiag_centroid",
+    "oracle_b200_plan_get_variants", "oracle_b200_plan_set_variants", "oracle_b200_plan_tune",
 )
+# kernel-variant choices of a plan, in OB_VAR_* order (include/oracle_b200.h)
+VARIANTS = ("zc2_fx", "zc2_fxs", "zc2_ix", "zc2_fy", "zc2_iy", "zc3_fx", "zc3_fxs", "zc3_ix",
+            "zc3_fxd", "zc3_fy", "zc3_fyd", "zc4_fx", "zc4_fxs", "zc4_ix", "zc4_fxd", "zc4_fy",
+            "zc4_iy", "slow_xw", "thomas_fast", "rzc2_fx", "rzc2_fy")
+OB_TUNE_FORCE = 1
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
 
 
@@ -147,6 +153,9 @@ def load(path: Path | None = None):
         "oracle_b200_vdiag_zpos": ([vp, vp, vp, c_int, c_double, vp], c_int),
         "oracle_b200_vdiag_centroid": ([vp, c_int, c_int, c_int, c_int, POINTER(c_double), vp],
                                        c_int),
+        "oracle_b200_plan_get_variants": ([vp, POINTER(c_int), c_int], c_int),
+        "oracle_b200_plan_set_variants": ([vp, POINTER(c_int), c_int], c_int),
+        "oracle_b200_plan_tune": ([vp, c_int, vp], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

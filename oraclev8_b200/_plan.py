@@ -68,6 +68,10 @@ class PlanSpec:
     # max|u| (m/s) above which the device's blow-up flag is raised; 0: only
     # non-finite values raise it (measure_lh82_phase3.py:129-130)
     blowup_u_max: float = 0.0
+    # time the kernel forms of each class at creation and keep the fastest
+    # (cached per grid, precision, component set and device); False keeps
+    # the built-in choice
+    autotune: bool = True
 
 
 def _f64(a):
@@ -108,6 +112,8 @@ class Plan:
         self.handle = h
         self.shape = (spec.nx, spec.ny, spec.nz)
         self.wshape = (spec.nx, spec.ny, spec.nz + 1)
+        if spec.autotune:
+            self.tune()
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -188,6 +194,37 @@ class Plan:
 
     def step_graph(self, ptrs: L.StatePtrs, dt: float, nsteps: int) -> "StepGraph":
         return StepGraph(self, ptrs, dt, nsteps)
+
+    # -- kernel variants ---------------------------------------------------------
+    def variants(self) -> dict:
+        """The plan's kernel-form choices, by OB_VAR_* name (0 = form off)."""
+        n = len(L.VARIANTS)
+        buf = (ctypes.c_int * n)()
+        L.check(self.lib.oracle_b200_plan_get_variants(self.handle, buf, n))
+        return dict(zip(L.VARIANTS, buf))
+
+    def set_variants(self, **kw) -> None:
+        """Change some choices (``plan.set_variants(zc4_ix=8)``); every value is
+        checked against the forms the plan's grid and precision allow."""
+        cur = self.variants()
+        for k, v in kw.items():
+            if k not in cur:
+                raise ValueError(f"unknown kernel variant {k!r}")
+            cur[k] = int(v)
+        vals = (ctypes.c_int * len(L.VARIANTS))(*[cur[k] for k in L.VARIANTS])
+        L.check(self.lib.oracle_b200_plan_set_variants(self.handle, vals, len(L.VARIANTS)))
+
+    def shared_memory_forms(self) -> None:
+        """Turn every register-resident and compile-time-chunk form off: the
+        runtime-chunk shared-memory Stockham kernels only."""
+        self.set_variants(**{k: 0 for k in L.VARIANTS if k.startswith(("zc3", "zc4"))})
+
+    def tune(self, force: bool = False) -> dict:
+        """Time the kernel forms of each class and keep the fastest (cached per
+        grid, precision, component set and device); returns the choices."""
+        L.check(self.lib.oracle_b200_plan_tune(self.handle, L.OB_TUNE_FORCE if force else 0,
+                                               self._stream()))
+        return self.variants()
 
     def read_diag(self) -> np.ndarray:
         """The diagnostics block (synchronises the current stream).  A raised
@@ -308,7 +345,7 @@ def _key(spec: PlanSpec) -> tuple:
             float(spec.drag_v_env), b(spec.drag_weight), spec.sponge, float(spec.sponge_u_env),
             float(spec.sponge_v_env), b(spec.sponge_alpha), b(spec.sponge_alpha_h),
             spec.diffusion, float(spec.diff_nu), float(spec.diff_dx2), float(spec.diff_dy2),
-            spec.cooling, float(spec.cool_alpha), float(spec.blowup_u_max))
+            spec.cooling, float(spec.cool_alpha), float(spec.blowup_u_max), spec.autotune)
 
 
 def cached_plan(spec: PlanSpec) -> Plan:

@@ -5,6 +5,9 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <array>
+#include <functional>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -13,6 +16,7 @@
 #include "kernels.cuh"
 #include "pencil.cuh"
 #include "xreg.cuh"
+#include "xreg4.cuh"
 #include "tracker.cuh"
 #include "vdiag.cuh"
 #include "init.cuh"
@@ -211,11 +215,18 @@ struct OraclePlan {
   int zc_fx = 1, zc_fy = 1, zc_iy = 1, zc_ix = 1;
   // x-pencil kernels with compile-time z-chunks (pencil.cuh); 0 = not used
   FftPlan px8{}, py8{};
+  bool px8_ok = false, py8_ok = false;  // nx/2 and ny factor into 8, 4, 2, 3, 5
   int zc2_fx = 0, zc2_fxs = 0, zc2_ix = 0, zc2_fy = 0, zc2_iy = 0;
   // register-resident x pencils of FP32 plans at nx = 512 (z-chunk, 0 = off): the
   // projection's forward and inverse kernels, and the FP64 residual transform
-  int zc3_fx = 0, zc3_ix = 0, zc3_fxd = 0;
+  int zc3_fx = 0, zc3_fxs = 0, zc3_ix = 0, zc3_fxd = 0;
   int zc3_fy = 0;  // register-resident FP32 y pencils (ny = 512): z-chunk, 0 = off
+  int zc3_fyd = 0;  // the FP64 residual y transform at ny = 512 (register form): 0 or 2
+  int thomas_fast = 1;  // FP32 short-wave sweep with a compile-time level count
+  // register-resident pencils of the 1024-point lines (xreg4.cuh), FP32 plans:
+  // forward x (stage / correction), inverse x, the FP64 residual x transform,
+  // and the y pencils (ny = 1024); z-chunk, 0 = off
+  int zc4_fxs = 0, zc4_fx = 0, zc4_ix = 0, zc4_fxd = 0, zc4_fy = 0, zc4_iy = 0;
   int slow_xw = 1;  // FP32 slow tendency marching along x (ORACLE_B200_SLOW_XW=0: gather form)
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
@@ -427,9 +438,35 @@ int yr_attrs() {
   return OB_OK;
 }
 
+template <class T, bool STAGE, int ZC>
+int xr4_attr_fx() {
+  OB_CUDA(cudaFuncSetAttribute(k_fx4<T, STAGE, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fx4_smem<T, STAGE, ZC>()));
+  return OB_OK;
+}
+template <int ZC>
+int xr4_attrs_zc() {
+  int rc;
+  if ((rc = xr4_attr_fx<float, false, ZC>()) || (rc = xr4_attr_fx<float, true, ZC>()))
+    return rc;
+  if constexpr (ZC == 2)
+    if ((rc = xr4_attr_fx<double, false, ZC>())) return rc;
+  for (auto k : {k_ix4<IX_CORRECT, ZC>, k_ix4<IX_STAGE, ZC>, k_ix4<IX_REFINE, ZC>})
+    OB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Ix4Size<ZC>::total));
+  OB_CUDA(cudaFuncSetAttribute(k_fy4<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Yr4Size<ZC>::total));
+  OB_CUDA(cudaFuncSetAttribute(k_iy4<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Yr4Size<ZC>::total));
+  return OB_OK;
+}
+
 template <class T>
 int set_x2_attrs() {
   int rc;
+  if constexpr (sizeof(T) == 4)
+    if ((rc = xr4_attrs_zc<2>()) || (rc = xr4_attrs_zc<4>()) || (rc = xr4_attrs_zc<8>()))
+      return rc;
   if constexpr (sizeof(T) == 4) {
     if ((rc = yr_attrs<2>()) || (rc = yr_attrs<4>()) || (rc = yr_attrs<8>())) return rc;
   } else {  // the defect correction's FP64 residual y transform
@@ -560,7 +597,6 @@ dim3 grid_y(const OraclePlan* p, int zc) { return dim3((p->g.nz + zc - 1) / zc, 
 // per step) than at ZC = 8 with two (1.48 ms).
 template <class T>
 size_t x2_smem_budget(int kind) {
-  if (const char* e = getenv("ORACLE_B200_X2_SMEM_KB")) return (size_t)atoi(e) * 1024;
   return (sizeof(T) == 4 && kind < 2) ? 74 * 1024 : 112 * 1024;
 }
 // y pencils (complex rows of ZC levels, at least 16-byte runs): three CTAs
@@ -597,8 +633,6 @@ size_t x2_smem(int kind, int zc, int nx) {
 // one; the FP32-refined step 60.9 ms with 2-level chunks and 46.2 ms with 4.
 template <class T, class TS>
 int pick_x2_zc(int kind, int nx, int nz) {
-  if (const char* e = getenv("ORACLE_B200_X2"))
-    if (atoi(e) == 0) return 0;
   int zc = 0;
   for (size_t cap : {x2_smem_budget<T>(kind), kSmemMax}) {
     for (int z : {8, 4, 2, 1}) {
@@ -629,8 +663,6 @@ size_t y2_smem_zc(int zc, int ny) {
 
 template <class T>
 int pick_y2_zc(int ny, int nz) {
-  if (const char* e = getenv("ORACLE_B200_X2"))
-    if (atoi(e) == 0) return 0;
   for (size_t cap : {y2_smem_budget<T>(), kSmemMax})
     for (int zc : {8, 4, 2, 1}) {
       if (zc > 1 && zc > nz) continue;
@@ -816,6 +848,66 @@ void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, co
   }
 }
 
+// ---- register-resident pencils of the 1024-point lines (xreg4.cuh) --------
+template <class T, bool STAGE, int ZC>
+void fx4_launch(const OraclePlan* q, const float* u, const float* v, const float* w,
+                const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
+  const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
+  k_fx4<T, STAGE, ZC><<<grid, 96 * ZC, fx4_smem<T, STAGE, ZC>(), st>>>(
+      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<T>*)q->twx, X0, X1);
+}
+// q's twiddles are of type T (the FP64 refiner plan for T = double)
+template <class T, bool STAGE>
+void fx4(const OraclePlan* q, int zc, const float* u, const float* v, const float* w,
+         const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    fx4_launch<T, false, 2>(q, u, v, w, bh, sdt, X0, X1, st);  // the FP64 residual form
+  } else {
+    switch (zc) {
+      case 2: fx4_launch<T, STAGE, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
+      case 4: fx4_launch<T, STAGE, 4>(q, u, v, w, bh, sdt, X0, X1, st); break;
+      default: fx4_launch<T, STAGE, 8>(q, u, v, w, bh, sdt, X0, X1, st); break;
+    }
+  }
+}
+template <int MODE, int ZC>
+void ix4_launch(const OraclePlan* p, const cplx<float>* phs, const cplx<float>* psi,
+                const float* u, const float* v, const float* w, const float* bh, double sdt,
+                float* uo, float* vo, float* wo, float* phio, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
+  k_ix4<MODE, ZC><<<grid, 32 * (3 * ZC + 1), Ix4Size<ZC>::total, st>>>(
+      p->g, phs, psi, p->kx, (const cplx<float>*)p->twx, u, v, w, bh, sdt, uo, vo, wo, phio);
+}
+template <int MODE>
+void ix4(const OraclePlan* p, int zc, const cplx<float>* phs, const cplx<float>* psi,
+         const float* u, const float* v, const float* w, const float* bh, double sdt,
+         float* uo, float* vo, float* wo, float* phio, cudaStream_t st) {
+  switch (zc) {
+    case 2: ix4_launch<MODE, 2>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    case 4: ix4_launch<MODE, 4>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+    default: ix4_launch<MODE, 8>(p, phs, psi, u, v, w, bh, sdt, uo, vo, wo, phio, st); break;
+  }
+}
+template <int ZC>
+void yr4_launch(const OraclePlan* p, bool inverse, const cplx<float>* in0,
+                const cplx<float>* in1, cplx<float>* out0, cplx<float>* out1, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.nxh);
+  const cplx<float>* tw = (const cplx<float>*)p->twy;
+  if (inverse)
+    k_iy4<ZC><<<grid, 64 * ZC, Yr4Size<ZC>::total, st>>>(p->g, in0, p->ky, tw, out0, out1);
+  else
+    k_fy4<ZC><<<grid, 64 * ZC, Yr4Size<ZC>::total, st>>>(p->g, in0, in1, p->ky, tw, out0);
+}
+// register-resident FP32 y pencils (ny = 1024): FY_DIV forward or the IY_GRAD inverse
+void yr4(const OraclePlan* p, bool inverse, const cplx<float>* in0, const cplx<float>* in1,
+         cplx<float>* out0, cplx<float>* out1, cudaStream_t st) {
+  switch (inverse ? p->zc4_iy : p->zc4_fy) {
+    case 2: yr4_launch<2>(p, inverse, in0, in1, out0, out1, st); break;
+    case 4: yr4_launch<4>(p, inverse, in0, in1, out0, out1, st); break;
+    default: yr4_launch<8>(p, inverse, in0, in1, out0, out1, st); break;
+  }
+}
+
 // The single-precision short-wave launch with a compile-time level count
 // (k_thomas_f32); false when nz has no instance.
 bool thomas_f32(OraclePlan* p, int cls, cplx<float>* S3, cudaStream_t st) {
@@ -874,7 +966,7 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
             p->g, thomas_args(p), S3, (cplx<T>*)p->S1, diag, slot_c, slot_d, nullptr, p->lw_flag); }
       OB_LAUNCHED();
     }
-    if (!thomas_f32(p, cls, (cplx<float>*)S3, st))
+    if (!p->thomas_fast || !thomas_f32(p, cls, (cplx<float>*)S3, st))
       { Launch L_(p, cls, st); k_thomas<T, kThomasCols, float><<<nb, kThomasCols, smem_thomas(p, 4), st>>>(
             p->g, thomas_args(p), S3, S3, nullptr, slot_c, slot_d, nullptr, p->lw_flag); }
     OB_LAUNCHED();
@@ -885,6 +977,142 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
 }
 
 // ---- projection pipeline -------------------------------------------------
+// One launcher per kernel class of the projection; each runs the variant the
+// plan's choice fields select (register-resident > compile-time-chunk pencils
+// > shared-memory Stockham), so that project_impl and the autotuner run the
+// same code.  stage: the inputs are the anchor state and the provisional
+// stage w + sdt * b_half (bh) is formed on the fly.
+
+template <class T>
+int proj_fx(OraclePlan* p, bool stage, const T* u, const T* v, const T* w, const T* th,
+            const T* bh, double sdt, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  Launch L_(p, 0, st);
+  if constexpr (sizeof(T) == 4) {
+    if (stage && bh && p->zc4_fxs) {
+      fx4<float, true>(p, p->zc4_fxs, u, v, w, bh, sdt, S1, S2, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+    if (!stage && p->zc4_fx) {
+      fx4<float, false>(p, p->zc4_fx, u, v, w, th, 0.0, S1, S2, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+    if (stage && bh && p->zc3_fxs) {
+      fx3<float, true>(p, p->zc3_fxs, u, v, w, bh, sdt, S1, S2, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+    if (!stage && p->zc3_fx) {
+      fx3<float, false>(p, p->zc3_fx, u, v, w, th, 0.0, S1, S2, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+  }
+  if (stage && bh && p->zc2_fxs)
+    fx2<T, true, T>(p, p->zc2_fxs, u, v, w, bh, sdt, S1, S2, st);
+  else if (!stage && p->zc2_fx)
+    fx2<T, false, T>(p, p->zc2_fx, u, v, w, th, 0.0, S1, S2, st);
+  else if (stage)
+    k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+        g, p->pxf, p->zc_fx, 3, u, v, w, th, sdt, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2, nullptr);
+  else
+    k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
+        g, p->pxf, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
+        (const C*)p->twx, S1, S2, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// forward y: (S1, S2) -> S3
+template <class T>
+int proj_fy(OraclePlan* p, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  C* S3 = (C*)p->S3;
+  Launch L_(p, 1, st);
+  if (sizeof(T) == 4 && p->zc4_fy)
+    yr4(p, false, (const cplx<float>*)S1, (const cplx<float>*)S2, (cplx<float>*)S3, nullptr, st);
+  else if (sizeof(T) == 4 && p->zc3_fy)
+    yr(p, false, (const cplx<float>*)S1, (const cplx<float>*)S2, (cplx<float>*)S3, nullptr, st);
+  else if (p->zc2_fy)
+    fy2<T, FY_DIV, T>(p, p->zc2_fy, S1, S2, S3, st);
+  else
+    k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
+        g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// inverse y: S3 -> (S1, S2); cls: the profile class the launch is counted in
+template <class T>
+int proj_iy(OraclePlan* p, int cls, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  C* S3 = (C*)p->S3;
+  Launch L_(p, cls, st);
+  if (sizeof(T) == 4 && p->zc4_iy)
+    yr4(p, true, (const cplx<float>*)S3, nullptr, (cplx<float>*)S1, (cplx<float>*)S2, st);
+  else if (sizeof(T) == 4 && p->zc3_fy)
+    yr(p, true, (const cplx<float>*)S3, nullptr, (cplx<float>*)S1, (cplx<float>*)S2, st);
+  else if (p->zc2_iy)
+    iy2<T>(p, p->zc2_iy, S3, S1, S2, st);
+  else
+    k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
+        g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// inverse x with the velocity correction: (S1, S2) and the state -> outputs
+template <class T>
+int proj_ix(OraclePlan* p, bool stage, const T* u, const T* v, const T* w, const T* th,
+            const T* bh, double sdt, T* uo, T* vo, T* wo, T* phio, cudaStream_t st) {
+  using C = cplx<T>;
+  const GridK g = p->g;
+  C* S1 = (C*)p->S1;
+  C* S2 = (C*)p->S2;
+  Launch L_(p, 4, st);
+  if constexpr (sizeof(T) == 4) {
+    if (p->zc4_ix && (bh || !stage)) {
+      if (stage) ix4<IX_STAGE>(p, p->zc4_ix, S1, S2, u, v, w, bh, sdt, uo, vo, wo, phio, st);
+      else ix4<IX_CORRECT>(p, p->zc4_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+    if (p->zc3_ix && (bh || !stage)) {
+      if (stage) ix3<IX_STAGE>(p, p->zc3_ix, S1, S2, u, v, w, bh, sdt, uo, vo, wo, phio, st);
+      else ix3<IX_CORRECT>(p, p->zc3_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st);
+      OB_LAUNCHED();
+      return OB_OK;
+    }
+  }
+  const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
+  if (p->zc2_ix && stage && bh)
+    ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, bh, sdt, uo, vo, wo, phio, st);
+  else if (p->zc2_ix && !stage)
+    ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st);
+  else if (stage)
+    k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th, sdt,
+        p->theta0, uo, vo, wo, phio);
+  else
+    k_ix<T, IX_CORRECT><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
+        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th, 0.0,
+        p->theta0, uo, vo, wo, phio);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
 // stage_sdt < 0: in-place projection of (u, v, w) with phi output.
 // stage_sdt >= 0: inputs are the anchor state (u, v, w, th); the provisional
 // stage state w + sdt * b_half is formed on the fly and the projected result
@@ -893,11 +1121,6 @@ template <class T>
 int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
                  double stage_sdt, T* uo, T* vo, T* wo, T* phio, int slot_c, int slot_d,
                  cudaStream_t st, const T* bh = nullptr) {
-  using C = cplx<T>;
-  const GridK g = p->g;
-  C* S1 = (C*)p->S1;
-  C* S2 = (C*)p->S2;
-  C* S3 = (C*)p->S3;
   p->solve_count += 1;
   const int de = p->diag_every < 1 ? 1 : p->diag_every;
   const bool log = !p->capturing && ((de == 1) || (p->solve_count % de == 1));
@@ -910,72 +1133,11 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
     OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
   }
   const bool stage = stage_sdt >= 0.0;
-  bool fx_done = false;
-  if constexpr (sizeof(T) == 4) {
-    if (p->zc3_fx && stage && bh) {
-      { Launch L_(p, 0, st); fx3<float, true>(p, p->zc3_fx, u, v, w, bh, stage_sdt, S1, S2, st); }
-      fx_done = true;
-    } else if (p->zc3_fx && !stage) {
-      { Launch L_(p, 0, st); fx3<float, false>(p, p->zc3_fx, u, v, w, th, 0.0, S1, S2, st); }
-      fx_done = true;
-    }
-  }
-  if (fx_done) {
-  } else if (stage && p->zc2_fxs && bh)
-    { Launch L_(p, 0, st); fx2<T, true, T>(p, p->zc2_fxs, u, v, w, bh, stage_sdt, S1, S2, st); }
-  else if (!stage && p->zc2_fx)
-    { Launch L_(p, 0, st); fx2<T, false, T>(p, p->zc2_fx, u, v, w, th, 0.0, S1, S2, st); }
-  else if (stage)
-    { Launch L_(p, 0, st); k_fx<T, FX_DIV_STAGE><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
-        g, p->pxf, p->zc_fx, 3, u, v, w, th, stage_sdt, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2, nullptr); }
-  else
-    { Launch L_(p, 0, st); k_fx<T, FX_DIV><<<grid_x(p, p->zc_fx), kFftThreads, smem_fx(p, 3), st>>>(
-        g, p->pxf, p->zc_fx, 3, u, v, w, th, 0.0, p->rho, p->rhoh, p->theta0, p->kx,
-        (const C*)p->twx, S1, S2, nullptr); }
-  OB_LAUNCHED();
-  if (sizeof(T) == 4 && p->zc3_fy)
-    { Launch L_(p, 1, st); yr(p, false, (const cplx<float>*)S1, (const cplx<float>*)S2, (cplx<float>*)S3, nullptr, st); }
-  else if (p->zc2_fy)
-    { Launch L_(p, 1, st); fy2<T, FY_DIV, T>(p, p->zc2_fy, S1, S2, S3, st); }
-  else
-    { Launch L_(p, 1, st); k_fy<T, FY_DIV><<<grid_y(p, p->zc_fy), kFftThreads, smem_fy(p, 2, p->zc_fy), st>>>(
-        g, p->pyf, p->zc_fy, 2, S1, S2, p->kx, p->ky, (const C*)p->twy, 1.0, S3, nullptr); }
-  OB_LAUNCHED();
-  RC(thomas_solve<T>(p, 2, S3, diag, slot_c, slot_d, st));
-  if (sizeof(T) == 4 && p->zc3_fy)
-    { Launch L_(p, 3, st); yr(p, true, (const cplx<float>*)S3, nullptr, (cplx<float>*)S1, (cplx<float>*)S2, st); }
-  else if (p->zc2_iy)
-    { Launch L_(p, 3, st); iy2<T>(p, p->zc2_iy, S3, S1, S2, st); }
-  else
-    { Launch L_(p, 3, st); k_iy<T, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-        g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const C*)p->twy, 1.0, S1, S2); }
-  OB_LAUNCHED();
-  const size_t sx = smem_ix(p, 3 * p->zc_ix + 1);
-  bool ix_done = false;
-  if constexpr (sizeof(T) == 4) {
-    if (p->zc3_ix && stage && bh) {
-      { Launch L_(p, 4, st); ix3<IX_STAGE>(p, p->zc3_ix, S1, S2, u, v, w, bh, stage_sdt, uo, vo, wo, phio, st); }
-      ix_done = true;
-    } else if (p->zc3_ix && !stage) {
-      { Launch L_(p, 4, st); ix3<IX_CORRECT>(p, p->zc3_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st); }
-      ix_done = true;
-    }
-  }
-  if (ix_done) {
-  } else if (p->zc2_ix && stage && bh)
-    { Launch L_(p, 4, st); ix2<T, IX_STAGE, T>(p, p->zc2_ix, S1, S2, u, v, w, bh, stage_sdt, uo, vo, wo, phio, st); }
-  else if (p->zc2_ix && !stage)
-    { Launch L_(p, 4, st); ix2<T, IX_CORRECT, T>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, uo, vo, wo, phio, st); }
-  else if (stage)
-    { Launch L_(p, 4, st); k_ix<T, IX_STAGE><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
-        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th,
-        stage_sdt, p->theta0, uo, vo, wo, phio); }
-  else
-    { Launch L_(p, 4, st); k_ix<T, IX_CORRECT><<<grid_x(p, p->zc_ix), kFftThreads, sx, st>>>(
-        g, p->px, p->zc_ix, 0, S1, S2, nullptr, p->kx, (const C*)p->twx, u, v, w, th, 0.0,
-        p->theta0, uo, vo, wo, phio); }
-  OB_LAUNCHED();
+  RC(proj_fx<T>(p, stage, u, v, w, th, bh, stage_sdt, st));
+  RC(proj_fy<T>(p, st));
+  RC(thomas_solve<T>(p, 2, (cplx<T>*)p->S3, diag, slot_c, slot_d, st));
+  RC(proj_iy<T>(p, 3, st));
+  RC(proj_ix<T>(p, stage, u, v, w, th, bh, stage_sdt, uo, vo, wo, phio, st));
   return OB_OK;
 }
 
@@ -987,45 +1149,65 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
 // is then solved and applied in single precision (it is small, so its
 // relative FP32 error is negligible against the state):
 // u, v, w -= grad(dphi), phi += dphi.
-int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStream_t st) {
+// The residual's x transform (FP32 state in, FP64 half-spectra R1, R2 out).
+int refine_fx(OraclePlan* p, const float* u, const float* v, const float* w, cudaStream_t st) {
   OraclePlan* q = p->dbl;
-  if (!q) return fail(OB_ERR_UNSUPPORTED, "defect correction needs a single-precision plan");
   using Cd = cplx<double>;
-  using Cf = cplx<float>;
   const GridK g = p->g;
   Cd* R1 = (Cd*)q->S1;
   Cd* R2 = (Cd*)q->S2;
+  Launch L_(p, OB_PROF_REFINE, st);
+  if (p->zc4_fxd)
+    fx4<double, false>(q, p->zc4_fxd, u, v, w, nullptr, 0.0, R1, R2, st);
+  else if (p->zc3_fxd)
+    fx3<double, false>(q, p->zc3_fxd, u, v, w, nullptr, 0.0, R1, R2, st);
+  else if (q->zc2_fx)
+    fx2<double, false, float>(q, q->zc2_fx, u, v, w, nullptr, 0.0, R1, R2, st);
+  else
+    k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
+        g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
+        (const Cd*)q->twx, R1, R2, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+// The residual's y transform (R1, R2 -> the FP32 residual in S3).
+int refine_fy(OraclePlan* p, cudaStream_t st) {
+  OraclePlan* q = p->dbl;
+  using Cd = cplx<double>;
+  const GridK g = p->g;
+  Cd* R1 = (Cd*)q->S1;
+  Cd* R2 = (Cd*)q->S2;
+  cplx<float>* S3 = (cplx<float>*)p->S3;
+  Launch L_(p, OB_PROF_REFINE, st);
+  if (p->zc3_fyd)
+    k_fy3<2, double, FY_RESID, float><<<dim3((g.nz + 1) / 2, g.nxh), 128,
+                                        YrSize<2, double>::total, st>>>(
+        g, R1, R2, q->ky, (const Cd*)q->twy, S3);
+  else if (q->zc2_fy)
+    fy2<double, FY_RESID, float>(q, q->zc2_fy, R1, R2, S3, st);
+  else
+    k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
+        g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr);
+  OB_LAUNCHED();
+  return OB_OK;
+}
+
+int refine_impl(OraclePlan* p, float* u, float* v, float* w, float* phi, cudaStream_t st) {
+  OraclePlan* q = p->dbl;
+  if (!q) return fail(OB_ERR_UNSUPPORTED, "defect correction needs a single-precision plan");
+  using Cf = cplx<float>;
+  const GridK g = p->g;
   Cf* S1 = (Cf*)p->S1;
   Cf* S2 = (Cf*)p->S2;
   Cf* S3 = (Cf*)p->S3;
-  if (p->zc3_fxd)
-    { Launch L_(p, OB_PROF_REFINE, st); fx3<double, false>(q, p->zc3_fxd, u, v, w, nullptr, 0.0, R1, R2, st); }
-  else if (q->zc2_fx)
-    { Launch L_(p, OB_PROF_REFINE, st); fx2<double, false, float>(q, q->zc2_fx, u, v, w, nullptr, 0.0, R1, R2, st); }
-  else
-    { Launch L_(p, OB_PROF_REFINE, st); k_fx<double, FX_DIV, float><<<grid_x(q, q->zc_fx), kFftThreads, smem_fx(q, 3), st>>>(
-        g, q->pxf, q->zc_fx, 3, u, v, w, nullptr, 0.0, q->rho, q->rhoh, q->theta0, q->kx,
-        (const Cd*)q->twx, R1, R2, nullptr); }
-  OB_LAUNCHED();
-  if (p->zc3_fy)
-    { Launch L_(p, OB_PROF_REFINE, st); k_fy3<2, double, FY_RESID, float><<<dim3((g.nz + 1) / 2, g.nxh), 128,
-          YrSize<2, double>::total, st>>>(g, R1, R2, q->ky, (const Cd*)q->twy, S3); }
-  else if (q->zc2_fy)
-    { Launch L_(p, OB_PROF_REFINE, st); fy2<double, FY_RESID, float>(q, q->zc2_fy, R1, R2, S3, st); }
-  else
-    { Launch L_(p, OB_PROF_REFINE, st); k_fy<double, FY_RESID, float><<<grid_y(q, q->zc_fy), kFftThreads, smem_fy(q, 2, q->zc_fy), st>>>(
-        g, q->pyf, q->zc_fy, 2, R1, R2, q->kx, q->ky, (const Cd*)q->twy, 1.0, S3, nullptr); }
-  OB_LAUNCHED();
+  RC(refine_fx(p, u, v, w, st));
+  RC(refine_fy(p, st));
   RC(thomas_solve<float>(p, OB_PROF_REFINE, S3, nullptr, 0, 0, st));
-  if (p->zc3_fy)
-    { Launch L_(p, OB_PROF_REFINE, st); yr(p, true, S3, nullptr, S1, S2, st); }
-  else if (p->zc2_iy)
-    { Launch L_(p, OB_PROF_REFINE, st); iy2<float>(p, p->zc2_iy, S3, S1, S2, st); }
-  else
-    { Launch L_(p, OB_PROF_REFINE, st); k_iy<float, IY_GRAD><<<grid_y(p, p->zc_iy), kFftThreads, smem_fy(p, 2, p->zc_iy), st>>>(
-        g, p->py, p->zc_iy, 2, S3, nullptr, p->ky, (const Cf*)p->twy, 1.0, S1, S2); }
-  OB_LAUNCHED();
-  if (p->zc3_ix)
+  RC(proj_iy<float>(p, OB_PROF_REFINE, st));
+  if (p->zc4_ix)
+    { Launch L_(p, OB_PROF_REFINE, st); ix4<IX_REFINE>(p, p->zc4_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
+  else if (p->zc3_ix)
     { Launch L_(p, OB_PROF_REFINE, st); ix3<IX_REFINE>(p, p->zc3_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
   else if (p->zc2_ix)
     { Launch L_(p, OB_PROF_REFINE, st); ix2<float, IX_REFINE, float>(p, p->zc2_ix, S1, S2, u, v, w, nullptr, 0.0, u, v, w, phi, st); }
@@ -1255,7 +1437,7 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
     const double alphas[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
     // the three stages share the buoyancy of the anchor theta'
     const T* bh = nullptr;
-    if (p->Bh && (p->zc2_fxs || p->zc2_ix)) {
+    if (p->Bh && (p->zc2_fxs || p->zc2_ix || p->zc4_fxs || p->zc4_ix)) {
       const long ncol = (long)p->g.nx * p->g.ny;
       { Launch L_(p, 7, st); k_bhalf<T><<<(unsigned)std::min<long>((ncol + 7) / 8, 65535), 256, 0, st>>>(
           p->g, ath, p->theta0, p->gth, (T*)p->Bh); }
@@ -1451,6 +1633,305 @@ int tendency_impl(OraclePlan* p, int mask, const OracleStatePtrs* s, T* du, T* d
 int check_plan(const OraclePlan* p) {
   if (!p) return fail(OB_ERR_ARG, "plan is NULL");
   return OB_OK;
+}
+
+// ---- kernel variants and the autotuner ---------------------------------------
+// The plan field behind each OB_VAR_* index (the refiner's compile-time
+// chunks live on its FP64 companion); nullptr where the plan has none.
+int* var_field(OraclePlan* p, int i) {
+  OraclePlan* q = p->dbl;
+  switch (i) {
+    case OB_VAR_ZC2_FX: return &p->zc2_fx;
+    case OB_VAR_ZC2_FXS: return &p->zc2_fxs;
+    case OB_VAR_ZC2_IX: return &p->zc2_ix;
+    case OB_VAR_ZC2_FY: return &p->zc2_fy;
+    case OB_VAR_ZC2_IY: return &p->zc2_iy;
+    case OB_VAR_ZC3_FX: return &p->zc3_fx;
+    case OB_VAR_ZC3_FXS: return &p->zc3_fxs;
+    case OB_VAR_ZC3_IX: return &p->zc3_ix;
+    case OB_VAR_ZC3_FXD: return &p->zc3_fxd;
+    case OB_VAR_ZC3_FY: return &p->zc3_fy;
+    case OB_VAR_ZC3_FYD: return &p->zc3_fyd;
+    case OB_VAR_ZC4_FX: return &p->zc4_fx;
+    case OB_VAR_ZC4_FXS: return &p->zc4_fxs;
+    case OB_VAR_ZC4_IX: return &p->zc4_ix;
+    case OB_VAR_ZC4_FXD: return &p->zc4_fxd;
+    case OB_VAR_ZC4_FY: return &p->zc4_fy;
+    case OB_VAR_ZC4_IY: return &p->zc4_iy;
+    case OB_VAR_SLOW_XW: return &p->slow_xw;
+    case OB_VAR_THOMAS_FAST: return &p->thomas_fast;
+    case OB_VAR_RZC2_FX: return q ? &q->zc2_fx : nullptr;
+    case OB_VAR_RZC2_FY: return q ? &q->zc2_fy : nullptr;
+  }
+  return nullptr;
+}
+
+// The values variant i may take on this plan: 0 (the form off) and the
+// z-chunks whose kernels exist for the plan's grid and precision and whose
+// tiles fit in shared memory.
+std::vector<int> var_values(const OraclePlan* p, int i) {
+  const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz;
+  const bool f32 = p->prec == OB_PREC_F32;
+  std::vector<int> v{0};
+  auto x2 = [&](int kind) {
+    if (!p->px8_ok) return;
+    for (int z : {1, 2, 4, 8}) {
+      if (z > 1 && z > nz) continue;
+      const size_t sm = f32 ? x2_smem<float, float>(kind, z, nx) : x2_smem<double, double>(kind, z, nx);
+      if (sm <= kSmemMax) v.push_back(z);
+    }
+  };
+  auto y2 = [&](bool dbl) {
+    if (!p->py8_ok) return;
+    for (int z : {1, 2, 4, 8}) {
+      if (z > 1 && z > nz) continue;
+      const size_t sm = dbl ? y2_smem_zc<double>(z, ny) : y2_smem_zc<float>(z, ny);
+      if (sm <= kSmemMax) v.push_back(z);
+    }
+  };
+  auto list = [&](bool ok, std::initializer_list<int> zs) {
+    if (ok)
+      for (int z : zs) v.push_back(z);
+  };
+  switch (i) {
+    case OB_VAR_ZC2_FX: x2(0); break;
+    case OB_VAR_ZC2_FXS: x2(1); break;
+    case OB_VAR_ZC2_IX: x2(2); break;
+    case OB_VAR_ZC2_FY:
+    case OB_VAR_ZC2_IY: y2(!f32); break;
+    case OB_VAR_ZC3_FX:
+    case OB_VAR_ZC3_FXS:
+    case OB_VAR_ZC3_IX: list(f32 && nx == kXrN, {2, 4, 8}); break;
+    case OB_VAR_ZC3_FXD: list(f32 && nx == kXrN, {2, 4}); break;
+    case OB_VAR_ZC3_FY: list(f32 && ny == kYrN, {2, 4, 8}); break;
+    case OB_VAR_ZC3_FYD: list(f32 && ny == kYrN && p->dbl, {2}); break;
+    case OB_VAR_ZC4_FX:
+    case OB_VAR_ZC4_FXS:
+    case OB_VAR_ZC4_IX: list(f32 && nx == kX4N, {2, 4, 8}); break;
+    case OB_VAR_ZC4_FXD: list(f32 && nx == kX4N && p->dbl, {2}); break;
+    case OB_VAR_ZC4_FY:
+    case OB_VAR_ZC4_IY: list(f32 && ny == kY4N, {2, 4, 8}); break;
+    case OB_VAR_SLOW_XW: list(true, {1}); break;
+    case OB_VAR_THOMAS_FAST: list(true, {1}); break;
+    case OB_VAR_RZC2_FX:
+      if (f32 && p->dbl && p->px8_ok)
+        for (int z : {1, 2, 4, 8})
+          if ((z == 1 || z <= nz) && x2_smem<double, float>(0, z, nx) <= kSmemMax) v.push_back(z);
+      break;
+    case OB_VAR_RZC2_FY:
+      if (f32 && p->dbl) y2(true);
+      break;
+  }
+  return v;
+}
+
+bool var_allowed(const OraclePlan* p, int i, int value) {
+  for (int z : var_values(p, i))
+    if (z == value) return true;
+  return false;
+}
+
+// Best device time (ms) of three launches of `f` after a warm-up one, with
+// CUDA events on st; +inf when a launch fails.
+template <class F>
+float time_launch(cudaStream_t st, F&& f) {
+  const float inf = INFINITY;
+  if (f() != OB_OK) return inf;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return inf;
+  float best = inf;
+  for (int r = 0; r < 3; ++r) {
+    cudaEventRecord(a, st);
+    if (f() != OB_OK) break;
+    cudaEventRecord(b, st);
+    if (cudaEventSynchronize(b) != cudaSuccess) break;
+    float ms = inf;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (cudaGetLastError() != cudaSuccess) return inf;
+  return best;
+}
+
+// One tuning group: variants that select among the forms of one kernel
+// class; a candidate turns one form on (one variant at one value) with the
+// group's other variants off, or every form off.
+template <class T>
+int tune_group(OraclePlan* p, std::initializer_list<int> vars, cudaStream_t st,
+               const std::function<int()>& launch) {
+  std::vector<std::pair<int, int>> cands{{-1, 0}};
+  for (int i : vars)
+    for (int z : var_values(p, i))
+      if (z) cands.push_back({i, z});
+  if (cands.size() == 1) return OB_OK;
+  float best = INFINITY;
+  std::pair<int, int> win{-1, 0};
+  for (const auto& c : cands) {
+    for (int i : vars)
+      if (int* f = var_field(p, i)) *f = (i == c.first) ? c.second : 0;
+    const float ms = time_launch(st, launch);
+    if (ms < best) {
+      best = ms;
+      win = c;
+    }
+  }
+  for (int i : vars)
+    if (int* f = var_field(p, i)) *f = (i == win.first) ? win.second : 0;
+  return OB_OK;
+}
+
+template <class T>
+int tune_impl(OraclePlan* p, cudaStream_t st) {
+  const size_t n = (size_t)p->g.nx * p->g.ny * p->g.nz;
+  const size_t nw = (size_t)p->g.nx * p->g.ny * (p->g.nz + 1);
+  const size_t e = p->esz;
+  // finite inputs: zero every buffer a candidate reads
+  for (void* b : {p->Au, p->Av, p->Ath, p->Aphi, p->Su, p->Sv, p->Sphi, p->Du, p->Dv})
+    OB_CUDA(cudaMemsetAsync(b, 0, n * e, st));
+  for (void* b : {p->Aw, p->Sw}) OB_CUDA(cudaMemsetAsync(b, 0, nw * e, st));
+  if (p->Bh) OB_CUDA(cudaMemsetAsync(p->Bh, 0, nw * e, st));
+  const T *u = (const T*)p->Au, *v = (const T*)p->Av, *w = (const T*)p->Aw,
+          *th = (const T*)p->Ath, *bh = (const T*)p->Bh;
+  T *uo = (T*)p->Su, *vo = (T*)p->Sv, *wo = (T*)p->Sw, *po = (T*)p->Sphi;
+  const bool stage = p->Bh && p->buoyancy && p->projection;
+  const double sdt = 10.0;
+  RC(tune_group<T>(p, {OB_VAR_ZC4_FX, OB_VAR_ZC3_FX, OB_VAR_ZC2_FX}, st,
+                   [&] { return proj_fx<T>(p, false, u, v, w, th, nullptr, 0.0, st); }));
+  if (stage)
+    RC(tune_group<T>(p, {OB_VAR_ZC4_FXS, OB_VAR_ZC3_FXS, OB_VAR_ZC2_FXS}, st,
+                     [&] { return proj_fx<T>(p, true, u, v, w, th, bh, sdt, st); }));
+  RC(tune_group<T>(p, {OB_VAR_ZC4_IX, OB_VAR_ZC3_IX, OB_VAR_ZC2_IX}, st, [&] {
+    return stage ? proj_ix<T>(p, true, u, v, w, th, bh, sdt, uo, vo, wo, po, st)
+                 : proj_ix<T>(p, false, u, v, w, th, nullptr, 0.0, uo, vo, wo, po, st);
+  }));
+  // forward and inverse y share the 512-point register form's chunk: time
+  // the two together for it, and each alone for the others
+  {
+    const int fy4 = p->zc4_fy, iy4 = p->zc4_iy;
+    std::vector<std::array<int, 5>> cands;  // zc4_fy, zc4_iy, zc3_fy, zc2_fy, zc2_iy
+    cands.push_back({0, 0, 0, 0, 0});
+    auto vals = [&](int i) {
+      std::vector<int> r;
+      for (int z : var_values(p, i))
+        if (z) r.push_back(z);
+      return r;
+    };
+    const auto f4 = vals(OB_VAR_ZC4_FY), i4 = vals(OB_VAR_ZC4_IY), y3 = vals(OB_VAR_ZC3_FY),
+               f2 = vals(OB_VAR_ZC2_FY), i2 = vals(OB_VAR_ZC2_IY);
+    for (int a : f4)
+      for (int b : i4) cands.push_back({a, b, 0, 0, 0});
+    for (int a : y3) cands.push_back({0, 0, a, 0, 0});
+    for (int a : f2)
+      for (int b : i2) cands.push_back({0, 0, 0, a, b});
+    (void)fy4;
+    (void)iy4;
+    if (cands.size() > 1) {
+      // time each forward and inverse form once, then pick the best pair
+      auto apply = [&](const std::array<int, 5>& c) {
+        p->zc4_fy = c[0];
+        p->zc4_iy = c[1];
+        p->zc3_fy = c[2];
+        p->zc2_fy = c[3];
+        p->zc2_iy = c[4];
+      };
+      float best = INFINITY;
+      std::array<int, 5> win = cands[0];
+      for (const auto& c : cands) {
+        apply(c);
+        const float t = time_launch(st, [&] { return proj_fy<T>(p, st); }) +
+                        time_launch(st, [&] { return proj_iy<T>(p, 3, st); });
+        if (t < best) {
+          best = t;
+          win = c;
+        }
+      }
+      apply(win);
+    }
+  }
+  if constexpr (sizeof(T) == 4) {
+    RC(tune_group<T>(p, {OB_VAR_THOMAS_FAST}, st, [&] {
+      return thomas_solve<T>(p, 2, (cplx<T>*)p->S3, nullptr, 0, 0, st);
+    }));
+    if (p->dbl) {
+      RC(tune_group<T>(p, {OB_VAR_ZC4_FXD, OB_VAR_ZC3_FXD, OB_VAR_RZC2_FX}, st,
+                       [&] { return refine_fx(p, (const float*)u, (const float*)v,
+                                              (const float*)w, st); }));
+      RC(tune_group<T>(p, {OB_VAR_ZC3_FYD, OB_VAR_RZC2_FY}, st,
+                       [&] { return refine_fy(p, st); }));
+    }
+    const bool slow = p->advection || p->coriolis || p->heating;
+    const bool extra = p->drag || p->sponge || p->diffusion || p->cooling;
+    const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_HEATING;
+    if (slow && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
+      RC(tune_group<T>(p, {OB_VAR_SLOW_XW}, st, [&] {
+        return slow_impl<T, 0>(p, all, 1.0, u, v, w, th, uo, vo, wo, (T*)p->Sphi, st);
+      }));
+  }
+  OB_CUDA(cudaStreamSynchronize(st));
+  return OB_OK;
+}
+
+// Tuned choices per (grid, precision, component set, device), for the life
+// of the process and optionally in a text file (ORACLE_B200_TUNE_CACHE):
+// one line "key | v0 v1 ..." per entry.
+std::mutex g_tune_mu;
+std::map<std::string, std::vector<int>> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_key(const OraclePlan* p) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, dev);
+  char buf[512];
+  snprintf(buf, sizeof buf, "v1 %dx%dx%d prec%d stage%d slow%d%d%d%d prod%d%d%d%d damp%d sm%d %s",
+           p->g.nx, p->g.ny, p->g.nz, p->prec, (int)(p->buoyancy && p->projection),
+           p->advection, p->coriolis, p->heating, p->damping, p->drag, p->sponge, p->diffusion,
+           p->cooling, p->damping, nsm, prop.name);
+  std::string k = buf;
+  for (char& c : k)
+    if (c == '|' || c == '\n') c = '_';
+  return k;
+}
+
+void tune_cache_load() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = getenv("ORACLE_B200_TUNE_CACHE");
+  if (!path || !*path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  char line[1024];
+  while (fgets(line, sizeof line, f)) {
+    char* bar = strchr(line, '|');
+    if (!bar) continue;
+    std::string key(line, bar - line);
+    while (!key.empty() && key.back() == ' ') key.pop_back();
+    std::vector<int> vals;
+    char* s = bar + 1;
+    char* end = nullptr;
+    for (long x = strtol(s, &end, 10); end != s; x = strtol(s, &end, 10)) {
+      vals.push_back((int)x);
+      s = end;
+    }
+    if (vals.size() == OB_VAR_COUNT) g_tune[key] = vals;
+  }
+  fclose(f);
+}
+
+void tune_cache_store(const std::string& key, const std::vector<int>& vals) {
+  g_tune[key] = vals;
+  const char* path = getenv("ORACLE_B200_TUNE_CACHE");
+  if (!path || !*path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s |", key.c_str());
+  for (int x : vals) fprintf(f, " %d", x);
+  fprintf(f, "\n");
+  fclose(f);
 }
 
 }  // namespace
@@ -2036,16 +2517,18 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     return bail(fail(OB_ERR_ARG, "grid (%d, %d, %d) exceeds shared-memory tiling limits", nx,
                      ny, nz));
   // compile-time-chunk x-pencil kernels where their tiles fit
-  if (factorize8(ny, p->py8)) {
+  p->py8_ok = factorize8(ny, p->py8);
+  p->px8_ok = factorize8(nx / 2, p->px8);
+  if (p->py8_ok) {
     p->zc2_fy = p->prec == OB_PREC_F64 ? pick_y2_zc<double>(ny, nz) : pick_y2_zc<float>(ny, nz);
     p->zc2_iy = p->zc2_fy;
   }
-  if (const char* e = getenv("ORACLE_B200_SLOW_XW")) p->slow_xw = atoi(e) != 0;
+  if (p->prec == OB_PREC_F32 && ny == kY4N) p->zc4_fy = p->zc4_iy = nz >= 4 ? 4 : 2;
   if (p->prec == OB_PREC_F32 && ny == kYrN) {
     p->zc3_fy = nz >= 4 ? 4 : 2;
-    if (const char* e = getenv("ORACLE_B200_FY3_ZC")) p->zc3_fy = atoi(e);
+    p->zc3_fyd = p->zc3_fy ? 2 : 0;
   }
-  if (factorize8(nx / 2, p->px8)) {
+  if (p->px8_ok) {
     if (p->prec == OB_PREC_F64) {
       p->zc2_fx = pick_x2_zc<double, double>(0, nx, nz);
       p->zc2_fxs = pick_x2_zc<double, double>(1, nx, nz);
@@ -2055,11 +2538,12 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       p->zc2_fxs = pick_x2_zc<float, float>(1, nx, nz);
       p->zc2_ix = pick_x2_zc<float, float>(2, nx, nz);
       if (nx == kXrN) {
-        p->zc3_fx = p->zc3_ix = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
-        if (const char* e = getenv("ORACLE_B200_FX3_ZC")) p->zc3_fx = atoi(e);
-        if (const char* e = getenv("ORACLE_B200_IX3_ZC")) p->zc3_ix = atoi(e);
+        p->zc3_fx = p->zc3_fxs = p->zc3_ix = nz >= 8 ? 8 : (nz >= 4 ? 4 : 2);
         p->zc3_fxd = nz >= 4 ? 4 : 2;
-        if (const char* e = getenv("ORACLE_B200_FXD3_ZC")) p->zc3_fxd = atoi(e);
+      }
+      if (nx == kX4N) {
+        p->zc4_fxs = p->zc4_fx = p->zc4_ix = nz >= 4 ? 4 : 2;
+        p->zc4_fxd = 2;
       }
     }
   }
@@ -2402,6 +2886,63 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
                 p->blowup_u);
   if (buf[OB_DIAG_BLOWUP] >= 1.0)
     return fail(OB_ERR_NONFINITE, "blow-up: a diagnosed state held a non-finite value");
+  return OB_OK;
+}
+
+int oracle_b200_plan_get_variants(const OraclePlan* p, int* out, int n) {
+  if (int rc = check_plan(p)) return rc;
+  if (!out || n < 0) return fail(OB_ERR_ARG, "plan_get_variants: bad output");
+  OraclePlan* q = const_cast<OraclePlan*>(p);
+  for (int i = 0; i < n && i < OB_VAR_COUNT; ++i) {
+    const int* f = var_field(q, i);
+    out[i] = f ? *f : 0;
+  }
+  return OB_OK;
+}
+
+int oracle_b200_plan_set_variants(OraclePlan* p, const int* in, int n) {
+  if (int rc = check_plan(p)) return rc;
+  if (!in || n < 0 || n > OB_VAR_COUNT) return fail(OB_ERR_ARG, "plan_set_variants: bad input");
+  for (int i = 0; i < n; ++i)
+    if (!var_allowed(p, i, in[i]))
+      return fail(OB_ERR_ARG, "plan_set_variants: variant %d cannot be %d on this plan", i, in[i]);
+  for (int i = 0; i < n; ++i)
+    if (int* f = var_field(p, i)) *f = in[i];
+  return OB_OK;
+}
+
+int oracle_b200_plan_tune(OraclePlan* p, int flags, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (flags & ~OB_TUNE_FORCE) return fail(OB_ERR_ARG, "plan_tune: unknown flags %d", flags);
+  if (p->capturing) return fail(OB_ERR_ARG, "plan_tune: not while a step graph is recorded");
+  const bool prof = p->profiling;
+  if (prof) return fail(OB_ERR_ARG, "plan_tune: switch profiling off first");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_cache_load();
+  const std::string key = tune_key(p);
+  auto it = g_tune.find(key);
+  if (it != g_tune.end() && !(flags & OB_TUNE_FORCE)) {
+    bool ok = true;
+    for (int i = 0; i < OB_VAR_COUNT; ++i) ok = ok && var_allowed(p, i, it->second[i]);
+    if (ok) {
+      for (int i = 0; i < OB_VAR_COUNT; ++i)
+        if (int* f = var_field(p, i)) *f = it->second[i];
+      return OB_OK;
+    }
+  }
+  // run after the caller's queued work, on the plan's private stream
+  OB_CUDA(cudaEventRecord(p->ev_fork, (cudaStream_t)stream));
+  OB_CUDA(cudaStreamWaitEvent(p->astream, p->ev_fork, 0));
+  const long l0 = p->launches;
+  const int rc = DISPATCH(p, tune_impl<double>(p, p->astream), tune_impl<float>(p, p->astream));
+  p->launches = l0;
+  if (rc) return rc;
+  std::vector<int> vals(OB_VAR_COUNT);
+  for (int i = 0; i < OB_VAR_COUNT; ++i) {
+    const int* f = var_field(p, i);
+    vals[i] = f ? *f : 0;
+  }
+  tune_cache_store(key, vals);
   return OB_OK;
 }
 

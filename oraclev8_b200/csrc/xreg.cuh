@@ -526,10 +526,12 @@ constexpr int kYrN = 512;
 constexpr int kYrEx = 16 * 33;  // exchange block of one column (complex)
 
 // ytw[32 k2 + n1] = W_512^(n1 k2) (forward sign), w32[j] = W_32^j.
+// yr_pass1 (DFT over n2 and the twiddles, registers only) and yr_pass2 (the
+// exchange through the column's block, the second DFT and the radix-2 step)
+// let a caller place a barrier between them when ex aliases other data.
 template <class T, bool INV>
-__device__ __forceinline__ void yr_fft(cplx<T> (&a)[16], int lane,
-                                       const cplx<T>* __restrict__ ytw,
-                                       const cplx<T>* __restrict__ w32, cplx<T>* ex) {
+__device__ __forceinline__ void yr_pass1(cplx<T> (&a)[16], int lane,
+                                         const cplx<T>* __restrict__ ytw) {
   dft16<T, INV>(a);
 #pragma unroll
   for (int k2 = 1; k2 < 16; ++k2) {
@@ -537,6 +539,10 @@ __device__ __forceinline__ void yr_fft(cplx<T> (&a)[16], int lane,
     if (INV) w.y = -w.y;
     a[k2] = mul(a[k2], w);
   }
+}
+template <class T, bool INV>
+__device__ __forceinline__ void yr_pass2(cplx<T> (&a)[16], int lane,
+                                         const cplx<T>* __restrict__ w32, cplx<T>* ex) {
 #pragma unroll
   for (int k2 = 0; k2 < 16; ++k2) ex[k2 * 33 + lane] = a[k2];
   __syncwarp();
@@ -554,6 +560,13 @@ __device__ __forceinline__ void yr_fft(cplx<T> (&a)[16], int lane,
     // p = 0 holds E, the partner O; p = 1 holds O, the partner E
     a[j] = p == 0 ? add(a[j], mul(w, other)) : sub(other, mul(w, a[j]));
   }
+}
+template <class T, bool INV>
+__device__ __forceinline__ void yr_fft(cplx<T> (&a)[16], int lane,
+                                       const cplx<T>* __restrict__ ytw,
+                                       const cplx<T>* __restrict__ w32, cplx<T>* ex) {
+  yr_pass1<T, INV>(a, lane, ytw);
+  yr_pass2<T, INV>(a, lane, w32, ex);
 }
 
 template <int ZC>

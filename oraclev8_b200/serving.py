@@ -235,6 +235,24 @@ class ServingEngine:
         self.realtime, self.keep_final = bool(realtime), bool(keep_final)
         self.max_active = int(max_active)
 
+    @staticmethod
+    def prepare_kernels(requests: "list[RunRequest]") -> int:
+        """Create (and drop) one plan per distinct grid and precision of
+        ``requests``, so that the kernel-form tuning of each grid (cached per
+        process) happens here and not while runs are being served.  Returns
+        the number of distinct grids."""
+        seen = set()
+        for r in requests:
+            key = (r.n, r.nz, r.precision)
+            if key in seen:
+                continue
+            seen.add(key)
+            integ, _, _ = build_run(r)
+            integ.plan.release()
+            del integ
+        torch.cuda.synchronize()
+        return len(seen)
+
     # -- run lifecycle ---------------------------------------------------------
     def _prepare(self, req: RunRequest) -> _Active:
         """Set a run up (plan, device initial state, step graphs): host work,

@@ -138,14 +138,16 @@ class RK3Integrator:
 
     def __init__(self, config, base, precision: str | None = None,
                  refine_passes: int | None = None, refine_every: int = 1,
-                 blowup_u_max: float = 0.0) -> None:
+                 blowup_u_max: float = 0.0, autotune: bool = True) -> None:
         """precision: "fp64", "fp32" or "fp32r".  "fp32r" is the FP32 step
         followed, every ``refine_every`` steps, by ``refine_passes`` (default 1)
         defect corrections of the final projection whose residual divergence
         is formed in FP64.  blowup_u_max > 0 also raises the device's blow-up
         flag (``StepDiagnostics.blowup``) when max|u| exceeds it; non-finite
         values always do.  Steps never raise on it, as the reference's step
-        does not: a harness tests the flag (measure_lh82_phase3.py:129-130)."""
+        does not: a harness tests the flag (measure_lh82_phase3.py:129-130).
+        autotune: time the kernel forms of each class for this grid once per
+        process and keep the fastest (``plan.variants()`` shows the choice)."""
         self.config = config
         self.base = wrap_base(base)
         self.precision = precision or backend.PRECISION
@@ -156,6 +158,7 @@ class RK3Integrator:
             refine_passes = 1 if self.precision == "fp32r" else 0
         self.spec = compile_config(config, self.base, plan_prec)
         self.spec.blowup_u_max = float(blowup_u_max)
+        self.spec.autotune = bool(autotune)
         self.plan = Plan(self.spec)
         self.refine_passes, self.refine_every = int(refine_passes), int(refine_every)
         if self.refine_passes:

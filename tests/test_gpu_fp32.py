@@ -114,7 +114,8 @@ def _vortex_case(nx, ny, nz):
                              z_peak=6e3, width_z=math.sqrt(2.0) * 2e3), noise_seed=3)
 
 
-@pytest.mark.parametrize("shape", [(96, 72, 16), (512, 40, 16), (48, 512, 16)])
+@pytest.mark.parametrize("shape", [(96, 72, 16), (512, 40, 16), (48, 512, 16), (1024, 32, 16),
+                                   (32, 1024, 16)])
 def test_fp32_steps_track_fp64(shape):
     """Ten full steps of the vortex configuration in FP32, FP32 with one
     correction per step, and FP64: per-field error of the single-precision
@@ -169,14 +170,29 @@ def test_refinement_controls():
         p64.refine(u, u.clone(), w, u.clone())
 
 
+def _register_forms(plan, nx, ny):
+    """Turn the register-resident pencil forms of the plan's grid on."""
+    kw = {}
+    if nx == 512:
+        kw.update(zc3_fx=4, zc3_fxs=4, zc3_ix=4, zc3_fxd=4)
+    if nx == 1024:
+        kw.update(zc4_fx=4, zc4_fxs=4, zc4_ix=4, zc4_fxd=2)
+    if ny == 512:
+        kw.update(zc3_fy=4, zc3_fyd=2)
+    if ny == 1024:
+        kw.update(zc4_fy=4, zc4_iy=4)
+    plan.set_variants(**kw)
+
+
 @pytest.mark.parametrize("nx, ny, nz", [(512, 40, 16), (512, 40, 13), (64, 512, 16),
-                                        (48, 512, 13)])
+                                        (48, 512, 13), (1024, 40, 16), (1024, 24, 13),
+                                        (64, 1024, 16), (48, 1024, 13), (1024, 1024, 8)])
 def test_register_pencils_match_stockham(nx, ny, nz, monkeypatch):
-    """At nx = 512 the FP32 x pencils run the register-resident FFT
-    (xreg.cuh), the defect correction's FP64 residual transform included,
-    and at ny = 512 the y pencils; with ORACLE_B200_FX3_ZC,
-    ORACLE_B200_IX3_ZC, ORACLE_B200_FXD3_ZC and ORACLE_B200_FY3_ZC at 0 the
-    plan keeps the shared-memory Stockham kernels.  Against the FP64
+    """At nx = 512 or 1024 the FP32 x pencils run the register-resident FFT
+    (xreg.cuh, xreg4.cuh), the defect correction's FP64 residual transform
+    included, and at ny = 512 or 1024 the y pencils (forced on here, whatever
+    the autotuner picks); with those forms off the plan keeps the
+    shared-memory Stockham kernels.  Against the FP64
     projection of the same input, the register path is as accurate as the
     Stockham path, field by field, before and after one correction pass; u
     and v of the two agree to a few FP32 ulp of the wind.  nz = 13 leaves a
@@ -187,14 +203,10 @@ def test_register_pencils_match_stockham(nx, ny, nz, monkeypatch):
     z, rho0, th0 = O.build_base_state(nz, Lz)
     mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
                                     projection=True))
-    knobs = ("ORACLE_B200_FX3_ZC", "ORACLE_B200_IX3_ZC", "ORACLE_B200_FXD3_ZC",
-             "ORACLE_B200_FY3_ZC")
-    for k in knobs:
-        monkeypatch.setenv(k, "0")
     p_ref = mk("fp32")
-    for k in knobs:
-        monkeypatch.delenv(k)
+    p_ref.shared_memory_forms()
     p_new = mk("fp32")
+    _register_forms(p_new, nx, ny)
     p64 = mk("fp64")
     u, v, w = _smooth_state(nx, ny, nz, seed=7 + nz)
     f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
@@ -225,8 +237,8 @@ def test_register_pencils_match_stockham(nx, ny, nz, monkeypatch):
 @pytest.mark.parametrize("shape", [(32, 16, 16), (48, 24, 40)])
 def test_slow_tendency_forms_agree(shape, monkeypatch):
     """For FP32 state the slow tendency runs marching along x (k_slow_xw)
-    where nx % 16 == 0 and ny % 8 == 0, else as a gather (k_slow_f32;
-    ORACLE_B200_SLOW_XW=0 forces it).  Same terms and operation order: one
+    where nx % 16 == 0 and ny % 8 == 0, else as a gather (k_slow_f32; the
+    plan's slow_xw variant at 0 forces it).  Same terms and operation order: one
     full step of the vortex configuration from the same state agrees to FP32
     rounding.  The shapes cover the periodic halo rows and columns (two tiles
     in x and in y) and, at nz = 40, two z-chunks with the lid in the second."""
@@ -237,9 +249,9 @@ def test_slow_tendency_forms_agree(shape, monkeypatch):
     base = Base(c["nz"], c["Lz"])
     cfg = b200_config(c)
     outs = []
-    for xw in ("0", "1"):
-        monkeypatch.setenv("ORACLE_B200_SLOW_XW", xw)
+    for xw in (0, 1):
         integ = RK3Integrator(cfg, base, precision="fp32")
+        integ.plan.set_variants(slow_xw=xw)
         d = lambda a: dev(a, torch.float32)
         s = State(d(s0.u), d(s0.v), d(s0.w), d(s0.theta_prime), d(s0.projection_potential), 0.0)
         for n in range(2):
@@ -260,8 +272,7 @@ def test_register_damper_matches_stockham(nx, ny, nz, monkeypatch):
     kernels where the grid allows: the x transforms at nx = 512 (the field
     forms of the forward and inverse x pencils) and the y stage at ny = 512
     (forward y transforms, the divergent-part multipliers and inverse y
-    transforms in one pass).  With ORACLE_B200_FX3_ZC, ORACLE_B200_IX3_ZC,
-    ORACLE_B200_FXD3_ZC and ORACLE_B200_FY3_ZC at 0 it keeps the
+    transforms in one pass).  With the register forms off it keeps the
     shared-memory kernels.  Against the FP64 damper tendency of the same
     input, the register forms are as accurate as the shared-memory ones, and
     the two FP32 forms agree to FP32 rounding.  nz = 13 leaves a partial
@@ -272,14 +283,10 @@ def test_register_damper_matches_stockham(nx, ny, nz, monkeypatch):
     z, rho0, th0 = O.build_base_state(nz, Lz)
     mk = lambda prec: Plan(PlanSpec(nx, ny, nz, Lx, Ly, Lz, rho0, th0, precision=prec,
                                     projection=True, damping=True, epsilon=0.5))
-    knobs = ("ORACLE_B200_FX3_ZC", "ORACLE_B200_IX3_ZC", "ORACLE_B200_FXD3_ZC",
-             "ORACLE_B200_FY3_ZC")
-    for k in knobs:
-        monkeypatch.setenv(k, "0")
     p_ref = mk("fp32")
-    for k in knobs:
-        monkeypatch.delenv(k)
+    p_ref.shared_memory_forms()
     p_new = mk("fp32")
+    _register_forms(p_new, nx, ny)
     p64 = mk("fp64")
     u, v, w = _smooth_state(nx, ny, nz, seed=31 + nz)
     f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
