@@ -983,16 +983,31 @@ def track_report(args):
     t0 = time.perf_counter()
     for h in range(hours + 1):
         for prec, r in runs.items():
+            if r.get("blew_h") is not None:
+                continue
             if h > 0:
                 for _ in range(sph // chunk):
                     r["graph"].launch()
+            mu = float(r["st"].u.abs().max())
+            # a state that is no longer finite (or past the blow-up speed) has
+            # no storm centre: the run stops there, as the reference's harness
+            # stops it (measure_lh82_phase3.py:129-130)
+            if not math.isfinite(mu) or mu > 400.0:
+                r["blew_h"] = h
+                continue
             (x, y), m, d = find_storm_centre(r["st"], r["base"], nx, ny, dx,
                                              last_pos=r["last"], u_env_ms=u_env,
                                              v_env_ms=v_env, dt_output_s=3600.0,
                                              return_diag=True, last_raw_pos=r["last_raw"])
             r["last"], r["last_raw"] = (x, y), d["theta_raw_m"]
             r["fixes"].append(dict(x=x, y=y, method=m, max_w=float(r["st"].w.abs().max()),
-                                   max_u=float(r["st"].u.abs().max())))
+                                   max_u=mu))
+        print(f"hour {h}: " + ", ".join(
+            f"{p} max|u| {r['fixes'][-1]['max_u']:.2f}" if r.get("blew_h") is None
+            else f"{p} blew up by hour {r['blew_h']}" for p, r in runs.items()),
+            file=sys.stderr, flush=True)
+        if all(r.get("blew_h") is not None for r in runs.values()):
+            break
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     f64, f32 = runs["fp64"]["fixes"], runs["fp32r"]["fixes"]
@@ -1003,16 +1018,19 @@ def track_report(args):
                          method_fp32r=a["method"], method_fp64=b["method"],
                          x_fp64_km=b["x"] / 1e3, y_fp64_km=b["y"] / 1e3))
     st32, st64 = runs["fp32r"]["st"], runs["fp64"]["st"]
-    rep = _precision_report(st32, st64, runs["fp64"]["integ"].plan)
+    both_finite = all(r.get("blew_h") is None for r in runs.values())
+    rep = _precision_report(st32, st64, runs["fp64"]["integ"].plan) if both_finite else None
     line = {"track": {
         "workload": f"{args.workload}: {nx}x{ny}x{nz}, dt={dt}s, {hours} h = {hours * sph} steps "
                     f"in each precision, step graphs of {chunk} steps",
+        "hours_compared": len(rows) - 1,
+        "blew_up_by_hour": {p: r.get("blew_h") for p, r in runs.items()},
         "hours": rows,
         "max_centre_diff_m": max(r["dist_m"] for r in rows),
         "max_w_rel_diff_max": max(r["max_w_rel"] for r in rows),
         "fp64_track_km": [(round(r["x_fp64_km"], 3), round(r["y_fp64_km"], 3)) for r in rows],
         "final": rep,
-        "blowup": {p: runs[p]["integ"].plan.blown_up() for p in runs},
+        "blowup_flag": {p: runs[p]["integ"].plan.blown_up() for p in runs},
         "wall_s": wall}}
     print(json.dumps(line), flush=True)
 

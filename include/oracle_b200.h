@@ -252,6 +252,13 @@ int oracle_b200_intensity_cap(const void *u, const void *v, int precision, long 
                               double v_cap, double tau, double u_env, double v_env,
                               void *du, void *dv, void *stream);
 
+/* Enqueue a copy of the first n raw diagnostics slots (the residual slots
+ * not yet normalised) into host_out on `stream`, without waiting.  No
+ * counterpart in the reference: the serving loop polls the blow-up flag
+ * (OB_DIAG_BLOWUP) this way while a run's later steps are already queued.
+ * host_out should be page-locked memory, or the copy waits for the stream. */
+int oracle_b200_read_diag_async(OraclePlan *plan, double *host_out, int n, void *stream);
+
 /* Kernel variants (OB_VAR_*).  No counterpart in the reference, which leaves
  * its transforms to the array library: these choose among this library's
  * kernel forms for the same operations.  get: the n first choices of the plan.

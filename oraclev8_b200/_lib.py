@@ -40,6 +40,7 @@ EXPORTS = (
     "oracle_b200_vdiag_speed_max", "oracle_b200_vdiag_vorticity", "oracle_b200_vdiag_ke",
     "oracle_b200_vdiag_rings", "oracle_b200_vdiag_zpos", "oracle_b200_vdiag_centroid",
     "oracle_b200_plan_get_variants", "oracle_b200_plan_set_variants", "oracle_b200_plan_tune",
+    "oracle_b200_read_diag_async",
 )
 # kernel-variant choices of a plan, in OB_VAR_* order (include/oracle_b200.h)
 VARIANTS = ("zc2_fx", "zc2_fxs", "zc2_ix", "zc2_fy", "zc2_iy", "zc3_fx", "zc3_fxs", "zc3_ix",
@@ -156,6 +157,7 @@ def load(path: Path | None = None):
         "oracle_b200_plan_get_variants": ([vp, POINTER(c_int), c_int], c_int),
         "oracle_b200_plan_set_variants": ([vp, POINTER(c_int), c_int], c_int),
         "oracle_b200_plan_tune": ([vp, c_int, vp], c_int),
+        "oracle_b200_read_diag_async": ([vp, vp, c_int, vp], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -237,6 +237,16 @@ class Plan:
             L.check(rc)
         return np.frombuffer(buf, dtype=np.float64).copy()
 
+    def read_diag_async(self, out: torch.Tensor) -> None:
+        """Enqueue a copy of the raw diagnostics block into ``out`` (a pinned
+        float64 host tensor of at least DIAG_COUNT elements) on the current
+        stream, without waiting; ``out[DIAG["blowup"]]`` is the blow-up flag
+        once the copy has landed."""
+        if out.dtype != torch.float64 or out.device.type != "cpu" or out.numel() < L.DIAG_COUNT:
+            raise ValueError("read_diag_async needs a float64 host tensor of DIAG_COUNT elements")
+        L.check(self.lib.oracle_b200_read_diag_async(
+            self.handle, ctypes.c_void_p(out.data_ptr()), L.DIAG_COUNT, self._stream()))
+
     def blown_up(self) -> int:
         """The plan's sticky blow-up flag as of its last diagnosed step: 0 none,
         1 a non-finite value, 2 max|u| above ``blowup_u_max``."""

@@ -449,7 +449,7 @@ int xr4_attrs_zc() {
   int rc;
   if ((rc = xr4_attr_fx<float, false, ZC>()) || (rc = xr4_attr_fx<float, true, ZC>()))
     return rc;
-  if constexpr (ZC == 2)
+  if constexpr (ZC <= 4)
     if ((rc = xr4_attr_fx<double, false, ZC>())) return rc;
   for (auto k : {k_ix4<IX_CORRECT, ZC>, k_ix4<IX_STAGE, ZC>, k_ix4<IX_REFINE, ZC>})
     OB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -860,8 +860,9 @@ void fx4_launch(const OraclePlan* q, const float* u, const float* v, const float
 template <class T, bool STAGE>
 void fx4(const OraclePlan* q, int zc, const float* u, const float* v, const float* w,
          const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
-  if constexpr (sizeof(T) == 8) {
-    fx4_launch<T, false, 2>(q, u, v, w, bh, sdt, X0, X1, st);  // the FP64 residual form
+  if constexpr (sizeof(T) == 8) {  // the FP64 residual form
+    if (zc == 4) fx4_launch<T, false, 4>(q, u, v, w, bh, sdt, X0, X1, st);
+    else fx4_launch<T, false, 2>(q, u, v, w, bh, sdt, X0, X1, st);
   } else {
     switch (zc) {
       case 2: fx4_launch<T, STAGE, 2>(q, u, v, w, bh, sdt, X0, X1, st); break;
@@ -920,7 +921,7 @@ bool thomas_f32(OraclePlan* p, int cls, cplx<float>* S3, cudaStream_t st) {
   case N: {                                                                                 \
     const size_t sm = N * sizeof(float4) + (size_t)kThomasCols * (N + 1) * sizeof(cplx<float>); \
     Launch L_(p, cls, st);                                                                  \
-    k_thomas_f32<N, kThomasCols><<<nb, kThomasCols, sm, st>>>(p->g, coef, p->kx, p->ky, scale, \
+    k_thomas_f32<N, kThomasCols><<<nb, 2 * kThomasCols, sm, st>>>(p->g, coef, p->kx, p->ky, scale, \
                                                              S3, S3, p->lw_flag);           \
     return true;                                                                            \
   }
@@ -1708,7 +1709,7 @@ std::vector<int> var_values(const OraclePlan* p, int i) {
     case OB_VAR_ZC4_FX:
     case OB_VAR_ZC4_FXS:
     case OB_VAR_ZC4_IX: list(f32 && nx == kX4N, {2, 4, 8}); break;
-    case OB_VAR_ZC4_FXD: list(f32 && nx == kX4N && p->dbl, {2}); break;
+    case OB_VAR_ZC4_FXD: list(f32 && nx == kX4N && p->dbl, {2, 4}); break;
     case OB_VAR_ZC4_FY:
     case OB_VAR_ZC4_IY: list(f32 && ny == kY4N, {2, 4, 8}); break;
     case OB_VAR_SLOW_XW: list(true, {1}); break;
@@ -2886,6 +2887,15 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
                 p->blowup_u);
   if (buf[OB_DIAG_BLOWUP] >= 1.0)
     return fail(OB_ERR_NONFINITE, "blow-up: a diagnosed state held a non-finite value");
+  return OB_OK;
+}
+
+int oracle_b200_read_diag_async(OraclePlan* p, double* host_out, int n, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!host_out || n < 0) return fail(OB_ERR_ARG, "read_diag_async: bad output");
+  if (n > OB_DIAG_COUNT) n = OB_DIAG_COUNT;
+  OB_CUDA(cudaMemcpyAsync(host_out, p->diag, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                          (cudaStream_t)stream));
   return OB_OK;
 }
 

@@ -497,106 +497,114 @@ __global__ void __launch_bounds__(TC) k_thomas(GridK g, ThomasK t, const cplx<T>
 // Single-precision tridiagonal solve over the short-wave column blocks, with
 // the level count NZ a compile-time constant: a twisted factorisation (one
 // elimination from the top and one from the bottom, two independent chains
-// per column, meeting at NZ/2 - 1) with its factors held in registers and
-// every loop unrolled, and each level's coefficients (negs, rho, a, c,
-// rounded to float on the host) one broadcast float4 from shared memory.
-// Shared memory holds only the staged (re, im) pairs of the CTA's columns, so
-// about 1.5x the columns of k_thomas<float, TC, float> are in flight per SM,
-// each with under half its instructions per level and half its dependent
-// chain.  The diagonal term b = negs - k^2 rho is formed in float.  Blocks flagged in `skip` (the
-// long-wave blocks, the zero mode's among them) are left to the double
-// launch.  No residual diagnostics: the solves that record them run k_thomas.
-// dh and ph may alias (a CTA reads only its own columns before writing them).
+// per column, meeting at NZ/2 - 1), each chain on its own thread: threads
+// [0, TC) run the top chains of the CTA's TC columns and [TC, 2 TC) the
+// bottom ones, with their factors in registers and every loop unrolled, and
+// each level's coefficients (negs, rho, a, c, rounded to float on the host)
+// one broadcast float4 from shared memory.  The two chains of a column meet
+// through shared memory (the 2 x 2 solve at levels NZ/2 - 1, NZ/2), then
+// substitute back each on its own half.  Same operations per chain as one
+// thread running both, so the same results; twice the warps per SM and half
+// the dependent chain per thread.  The diagonal term b = negs - k^2 rho is
+// formed in float.  Blocks flagged in `skip` (the long-wave blocks, the zero
+// mode's among them) are left to the double launch.  No residual
+// diagnostics: the solves that record them run k_thomas.  dh and ph may
+// alias (a CTA reads only its own columns before writing them).
 // CTAs per SM that the staged columns' shared memory allows (TC = 32), which
 // the register bound matches
 template <int NZ>
 constexpr int thomas_f32_blocks() { return NZ <= 64 ? 12 : 10; }
 template <int NZ, int TC>
-__global__ void __launch_bounds__(TC, thomas_f32_blocks<NZ>()) k_thomas_f32(GridK g, const float4* __restrict__ coef,
-                                                   const double* __restrict__ kxd,
-                                                   const double* __restrict__ kyd, float scale,
-                                                   const cplx<float>* dh, cplx<float>* ph,
-                                                   const unsigned char* __restrict__ skip) {
+__global__ void __launch_bounds__(2 * TC, thomas_f32_blocks<NZ>()) k_thomas_f32(
+    GridK g, const float4* __restrict__ coef, const double* __restrict__ kxd,
+    const double* __restrict__ kyd, float scale, const cplx<float>* dh, cplx<float>* ph,
+    const unsigned char* __restrict__ skip) {
   constexpr int P = NZ + 1;  // padded column stride (bank spread)
+  constexpr int MT = NZ / 2 - 1;
+  constexpr int NT = 2 * TC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sco = reinterpret_cast<float4*>(smem_raw);          // NZ coefficient quadruples
   cplx<float>* sc = reinterpret_cast<cplx<float>*>(sco + NZ);  // TC * P staged pairs
+  __shared__ float meet[2][TC][3];  // (f, d'.re, d'.im) of each chain at its last level
   const long blk = blockIdx.x;
   if (skip[blk]) return;  // uniform across the block
   const long ncols = (long)g.nxh * g.ny;
   const long c0 = blk * TC;
   const int ncl = (int)min((long)TC, ncols - c0);
   const long base = c0 * NZ;
-  for (int k = threadIdx.x; k < NZ; k += TC) cp_async(&sco[k], &coef[k], 16);
-  for (int cl = 0; cl < ncl; ++cl)
-    for (int k = threadIdx.x; k < NZ; k += TC)
-      cp_async(&sc[cl * P + k], dh + base + (long)cl * NZ + k, 8);
+  for (int k = threadIdx.x; k < NZ; k += NT) cp_async(&sco[k], &coef[k], 16);
+  for (int e = threadIdx.x; e < ncl * NZ; e += NT) {
+    const int cl = e / NZ, k = e - cl * NZ;
+    cp_async(&sc[cl * P + k], dh + base + e, 8);
+  }
   cp_commit();
   cp_wait<0>();
   __syncthreads();
-  const int cl = threadIdx.x;
+  const int cl = threadIdx.x % TC;
+  const int h = threadIdx.x / TC;  // 0: top chain, 1: bottom chain
+  const bool top = h == 0;
+  float f[MT + 1];  // top: cp at level t; bottom: ap at level NZ - 1 - t
+  float dr = 0.0f, di = 0.0f;
+  cplx<float>* s = sc + cl * P;
   if (cl < ncl) {
     const long col = c0 + cl;
     const int kxi = (int)(col / g.ny);
     const int kyi = (int)(col - (long)kxi * g.ny);
     const double kx = kxd[kxi], ky = kyd[kyi];
     const float ksq = (float)arn(mrn(kx, kx), mrn(ky, ky));
-    cplx<float>* s = sc + cl * P;
-    // twisted factorisation: elimination from the top over levels 0 .. MT
-    // and from the bottom over NZ-1 .. MT+1, two independent chains; x_MT
-    // from the 2 x 2 system where they meet, then substitution both ways.
-    //   top:    cp_k = c_k / (b_k - a_k cp_{k-1}),  x_k = dp_k - cp_k x_{k+1}
-    //   bottom: ap_k = a_k / (b_k - c_k ap_{k+1}),  x_k = dq_k - ap_k x_{k-1}
-    constexpr int MT = NZ / 2 - 1;
-    float f[NZ];  // cp (k <= MT) and ap (k > MT)
-    float tr = 0.0f, ti = 0.0f, br = 0.0f, bi = 0.0f;
+    //   top:    cp_k = c_k / (b_k - a_k cp_{k-1}),  dp_k = (d_k - a_k dp_{k-1}) / (...)
+    //   bottom: ap_k = a_k / (b_k - c_k ap_{k+1}),  dq_k = (d_k - c_k dq_{k+1}) / (...)
 #pragma unroll
     for (int t = 0; t <= MT; ++t) {
-      const int kt = t, kb = NZ - 1 - t;
-      const float4 qt = sco[kt], qb = sco[kb];  // (negs, rho, a, c)
-      const float btt = srn(qt.x, mrn(ksq, qt.y)), bbb = srn(qb.x, mrn(ksq, qb.y));
-      const float it = rcprn(t == 0 ? btt : srn(btt, mrn(qt.z, f[kt - (t > 0)])));
-      const float ib = rcprn(t == 0 ? bbb : srn(bbb, mrn(qb.w, f[kb + (t > 0)])));
-      f[kt] = mrn(qt.w, it);
-      f[kb] = mrn(qb.z, ib);
-      const cplx<float> dt = s[kt], db = s[kb];
-      tr = mrn(t == 0 ? dt.x : srn(dt.x, mrn(qt.z, tr)), it);
-      ti = mrn(t == 0 ? dt.y : srn(dt.y, mrn(qt.z, ti)), it);
-      br = mrn(t == 0 ? db.x : srn(db.x, mrn(qb.w, br)), ib);
-      bi = mrn(t == 0 ? db.y : srn(db.y, mrn(qb.w, bi)), ib);
-      s[kt] = mk<float>(tr, ti);
-      s[kb] = mk<float>(br, bi);
+      const int k = top ? t : NZ - 1 - t;
+      const float4 q = sco[k];  // (negs, rho, a, c)
+      const float el = top ? q.z : q.w, fa = top ? q.w : q.z;
+      const float bk = srn(q.x, mrn(ksq, q.y));
+      const float iv = rcprn(t == 0 ? bk : srn(bk, mrn(el, f[t > 0 ? t - 1 : 0])));
+      f[t] = mrn(fa, iv);
+      const cplx<float> d = s[k];
+      dr = mrn(t == 0 ? d.x : srn(d.x, mrn(el, dr)), iv);
+      di = mrn(t == 0 ? d.y : srn(d.y, mrn(el, di)), iv);
+      s[k] = mk<float>(dr, di);
       // loads may run ahead within a group of four levels, not further: the
       // unrolled sweep would otherwise hoist every level's loads into
       // registers that the factors need
       if ((t & 3) == 3) asm volatile("" ::: "memory");
     }
+    meet[h][cl][0] = f[MT];
+    meet[h][cl][1] = dr;
+    meet[h][cl][2] = di;
+  }
+  __syncthreads();
+  if (cl < ncl) {
     // meeting point: x_MT = dp_MT - cp_MT x_{MT+1},  x_{MT+1} = dq_{MT+1} - ap_{MT+1} x_MT
-    const float den = rcprn(srn(1.0f, mrn(f[MT], f[MT + 1])));
-    float xr = mrn(srn(tr, mrn(f[MT], br)), den);
-    float xi = mrn(srn(ti, mrn(f[MT], bi)), den);
-    float yr = srn(br, mrn(f[MT + 1], xr)), yi = srn(bi, mrn(f[MT + 1], xi));
-    s[MT] = mk<float>(xr, xi);
-    s[MT + 1] = mk<float>(yr, yi);
+    const float cpm = meet[0][cl][0], tr = meet[0][cl][1], ti = meet[0][cl][2];
+    const float apm = meet[1][cl][0], br = meet[1][cl][1], bi = meet[1][cl][2];
+    const float den = rcprn(srn(1.0f, mrn(cpm, apm)));
+    float xr = mrn(srn(tr, mrn(cpm, br)), den);
+    float xi = mrn(srn(ti, mrn(cpm, bi)), den);
+    if (!top) {
+      xr = srn(br, mrn(apm, xr));
+      xi = srn(bi, mrn(apm, xi));
+    }
+    s[top ? MT : MT + 1] = mk<float>(xr, xi);
 #pragma unroll
     for (int t = 1; t <= MT; ++t) {
-      const int kt = MT - t, kb = MT + 1 + t;
-      const cplx<float> dt = s[kt], db = s[kb];
-      xr = srn(dt.x, mrn(f[kt], xr));
-      xi = srn(dt.y, mrn(f[kt], xi));
-      yr = srn(db.x, mrn(f[kb], yr));
-      yi = srn(db.y, mrn(f[kb], yi));
-      s[kt] = mk<float>(xr, xi);
-      s[kb] = mk<float>(yr, yi);
+      const int k = top ? MT - t : MT + 1 + t;
+      const cplx<float> d = s[k];
+      const float fk = f[MT - t];
+      xr = srn(d.x, mrn(fk, xr));
+      xi = srn(d.y, mrn(fk, xi));
+      s[k] = mk<float>(xr, xi);
       if ((t & 3) == 0) asm volatile("" ::: "memory");
     }
   }
   __syncthreads();
-  for (int c = 0; c < ncl; ++c)
-    for (int k = threadIdx.x; k < NZ; k += TC) {
-      const cplx<float> v = sc[c * P + k];
-      ph[base + (long)c * NZ + k] = mk<float>(v.x * scale, v.y * scale);
-    }
+  for (int e = threadIdx.x; e < ncl * NZ; e += NT) {
+    const int c = e / NZ, k = e - c * NZ;
+    const cplx<float> v = sc[c * P + k];
+    ph[base + e] = mk<float>(v.x * scale, v.y * scale);
+  }
 }
 
 enum IyMode { IY_GRAD = 0, IY_FIELDS = 1 };
@@ -1353,6 +1361,9 @@ __global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, 
   for (int k0 = 0; k0 < nz; k0 += 32) {
     const int k = k0 + lane;
     const bool kin = k < nz;
+    // per-level constants of this thread's level, once per chunk
+    const float dth0k = (adv && kin) ? (float)s.dth0[k] : 0.0f;
+    const float heatz = (heat && kin) ? (float)s.heat_z[k] : 0.0f;
     auto at = [&](int ii, int jj, int f_) -> float {  // cell (ii, jj, k) of field f_
       return f_ < 3 ? fptr(f_)[(ii * ny + jj) * nz + k] : w[(ii * ny + jj) * nzw + k];
     };
@@ -1469,7 +1480,7 @@ __global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, 
             xv = (qv[4] - qv[2]) * inv2dx;
             yv = (Pv[pc + kXwCols] - Pv[pc - kXwCols]) * inv2dy;
           }
-          tt = -(uc * xt + vc * yt + wc * (czt + (float)s.dth0[k]));
+          tt = -(uc * xt + vc * yt + wc * (czt + dth0k));
           tu = -(uc * xu + vc * yu + wc * czu);
           tv = -(uc * xv + vc * yv + wc * czv);
         }
@@ -1481,7 +1492,7 @@ __global__ void __launch_bounds__(256, 3) k_slow_xw(GridK g, SlowK s, int mask, 
           tu = tu + dmp_u[o];
           tv = tv + dmp_v[o];
         }
-        if (heat) tt = tt + (float)s.heat_r[col] * (float)s.heat_z[k];
+        if (heat) tt = tt + (float)s.heat_r[col] * heatz;
         if (OUTMODE == 0) {
           uo[o] = uc + dts * tu;
           vo[o] = vc + dts * tv;

@@ -67,7 +67,7 @@ __host__ __device__ constexpr size_t fx4_smem() {
   return (size_t)kX4Tw * sizeof(cplx<T>) + (r1 > xs ? r1 : xs);
 }
 template <class T, int ZC>
-constexpr int fx4_min_blocks() { return ZC >= 8 ? 1 : 2; }
+constexpr int fx4_min_blocks() { return (sizeof(T) == 8 || ZC >= 8) ? 1 : 2; }
 
 // Forward x-pencil kernel (k_fx3 semantics at nx = 1024): rho-weighting,
 // vertical flux divergence (STAGE: of w + sdt b_half), R2C along x;
@@ -179,18 +179,20 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
   __syncthreads();  // every gather done: the exchange blocks reuse the tiles' space
   yr_pass2<T, false>(a, t, w32, ex + grp * kWEx);
 
-  // 3. R2C split: a[s] = Z[k], k = 16 (s + 16 p) + k2
+  // 3. R2C split: a[s] = Z[k], k = 16 (s + 16 p) + k2.  The lanes with
+  //    k2 > 0 read their partner values only from lanes with k2 > 0, and the
+  //    two lanes with k2 = 0 only from each other, so each lane offers the
+  //    register its readers need and one shuffle pair per slot serves all.
   const int k2 = t & 15, p = t >> 4;
-  const int partner = k2 ? (16 - k2) + 16 * (1 - p) : t;
+  const int partner = k2 ? (16 - k2) + 16 * (1 - p) : (t ^ 16);
   __syncthreads();  // every exchange read: the spectra reuse their space
 #pragma unroll
   for (int s = 0; s < 16; ++s) {
-    const T p1x = __shfl_sync(0xffffffffu, a[15 - s].x, partner);
-    const T p1y = __shfl_sync(0xffffffffu, a[15 - s].y, partner);
-    const T p2x = __shfl_sync(0xffffffffu, a[(16 - s) & 15].x, t ^ 16);
-    const T p2y = __shfl_sync(0xffffffffu, a[(16 - s) & 15].y, t ^ 16);
+    const cplx<T> offer = k2 ? a[15 - s] : a[(16 - s) & 15];
+    const T px = __shfl_sync(0xffffffffu, offer.x, partner);
+    const T py = __shfl_sync(0xffffffffu, offer.y, partner);
     const cplx<T> zk = a[s];
-    const cplx<T> zm = k2 ? mk<T>(p1x, p1y) : (s == 0 ? a[0] : mk<T>(p2x, p2y));
+    const cplx<T> zm = (k2 == 0 && s == 0) ? a[0] : mk<T>(px, py);
     const cplx<T> zc = conjg(zm);
     const cplx<T> E = scl(add(zk, zc), (T)0.5);
     const cplx<T> D = sub(zk, zc);
@@ -203,13 +205,18 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
   __syncthreads();
 
   // 4. X0 = i kx' U + D, X1 = V, two adjacent levels per thread (16-byte
-  //    stores of FP32 pairs where the levels start on an even index)
+  //    stores of FP32 pairs where the levels start on an even index).  Each
+  //    group of 8 ZC threads covers 16 consecutive k at every level pair:
+  //    a half-warp reads 16 k of one pair (distinct banks, BP odd), a warp
+  //    stores whole 32-byte runs of two pairs per k.
   const bool st2 = sizeof(T) == 4 && (nz & 1) == 0 &&
                    ((reinterpret_cast<size_t>(X0) | reinterpret_cast<size_t>(X1)) & 15) == 0;
-  for (int e = tid; e < (M + 1) * (ZC / 2); e += NT) {
-    const int k = e / (ZC / 2), jj = 2 * (e - k * (ZC / 2));
+  constexpr int G = 16 * (ZC / 2);  // threads of one 16-k group
+  for (int e = tid; e < ((M + 1 + 15) / 16) * G; e += NT) {
+    const int grp16 = e / G, r = e - grp16 * G;
+    const int k = 16 * grp16 + (r & 15), jj = 2 * (r >> 4);
     const int z = z0 + jj;
-    if (z >= nz) continue;
+    if (k > M || z >= nz) continue;
     const bool two = z + 1 < nz;
     const T kk = (k == M) ? (T)0 : (T)kxd[k];
     const int o = (k * ny + y) * nz + z;
@@ -234,11 +241,14 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
 
 // ---- inverse x: k_ix4 -------------------------------------------------------------
 // Columns (warps): [0, ZC] phi at levels z0-1 .. z0+ZC-1 (one halo level),
-// [ZC+1, 2ZC] d/dx phi, [2ZC+1, 3ZC] d/dy phi (psi~).  The state the
-// correction reads is not staged in shared memory: it is prefetched into L2
-// when the CTA starts and loaded once the transforms are done.
+// [ZC+1, 2ZC] d/dx phi, [2ZC+1, 3ZC] d/dy phi (psi~).  At ZC = 8 the CTA has
+// the SM to itself (registers), so the state tiles the correction reads
+// (u, v, w) are staged in shared memory too, requested with the spectra and
+// landing during the transforms; at ZC = 2 and 4 (several CTAs per SM) they
+// are prefetched into L2 and loaded into registers before the last barrier.
 template <int ZC>
 struct Ix4Size {
+  static constexpr bool SST = (ZC == 8);  // state tiles in shared memory
   static constexpr int BG = 3 * ZC + 1;  // columns (warps)
   static constexpr int BI = 2 * ZC + 1;  // loaded spectral columns: phi (with halo), psi
   static constexpr int SR = x4_stride<ZC>();
@@ -246,8 +256,9 @@ struct Ix4Size {
   static constexpr size_t xi = (size_t)(kX4M + 1) * BI * 8;
   static constexpr size_t ex = (size_t)BG * kWEx * 8;
   static constexpr size_t zr = (size_t)BG * SR * 4;
-  static constexpr size_t total =
-      tables + (xi > ex ? (xi > zr ? xi : zr) : (ex > zr ? ex : zr));
+  static constexpr size_t regA = xi > ex ? (xi > zr ? xi : zr) : (ex > zr ? ex : zr);
+  static constexpr size_t state = SST ? (size_t)kX4N * (3 * ZC + 1) * 4 : 0;
+  static constexpr size_t total = tables + regA + state;
 };
 template <int ZC>
 constexpr int ix4_min_blocks() { return ZC >= 8 ? 1 : 2; }
@@ -275,6 +286,10 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
   cplx<float>* XI = reinterpret_cast<cplx<float>*>(regA);  // [M + 1][BI]
   cplx<float>* ex = reinterpret_cast<cplx<float>*>(regA);  // BG x 16 x 33
   float* ZR = reinterpret_cast<float*>(regA);              // [BG][SR] real outputs
+  constexpr bool SST = SZ::SST;
+  float* SU = reinterpret_cast<float*>(regA + SZ::regA);  // [x][ZC] (SST)
+  float* SV = SU + N * ZC;                                // [x][ZC]
+  float* SW = SV + N * ZC;                                // [x][ZC + 1]
   const int ny = g.ny, nz = g.nz;
   const int y = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
@@ -297,17 +312,52 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
     }
   }
   cp_commit();
+  if constexpr (SST) {
+    // u, v: 16-byte copies where the chunk is whole and the rows start on 16
+    // bytes, 4-byte copies otherwise; w: 4-byte copies (row stride nz + 1)
+    const bool vec = z0 + ZC <= nz && (nz & 3) == 0 &&
+                     ((reinterpret_cast<size_t>(u_in) | reinterpret_cast<size_t>(v_in)) & 15) == 0;
+    if (vec) {
+      for (int e = tid; e < N * (ZC / 4); e += NT) {
+        const int x = e / (ZC / 4), q = e - x * (ZC / 4);
+        const int gi = (x * ny + y) * nz + z0 + 4 * q;
+        cp_async(&SU[x * ZC + 4 * q], u_in + gi, 16);
+        cp_async(&SV[x * ZC + 4 * q], v_in + gi, 16);
+      }
+    } else {
+      for (int e = tid; e < N * ZC; e += NT) {
+        const int x = e / ZC, j = e - x * ZC;
+        const int z = z0 + j;
+        const bool ok = z < nz;
+        const int gi = (x * ny + y) * nz + (ok ? z : 0);
+        copy_or_zero(&SU[e], u_in + gi, ok);
+        copy_or_zero(&SV[e], v_in + gi, ok);
+      }
+    }
+    for (int e = tid; e < N * (ZC + 1); e += NT) {
+      const int x = e / (ZC + 1), j = e - x * (ZC + 1);
+      const int z = z0 + j;  // half levels z0 .. z0+ZC
+      const bool ok = z <= nz;
+      copy_or_zero(&SW[e], w_in + (x * ny + y) * (nz + 1) + (ok ? z : 0), ok);
+    }
+    cp_commit();
+  }
   for (int x = tid; x < N; x += NT) {
     const int c = x * ny + y;
-    prefetch_run(u_in + c * nz + z0, u_in + c * nz + zl);
-    prefetch_run(v_in + c * nz + z0, v_in + c * nz + zl);
-    prefetch_run(w_in + c * (nz + 1) + z0, w_in + c * (nz + 1) + zl + 1);
+    if (!SST) {
+      prefetch_run(u_in + c * nz + z0, u_in + c * nz + zl);
+      prefetch_run(v_in + c * nz + z0, v_in + c * nz + zl);
+      prefetch_run(w_in + c * (nz + 1) + z0, w_in + c * (nz + 1) + zl + 1);
+    }
     if (STAGE) prefetch_run(bh + c * (nz + 1) + z0, bh + c * (nz + 1) + zl + 1);
     if (MODE == IX_REFINE) prefetch_run(phi_out + c * nz + z0, phi_out + c * nz + zl);
   }
   x4_tables<float>(ytw, twN, w32, twx, tid, NT);
   for (int i = tid; i <= M; i += NT) kxs[i] = (i == M) ? 0.0f : (float)kxd[i];
-  cp_wait<0>();
+  if constexpr (SST)
+    cp_wait<1>();  // the spectra (the state tiles may still be in flight)
+  else
+    cp_wait<0>();
   __syncthreads();
 
   // 2. gather with the C2R pre-process fused: a[q] = Z[t + 32 q] of column grp
@@ -361,54 +411,74 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
                                       reinterpret_cast<size_t>(u_in) |
                                       reinterpret_cast<size_t>(v_in)) & 7) == 0;
   float su[NP][2], sv[NP][2], sw[NP][2], gg[NP][2], lid[NP];
-#pragma unroll
-  for (int i = 0; i < NP; ++i) {
-    const int e = tid + i * NT;
-    const int x = e / (ZC / 2), j = 2 * (e - x * (ZC / 2));
-    const int z = z0 + j;
-    su[i][0] = su[i][1] = sv[i][0] = sv[i][1] = sw[i][0] = sw[i][1] = 0.0f;
-    gg[i][0] = gg[i][1] = lid[i] = 0.0f;
-    if (e >= NPR || z >= nz) continue;
-    const bool two = z + 1 < nz;
-    const int col = x * ny + y;
-    const int idx = col * nz + z;
-    const int wi = col * (nz + 1) + z;
-    if (two && st2) {
-      const float2 a2 = *reinterpret_cast<const float2*>(&u_in[idx]);
-      const float2 b2 = *reinterpret_cast<const float2*>(&v_in[idx]);
-      su[i][0] = a2.x;
-      su[i][1] = a2.y;
-      sv[i][0] = b2.x;
-      sv[i][1] = b2.y;
-    } else {
-      su[i][0] = u_in[idx];
-      sv[i][0] = v_in[idx];
-      if (two) {
-        su[i][1] = u_in[idx + 1];
-        sv[i][1] = v_in[idx + 1];
+  auto load_state = [&]() {
+  #pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      const int e = tid + i * NT;
+      const int x = e / (ZC / 2), j = 2 * (e - x * (ZC / 2));
+      const int z = z0 + j;
+      su[i][0] = su[i][1] = sv[i][0] = sv[i][1] = sw[i][0] = sw[i][1] = 0.0f;
+      gg[i][0] = gg[i][1] = lid[i] = 0.0f;
+      if (e >= NPR || z >= nz) continue;
+      const bool two = z + 1 < nz;
+      const int col = x * ny + y;
+      const int idx = col * nz + z;
+      const int wi = col * (nz + 1) + z;
+      if constexpr (SST) {
+        // the state comes from the shared tiles; the lid too
+        if ((two ? z + 1 : z) == nz - 1 && STAGE) lid[i] = bh[col * (nz + 1) + nz];
+        if (STAGE) {
+          gg[i][0] = bh[wi];
+          if (two) gg[i][1] = bh[wi + 1];
+        } else if (MODE == IX_REFINE) {
+          gg[i][0] = phi_out[idx];
+          if (two) gg[i][1] = phi_out[idx + 1];
+        }
+        continue;
+      }
+      if (two && st2) {
+        const float2 a2 = *reinterpret_cast<const float2*>(&u_in[idx]);
+        const float2 b2 = *reinterpret_cast<const float2*>(&v_in[idx]);
+        su[i][0] = a2.x;
+        su[i][1] = a2.y;
+        sv[i][0] = b2.x;
+        sv[i][1] = b2.y;
+      } else {
+        su[i][0] = u_in[idx];
+        sv[i][0] = v_in[idx];
+        if (two) {
+          su[i][1] = u_in[idx + 1];
+          sv[i][1] = v_in[idx + 1];
+        }
+      }
+      sw[i][0] = w_in[wi];
+      if (two) sw[i][1] = w_in[wi + 1];
+      if (STAGE) {
+        gg[i][0] = bh[wi];
+        if (two) gg[i][1] = bh[wi + 1];
+      } else if (MODE == IX_REFINE) {
+        gg[i][0] = phi_out[idx];
+        if (two) gg[i][1] = phi_out[idx + 1];
+      }
+      // the lid, level nz, follows the column's top level nz - 1
+      if ((two ? z + 1 : z) == nz - 1) {
+        lid[i] = w_in[col * (nz + 1) + nz];
+        if (STAGE) lid[i] = (float)arn((double)lid[i], mrn(sdt, (double)bh[col * (nz + 1) + nz]));
       }
     }
-    sw[i][0] = w_in[wi];
-    if (two) sw[i][1] = w_in[wi + 1];
-    if (STAGE) {
-      gg[i][0] = bh[wi];
-      if (two) gg[i][1] = bh[wi + 1];
-    } else if (MODE == IX_REFINE) {
-      gg[i][0] = phi_out[idx];
-      if (two) gg[i][1] = phi_out[idx + 1];
-    }
-    // the lid, level nz, follows the column's top level nz - 1
-    if ((two ? z + 1 : z) == nz - 1) {
-      lid[i] = w_in[col * (nz + 1) + nz];
-      if (STAGE) lid[i] = (float)arn((double)lid[i], mrn(sdt, (double)bh[col * (nz + 1) + nz]));
-    }
-  }
+  };
+  // SST: only b_half or phi come from global memory, loaded before the
+  // barrier; otherwise the state is loaded after it, once the transform's
+  // registers are free (several CTAs per SM cover the latency)
+  if constexpr (SST) load_state();
   __syncthreads();  // every exchange read: the outputs reuse their space
   float* zr = ZR + grp * SR + 2 * k2 + 512 * p;
 #pragma unroll
   for (int jj = 0; jj < 16; ++jj)
     *reinterpret_cast<float2*>(zr + 32 * jj) = make_float2(a[jj].x, a[jj].y);
+  if constexpr (SST) cp_wait<0>();  // this thread's state copies have landed
   __syncthreads();
+  if constexpr (!SST) load_state();
 
   // 3. velocity correction
   const float dzt = (float)g.dz;
@@ -430,7 +500,20 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
     const float gy0 = ZR[(2 * ZC + 1 + j) * SR + x], gy1 = ZR[(2 * ZC + 2 + j) * SR + x];
     const float gz0 = (z >= 1) ? drn(srn(ph0, phb), dzt) : 0.0f;
     const float gz1 = drn(srn(ph1, ph0), dzt);
-    float w0 = sw[i][0], w1 = sw[i][1];
+    float w0, w1;
+    if constexpr (SST) {
+      const float2 u2 = *reinterpret_cast<const float2*>(&SU[x * ZC + j]);
+      const float2 v2 = *reinterpret_cast<const float2*>(&SV[x * ZC + j]);
+      su[i][0] = u2.x;
+      su[i][1] = u2.y;
+      sv[i][0] = v2.x;
+      sv[i][1] = v2.y;
+      w0 = SW[x * (ZC + 1) + j];
+      w1 = SW[x * (ZC + 1) + j + 1];
+    } else {
+      w0 = sw[i][0];
+      w1 = sw[i][1];
+    }
     if (STAGE) {
       w0 = (float)arn((double)w0, mrn(sdt, (double)gg[i][0]));
       w1 = (float)arn((double)w1, mrn(sdt, (double)gg[i][1]));
@@ -454,7 +537,16 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
     w_out[wi] = w0 - gz0;
     if (two) w_out[wi + 1] = w1 - gz1;
     const int zt = two ? z + 1 : z;
-    if (zt == nz - 1 && (STAGE || w_out != w_in)) w_out[col * (nz + 1) + nz] = lid[i];
+    if (zt == nz - 1 && (STAGE || w_out != w_in)) {
+      // SST: lid holds b_half at the lid (STAGE) and the level-nz w is in
+      // the tile; otherwise lid is the finished lid value
+      float wt = lid[i];
+      if constexpr (SST) {
+        const float wl = SW[x * (ZC + 1) + (nz - z0)];
+        wt = STAGE ? (float)arn((double)wl, mrn(sdt, (double)lid[i])) : wl;
+      }
+      w_out[col * (nz + 1) + nz] = wt;
+    }
   }
 }
 

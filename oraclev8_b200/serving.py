@@ -55,6 +55,7 @@ class RunRequest:
     dx: float = 10e3
     lz: float = 16e3
     resume: Optional[dict] = None  # snapshot (oraclev8_b200.snapshot) to continue from
+    cfl: float = 0.8               # advective CFL number of the time step
 
     @property
     def start_step(self) -> int:
@@ -70,7 +71,7 @@ class RunRequest:
 
     @property
     def nsteps(self) -> int:
-        return max(1, math.ceil(self.hours * 3600.0 / (0.8 * self.dx / self.vmax) - 1e-9))
+        return max(1, math.ceil(self.hours * 3600.0 / (self.cfl * self.dx / self.vmax) - 1e-9))
 
     @property
     def dt(self) -> float:
@@ -86,11 +87,12 @@ class RunRequest:
 
 
 def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: float = 0.0,
-                  fp32r_frac: float = 1.0) -> "list[RunRequest]":
+                  fp32r_frac: float = 1.0, cfl: float = 0.8) -> "list[RunRequest]":
     """``count`` requests from a seeded stream.  ``hours``: a fixed run length
     or a (lo, hi) uniform range.  ``rate`` > 0 gives Poisson arrivals at that
     many requests per second (else all arrive at 0); ``fp32r_frac`` < 1 tags
-    that fraction FP32-refined and the rest FP64 (``precision`` ignored)."""
+    that fraction FP32-refined and the rest FP64 (``precision`` ignored).
+    ``cfl``: dt = cfl dx / Vmax (0.8 in the ensemble and serving workloads)."""
     rng = np.random.default_rng(seed)
     t, out = 0.0, []
     for i in range(count):
@@ -106,7 +108,7 @@ def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: fl
             prec = "fp32r" if rng.uniform() < fp32r_frac else "fp64"
         if rate > 0.0:
             t += float(rng.exponential(1.0 / rate))
-        out.append(RunRequest(i, n, nz, vmax, rmax, b, lat, h, prec, t))
+        out.append(RunRequest(i, n, nz, vmax, rmax, b, lat, h, prec, t, cfl=cfl))
     return out
 
 
@@ -201,6 +203,9 @@ class _Active:
     bytes: int = 0
     t: float = 0.0           # model time after the launched steps
     snaps: list = field(default_factory=list)  # snapshot copies in flight
+    flag: Optional[torch.Tensor] = None  # pinned copy of the diagnostics block
+    blown: bool = False      # the blow-up flag was seen: no further chunks
+    launched: int = 0        # steps launched
 
 
 class ServingEngine:
@@ -272,8 +277,10 @@ class ServingEngine:
                 graphs[tail] = integ.capture(state, req.dt, tail)
         rec = RunRecord(req.rid, req.n, req.nz, req.precision, req.nsteps, req.cells,
                         req.arrival_s)
+        from . import _lib as L
+        flag = torch.zeros(L.DIAG_COUNT, dtype=torch.float64, pin_memory=True)
         return _Active(req, rec, integ, state, stream, graphs, left,
-                       bytes=footprint_bytes(req), t=float(state.t))
+                       bytes=footprint_bytes(req), t=float(state.t), flag=flag)
 
     def _launch(self, a: _Active) -> None:
         k = min(self.chunk, a.left)
@@ -282,10 +289,15 @@ class ServingEngine:
         if a.integ._fast:  # t advances once per step, as the step loop adds it
             for _ in range(k):
                 a.t = a.t + a.req.dt
+        # the graph's last step updated the plan's blow-up flag: copy the
+        # diagnostics block to the run's pinned buffer behind it
+        with torch.cuda.stream(a.stream):
+            a.integ.plan.read_diag_async(a.flag)
         ev = torch.cuda.Event()
         ev.record(a.stream)
         a.events.append(ev)
         a.left -= k
+        a.launched += k
         n = self.snapshot_every
         if n and (a.req.nsteps - a.left) // n > before // n:
             with torch.cuda.stream(a.stream):
@@ -298,6 +310,7 @@ class ServingEngine:
 
     def _retire(self, a: _Active, now: float) -> RunRecord:
         a.rec.done_s = now
+        a.rec.steps = a.launched  # steps this engine ran (fewer for a blown-up run)
         self._drain_snapshots(a, wait=True)
         # the last step of every step graph runs the diagnostics reductions,
         # which keep the plan's sticky blow-up flag (the run's work is done,
@@ -391,6 +404,12 @@ class ServingEngine:
                         a.events = [e for e in a.events if not e.query()]
                     if a.snaps:
                         self._drain_snapshots(a)
+                    # a blown-up run gets no further chunks: it retires once
+                    # the chunks already queued are done, and its slot is
+                    # backfilled (the flag of a completed chunk's copy)
+                    if not a.blown and a.left > 0 and float(a.flag[14]) > 0.0:
+                        a.blown = True
+                        a.left = 0
                 busy = sum(a.req.cells for a in active if a.events)
                 for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
                     if a.left > 0 and (a.events or busy < self.inflight_cells):
@@ -480,12 +499,18 @@ def serve_serial_plain(requests: "list[RunRequest]", realtime: bool = True
         r64 = RunRequest(**{**req.__dict__, "precision": "fp64"})
         admit = time.perf_counter() - t0
         integ, state, _ = build_run(r64)
+        done, flag = 0, 0
         for n in range(r64.nsteps):
-            state, _ = integ.step(state, r64.dt, n)
+            state, dg = integ.step(state, r64.dt, n)
+            done += 1
+            # the reference's harnesses stop a run here (measure_lh82_phase3.py:
+            # 129-130): max|u| above the limit or not finite
+            if dg.blowup:
+                flag = dg.blowup
+                break
         torch.cuda.synchronize()
-        rec = RunRecord(req.rid, req.n, req.nz, "fp64", r64.nsteps, r64.cells,
+        rec = RunRecord(req.rid, req.n, req.nz, "fp64", done, r64.cells,
                         req.arrival_s, admit_s=admit, done_s=time.perf_counter() - t0)
-        flag = integ.plan.blown_up()
         if flag:
             rec.error = "non-finite state" if flag == 1 else "max|u| above the limit"
         recs.append(rec)
