@@ -968,17 +968,44 @@ def track_report(args):
     chunk = _hour_chunk(sph)
     u_env = w["coriolis"].get("u_env", 0.0)
     v_env = w["coriolis"].get("v_env", 0.0)
+    prod = args.track_physics == "production"
     runs = {}
     hs = None
     for prec in ("fp64", "fp32r"):
-        integ, base = b200_integrator(w, prec, blowup_u_max=400.0)
+        if prod:
+            # the reference's production physics (build_production_config) with
+            # the intensity cap added after every step (run_storm.py:146-172)
+            from oraclev8_b200.production_config import (TAU_CAP, VMAX_CAP_MS, BaseState,
+                                                         build_production_config)
+            from oraclev8_b200.solver import IntensityCapComponent, RK3Integrator
+            base = BaseState(nz, Lz)
+            integ = RK3Integrator(build_production_config(nx, ny, nz, Lx, Ly, Lz,
+                                                          w["coriolis"]["f"], u_env, v_env),
+                                  base, precision=prec, blowup_u_max=400.0)
+            cap = IntensityCapComponent(v_cap=VMAX_CAP_MS, tau=TAU_CAP, u_env=u_env,
+                                        v_env=v_env)
+        else:
+            integ, base = b200_integrator(w, prec, blowup_u_max=400.0)
+            cap = None
         if hs is None:
             hs = host_initial_state(w, base)
         ty = integ.dtype
         st = State(*(torch.as_tensor(a, dtype=ty).cuda() for a in
                      (hs.u, hs.v, hs.w, hs.theta_prime, hs.projection_potential)), 0.0)
-        runs[prec] = dict(integ=integ, base=base, st=st, graph=integ.capture(st, dt, chunk),
-                          last=None, last_raw=None, fixes=[])
+        runs[prec] = dict(integ=integ, base=base, st=st, cap=cap, last=None, last_raw=None,
+                          fixes=[], graph=None if prod else integ.capture(st, dt, chunk))
+
+    def advance_hour(r):
+        if r["graph"] is not None:
+            for _ in range(sph // chunk):
+                r["graph"].launch()
+            return
+        st = r["st"]
+        for _ in range(sph):
+            r["integ"].step_(st, dt)
+            ct = r["cap"].compute_tendency(st, None, None, r["base"], dt)
+            st.u.add_(ct.du_dt, alpha=dt)
+            st.v.add_(ct.dv_dt, alpha=dt)
     hours = int(args.track_hours)
     t0 = time.perf_counter()
     for h in range(hours + 1):
@@ -986,8 +1013,7 @@ def track_report(args):
             if r.get("blew_h") is not None:
                 continue
             if h > 0:
-                for _ in range(sph // chunk):
-                    r["graph"].launch()
+                advance_hour(r)
             mu = float(r["st"].u.abs().max())
             # a state that is no longer finite (or past the blow-up speed) has
             # no storm centre: the run stops there, as the reference's harness
@@ -1022,7 +1048,9 @@ def track_report(args):
     rep = _precision_report(st32, st64, runs["fp64"]["integ"].plan) if both_finite else None
     line = {"track": {
         "workload": f"{args.workload}: {nx}x{ny}x{nz}, dt={dt}s, {hours} h = {hours * sph} steps "
-                    f"in each precision, step graphs of {chunk} steps",
+                    f"in each precision, "
+                    + ("production physics (build_production_config) + intensity cap per step"
+                       if prod else f"the workload's physics, step graphs of {chunk} steps"),
         "hours_compared": len(rows) - 1,
         "blew_up_by_hour": {p: r.get("blew_h") for p, r in runs.items()},
         "hours": rows,
@@ -1093,6 +1121,9 @@ def main():
     ap.add_argument("--serving-scale", type=float, default=4.0)
     ap.add_argument("--track-hours", type=float, default=0.0,
                     help="run the FP32-refined vs FP64 hourly track comparison instead")
+    ap.add_argument("--track-physics", default="workload", choices=["workload", "production"],
+                    help="physics of the track comparison: the workload's (LH82 WS5 + buoyancy) "
+                         "or the reference's production configuration")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
     args = ap.parse_args()
     if args.track_hours > 0:

@@ -114,7 +114,8 @@ extern "C" {
 #define OB_VAR_THOMAS_FAST 18 /* FP32 sweep with a compile-time level count (1) */
 #define OB_VAR_RZC2_FX 19
 #define OB_VAR_RZC2_FY 20
-#define OB_VAR_COUNT 21
+#define OB_VAR_ZC4_FYD 21   /* FP64 residual y at ny = 1024 (register form, 0 or 2) */
+#define OB_VAR_COUNT 22
 
 #define OB_TUNE_FORCE 1  /* time the candidates even when a choice is cached */
 

@@ -226,7 +226,7 @@ struct OraclePlan {
   // register-resident pencils of the 1024-point lines (xreg4.cuh), FP32 plans:
   // forward x (stage / correction), inverse x, the FP64 residual x transform,
   // and the y pencils (ny = 1024); z-chunk, 0 = off
-  int zc4_fxs = 0, zc4_fx = 0, zc4_ix = 0, zc4_fxd = 0, zc4_fy = 0, zc4_iy = 0;
+  int zc4_fxs = 0, zc4_fx = 0, zc4_ix = 0, zc4_fxd = 0, zc4_fy = 0, zc4_iy = 0, zc4_fyd = 0;
   int slow_xw = 1;  // FP32 slow tendency marching along x (ORACLE_B200_SLOW_XW=0: gather form)
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
@@ -456,6 +456,9 @@ int xr4_attrs_zc() {
                                  (int)Ix4Size<ZC>::total));
   OB_CUDA(cudaFuncSetAttribute(k_fy4<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)Yr4Size<ZC>::total));
+  if constexpr (ZC == 2)
+    OB_CUDA(cudaFuncSetAttribute(k_fy4d, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Yr4dSize::total));
   OB_CUDA(cudaFuncSetAttribute(k_iy4<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)Yr4Size<ZC>::total));
   return OB_OK;
@@ -849,6 +852,9 @@ void ix2(const OraclePlan* p, int zc, const cplx<T>* phs, const cplx<T>* psi, co
 }
 
 // ---- register-resident pencils of the 1024-point lines (xreg4.cuh) --------
+template <class K>
+int resident_ctas(K kernel, int threads, size_t smem);
+
 template <class T, bool STAGE, int ZC>
 void fx4_launch(const OraclePlan* q, const float* u, const float* v, const float* w,
                 const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
@@ -871,6 +877,35 @@ void fx4(const OraclePlan* q, int zc, const float* u, const float* v, const floa
     }
   }
 }
+// Resident CTAs of a persistent kernel on the current device (occupancy API x
+// SM count), cached per (kernel, device): kernels of one signature share a
+// function-pointer type, so the cache is keyed by the pointer itself.
+std::mutex g_resident_mu;
+std::map<std::pair<const void*, int>, int> g_resident;
+
+template <class K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  {
+    std::lock_guard<std::mutex> lk(g_resident_mu);
+    auto it = g_resident.find(key);
+    if (it != g_resident.end()) return it->second;
+  }
+  int nsm = 148, per = 1;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess ||
+      per < 1) {
+    cudaGetLastError();
+    per = 1;
+  }
+  const int n = per * nsm;
+  std::lock_guard<std::mutex> lk(g_resident_mu);
+  g_resident[key] = n;
+  return n;
+}
+
 template <int MODE, int ZC>
 void ix4_launch(const OraclePlan* p, const cplx<float>* phs, const cplx<float>* psi,
                 const float* u, const float* v, const float* w, const float* bh, double sdt,
@@ -1181,7 +1216,11 @@ int refine_fy(OraclePlan* p, cudaStream_t st) {
   Cd* R2 = (Cd*)q->S2;
   cplx<float>* S3 = (cplx<float>*)p->S3;
   Launch L_(p, OB_PROF_REFINE, st);
-  if (p->zc3_fyd)
+  if (p->zc4_fyd) {
+    const int items = ((g.nz + 1) / 2) * g.nxh;
+    const int grid = std::min(items, resident_ctas(k_fy4d, 128, Yr4dSize::total));
+    k_fy4d<<<grid, 128, Yr4dSize::total, st>>>(g, R1, R2, q->ky, (const Cd*)q->twy, S3);
+  } else if (p->zc3_fyd)
     k_fy3<2, double, FY_RESID, float><<<dim3((g.nz + 1) / 2, g.nxh), 128,
                                         YrSize<2, double>::total, st>>>(
         g, R1, R2, q->ky, (const Cd*)q->twy, S3);
@@ -1663,6 +1702,7 @@ int* var_field(OraclePlan* p, int i) {
     case OB_VAR_THOMAS_FAST: return &p->thomas_fast;
     case OB_VAR_RZC2_FX: return q ? &q->zc2_fx : nullptr;
     case OB_VAR_RZC2_FY: return q ? &q->zc2_fy : nullptr;
+    case OB_VAR_ZC4_FYD: return &p->zc4_fyd;
   }
   return nullptr;
 }
@@ -1722,6 +1762,7 @@ std::vector<int> var_values(const OraclePlan* p, int i) {
     case OB_VAR_RZC2_FY:
       if (f32 && p->dbl) y2(true);
       break;
+    case OB_VAR_ZC4_FYD: list(f32 && ny == kY4N && p->dbl, {2}); break;
   }
   return v;
 }
@@ -1859,7 +1900,7 @@ int tune_impl(OraclePlan* p, cudaStream_t st) {
       RC(tune_group<T>(p, {OB_VAR_ZC4_FXD, OB_VAR_ZC3_FXD, OB_VAR_RZC2_FX}, st,
                        [&] { return refine_fx(p, (const float*)u, (const float*)v,
                                               (const float*)w, st); }));
-      RC(tune_group<T>(p, {OB_VAR_ZC3_FYD, OB_VAR_RZC2_FY}, st,
+      RC(tune_group<T>(p, {OB_VAR_ZC4_FYD, OB_VAR_ZC3_FYD, OB_VAR_RZC2_FY}, st,
                        [&] { return refine_fy(p, st); }));
     }
     const bool slow = p->advection || p->coriolis || p->heating;
@@ -2524,7 +2565,10 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     p->zc2_fy = p->prec == OB_PREC_F64 ? pick_y2_zc<double>(ny, nz) : pick_y2_zc<float>(ny, nz);
     p->zc2_iy = p->zc2_fy;
   }
-  if (p->prec == OB_PREC_F32 && ny == kY4N) p->zc4_fy = p->zc4_iy = nz >= 4 ? 4 : 2;
+  if (p->prec == OB_PREC_F32 && ny == kY4N) {
+    p->zc4_fy = p->zc4_iy = nz >= 4 ? 4 : 2;
+    p->zc4_fyd = 2;
+  }
   if (p->prec == OB_PREC_F32 && ny == kYrN) {
     p->zc3_fy = nz >= 4 ? 4 : 2;
     p->zc3_fyd = p->zc3_fy ? 2 : 0;

@@ -568,23 +568,22 @@ constexpr int yr4_min_blocks() { return ZC >= 8 ? 1 : 2; }
 // One 1024-point transform of a warp's column.  e[q] = x[2 (L + 32 q)],
 // o[q] = x[2 (L + 32 q) + 1] on entry; on exit e[j] = X[k], o[j] = X[k + 512],
 // k = 16 (j + 16 p) + k2.  ex: the warp's exchange block (free on entry).
-template <bool INV>
-__device__ __forceinline__ void y4_fft(cplx<float> (&e)[16], cplx<float> (&o)[16], int lane,
-                                       const cplx<float>* __restrict__ ytw,
-                                       const cplx<float>* __restrict__ w32,
-                                       const cplx<float>* __restrict__ tw1k,
-                                       cplx<float>* ex) {
-  yr_pass1<float, INV>(e, lane, ytw);
-  yr_pass2<float, INV>(e, lane, w32, ex);
+template <bool INV, class T = float>
+__device__ __forceinline__ void y4_fft(cplx<T> (&e)[16], cplx<T> (&o)[16], int lane,
+                                       const cplx<T>* __restrict__ ytw,
+                                       const cplx<T>* __restrict__ w32,
+                                       const cplx<T>* __restrict__ tw1k, cplx<T>* ex) {
+  yr_pass1<T, INV>(e, lane, ytw);
+  yr_pass2<T, INV>(e, lane, w32, ex);
   __syncwarp();  // every lane has read its pass-2 values out of ex
-  yr_pass1<float, INV>(o, lane, ytw);
-  yr_pass2<float, INV>(o, lane, w32, ex);
+  yr_pass1<T, INV>(o, lane, ytw);
+  yr_pass2<T, INV>(o, lane, w32, ex);
   const int k2 = lane & 15, p = lane >> 4;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    cplx<float> w = tw1k[16 * (j + 16 * p) + k2];
+    cplx<T> w = tw1k[16 * (j + 16 * p) + k2];
     if (INV) w.y = -w.y;
-    const cplx<float> wo = mul(w, o[j]);
+    const cplx<T> wo = mul(w, o[j]);
     o[j] = sub(e[j], wo);
     e[j] = add(e[j], wo);
   }
@@ -710,6 +709,92 @@ __global__ void __launch_bounds__(64 * ZC, yr4_min_blocks<ZC>()) k_iy4(
     out0[o2] = R[y * BP + j];
     out1[o2] = R[y * BP + ZC + j];
   }
+}
+
+// The defect correction's FP64 residual y transform at ny = 1024 (k_fy3
+// FY_RESID at ny = 512): d^ = FFTy(X0) + i ky' FFTy(X1) in double, zero on
+// the Nyquist rows (ky = ny/2 or kx = nx/2), stored as float.  Two levels of
+// the two fields, one warp per column: 128 threads, 32 complex doubles per
+// lane.  Rows of 2 levels (32-byte runs) against the 16-byte runs of the
+// compile-time-chunk Stockham kernel, whose FP64 tiles fit only one level.
+struct Yr4dSize {
+  static constexpr int ZC = 2, B = 2 * ZC, BP = B + 1;
+  static constexpr size_t tables = (size_t)kX4Tw * sizeof(cplx<double>);
+  static constexpr size_t rows = (size_t)kY4N * BP * sizeof(cplx<double>);
+  static constexpr size_t ex = (size_t)B * kWEx * sizeof(cplx<double>);
+  static constexpr size_t total = tables + (rows > ex ? rows : ex);
+};
+
+__global__ void __launch_bounds__(128, 2) k_fy4d(GridK g, const cplx<double>* __restrict__ in0,
+                                                 const cplx<double>* __restrict__ in1,
+                                                 const double* __restrict__ kyd,
+                                                 const cplx<double>* __restrict__ twy,
+                                                 cplx<float>* __restrict__ out0) {
+  using SZ = Yr4dSize;
+  constexpr int ZC = SZ::ZC, B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kY4N;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  cplx<double>* ytw = reinterpret_cast<cplx<double>*>(smem_dyn);
+  cplx<double>* tw1k = ytw + 512;
+  cplx<double>* w32 = tw1k + 512;
+  cplx<double>* R = reinterpret_cast<cplx<double>*>(smem_dyn + SZ::tables);  // [N][BP]
+  cplx<double>* ex = R;                                                     // B x 16 x 33
+  const int ny = g.ny, nz = g.nz;
+  const int tid = threadIdx.x;
+  const int nzc = (nz + ZC - 1) / ZC;
+  const int nitems = g.nxh * nzc;
+  x4_tables<double>(ytw, tw1k, w32, twy, tid, NT);
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+  const int kx = item / nzc;
+  const int z0 = (item - kx * nzc) * ZC;
+  if (item + (int)gridDim.x < nitems) {
+    const int nit = item + gridDim.x;
+    const int k2_ = nit / nzc, za = (nit - k2_ * nzc) * ZC, zb = min(za + ZC, nz) - 1;
+    for (int y = tid; y < N; y += NT) {
+      const int ob = (k2_ * ny + y) * nz;
+      prefetch_run(in0 + ob + za, in0 + ob + zb);
+      prefetch_run(in1 + ob + za, in1 + ob + zb);
+    }
+  }
+  for (int e = tid; e < N * B; e += NT) {
+    const int y = e / B, b = e - y * B;
+    const int f = b / ZC, j = b - f * ZC;
+    const int z = z0 + j;
+    const bool ok = z < nz;
+    copy_or_zero(&R[y * BP + b], (f == 0 ? in0 : in1) + (kx * ny + y) * nz + (ok ? z : 0), ok);
+  }
+  cp_commit();
+  cp_wait<0>();
+  __syncthreads();
+  const int c = tid >> 5, lane = tid & 31;
+  cplx<double> e[16], o[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int n = 2 * (lane + 32 * q);
+    e[q] = R[n * BP + c];
+    o[q] = R[(n + 1) * BP + c];
+  }
+  __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
+  y4_fft<false, double>(e, o, lane, ytw, w32, tw1k, ex + c * kWEx);
+  __syncthreads();  // every exchange read: the output rows reuse their space
+  const int k2 = lane & 15, p = lane >> 4;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int k = 16 * (j + 16 * p) + k2;
+    R[k * BP + c] = e[j];
+    R[(k + 512) * BP + c] = o[j];
+  }
+  __syncthreads();
+  for (int e2 = tid; e2 < N * ZC; e2 += NT) {
+    const int ky = e2 / ZC, j = e2 - ky * ZC;
+    const int z = z0 + j;
+    if (z >= nz) continue;
+    const double kk = (ky == N / 2) ? 0.0 : kyd[ky];
+    cplx<double> d = add(R[ky * BP + j], ik(kk, R[ky * BP + ZC + j]));
+    if (ky == N / 2 || kx == g.nx / 2) d = mk<double>(0.0, 0.0);
+    out0[(kx * ny + ky) * nz + z] = mk<float>((float)d.x, (float)d.y);
+  }
+  __syncthreads();  // the next item's copies reuse the rows
+  }  // item
 }
 
 }  // namespace ob

@@ -637,11 +637,50 @@ def gen_config0_long():
     np.savez_compressed(OUT / "config0_6h.npz", **out)
 
 
+# ---------------------------------------------------------------------------
+# Blow-up of the LH82 physics: config-1 parameters (dx 5 km, dz 250 m,
+# beta-plane at 20N, Holland 50 m/s / 40 km / 1.6 with the 12-km linear wind
+# decay, eyewall heating, seeded theta' noise, dt 20 s) on a 96 x 96 x 64
+# grid, stepped by the reference until max|u| exceeds 400 m/s or is not
+# finite (the test of measure_lh82_phase3.py:129-130).  Every step's max|u|
+# and max|w| are kept.  About 12 minutes on one core (--blowup).
+# ---------------------------------------------------------------------------
+
+BLOWUP = dict(nx=96, ny=96, nz=64, Lx=96 * 5e3, Ly=96 * 5e3, Lz=16e3, dt=20.0,
+              vortex=dict(Vmax=50.0, Rmax=40e3, B=1.6, f=4.99e-5),
+              coriolis=dict(f=4.99e-5, mode="beta_plane", beta=2.15e-11, periodic_taper=True),
+              advection="upwind5h", buoyancy=True,
+              heating=dict(Q_max=3.0 / 3600.0, r_eyewall=40e3, width_r=math.sqrt(2.0) * 15e3,
+                           z_peak=6e3, width_z=math.sqrt(2.0) * 2e3),
+              noise_seed=20261203, max_steps=800)
+
+
+def gen_blowup():
+    c = BLOWUP
+    base = Base(c["nz"], c["Lz"])
+    s = initial_state(c, base)
+    integ = RK3Integrator(config=build_ref_config(c), base=base)
+    mu, mw = [], []
+    blew = -1
+    for n in range(c["max_steps"]):
+        s, dg = integ.step(s, dt=c["dt"], step_number=n)
+        mu.append(float(dg.max_u))
+        mw.append(float(dg.max_w))
+        if n % 50 == 0:
+            print("step", n, mu[-1], mw[-1], flush=True)
+        if not math.isfinite(mu[-1]) or mu[-1] > 400.0:
+            blew = n
+            break
+    np.savez_compressed(OUT / "blowup_lh82.npz", config_json=np.array(json.dumps(c)),
+                        max_u=np.array(mu), max_w=np.array(mw), blew_step=np.int64(blew))
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--long", action="store_true")
     ap.add_argument("--reference", default=None, help="root of the reference tree (read above)")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--blowup", action="store_true")
     a = ap.parse_args()
     jobs = dict(components=gen_components, production=gen_production, steps=gen_steps,
                 production_storm=gen_production_storm, diagnostics=gen_diagnostics,
@@ -655,3 +694,6 @@ if __name__ == "__main__":
     if a.long:
         gen_config0_long()
         print("wrote config0_6h", flush=True)
+    if a.blowup:
+        gen_blowup()
+        print("wrote blowup_lh82", flush=True)

@@ -122,3 +122,34 @@ def test_serving_retires_a_blown_up_run_and_backfills():
     assert recs[0].error is None and recs[2].error is None
     for rid in (0, 2):
         assert all(np.isfinite(recs[rid].final[f]).all() for f in ("u", "v", "w"))
+
+
+def test_lh82_blowup_matches_the_reference(golden_dir):
+    """The LH82 physics of the mid-size workload (WS5, buoyancy, heating,
+    theta' noise, dt 20 s) on a 96 x 96 x 64 grid blows up in the reference
+    itself (blowup_lh82.npz: the reference's max|u| and max|w| of every step,
+    generated by make_golden.py --blowup).  The plain FP64 step follows the
+    reference's diagnostics step for step (within 1e-6 until 30 steps before
+    the blow-up, while round-off differences are still small against the
+    growing mode) and raises its blow-up flag at the same step."""
+    import json as _json
+    from tests.test_oracle_golden import oracle_initial_state
+    from tests.gpu_helpers import b200_config
+    from oraclev8_b200.solver import RK3Integrator
+    g = np.load(golden_dir / "blowup_lh82.npz")
+    c = _json.loads(str(g["config_json"]))
+    ref_u, ref_w, blew = g["max_u"], g["max_w"], int(g["blew_step"])
+    assert blew > 0
+    s0, _ = oracle_initial_state(c)
+    integ = RK3Integrator(b200_config(c), Base(c["nz"], c["Lz"]), precision="fp64",
+                          blowup_u_max=400.0)
+    st = _dev_state(s0, torch.float64)
+    flagged = -1
+    for n in range(blew + 1):
+        st, dg = integ.step(st, c["dt"], n)
+        if n < blew - 30:
+            assert abs(dg.max_u - ref_u[n]) <= 1e-6 * ref_u[n], (n, dg.max_u, ref_u[n])
+            assert abs(dg.max_w - ref_w[n]) <= 1e-6 * max(ref_w[n], 1.0), (n, dg.max_w, ref_w[n])
+        if dg.blowup and flagged < 0:
+            flagged = n
+    assert flagged == blew, (flagged, blew)

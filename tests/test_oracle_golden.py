@@ -314,3 +314,19 @@ def test_vortex_diagnostics_match_reference(golden_dir):
             assert same(got, c["out"]), (name, c["fn"], c["kw"], got, c["out"])
             n += 1
     assert n == 78
+
+
+def test_blowup_run_first_steps(golden_dir):
+    """The first steps of the reference's LH82 blow-up run (blowup_lh82.npz:
+    the reference stepped until max|u| > 400 m/s, make_golden.py --blowup):
+    the oracle's max|u| and max|w| follow the recorded ones."""
+    g = np.load(golden_dir / "blowup_lh82.npz")
+    c = json.loads(str(g["config_json"]))
+    assert int(g["blew_step"]) > 0 and len(g["max_u"]) == int(g["blew_step"]) + 1
+    assert not math.isfinite(g["max_u"][-1]) or g["max_u"][-1] > 400.0
+    s, (z, rho0, th0) = oracle_initial_state(c)
+    integ = O.Integrator(oracle_config(c), z, rho0, th0)
+    for n in range(3):
+        s, dg = integ.step(s, c["dt"], step_number=n)
+        np.testing.assert_allclose([dg.max_u, dg.max_w], [g["max_u"][n], g["max_w"][n]],
+                                   rtol=1e-12, atol=0)
