@@ -589,6 +589,12 @@ def run_b200(args):
                      "bytes_per_launch": kb[dom], "avg_launch_ms": dms / dn},
         "step_roofline": {"passes_per_cell": passes, "achieved": step_gbs, "peak": peak,
                           "unit": "GB/s", "frac": step_gbs / peak},
+        # every kernel class against the same peak: algorithmic bytes per
+        # launch / mean launch time (classes with a byte model only)
+        "kernel_rooflines": {c: {"achieved_gbs": kb[c] / (prof[c][0] / prof[c][1] / 1e3) / 1e9,
+                                 "frac": kb[c] / (prof[c][0] / prof[c][1] / 1e3) / 1e9 / peak,
+                                 "launches_per_step": prof[c][1] / args.steps}
+                             for c in kb if c in prof and prof[c][1] > 0},
         "kernels_ms_per_step": {c: prof[c][0] / args.steps for c in prof if prof[c][1]},
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d + 8 * 6,

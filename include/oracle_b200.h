@@ -83,6 +83,10 @@ extern "C" {
  * blow-up test of oracle_v8/measure_lh82_phase3.py:129-130).  The maxima in
  * slots 0-3 propagate NaN as NumPy's max does. */
 #define OB_DIAG_BLOWUP 14
+/* Non-zero once a kernel's bounded wait for its own staged copies ran out (it
+ * then stops early and its outputs are incomplete); oracle_b200_read_diag
+ * reports it as OB_ERR_CUDA.  It cannot happen with in-bounds copies. */
+#define OB_DIAG_STALL 15
 #define OB_DIAG_COUNT 16
 
 /* Kernel-variant choices of a plan, in this order (oracle_b200_plan_get_variants,

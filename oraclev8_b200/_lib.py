@@ -19,7 +19,7 @@ OB_TEND_ADVECTION, OB_TEND_CORIOLIS, OB_TEND_DAMPING, OB_TEND_HEATING = 1, 2, 4,
 OB_TEND_DRAG, OB_TEND_SPONGE, OB_TEND_DIFFUSION, OB_TEND_COOLING = 16, 32, 64, 128
 OB_DIFF_NONE, OB_DIFF_LAPLACIAN, OB_DIFF_BIHARMONIC = 0, 1, 2
 DIAG = dict(max_u=0, max_v=1, max_w=2, max_th=3, phi_min=4, phi_max=5, compat0=6, disc0=9,
-            last_compat=12, last_disc=13, blowup=14)
+            last_compat=12, last_disc=13, blowup=14, stall=15)
 DIAG_COUNT = 16
 
 LIB_PATH = Path(__file__).resolve().parent / "liboracle_b200.so"

@@ -17,6 +17,7 @@
 #include "pencil.cuh"
 #include "xreg.cuh"
 #include "xreg4.cuh"
+#include "slowx.cuh"
 #include "tracker.cuh"
 #include "vdiag.cuh"
 #include "init.cuh"
@@ -227,7 +228,9 @@ struct OraclePlan {
   // forward x (stage / correction), inverse x, the FP64 residual x transform,
   // and the y pencils (ny = 1024); z-chunk, 0 = off
   int zc4_fxs = 0, zc4_fx = 0, zc4_ix = 0, zc4_fxd = 0, zc4_fy = 0, zc4_iy = 0, zc4_fyd = 0;
-  int slow_xw = 1;  // FP32 slow tendency marching along x (ORACLE_B200_SLOW_XW=0: gather form)
+  // FP32 slow tendency: 0 the gather form, 1 marching along x (k_slow_xw),
+  // 4 / 8 marching along x over bulk-copied planes of 4 / 8 rows (k_slow_xt)
+  int slow_xw = 1;
   // FP64 defect correction of single-precision plans: a double-precision
   // shadow descriptor (own twiddles and spectral buffers, shared tables)
   OraclePlan* dbl = nullptr;
@@ -500,9 +503,14 @@ int set_x2_attrs() {
   return OB_OK;
 }
 
+int slow_xt_attrs(int nz);
+
 template <class T>
 int set_smem_attrs() {
   const int mx = (int)kSmemMax;
+  if constexpr (sizeof(T) == 4)
+    for (int nz : {32, 48, 64, 80})
+      if (int rc = slow_xt_attrs(nz)) return rc;
   OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_DIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_DIV_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   OB_CUDA(cudaFuncSetAttribute(k_fx<T, FX_FIELDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -1383,6 +1391,84 @@ SlowK slow_args(const OraclePlan* p) {
   return s;
 }
 
+// ---- x-marching slow tendency over bulk-copied planes (slowx.cuh) ---------
+bool slow_xt_grid(const OraclePlan* p, int r) {
+  const int nz = p->g.nz;
+  return p->prec == OB_PREC_F32 && p->advection == OB_ADV_UPWIND5H &&
+         (nz == 32 || nz == 48 || nz == 64 || nz == 80) && (r == 4 || r == 8) &&
+         p->g.ny % r == 0 && p->g.ny >= r + 6 && p->g.nx >= 7;
+}
+template <int NZ, int R>
+int slow_xt_attr() {
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<0, NZ, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SlowXt<NZ, R>::smem));
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<1, NZ, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SlowXt<NZ, R>::smem));
+  return OB_OK;
+}
+int slow_xt_attrs(int nz) {
+  int rc = OB_OK;
+  switch (nz) {
+    case 32: (rc = slow_xt_attr<32, 4>()) || (rc = slow_xt_attr<32, 8>()); break;
+    case 48: (rc = slow_xt_attr<48, 4>()) || (rc = slow_xt_attr<48, 8>()); break;
+    case 64: (rc = slow_xt_attr<64, 4>()) || (rc = slow_xt_attr<64, 8>()); break;
+    case 80: (rc = slow_xt_attr<80, 4>()) || (rc = slow_xt_attr<80, 8>()); break;
+  }
+  return rc;
+}
+// x-segment of one CTA: a multiple of 7 steps, short enough that the grid
+// holds about eight CTAs per SM (each segment re-reads 6 planes of its
+// neighbours' columns, from L2)
+int slow_xt_seg(const OraclePlan* p, int r) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int nrow = p->g.ny / r;
+  const int nseg = std::max(1, (8 * nsm + nrow - 1) / nrow);
+  int seg = (p->g.nx + nseg - 1) / nseg;
+  seg = std::max(21, (seg + 6) / 7 * 7);
+  return std::min(seg, (p->g.nx + 6) / 7 * 7);
+}
+template <int OUT, int NZ, int R>
+void slow_xt_launch(OraclePlan* p, int mask, double dts, const float* u, const float* v,
+                    const float* w, const float* th, float* uo, float* vo, float* wo,
+                    float* tho, cudaStream_t st) {
+  const int seg = slow_xt_seg(p, R);
+  const dim3 grid(p->g.ny / R, (p->g.nx + seg - 1) / seg);
+  k_slow_xt<OUT, NZ, R><<<grid, R * NZ, SlowXt<NZ, R>::smem, st>>>(
+      p->g, slow_args(p), mask, dts, seg, u, v, w, th, (const float*)p->Du, (const float*)p->Dv,
+      uo, vo, wo, tho, p->diag + OB_DIAG_STALL);
+}
+// k_slow_xt for this call, if the plan selected it and the call allows it:
+// advection on and 16-byte aligned fields (the bulk copies' rule)
+bool slow_xt_call(const OraclePlan* p, int mask, const void* u, const void* v, const void* w,
+                  const void* th) {
+  return (mask & OB_TEND_ADVECTION) && slow_xt_grid(p, p->slow_xw) &&
+         !((reinterpret_cast<size_t>(u) | reinterpret_cast<size_t>(v) |
+            reinterpret_cast<size_t>(w) | reinterpret_cast<size_t>(th)) & 15);
+}
+template <int OUT>
+bool slow_xt_launch_any(OraclePlan* p, int mask, double dts, const float* u, const float* v,
+                        const float* w, const float* th, float* uo, float* vo, float* wo,
+                        float* tho, cudaStream_t st) {
+  const int r = p->slow_xw;
+#define OB_XT(NZ)                                                                  \
+  case NZ:                                                                         \
+    if (r == 4)                                                                    \
+      slow_xt_launch<OUT, NZ, 4>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);       \
+    else                                                                           \
+      slow_xt_launch<OUT, NZ, 8>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);       \
+    return true;
+  switch (p->g.nz) {
+    OB_XT(32)
+    OB_XT(48)
+    OB_XT(64)
+    OB_XT(80)
+  }
+#undef OB_XT
+  return false;
+}
+
 template <class T, int OUT>
 int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const T* w,
               const T* th, T* uo, T* vo, T* wo, T* tho, cudaStream_t st) {
@@ -1400,7 +1486,9 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
                      (p->drag || p->sponge || p->diffusion || p->cooling);
   if constexpr (sizeof(T) == 4) {
     // the x-marching form where the grid tiles it; the gather form otherwise
-    if (p->slow_xw && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
+    if (!extra && slow_xt_call(p, mask, u, v, w, th))
+      { Launch L_(p, 5, st); slow_xt_launch_any<OUT>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st); }
+    else if (p->slow_xw && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
       { Launch L_(p, 5, st); k_slow_xw<OUT><<<dim3(p->g.ny / 8, p->g.nx / KXW), blk, 0, st>>>(
             p->g, slow_args(p), mask, dts, u, v, w, th, (const T*)p->Du, (const T*)p->Dv, uo, vo, wo, tho); }
     else if (extra)
@@ -1752,7 +1840,11 @@ std::vector<int> var_values(const OraclePlan* p, int i) {
     case OB_VAR_ZC4_FXD: list(f32 && nx == kX4N && p->dbl, {2, 4}); break;
     case OB_VAR_ZC4_FY:
     case OB_VAR_ZC4_IY: list(f32 && ny == kY4N, {2, 4, 8}); break;
-    case OB_VAR_SLOW_XW: list(true, {1}); break;
+    case OB_VAR_SLOW_XW:
+      list(true, {1});
+      list(slow_xt_grid(p, 4), {4});
+      list(slow_xt_grid(p, 8), {8});
+      break;
     case OB_VAR_THOMAS_FAST: list(true, {1}); break;
     case OB_VAR_RZC2_FX:
       if (f32 && p->dbl && p->px8_ok)
@@ -2569,6 +2661,7 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
     p->zc4_fy = p->zc4_iy = nz >= 4 ? 4 : 2;
     p->zc4_fyd = 2;
   }
+  if (slow_xt_grid(p, 4)) p->slow_xw = 4;
   if (p->prec == OB_PREC_F32 && ny == kYrN) {
     p->zc3_fy = nz >= 4 ? 4 : 2;
     p->zc3_fyd = p->zc3_fy ? 2 : 0;
@@ -2926,6 +3019,9 @@ int oracle_b200_read_diag(OraclePlan* p, double* host_out, int n, void* stream) 
   for (int s : {OB_DIAG_DISC0, OB_DIAG_DISC0 + 1, OB_DIAG_DISC0 + 2, OB_DIAG_LAST_DISC})
     buf[s] = std::sqrt(std::fmax(buf[s], 0.0) / norm);
   std::memcpy(host_out, buf, n * sizeof(double));
+  if (buf[OB_DIAG_STALL] != 0.0)
+    return fail(OB_ERR_CUDA, "a kernel's bounded wait for its staged copies ran out: the "
+                "results of the steps since are incomplete");
   if (buf[OB_DIAG_BLOWUP] >= 2.0)
     return fail(OB_ERR_NONFINITE, "blow-up: max|u| exceeded %g m/s in a diagnosed step",
                 p->blowup_u);

@@ -1,0 +1,386 @@
+// Slow tendency + forward-Euler half step for FP32 state with WS5 advection,
+// marching along x over planes staged in shared memory by the bulk-copy
+// (TMA) engine: k_slow_xt.  Same terms per cell as k_slow_xw / k_slow_f32
+// (advection tendency.py:965-1062, Coriolis :1220-1234, divergence damping,
+// heating :1731-1732; the half step integrator.py:346-370), in single
+// precision held to its rounding rather than to the reference's operation
+// order: the WS5 derivative is formed as its centred sixth-order part less
+// sgn(a) times its dissipative part, two fields at a time with the paired
+// FP32 instructions (u with v, theta' with w).
+//
+// A CTA owns R rows (y) by all NZ levels of one x-segment.  Thread t is cell
+// (row t / NZ, level t % NZ): the CTA's rows j0..j0+R-1 are consecutive in
+// memory for a fixed x, so one x-plane of the CTA with its y-halo (rows
+// j0-3..j0+R+2, periodic) is one or two contiguous runs per field.
+//
+// * The planes arrive by cp.async.bulk, one instruction per run, issued by
+//   one thread, completion counted on an mbarrier per ring slot.  w's rows of
+//   NZ + 1 floats do not start on 16 bytes: its run is copied as the 16-byte
+//   aligned range around it and read from `lead` floats into the slot.  With
+//   ny % 4 == 0 a run that wraps in y ends (row ny - 1) and restarts (row 0)
+//   on 16 bytes, so its second piece lands, aligned, right after the first;
+//   and a run that does not wrap ends at least one row before the array's
+//   end, so its aligned range stays inside the array.
+// * A ring of 7 plane slots: at step x = i the CTA reads plane i (y- and
+//   z-neighbours) and plane i + 3 (the x-window's new column), while planes
+//   up to i + 6 are in flight: the copies are issued three steps ahead.
+// * Each thread keeps 7-point x-windows of the four fields in registers.
+//   Steps run in groups of 7 with the group unrolled, so the window's
+//   rotation and the ring's slot indices are compile-time: every shared-
+//   memory read is a register base plus an immediate (NZ is a template
+//   parameter for the same reason).
+// * No CTA-wide barrier per step: each slot has a "full" mbarrier (the
+//   copies landed) and an "empty" one, on which every warp arrives once it has
+//   read the slot's plane for the last time.  Only the thread that issues the
+//   next copies into a slot waits for it to be empty, so the warps of a CTA
+//   run up to three steps apart.  The issuing passes from warp to warp, step
+//   by step, so that no warp carries it all and lags the others.
+// * Every wait on an mbarrier is bounded.  A wait that runs out (it cannot
+//   by construction: every copy is in bounds) sets stall[0] = 1, waits for
+//   the CTA's copies in flight with the same bound, and returns.
+#pragma once
+#include "kernels.cuh"
+
+namespace ob {
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+// Bounded wait for the phase of parity `parity`: false when it did not
+// complete within 2^22 tests (each test suspends the thread for up to a
+// hardware time limit while the phase is incomplete: about a second or more
+// in all).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_test(b, parity)) return true;
+  return false;
+}
+// orders this thread's earlier shared-memory accesses before its later
+// bulk copies (the slot being refilled was read by the generic proxy)
+__device__ __forceinline__ void fence_proxy() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// 60 d times the WS5 upwind derivative of two fields at once (q[r]: the
+// values at offsets r - 3; nsg = -sgn(a) per field, sgn(0) = +1).  The
+// stencils of tendency.py:940-959 are C6 - D (a >= 0) and C6 + D (a < 0) with
+// C6 = 45 (q1 - q-1) - 9 (q2 - q-2) + (q3 - q-3) and
+// D = (q3 + q-3) - 6 (q2 + q-2) + 15 (q1 + q-1) - 20 q0.
+__device__ __forceinline__ float2 ws5_pair(const float2 (&q)[7], float2 nsg) {
+  const float2 m1 = make_float2(-1.0f, -1.0f);
+  const float2 d1 = __ffma2_rn(q[2], m1, q[4]);
+  const float2 d2 = __ffma2_rn(q[1], m1, q[5]);
+  const float2 d3 = __ffma2_rn(q[0], m1, q[6]);
+  const float2 s1 = __fadd2_rn(q[2], q[4]);
+  const float2 s2 = __fadd2_rn(q[1], q[5]);
+  const float2 s3 = __fadd2_rn(q[0], q[6]);
+  float2 c = __ffma2_rn(make_float2(45.0f, 45.0f), d1, d3);
+  c = __ffma2_rn(make_float2(-9.0f, -9.0f), d2, c);
+  float2 d = __ffma2_rn(make_float2(15.0f, 15.0f), s1, s3);
+  d = __ffma2_rn(make_float2(-6.0f, -6.0f), s2, d);
+  d = __ffma2_rn(make_float2(-20.0f, -20.0f), q[3], d);
+  return __ffma2_rn(nsg, d, c);
+}
+__device__ __forceinline__ float nsgn(float a) { return a >= 0.0f ? -1.0f : 1.0f; }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+// Shared-memory plan of k_slow_xt (floats unless stated).
+template <int NZ, int R>
+struct SlowXt {
+  static constexpr int NT = R * NZ;                 // threads
+  static constexpr int RH = R + 6;                  // plane rows j0-3 .. j0+R+2
+  static constexpr int NW = NZ + 1;                 // w levels
+  static constexpr int FS = RH * NZ;                // one u / v / theta' plane
+  static constexpr int WS = (RH * NW + 8 + 3) / 4 * 4;  // the w run with its 16-byte margins
+  static constexpr int SLOT = 3 * FS + WS;
+  static constexpr int NSLOT = 7;
+  static constexpr size_t smem = (size_t)NSLOT * SLOT * 4 + 2 * NSLOT * 8;  // + mbarriers
+  // CTAs per SM: what the shared memory allows (228 KB per SM, 1 KB reserved
+  // per CTA), at most 2048 threads, and at least 72 registers a thread
+  static constexpr int by_smem = (int)(233472 / (smem + 1024));
+  static constexpr int by_regs = 65536 / (72 * NT);
+  static constexpr int by_thr = 2048 / NT;
+  static constexpr int per_sm_min = by_smem < by_regs ? by_smem : by_regs;
+  static constexpr int per_sm_cap = per_sm_min < by_thr ? per_sm_min : by_thr;
+  static constexpr int per_sm = per_sm_cap < 1 ? 1 : per_sm_cap;
+  static_assert(NZ % 4 == 0, "u, v, theta' rows must be whole 16-byte runs");
+  // (and ny % 4 == 0, checked by the host, for w's runs)
+  static_assert(NT % 32 == 0 && NT <= 1024, "whole warps, one CTA");
+};
+
+// grid = (ny / R, ceil(nx / seg)), block = R * NZ; seg is a multiple of 7.
+// OUTMODE 0: out = in + dts * tendency (the half step); 1: out = tendency.
+// stall: one double (the plan's OB_DIAG_STALL slot).
+template <int OUTMODE, int NZ, int R>
+__global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
+    GridK g, SlowK s, int mask, double dts_d, int seg, const float* __restrict__ u,
+    const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ th,
+    const float* __restrict__ dmp_u, const float* __restrict__ dmp_v, float* __restrict__ uo,
+    float* __restrict__ vo, float* __restrict__ wo, float* __restrict__ tho,
+    double* __restrict__ stall) {
+  using C = SlowXt<NZ, R>;
+  constexpr int NT = C::NT, RH = C::RH, NW = C::NW, FS = C::FS, SLOT = C::SLOT;
+  extern __shared__ __align__(16) float smx[];
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smx + C::NSLOT * SLOT);
+  const int nx = g.nx, ny = g.ny;
+  const int t = threadIdx.x;
+  const int row = t / NZ, k = t - row * NZ;
+  const int j0 = blockIdx.x * R, j = j0 + row;
+  const int i0 = blockIdx.y * seg;
+  const int len = min(seg, nx - i0);
+  const int qmax = len + 5;  // last plane (ring index q = x - i0 + 3) the segment reads
+  const bool cor = (mask & 2) && s.cor;
+  const bool dmp = (mask & 4) && s.damp;
+  const bool heat = (mask & 8) && s.heat;
+  const float dts = (float)dts_d;
+  const float inv60dx = (float)s.inv60dx, inv60dy = (float)s.inv60dy;
+  const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
+  const float f = cor ? (float)((s.cor == 2) ? s.fy[j] : s.f0) : 0.0f;
+  const float u_env = (float)s.u_env, v_env = (float)s.v_env;
+  const float dth0k = (float)s.dth0[k];
+  const float heatz = heat ? (float)s.heat_z[k] : 0.0f;
+
+  // the y-halo'd row block [j0 - 3, j0 + R + 3) mod ny as one or two runs
+  // (ny >= R + 6): na rows from global row ga, then nb rows from row 0, which
+  // land at plane row na
+  int ga = j0 - 3, na = RH, nb = 0;
+  if (ga < 0) {
+    na = -ga;
+    ga += ny;
+    nb = RH - na;
+  } else if (ga + RH > ny) {
+    na = ny - ga;
+    nb = RH - na;
+  }
+  // x-plane of ring plane q (x = i0 - 3 + q, periodic)
+  auto plane_x = [&](int q) {
+    int px = i0 - 3 + q;
+    px += (px < 0) ? nx : 0;
+    px -= (px >= nx) ? nx : 0;
+    return px;
+  };
+  // where w's run starts in its slot: its first float's offset mod 4 (the
+  // 16-byte aligned copy starts that many floats before it; exact mod 4 in
+  // 32-bit arithmetic)
+  auto lead_of = [&](int px) { return ((px * ny + ga) * NW) & 3; };
+  unsigned long long* full = bar;
+  unsigned long long* empty = bar + C::NSLOT;
+  // w's run of plane px: floats [wa, we) and, wrapped, [w2, w2e); piece 1
+  // ends at the plane's end (wrapped: aligned there) or at the run's aligned end
+  struct WRun {
+    size_t wa, we, w2, w2e;
+  };
+  auto w_run = [&](size_t cb) {
+    const size_t w0 = (cb + ga) * NW;
+    const size_t w2 = cb * NW;
+    return WRun{w0 & ~(size_t)3, nb ? (cb + ny) * NW : (w0 + RH * NW + 3) & ~(size_t)3, w2,
+                (w2 + nb * NW + 3) & ~(size_t)3};
+  };
+  // issue the copies of ring plane q into slot `slot` (free: the caller
+  // waited); one thread
+  auto issue = [&](int q, int slot) {
+    const int px = plane_x(q);
+    float* sl = smx + slot * SLOT;
+    const size_t cb = (size_t)px * ny;
+    const WRun r = w_run(cb);
+    const size_t wa = r.wa, we = r.we, w2 = r.w2, w2e = r.w2e;
+    const unsigned wbytes = (unsigned)((we - wa) + (nb ? w2e - w2 : 0)) * 4u;
+    fence_proxy();
+    mbar_expect_tx(&full[slot], 3u * FS * 4u + wbytes);
+    const float* src[3] = {u, v, th};
+#pragma unroll
+    for (int fi = 0; fi < 3; ++fi) {
+      bulk_load(sl + fi * FS, src[fi] + (cb + ga) * NZ, (unsigned)(na * NZ * 4), &full[slot]);
+      if (nb) bulk_load(sl + fi * FS + na * NZ, src[fi] + cb * NZ, (unsigned)(nb * NZ * 4),
+                        &full[slot]);
+    }
+    float* sw = sl + 3 * FS;
+    bulk_load(sw, w + wa, (unsigned)(we - wa) * 4u, &full[slot]);
+    if (nb) bulk_load(sw + (we - wa), w + w2, (unsigned)(w2e - w2) * 4u, &full[slot]);
+  };
+  const int lane = t & 31, warp = t >> 5;
+  constexpr int NWARP = NT / 32;
+  // this warp has read plane q for the last time
+  auto release = [&](int q) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[q % 7]);
+  };
+
+  if (t == 0) {
+#pragma unroll
+    for (int sl = 0; sl < C::NSLOT; ++sl) {
+      mbar_init(&full[sl], 1);
+      mbar_init(&empty[sl], NWARP);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  int qlast = min(6, qmax);  // the last plane issued
+  // planes q = 0..6 (x = i0-3 .. i0+3) into the fresh slots
+  if (t == 0)
+    for (int q = 0; q <= qlast; ++q) issue(q, q);
+  // the windows' first six columns: planes 0..5
+  bool ok = true;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) ok = ok && mbar_wait(&full[q], 0);
+  const int pc = (row + 3) * NZ + k;  // own cell in a u / v / theta' plane
+  const int pw = (row + 3) * NW + k;  // own level in the w plane (from its lead)
+  // x-windows, plane q at index q % 7: (u, v) and (theta', w) pairs
+  float2 quv[7], qtw[7];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const float* P = smx + q * SLOT;
+    quv[q] = f2(P[pc], P[FS + pc]);
+    qtw[q] = f2(P[2 * FS + pc], P[3 * FS + lead_of(plane_x(q)) + pw]);
+  }
+  // planes 0..2 are read only here; 7 and 8 refill the slots of 0 and 1
+#pragma unroll
+  for (int q = 0; q < 3; ++q) release(q);
+  for (int q = 7; q < 9; ++q)
+    if (q <= qmax) {
+      if (t == 0) {
+        ok = ok && mbar_wait(&empty[q - 7], 0);
+        if (ok) issue(q, q - 7);
+      }
+      qlast = q;
+    }
+  // z-neighbours: one-sided differences at the bottom and top levels
+  // (tendency.py:1000-1011), as offsets fixed for the thread
+  const int zm = (k > 0) ? -1 : 0, zp = (k < NZ - 1) ? 1 : 0;
+  const float fz = (k == 0 || k == NZ - 1) ? invdz : inv2dz;
+  const size_t plane_cells = (size_t)ny * NZ, plane_w = (size_t)ny * NW;
+  size_t o = ((size_t)i0 * ny + j) * NZ + k;
+  size_t ow = ((size_t)i0 * ny + j) * NW + k;
+  size_t col = (size_t)i0 * ny + j;
+
+  int iw = 0;  // the warp that issues this step's copies (lane 0)
+  for (int s0 = 0; ok && s0 < len; s0 += 7) {
+#pragma unroll
+    for (int uu = 0; uu < 7; ++uu) {
+      const int st = s0 + uu;  // step: x = i0 + st
+      if (ok && st < len) {
+        // plane st + 6 (the window's new column) must have landed
+        const int qn = st + 6;
+        ok = mbar_wait(&full[(uu + 6) % 7], (unsigned)((qn / 7) & 1));
+        // refill the slot of plane st + 2 (last read in the previous step)
+        // with plane st + 9, once every warp has released it
+        if (st + 9 <= qmax) {
+          if (warp == iw && lane == 0 && ok) {
+            ok = mbar_wait(&empty[(uu + 2) % 7], (unsigned)(((st + 2) / 7) & 1));
+            if (ok) issue(st + 9, (uu + 2) % 7);
+          }
+          qlast = st + 9;
+        }
+        iw = (iw + 1 == NWARP) ? 0 : iw + 1;
+        if (!ok) break;
+
+        const float* P = smx + ((uu + 3) % 7) * SLOT;  // plane x
+        const float* N = smx + ((uu + 6) % 7) * SLOT;  // plane x + 3
+        const int x = i0 + st;
+        const int pwx = pw + lead_of(x);
+        const int xn = x + 3 - ((x + 3 >= nx) ? nx : 0);
+        quv[(uu + 6) % 7] = f2(N[pc], N[FS + pc]);
+        qtw[(uu + 6) % 7] = f2(N[2 * FS + pc], N[3 * FS + pw + lead_of(xn)]);
+        // the windows in x order: x-3 .. x+3
+        float2 wuv[7], wtw[7];
+#pragma unroll
+        for (int r = 0; r < 7; ++r) {
+          wuv[r] = quv[(uu + r) % 7];
+          wtw[r] = qtw[(uu + r) % 7];
+        }
+        const float* Pu = P;
+        const float* Pv = P + FS;
+        const float* Pt = P + 2 * FS;
+        const float* Pw = P + 3 * FS;
+        const float uc = wuv[3].x, vc = wuv[3].y, wk = wtw[3].y;
+        // y-columns of this plane, rows -3..+3
+        float2 cuv[7], ctw[7];
+#pragma unroll
+        for (int r = 0; r < 7; ++r) {
+          if (r == 3) continue;  // the centre is the window's
+          cuv[r] = f2(Pu[pc + (r - 3) * NZ], Pv[pc + (r - 3) * NZ]);
+          ctw[r] = f2(Pt[pc + (r - 3) * NZ], Pw[pwx + (r - 3) * NW]);
+        }
+        cuv[3] = wuv[3];
+        ctw[3] = wtw[3];
+        const float um = Pu[pc + zm], vm = Pv[pc + zm], tm = Pt[pc + zm];
+        const float wp1 = Pw[pwx + 1], wm1 = Pw[pwx - 1];
+        const float wc = 0.5f * (wk + wp1);
+        const float uh = 0.5f * (um + uc), vh = 0.5f * (vm + vc);
+        const float2 m1 = f2(-1.0f, -1.0f);
+        // vertical differences: (u, v) one-sided at the bottom and top levels,
+        // (theta' + its base gradient, w on half levels)
+        const float2 cuvz = __fmul2_rn(__ffma2_rn(f2(um, vm), m1, f2(Pu[pc + zp], Pv[pc + zp])),
+                                       f2(fz, fz));
+        const float2 ctwz = __ffma2_rn(__ffma2_rn(f2(tm, wm1), m1, f2(Pt[pc + zp], wp1)),
+                                       f2(fz, inv2dz), f2(dth0k, 0.0f));
+        const float2 Xuv = ws5_pair(wuv, f2(nsgn(uc), nsgn(uc)));
+        const float2 Yuv = ws5_pair(cuv, f2(nsgn(vc), nsgn(vc)));
+        const float2 Xtw = ws5_pair(wtw, f2(nsgn(uc), nsgn(uh)));
+        const float2 Ytw = ws5_pair(ctw, f2(nsgn(vc), nsgn(vh)));
+        // tendencies -(u d/dx + v d/dy + w d/dz): (u, v) advected by (uc, vc, wc),
+        // (theta', w) by (uc, vc, wc) and (uh, vh, wk)
+        const float nux = -uc * inv60dx, nvy = -vc * inv60dy;
+        float2 tuv = __fmul2_rn(f2(nux, nux), Xuv);
+        tuv = __ffma2_rn(f2(nvy, nvy), Yuv, tuv);
+        tuv = __ffma2_rn(f2(-wc, -wc), cuvz, tuv);
+        float2 ttw = __fmul2_rn(f2(nux, -uh * inv60dx), Xtw);
+        ttw = __ffma2_rn(f2(nvy, -vh * inv60dy), Ytw, ttw);
+        ttw = __ffma2_rn(f2(-wc, -wk), ctwz, ttw);
+        if (cor) tuv = __ffma2_rn(f2(f, -f), f2(vc - v_env, uc - u_env), tuv);
+        if (dmp) tuv = __fadd2_rn(tuv, f2(dmp_u[o], dmp_v[o]));
+        if (heat) ttw.x = ttw.x + (float)s.heat_r[col] * heatz;
+        if (k == 0) ttw.y = 0.0f;  // w: no tendency at the surface
+        if (OUTMODE == 0) {
+          tuv = __ffma2_rn(f2(dts, dts), tuv, wuv[3]);
+          ttw = __ffma2_rn(f2(dts, dts), ttw, wtw[3]);
+        }
+        uo[o] = tuv.x;
+        vo[o] = tuv.y;
+        tho[o] = ttw.x;
+        wo[ow] = ttw.y;
+        if (k == NZ - 1) wo[ow + 1] = OUTMODE == 0 ? wp1 : 0.0f;  // the lid, level nz: no tendency
+        release(st + 3);  // plane x: read for the last time
+        o += plane_cells;
+        ow += plane_w;
+        col += ny;
+      }
+    }
+  }
+  if (!ok) {
+    // a wait ran out: flag it, and wait with the same bound for the copies
+    // into every slot whose latest plane was issued
+    *stall = 1.0;
+    for (int q = max(0, qlast - 6); q <= qlast; ++q) mbar_wait(&full[q % 7], (q / 7) & 1);
+  }
+}
+
+}  // namespace ob
