@@ -56,6 +56,10 @@ class RunRequest:
     lz: float = 16e3
     resume: Optional[dict] = None  # snapshot (oraclev8_b200.snapshot) to continue from
     cfl: float = 0.8               # advective CFL number of the time step
+    # "lh82": WS5 advection, beta-plane, buoyancy, projection; "production": the
+    # reference's build_production_config (centred advection, beta-plane,
+    # biharmonic diffusion, divergence damping, cooling, drag, projection)
+    physics: str = "lh82"
 
     @property
     def start_step(self) -> int:
@@ -87,12 +91,14 @@ class RunRequest:
 
 
 def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: float = 0.0,
-                  fp32r_frac: float = 1.0, cfl: float = 0.8) -> "list[RunRequest]":
+                  fp32r_frac: float = 1.0, cfl: float = 0.8,
+                  physics: str = "lh82") -> "list[RunRequest]":
     """``count`` requests from a seeded stream.  ``hours``: a fixed run length
     or a (lo, hi) uniform range.  ``rate`` > 0 gives Poisson arrivals at that
     many requests per second (else all arrive at 0); ``fp32r_frac`` < 1 tags
     that fraction FP32-refined and the rest FP64 (``precision`` ignored).
-    ``cfl``: dt = cfl dx / Vmax (0.8 in the ensemble and serving workloads)."""
+    ``cfl``: dt = cfl dx / Vmax (0.8 in the ensemble and serving workloads).
+    ``physics``: the step's components, as ``RunRequest.physics``."""
     rng = np.random.default_rng(seed)
     t, out = 0.0, []
     for i in range(count):
@@ -108,7 +114,8 @@ def draw_requests(count: int, seed: int, hours=24.0, precision="fp32r", rate: fl
             prec = "fp32r" if rng.uniform() < fp32r_frac else "fp64"
         if rate > 0.0:
             t += float(rng.exponential(1.0 / rate))
-        out.append(RunRequest(i, n, nz, vmax, rmax, b, lat, h, prec, t, cfl=cfl))
+        out.append(RunRequest(i, n, nz, vmax, rmax, b, lat, h, prec, t, cfl=cfl,
+                              physics=physics))
     return out
 
 
@@ -120,11 +127,12 @@ BLOWUP_U_MAX = 400.0
 def build_run(req: RunRequest, device_dtype=None, blowup_u_max: float = BLOWUP_U_MAX):
     """Integrator and device initial state of a request: WS5 advection,
     beta-plane Coriolis (periodic taper), buoyancy and the anelastic
-    projection; Holland vortex at the domain centre with the 12-km linear
-    wind decay.  The plan raises its blow-up flag on non-finite values or
-    max|u| > ``blowup_u_max``."""
+    projection, or with ``physics="production"`` the reference's production
+    configuration (build_production_config, no steering wind); Holland vortex
+    at the domain centre with the 12-km linear wind decay.  The plan raises
+    its blow-up flag on non-finite values or max|u| > ``blowup_u_max``."""
     from .grid import LorenzStaggering
-    from .production_config import BaseState
+    from .production_config import BaseState, build_production_config
     from .solver import (AdvectionComponent, AnelasticProjection, BuoyancyComponent,
                          CoriolisComponent, LH82AnelasticEquationSet, OperatorConfig,
                          RK3Integrator)
@@ -132,12 +140,17 @@ def build_run(req: RunRequest, device_dtype=None, blowup_u_max: float = BLOWUP_U
     n, nz = req.n, req.nz
     L = n * req.dx
     base = BaseState(nz, req.lz)
-    cfg = OperatorConfig(
-        equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
-        buoyancy=BuoyancyComponent(), projection=AnelasticProjection(n, n, nz, L, L, req.lz),
-        advection=AdvectionComponent(n, n, nz, L, L, req.lz, scheme="upwind5h"),
-        coriolis=CoriolisComponent(f=req.f0, mode="beta_plane", beta=req.beta, Ly=L, ny=n,
-                                   periodic_taper=True))
+    if req.physics == "production":
+        cfg = build_production_config(n, n, nz, L, L, req.lz, req.f0, 0.0, 0.0)
+    elif req.physics == "lh82":
+        cfg = OperatorConfig(
+            equation_set=LH82AnelasticEquationSet(), staggering=LorenzStaggering(),
+            buoyancy=BuoyancyComponent(), projection=AnelasticProjection(n, n, nz, L, L, req.lz),
+            advection=AdvectionComponent(n, n, nz, L, L, req.lz, scheme="upwind5h"),
+            coriolis=CoriolisComponent(f=req.f0, mode="beta_plane", beta=req.beta, Ly=L, ny=n,
+                                       periodic_taper=True))
+    else:
+        raise ValueError(f"physics must be 'lh82' or 'production', not {req.physics!r}")
     integ = RK3Integrator(cfg, base, precision=req.precision, blowup_u_max=blowup_u_max)
     if req.resume is not None:
         from .snapshot import state_from_snapshot
@@ -155,11 +168,14 @@ def footprint_bytes(req: RunRequest) -> int:
     """HBM a resident run holds: 5 state fields and the plan's scratch (3
     half-spectrum buffers, 5 anchor and 4 stage fields, 2 temporaries and the
     half-level buoyancy; plus two FP64 spectra for the FP32-refined
-    correction), in the state dtype."""
+    correction; the production physics adds the damper's two tendency fields
+    and the biharmonic's two inner Laplacians), in the state dtype."""
     S = 8 if req.precision == "fp64" else 4
     n = req.cells
     ns = (req.n // 2 + 1) * req.n * req.nz
     b = S * (5 * n + 12 * n) + 3 * ns * 2 * S
+    if req.physics == "production":  # damper tendencies and the inner Laplacians
+        b += 4 * n * S
     if req.precision != "fp64":
         b += 2 * ns * 16
     return int(b * 1.05) + (8 << 20)

@@ -88,6 +88,36 @@ def test_runs_equal_alone_and_in_the_mix():
         assert np.array_equal(a, host(getattr(s, f))), f
 
 
+def test_production_physics_runs_equal_alone_and_in_the_mix():
+    """Runs with the reference's production physics (build_production_config:
+    centred advection, biharmonic diffusion, divergence damping, cooling,
+    drag) served together end in the state each reaches alone, and the FP64
+    run equals the plain public step loop; all stay finite."""
+    from oraclev8_b200.serving import RunRequest, ServingEngine, build_run
+    reqs = [RunRequest(0, 96, 32, 45.0, 40e3, 1.5, 20.0, 0.5, "fp32r", physics="production"),
+            RunRequest(1, 128, 48, 30.0, 60e3, 1.2, 12.0, 0.4, "fp64", physics="production"),
+            RunRequest(2, 96, 64, 60.0, 25e3, 1.9, 28.0, 0.6, "fp32r", physics="production",
+                       arrival_s=0.05)]
+    eng = ServingEngine(hbm_budget=40e9, chunk=6, keep_final=True)
+    mix = {r.rid: r for r in eng.run(reqs)}
+    assert sorted(mix) == [0, 1, 2]
+    for req in reqs:
+        rec = mix[req.rid]
+        assert rec.error is None and rec.steps == req.nsteps
+        alone = ServingEngine(chunk=5, keep_final=True, realtime=False).run([req])[0]
+        for f, a in alone.final.items():
+            assert np.isfinite(a).all(), (req.rid, f)
+            assert np.array_equal(a, rec.final[f]), (req.rid, f)
+    req = reqs[1]
+    integ, s, _ = build_run(req)
+    for n in range(req.nsteps):
+        s, _ = integ.step(s, req.dt, n)
+    for f, a in mix[req.rid].final.items():
+        assert np.array_equal(a, host(getattr(s, f))), f
+    with pytest.raises(ValueError):
+        build_run(RunRequest(9, 96, 32, 45.0, 40e3, 1.5, 20.0, 0.1, "fp64", physics="dry"))
+
+
 def test_admission_respects_the_budget():
     """With room for one run at a time the runs are served one after the
     other, each admitted only once the previous one retired."""
