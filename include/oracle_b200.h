@@ -114,7 +114,10 @@ extern "C" {
 #define OB_VAR_ZC4_FXD 14
 #define OB_VAR_ZC4_FY 15
 #define OB_VAR_ZC4_IY 16
-#define OB_VAR_SLOW_XW 17   /* FP32 slow tendency marching along x (1) or gathering (0) */
+#define OB_VAR_SLOW_XW 17   /* FP32 slow tendency: 0 gathering, 1 marching along x with rows
+                               loaded per step, 4 / 8 marching over bulk-copied planes of 4 / 8
+                               rows (one cell per thread), 24 / 28 the same with two cells per
+                               thread (nz in {32, 48, 64, 80}, WS5 advection) */
 #define OB_VAR_THOMAS_FAST 18 /* FP32 sweep with a compile-time level count (1) */
 #define OB_VAR_RZC2_FX 19
 #define OB_VAR_RZC2_FY 20

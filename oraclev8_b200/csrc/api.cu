@@ -1392,29 +1392,41 @@ SlowK slow_args(const OraclePlan* p) {
 }
 
 // ---- x-marching slow tendency over bulk-copied planes (slowx.cuh) ---------
-bool slow_xt_grid(const OraclePlan* p, int r) {
-  const int nz = p->g.nz;
+// The plan's slow_xw value v selects k_slow_xt with R = v % 10 rows per CTA
+// and KC = v / 10 cells per thread (4, 8: one cell; 24, 28: two).
+bool slow_xt_grid(const OraclePlan* p, int v) {
+  const int nz = p->g.nz, r = v % 10;
   return p->prec == OB_PREC_F32 && p->advection == OB_ADV_UPWIND5H &&
-         (nz == 32 || nz == 48 || nz == 64 || nz == 80) && (r == 4 || r == 8) &&
+         (nz == 32 || nz == 48 || nz == 64 || nz == 80) && (v == 4 || v == 8 || v == 24 ||
+                                                            v == 28) &&
          p->g.ny % r == 0 && p->g.ny >= r + 6 && p->g.nx >= 7;
 }
-template <int NZ, int R>
+template <int NZ, int R, int KC>
 int slow_xt_attr() {
-  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<0, NZ, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)SlowXt<NZ, R>::smem));
-  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<1, NZ, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)SlowXt<NZ, R>::smem));
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<0, NZ, R, KC>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SlowXt<NZ, R, KC>::smem));
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<1, NZ, R, KC>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SlowXt<NZ, R, KC>::smem));
+  return OB_OK;
+}
+template <int NZ>
+int slow_xt_attrs_nz() {
+  int rc;
+  if ((rc = slow_xt_attr<NZ, 4, 1>()) || (rc = slow_xt_attr<NZ, 8, 1>()) ||
+      (rc = slow_xt_attr<NZ, 4, 2>()) || (rc = slow_xt_attr<NZ, 8, 2>()))
+    return rc;
   return OB_OK;
 }
 int slow_xt_attrs(int nz) {
-  int rc = OB_OK;
   switch (nz) {
-    case 32: (rc = slow_xt_attr<32, 4>()) || (rc = slow_xt_attr<32, 8>()); break;
-    case 48: (rc = slow_xt_attr<48, 4>()) || (rc = slow_xt_attr<48, 8>()); break;
-    case 64: (rc = slow_xt_attr<64, 4>()) || (rc = slow_xt_attr<64, 8>()); break;
-    case 80: (rc = slow_xt_attr<80, 4>()) || (rc = slow_xt_attr<80, 8>()); break;
+    case 32: return slow_xt_attrs_nz<32>();
+    case 48: return slow_xt_attrs_nz<48>();
+    case 64: return slow_xt_attrs_nz<64>();
+    case 80: return slow_xt_attrs_nz<80>();
   }
-  return rc;
+  return OB_OK;
 }
 // x-segment of one CTA: a multiple of 7 steps, short enough that the grid
 // holds about eight CTAs per SM (each segment re-reads 6 planes of its
@@ -1429,13 +1441,13 @@ int slow_xt_seg(const OraclePlan* p, int r) {
   seg = std::max(21, (seg + 6) / 7 * 7);
   return std::min(seg, (p->g.nx + 6) / 7 * 7);
 }
-template <int OUT, int NZ, int R>
+template <int OUT, int NZ, int R, int KC>
 void slow_xt_launch(OraclePlan* p, int mask, double dts, const float* u, const float* v,
                     const float* w, const float* th, float* uo, float* vo, float* wo,
                     float* tho, cudaStream_t st) {
   const int seg = slow_xt_seg(p, R);
   const dim3 grid(p->g.ny / R, (p->g.nx + seg - 1) / seg);
-  k_slow_xt<OUT, NZ, R><<<grid, R * NZ, SlowXt<NZ, R>::smem, st>>>(
+  k_slow_xt<OUT, NZ, R, KC><<<grid, R * NZ / KC, SlowXt<NZ, R, KC>::smem, st>>>(
       p->g, slow_args(p), mask, dts, seg, u, v, w, th, (const float*)p->Du, (const float*)p->Dv,
       uo, vo, wo, tho, p->diag + OB_DIAG_STALL);
 }
@@ -1455,9 +1467,13 @@ bool slow_xt_launch_any(OraclePlan* p, int mask, double dts, const float* u, con
 #define OB_XT(NZ)                                                                  \
   case NZ:                                                                         \
     if (r == 4)                                                                    \
-      slow_xt_launch<OUT, NZ, 4>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);       \
+      slow_xt_launch<OUT, NZ, 4, 1>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
+    else if (r == 8)                                                               \
+      slow_xt_launch<OUT, NZ, 8, 1>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
+    else if (r == 24)                                                              \
+      slow_xt_launch<OUT, NZ, 4, 2>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
     else                                                                           \
-      slow_xt_launch<OUT, NZ, 8>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);       \
+      slow_xt_launch<OUT, NZ, 8, 2>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
     return true;
   switch (p->g.nz) {
     OB_XT(32)
@@ -1842,8 +1858,7 @@ std::vector<int> var_values(const OraclePlan* p, int i) {
     case OB_VAR_ZC4_IY: list(f32 && ny == kY4N, {2, 4, 8}); break;
     case OB_VAR_SLOW_XW:
       list(true, {1});
-      list(slow_xt_grid(p, 4), {4});
-      list(slow_xt_grid(p, 8), {8});
+      for (int v : {4, 8, 24, 28}) list(slow_xt_grid(p, v), {v});
       break;
     case OB_VAR_THOMAS_FAST: list(true, {1}); break;
     case OB_VAR_RZC2_FX:

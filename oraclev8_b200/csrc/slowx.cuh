@@ -112,10 +112,11 @@ __device__ __forceinline__ float2 ws5_pair(const float2 (&q)[7], float2 nsg) {
 }
 __device__ __forceinline__ float nsgn(float a) { return a >= 0.0f ? -1.0f : 1.0f; }
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-// Shared-memory plan of k_slow_xt (floats unless stated).
-template <int NZ, int R>
+// Shared-memory plan of k_slow_xt (floats unless stated); KC cells (levels
+// k and k + NZ / 2 when KC = 2) per thread.
+template <int NZ, int R, int KC = 1>
 struct SlowXt {
-  static constexpr int NT = R * NZ;                 // threads
+  static constexpr int NT = R * NZ / KC;            // threads
   static constexpr int RH = R + 6;                  // plane rows j0-3 .. j0+R+2
   static constexpr int NW = NZ + 1;                 // w levels
   static constexpr int FS = RH * NZ;                // one u / v / theta' plane
@@ -124,9 +125,10 @@ struct SlowXt {
   static constexpr int NSLOT = 7;
   static constexpr size_t smem = (size_t)NSLOT * SLOT * 4 + 2 * NSLOT * 8;  // + mbarriers
   // CTAs per SM: what the shared memory allows (228 KB per SM, 1 KB reserved
-  // per CTA), at most 2048 threads, and at least 72 registers a thread
+  // per CTA), at most 2048 threads, and at least 72 registers a thread (136
+  // with two cells per thread)
   static constexpr int by_smem = (int)(233472 / (smem + 1024));
-  static constexpr int by_regs = 65536 / (72 * NT);
+  static constexpr int by_regs = 65536 / ((KC == 2 ? 136 : 72) * NT);
   static constexpr int by_thr = 2048 / NT;
   static constexpr int per_sm_min = by_smem < by_regs ? by_smem : by_regs;
   static constexpr int per_sm_cap = per_sm_min < by_thr ? per_sm_min : by_thr;
@@ -134,25 +136,29 @@ struct SlowXt {
   static_assert(NZ % 4 == 0, "u, v, theta' rows must be whole 16-byte runs");
   // (and ny % 4 == 0, checked by the host, for w's runs)
   static_assert(NT % 32 == 0 && NT <= 1024, "whole warps, one CTA");
+  static_assert(KC == 1 || (KC == 2 && NZ % 2 == 0), "one or two cells per thread");
 };
 
-// grid = (ny / R, ceil(nx / seg)), block = R * NZ; seg is a multiple of 7.
+// grid = (ny / R, ceil(nx / seg)), block = R * NZ / KC; seg is a multiple of 7.
 // OUTMODE 0: out = in + dts * tendency (the half step); 1: out = tendency.
+// KC = 2: each thread computes levels k and k + NZ / 2 of its row (twice the
+// work between waits, so that a step outlasts more of the copies' latency).
 // stall: one double (the plan's OB_DIAG_STALL slot).
-template <int OUTMODE, int NZ, int R>
-__global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
+template <int OUTMODE, int NZ, int R, int KC>
+__global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow_xt(
     GridK g, SlowK s, int mask, double dts_d, int seg, const float* __restrict__ u,
     const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ th,
     const float* __restrict__ dmp_u, const float* __restrict__ dmp_v, float* __restrict__ uo,
     float* __restrict__ vo, float* __restrict__ wo, float* __restrict__ tho,
     double* __restrict__ stall) {
-  using C = SlowXt<NZ, R>;
+  using C = SlowXt<NZ, R, KC>;
+  constexpr int NZC = NZ / KC;  // levels between a thread's cells
   constexpr int NT = C::NT, RH = C::RH, NW = C::NW, FS = C::FS, SLOT = C::SLOT;
   extern __shared__ __align__(16) float smx[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smx + C::NSLOT * SLOT);
   const int nx = g.nx, ny = g.ny;
   const int t = threadIdx.x;
-  const int row = t / NZ, k = t - row * NZ;
+  const int row = t / NZC, kb = t - row * NZC;
   const int j0 = blockIdx.x * R, j = j0 + row;
   const int i0 = blockIdx.y * seg;
   const int len = min(seg, nx - i0);
@@ -165,8 +171,12 @@ __global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
   const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
   const float f = cor ? (float)((s.cor == 2) ? s.fy[j] : s.f0) : 0.0f;
   const float u_env = (float)s.u_env, v_env = (float)s.v_env;
-  const float dth0k = (float)s.dth0[k];
-  const float heatz = heat ? (float)s.heat_z[k] : 0.0f;
+  float dth0k[KC], heatz[KC];
+#pragma unroll
+  for (int c = 0; c < KC; ++c) {
+    dth0k[c] = (float)s.dth0[kb + c * NZC];
+    heatz[c] = heat ? (float)s.heat_z[kb + c * NZC] : 0.0f;
+  }
 
   // the y-halo'd row block [j0 - 3, j0 + R + 3) mod ny as one or two runs
   // (ny >= R + 6): na rows from global row ga, then nb rows from row 0, which
@@ -251,15 +261,19 @@ __global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
   bool ok = true;
 #pragma unroll
   for (int q = 0; q < 6; ++q) ok = ok && mbar_wait(&full[q], 0);
-  const int pc = (row + 3) * NZ + k;  // own cell in a u / v / theta' plane
-  const int pw = (row + 3) * NW + k;  // own level in the w plane (from its lead)
-  // x-windows, plane q at index q % 7: (u, v) and (theta', w) pairs
-  float2 quv[7], qtw[7];
+  const int pc = (row + 3) * NZ + kb;  // own first cell in a u / v / theta' plane
+  const int pw = (row + 3) * NW + kb;  // its level in the w plane (from the lead)
+  // x-windows per cell, plane q at index q % 7: (u, v) and (theta', w) pairs
+  float2 quv[KC][7], qtw[KC][7];
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     const float* P = smx + q * SLOT;
-    quv[q] = f2(P[pc], P[FS + pc]);
-    qtw[q] = f2(P[2 * FS + pc], P[3 * FS + lead_of(plane_x(q)) + pw]);
+    const int ld = lead_of(plane_x(q));
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+      quv[c][q] = f2(P[pc + c * NZC], P[FS + pc + c * NZC]);
+      qtw[c][q] = f2(P[2 * FS + pc + c * NZC], P[3 * FS + ld + pw + c * NZC]);
+    }
   }
   // planes 0..2 are read only here; 7 and 8 refill the slots of 0 and 1
 #pragma unroll
@@ -274,11 +288,18 @@ __global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
     }
   // z-neighbours: one-sided differences at the bottom and top levels
   // (tendency.py:1000-1011), as offsets fixed for the thread
-  const int zm = (k > 0) ? -1 : 0, zp = (k < NZ - 1) ? 1 : 0;
-  const float fz = (k == 0 || k == NZ - 1) ? invdz : inv2dz;
+  int zm[KC], zp[KC];
+  float fz[KC];
+#pragma unroll
+  for (int c = 0; c < KC; ++c) {
+    const int k = kb + c * NZC;
+    zm[c] = (k > 0) ? -1 : 0;
+    zp[c] = (k < NZ - 1) ? 1 : 0;
+    fz[c] = (k == 0 || k == NZ - 1) ? invdz : inv2dz;
+  }
   const size_t plane_cells = (size_t)ny * NZ, plane_w = (size_t)ny * NW;
-  size_t o = ((size_t)i0 * ny + j) * NZ + k;
-  size_t ow = ((size_t)i0 * ny + j) * NW + k;
+  size_t o = ((size_t)i0 * ny + j) * NZ + kb;
+  size_t ow = ((size_t)i0 * ny + j) * NW + kb;
   size_t col = (size_t)i0 * ny + j;
 
   int iw = 0;  // the warp that issues this step's copies (lane 0)
@@ -307,67 +328,75 @@ __global__ void __launch_bounds__(R * NZ, SlowXt<NZ, R>::per_sm) k_slow_xt(
         const int x = i0 + st;
         const int pwx = pw + lead_of(x);
         const int xn = x + 3 - ((x + 3 >= nx) ? nx : 0);
-        quv[(uu + 6) % 7] = f2(N[pc], N[FS + pc]);
-        qtw[(uu + 6) % 7] = f2(N[2 * FS + pc], N[3 * FS + pw + lead_of(xn)]);
-        // the windows in x order: x-3 .. x+3
-        float2 wuv[7], wtw[7];
-#pragma unroll
-        for (int r = 0; r < 7; ++r) {
-          wuv[r] = quv[(uu + r) % 7];
-          wtw[r] = qtw[(uu + r) % 7];
-        }
+        const int pwn = pw + lead_of(xn);
         const float* Pu = P;
         const float* Pv = P + FS;
         const float* Pt = P + 2 * FS;
         const float* Pw = P + 3 * FS;
-        const float uc = wuv[3].x, vc = wuv[3].y, wk = wtw[3].y;
-        // y-columns of this plane, rows -3..+3
-        float2 cuv[7], ctw[7];
+        const float hr = heat ? (float)s.heat_r[col] : 0.0f;
 #pragma unroll
-        for (int r = 0; r < 7; ++r) {
-          if (r == 3) continue;  // the centre is the window's
-          cuv[r] = f2(Pu[pc + (r - 3) * NZ], Pv[pc + (r - 3) * NZ]);
-          ctw[r] = f2(Pt[pc + (r - 3) * NZ], Pw[pwx + (r - 3) * NW]);
+        for (int c = 0; c < KC; ++c) {
+          const int cp = pc + c * NZC, cw = pwx + c * NZC;
+          quv[c][(uu + 6) % 7] = f2(N[cp], N[FS + cp]);
+          qtw[c][(uu + 6) % 7] = f2(N[2 * FS + cp], N[3 * FS + pwn + c * NZC]);
+          // the windows in x order: x-3 .. x+3
+          float2 wuv[7], wtw[7];
+#pragma unroll
+          for (int r = 0; r < 7; ++r) {
+            wuv[r] = quv[c][(uu + r) % 7];
+            wtw[r] = qtw[c][(uu + r) % 7];
+          }
+          const float uc = wuv[3].x, vc = wuv[3].y, wk = wtw[3].y;
+          // y-columns of this plane, rows -3..+3
+          float2 cuv[7], ctw[7];
+#pragma unroll
+          for (int r = 0; r < 7; ++r) {
+            if (r == 3) continue;  // the centre is the window's
+            cuv[r] = f2(Pu[cp + (r - 3) * NZ], Pv[cp + (r - 3) * NZ]);
+            ctw[r] = f2(Pt[cp + (r - 3) * NZ], Pw[cw + (r - 3) * NW]);
+          }
+          cuv[3] = wuv[3];
+          ctw[3] = wtw[3];
+          const float um = Pu[cp + zm[c]], vm = Pv[cp + zm[c]], tm = Pt[cp + zm[c]];
+          const float wp1 = Pw[cw + 1], wm1 = Pw[cw - 1];
+          const float wc = 0.5f * (wk + wp1);
+          const float uh = 0.5f * (um + uc), vh = 0.5f * (vm + vc);
+          const float2 m1 = f2(-1.0f, -1.0f);
+          // vertical differences: (u, v) one-sided at the bottom and top
+          // levels, (theta' + its base gradient, w on half levels)
+          const float2 cuvz = __fmul2_rn(
+              __ffma2_rn(f2(um, vm), m1, f2(Pu[cp + zp[c]], Pv[cp + zp[c]])), f2(fz[c], fz[c]));
+          const float2 ctwz = __ffma2_rn(__ffma2_rn(f2(tm, wm1), m1, f2(Pt[cp + zp[c]], wp1)),
+                                         f2(fz[c], inv2dz), f2(dth0k[c], 0.0f));
+          const float2 Xuv = ws5_pair(wuv, f2(nsgn(uc), nsgn(uc)));
+          const float2 Yuv = ws5_pair(cuv, f2(nsgn(vc), nsgn(vc)));
+          const float2 Xtw = ws5_pair(wtw, f2(nsgn(uc), nsgn(uh)));
+          const float2 Ytw = ws5_pair(ctw, f2(nsgn(vc), nsgn(vh)));
+          // tendencies -(u d/dx + v d/dy + w d/dz): (u, v) advected by
+          // (uc, vc, wc), (theta', w) by (uc, vc, wc) and (uh, vh, wk)
+          const float nux = -uc * inv60dx, nvy = -vc * inv60dy;
+          float2 tuv = __fmul2_rn(f2(nux, nux), Xuv);
+          tuv = __ffma2_rn(f2(nvy, nvy), Yuv, tuv);
+          tuv = __ffma2_rn(f2(-wc, -wc), cuvz, tuv);
+          float2 ttw = __fmul2_rn(f2(nux, -uh * inv60dx), Xtw);
+          ttw = __ffma2_rn(f2(nvy, -vh * inv60dy), Ytw, ttw);
+          ttw = __ffma2_rn(f2(-wc, -wk), ctwz, ttw);
+          const size_t oc = o + c * NZC, owc = ow + c * NZC;
+          if (cor) tuv = __ffma2_rn(f2(f, -f), f2(vc - v_env, uc - u_env), tuv);
+          if (dmp) tuv = __fadd2_rn(tuv, f2(dmp_u[oc], dmp_v[oc]));
+          if (heat) ttw.x = ttw.x + hr * heatz[c];
+          if (kb + c * NZC == 0) ttw.y = 0.0f;  // w: no tendency at the surface
+          if (OUTMODE == 0) {
+            tuv = __ffma2_rn(f2(dts, dts), tuv, wuv[3]);
+            ttw = __ffma2_rn(f2(dts, dts), ttw, wtw[3]);
+          }
+          uo[oc] = tuv.x;
+          vo[oc] = tuv.y;
+          tho[oc] = ttw.x;
+          wo[owc] = ttw.y;
+          if (kb + c * NZC == NZ - 1)  // the lid, level nz: no tendency
+            wo[owc + 1] = OUTMODE == 0 ? wp1 : 0.0f;
         }
-        cuv[3] = wuv[3];
-        ctw[3] = wtw[3];
-        const float um = Pu[pc + zm], vm = Pv[pc + zm], tm = Pt[pc + zm];
-        const float wp1 = Pw[pwx + 1], wm1 = Pw[pwx - 1];
-        const float wc = 0.5f * (wk + wp1);
-        const float uh = 0.5f * (um + uc), vh = 0.5f * (vm + vc);
-        const float2 m1 = f2(-1.0f, -1.0f);
-        // vertical differences: (u, v) one-sided at the bottom and top levels,
-        // (theta' + its base gradient, w on half levels)
-        const float2 cuvz = __fmul2_rn(__ffma2_rn(f2(um, vm), m1, f2(Pu[pc + zp], Pv[pc + zp])),
-                                       f2(fz, fz));
-        const float2 ctwz = __ffma2_rn(__ffma2_rn(f2(tm, wm1), m1, f2(Pt[pc + zp], wp1)),
-                                       f2(fz, inv2dz), f2(dth0k, 0.0f));
-        const float2 Xuv = ws5_pair(wuv, f2(nsgn(uc), nsgn(uc)));
-        const float2 Yuv = ws5_pair(cuv, f2(nsgn(vc), nsgn(vc)));
-        const float2 Xtw = ws5_pair(wtw, f2(nsgn(uc), nsgn(uh)));
-        const float2 Ytw = ws5_pair(ctw, f2(nsgn(vc), nsgn(vh)));
-        // tendencies -(u d/dx + v d/dy + w d/dz): (u, v) advected by (uc, vc, wc),
-        // (theta', w) by (uc, vc, wc) and (uh, vh, wk)
-        const float nux = -uc * inv60dx, nvy = -vc * inv60dy;
-        float2 tuv = __fmul2_rn(f2(nux, nux), Xuv);
-        tuv = __ffma2_rn(f2(nvy, nvy), Yuv, tuv);
-        tuv = __ffma2_rn(f2(-wc, -wc), cuvz, tuv);
-        float2 ttw = __fmul2_rn(f2(nux, -uh * inv60dx), Xtw);
-        ttw = __ffma2_rn(f2(nvy, -vh * inv60dy), Ytw, ttw);
-        ttw = __ffma2_rn(f2(-wc, -wk), ctwz, ttw);
-        if (cor) tuv = __ffma2_rn(f2(f, -f), f2(vc - v_env, uc - u_env), tuv);
-        if (dmp) tuv = __fadd2_rn(tuv, f2(dmp_u[o], dmp_v[o]));
-        if (heat) ttw.x = ttw.x + (float)s.heat_r[col] * heatz;
-        if (k == 0) ttw.y = 0.0f;  // w: no tendency at the surface
-        if (OUTMODE == 0) {
-          tuv = __ffma2_rn(f2(dts, dts), tuv, wuv[3]);
-          ttw = __ffma2_rn(f2(dts, dts), ttw, wtw[3]);
-        }
-        uo[o] = tuv.x;
-        vo[o] = tuv.y;
-        tho[o] = ttw.x;
-        wo[ow] = ttw.y;
-        if (k == NZ - 1) wo[ow + 1] = OUTMODE == 0 ? wp1 : 0.0f;  // the lid, level nz: no tendency
         release(st + 3);  // plane x: read for the last time
         o += plane_cells;
         ow += plane_w;

@@ -241,7 +241,8 @@ def test_slow_tendency_forms_agree(shape, monkeypatch):
     the plan's slow_xw variant at 0), marching along x with the neighbour rows
     loaded per step (k_slow_xw, variant 1; nx % 16 == 0, ny % 8 == 0), and
     marching along x over planes of 4 or 8 rows staged by bulk copies
-    (k_slow_xt, variants 4 and 8; nz in {32, 48, 64, 80}).  The first two share
+    (k_slow_xt, variants 4 and 8, and 24 and 28 with two cells per thread;
+    nz in {32, 48, 64, 80}).  The first two share
     the gather's operation order and agree with it to FP32 rounding; the
     plane-staged form forms the WS5 derivative as a centred part less the
     upwind sign times a dissipative part, so two full steps of the vortex
@@ -274,7 +275,7 @@ def test_slow_tendency_forms_agree(shape, monkeypatch):
 
     ref = run("fp64")
     outs = {}
-    for xw in (0, 1, 4, 8):
+    for xw in (0, 1, 4, 8, 24, 28):
         try:
             outs[xw] = run("fp32", xw)
         except ValueError:  # the form does not exist for this grid
@@ -318,7 +319,7 @@ def test_slow_tendency_forms_against_fp64(shape):
     ref = [host(t) for t in p64.tendency(mask, *(dev(a, torch.float64) for a in fields), c["dt"])]
     scale = [np.abs(r).max() for r in ref]
     errs, outs = {}, {}
-    for xw in (0, 1, 4, 8):
+    for xw in (0, 1, 4, 8, 24, 28):
         p = RK3Integrator(cfg, base, precision="fp32").plan
         try:
             p.set_variants(slow_xw=xw)
@@ -332,7 +333,7 @@ def test_slow_tendency_forms_against_fp64(shape):
     assert 0 in errs and 4 in errs, sorted(errs)
     for xw, e in errs.items():
         assert max(e) <= 1e-5, (xw, e)
-    for xw in (4, 8):
+    for xw in (4, 8, 24, 28):
         if xw not in errs:
             continue
         for n in range(4):
