@@ -1165,6 +1165,12 @@ template <class T>
 int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
                  double stage_sdt, T* uo, T* vo, T* wo, T* phio, int slot_c, int slot_d,
                  cudaStream_t st, const T* bh = nullptr) {
+  // a stage projection reads the half-level buoyancy in every form but the
+  // generic one; without it a selected form would silently fall back
+  if (stage_sdt >= 0.0 && !bh && (p->zc2_fxs || p->zc2_ix || p->zc3_fxs || p->zc3_ix || p->zc4_fxs ||
+                    p->zc4_ix))
+    return fail(OB_ERR_CUDA, "stage projection without the half-level buoyancy its "
+                "kernel forms read");
   p->solve_count += 1;
   const int de = p->diag_every < 1 ? 1 : p->diag_every;
   const bool log = !p->capturing && ((de == 1) || (p->solve_count % de == 1));
@@ -1579,9 +1585,12 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
   const T *su = au, *sv = av, *sw = aw, *sphi = aphi;
   if (p->buoyancy && p->projection) {
     const double alphas[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
-    // the three stages share the buoyancy of the anchor theta'
+    // the three stages share the buoyancy of the anchor theta', formed once
+    // on half levels for every stage form that reads it (all but the generic
+    // shared-memory kernels, which form it on the fly; whichever form the
+    // autotuner kept, the stage projections must not fall back to those)
     const T* bh = nullptr;
-    if (p->Bh && (p->zc2_fxs || p->zc2_ix || p->zc4_fxs || p->zc4_ix)) {
+    if (p->Bh) {
       const long ncol = (long)p->g.nx * p->g.ny;
       { Launch L_(p, 7, st); k_bhalf<T><<<(unsigned)std::min<long>((ncol + 7) / 8, 65535), 256, 0, st>>>(
           p->g, ath, p->theta0, p->gth, (T*)p->Bh); }
