@@ -1399,29 +1399,36 @@ SlowK slow_args(const OraclePlan* p) {
 
 // ---- x-marching slow tendency over bulk-copied planes (slowx.cuh) ---------
 // The plan's slow_xw value v selects k_slow_xt with R = v % 10 rows per CTA
-// and KC = v / 10 cells per thread (4, 8: one cell; 24, 28: two).
+// and KC = v / 10 cells per thread (4, 8: one cell; 24, 28: two).  Plans with
+// production components or centred advection run its production form, which
+// has one cell per thread.
+bool slow_xt_prod(const OraclePlan* p) {
+  return p->drag || p->sponge || p->diffusion || p->cooling ||
+         p->advection != OB_ADV_UPWIND5H;
+}
 bool slow_xt_grid(const OraclePlan* p, int v) {
   const int nz = p->g.nz, r = v % 10;
-  return p->prec == OB_PREC_F32 && p->advection == OB_ADV_UPWIND5H &&
-         (nz == 32 || nz == 48 || nz == 64 || nz == 80) && (v == 4 || v == 8 || v == 24 ||
-                                                            v == 28) &&
+  const bool adv = p->advection == OB_ADV_UPWIND5H || p->advection == OB_ADV_CENTERED2;
+  return p->prec == OB_PREC_F32 && adv && (nz == 32 || nz == 48 || nz == 64 || nz == 80) &&
+         (v == 4 || v == 8 || ((v == 24 || v == 28) && !slow_xt_prod(p))) &&
          p->g.ny % r == 0 && p->g.ny >= r + 6 && p->g.nx >= 7;
 }
-template <int NZ, int R, int KC>
+template <int NZ, int R, int KC, bool PROD = false>
 int slow_xt_attr() {
-  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<0, NZ, R, KC>,
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<0, NZ, R, KC, PROD>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)SlowXt<NZ, R, KC>::smem));
-  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<1, NZ, R, KC>,
+                               (int)SlowXt<NZ, R, KC, PROD>::smem));
+  OB_CUDA(cudaFuncSetAttribute(k_slow_xt<1, NZ, R, KC, PROD>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)SlowXt<NZ, R, KC>::smem));
+                               (int)SlowXt<NZ, R, KC, PROD>::smem));
   return OB_OK;
 }
 template <int NZ>
 int slow_xt_attrs_nz() {
   int rc;
   if ((rc = slow_xt_attr<NZ, 4, 1>()) || (rc = slow_xt_attr<NZ, 8, 1>()) ||
-      (rc = slow_xt_attr<NZ, 4, 2>()) || (rc = slow_xt_attr<NZ, 8, 2>()))
+      (rc = slow_xt_attr<NZ, 4, 2>()) || (rc = slow_xt_attr<NZ, 8, 2>()) ||
+      (rc = slow_xt_attr<NZ, 4, 1, true>()) || (rc = slow_xt_attr<NZ, 8, 1, true>()))
     return rc;
   return OB_OK;
 }
@@ -1447,13 +1454,13 @@ int slow_xt_seg(const OraclePlan* p, int r) {
   seg = std::max(21, (seg + 6) / 7 * 7);
   return std::min(seg, (p->g.nx + 6) / 7 * 7);
 }
-template <int OUT, int NZ, int R, int KC>
+template <int OUT, int NZ, int R, int KC, bool PROD = false>
 void slow_xt_launch(OraclePlan* p, int mask, double dts, const float* u, const float* v,
                     const float* w, const float* th, float* uo, float* vo, float* wo,
                     float* tho, cudaStream_t st) {
   const int seg = slow_xt_seg(p, R);
   const dim3 grid(p->g.ny / R, (p->g.nx + seg - 1) / seg);
-  k_slow_xt<OUT, NZ, R, KC><<<grid, R * NZ / KC, SlowXt<NZ, R, KC>::smem, st>>>(
+  k_slow_xt<OUT, NZ, R, KC, PROD><<<grid, R * NZ / KC, SlowXt<NZ, R, KC, PROD>::smem, st>>>(
       p->g, slow_args(p), mask, dts, seg, u, v, w, th, (const float*)p->Du, (const float*)p->Dv,
       uo, vo, wo, tho, p->diag + OB_DIAG_STALL);
 }
@@ -1470,9 +1477,14 @@ bool slow_xt_launch_any(OraclePlan* p, int mask, double dts, const float* u, con
                         const float* w, const float* th, float* uo, float* vo, float* wo,
                         float* tho, cudaStream_t st) {
   const int r = p->slow_xw;
+  const bool prod = slow_xt_prod(p);
 #define OB_XT(NZ)                                                                  \
   case NZ:                                                                         \
-    if (r == 4)                                                                    \
+    if (prod && r == 4)                                                            \
+      slow_xt_launch<OUT, NZ, 4, 1, true>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st); \
+    else if (prod)                                                                 \
+      slow_xt_launch<OUT, NZ, 8, 1, true>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st); \
+    else if (r == 4)                                                               \
       slow_xt_launch<OUT, NZ, 4, 1>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
     else if (r == 8)                                                               \
       slow_xt_launch<OUT, NZ, 8, 1>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st);  \
@@ -1508,7 +1520,7 @@ int slow_impl(OraclePlan* p, int mask, double dts, const T* u, const T* v, const
                      (p->drag || p->sponge || p->diffusion || p->cooling);
   if constexpr (sizeof(T) == 4) {
     // the x-marching form where the grid tiles it; the gather form otherwise
-    if (!extra && slow_xt_call(p, mask, u, v, w, th))
+    if (slow_xt_call(p, mask, u, v, w, th))
       { Launch L_(p, 5, st); slow_xt_launch_any<OUT>(p, mask, dts, u, v, w, th, uo, vo, wo, tho, st); }
     else if (p->slow_xw && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
       { Launch L_(p, 5, st); k_slow_xw<OUT><<<dim3(p->g.ny / 8, p->g.nx / KXW), blk, 0, st>>>(
@@ -2021,8 +2033,10 @@ int tune_impl(OraclePlan* p, cudaStream_t st) {
     }
     const bool slow = p->advection || p->coriolis || p->heating;
     const bool extra = p->drag || p->sponge || p->diffusion || p->cooling;
-    const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_HEATING;
-    if (slow && !extra && p->g.ny % 8 == 0 && p->g.nx % KXW == 0)
+    const int all = OB_TEND_ADVECTION | OB_TEND_CORIOLIS | OB_TEND_HEATING |
+                    (extra ? (OB_TEND_DRAG | OB_TEND_SPONGE | OB_TEND_DIFFUSION |
+                              OB_TEND_COOLING) : 0);
+    if (slow && var_values(p, OB_VAR_SLOW_XW).size() > 1)
       RC(tune_group<T>(p, {OB_VAR_SLOW_XW}, st, [&] {
         return slow_impl<T, 0>(p, all, 1.0, u, v, w, th, uo, vo, wo, (T*)p->Sphi, st);
       }));

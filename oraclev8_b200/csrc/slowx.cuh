@@ -113,22 +113,24 @@ __device__ __forceinline__ float2 ws5_pair(const float2 (&q)[7], float2 nsg) {
 __device__ __forceinline__ float nsgn(float a) { return a >= 0.0f ? -1.0f : 1.0f; }
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 // Shared-memory plan of k_slow_xt (floats unless stated); KC cells (levels
-// k and k + NZ / 2 when KC = 2) per thread.
-template <int NZ, int R, int KC = 1>
+// k and k + NZ / 2 when KC = 2) per thread; PROD: the production form, whose
+// planes also carry the biharmonic's inner Laplacians of u and v.
+template <int NZ, int R, int KC = 1, bool PROD = false>
 struct SlowXt {
   static constexpr int NT = R * NZ / KC;            // threads
   static constexpr int RH = R + 6;                  // plane rows j0-3 .. j0+R+2
   static constexpr int NW = NZ + 1;                 // w levels
   static constexpr int FS = RH * NZ;                // one u / v / theta' plane
   static constexpr int WS = (RH * NW + 8 + 3) / 4 * 4;  // the w run with its 16-byte margins
-  static constexpr int SLOT = 3 * FS + WS;
+  static constexpr int NF = PROD ? 5 : 3;           // full-level fields per plane
+  static constexpr int SLOT = NF * FS + WS;
   static constexpr int NSLOT = 7;
   static constexpr size_t smem = (size_t)NSLOT * SLOT * 4 + 2 * NSLOT * 8;  // + mbarriers
   // CTAs per SM: what the shared memory allows (228 KB per SM, 1 KB reserved
   // per CTA), at most 2048 threads, and at least 72 registers a thread (136
-  // with two cells per thread)
+  // with two cells per thread, 104 in the production form)
   static constexpr int by_smem = (int)(233472 / (smem + 1024));
-  static constexpr int by_regs = 65536 / ((KC == 2 ? 136 : 72) * NT);
+  static constexpr int by_regs = 65536 / ((KC == 2 ? 136 : PROD ? 104 : 72) * NT);
   static constexpr int by_thr = 2048 / NT;
   static constexpr int per_sm_min = by_smem < by_regs ? by_smem : by_regs;
   static constexpr int per_sm_cap = per_sm_min < by_thr ? per_sm_min : by_thr;
@@ -143,17 +145,21 @@ struct SlowXt {
 // OUTMODE 0: out = in + dts * tendency (the half step); 1: out = tendency.
 // KC = 2: each thread computes levels k and k + NZ / 2 of its row (twice the
 // work between waits, so that a step outlasts more of the copies' latency).
+// PROD: the production components as well (k_slow_f32<OUTMODE, true>):
+// surface drag, sponge, Laplacian or biharmonic diffusion, Newtonian cooling,
+// and centred (C2) or WS5 advection chosen at run time.
 // stall: one double (the plan's OB_DIAG_STALL slot).
-template <int OUTMODE, int NZ, int R, int KC>
-__global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow_xt(
+template <int OUTMODE, int NZ, int R, int KC, bool PROD = false>
+__global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) k_slow_xt(
     GridK g, SlowK s, int mask, double dts_d, int seg, const float* __restrict__ u,
     const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ th,
     const float* __restrict__ dmp_u, const float* __restrict__ dmp_v, float* __restrict__ uo,
     float* __restrict__ vo, float* __restrict__ wo, float* __restrict__ tho,
     double* __restrict__ stall) {
-  using C = SlowXt<NZ, R, KC>;
+  using C = SlowXt<NZ, R, KC, PROD>;
+  static_assert(!PROD || KC == 1, "the production form has one cell per thread");
   constexpr int NZC = NZ / KC;  // levels between a thread's cells
-  constexpr int NT = C::NT, RH = C::RH, NW = C::NW, FS = C::FS, SLOT = C::SLOT;
+  constexpr int NT = C::NT, RH = C::RH, NW = C::NW, FS = C::FS, SLOT = C::SLOT, NF = C::NF;
   extern __shared__ __align__(16) float smx[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smx + C::NSLOT * SLOT);
   const int nx = g.nx, ny = g.ny;
@@ -166,6 +172,15 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
   const bool cor = (mask & 2) && s.cor;
   const bool dmp = (mask & 4) && s.damp;
   const bool heat = (mask & 8) && s.heat;
+  // production components (k_slow_f32<_, true>)
+  const bool ws5 = !PROD || s.adv == 2;
+  const bool drg = PROD && (mask & kTendDrag) && s.drag;
+  const bool spg = PROD && (mask & kTendSponge) && s.sponge;
+  const int dif = (PROD && (mask & kTendDiffusion)) ? s.diff : 0;
+  const bool cool = PROD && (mask & kTendCooling) && s.cool;
+  const float* lap_u = static_cast<const float*>(s.lap_u);
+  const float* lap_v = static_cast<const float*>(s.lap_v);
+  const bool lapf = PROD && dif == 2;  // the inner Laplacians ride in the planes
   const float dts = (float)dts_d;
   const float inv60dx = (float)s.inv60dx, inv60dy = (float)s.inv60dy;
   const float inv2dz = (float)s.inv2dz, invdz = (float)s.invdz;
@@ -224,15 +239,17 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
     const size_t wa = r.wa, we = r.we, w2 = r.w2, w2e = r.w2e;
     const unsigned wbytes = (unsigned)((we - wa) + (nb ? w2e - w2 : 0)) * 4u;
     fence_proxy();
-    mbar_expect_tx(&full[slot], 3u * FS * 4u + wbytes);
-    const float* src[3] = {u, v, th};
+    const int nfc = lapf ? 5 : 3;  // full-level fields copied
+    mbar_expect_tx(&full[slot], (unsigned)nfc * FS * 4u + wbytes);
+    const float* src[5] = {u, v, th, lap_u, lap_v};
 #pragma unroll
-    for (int fi = 0; fi < 3; ++fi) {
+    for (int fi = 0; fi < NF; ++fi) {
+      if (fi >= nfc) break;
       bulk_load(sl + fi * FS, src[fi] + (cb + ga) * NZ, (unsigned)(na * NZ * 4), &full[slot]);
       if (nb) bulk_load(sl + fi * FS + na * NZ, src[fi] + cb * NZ, (unsigned)(nb * NZ * 4),
                         &full[slot]);
     }
-    float* sw = sl + 3 * FS;
+    float* sw = sl + NF * FS;
     bulk_load(sw, w + wa, (unsigned)(we - wa) * 4u, &full[slot]);
     if (nb) bulk_load(sw + (we - wa), w + w2, (unsigned)(w2e - w2) * 4u, &full[slot]);
   };
@@ -272,9 +289,22 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
 #pragma unroll
     for (int c = 0; c < KC; ++c) {
       quv[c][q] = f2(P[pc + c * NZC], P[FS + pc + c * NZC]);
-      qtw[c][q] = f2(P[2 * FS + pc + c * NZC], P[3 * FS + ld + pw + c * NZC]);
+      qtw[c][q] = f2(P[2 * FS + pc + c * NZC], P[NF * FS + ld + pw + c * NZC]);
     }
   }
+  // the inner Laplacians of u, v at x-1 and x (planes 2 and 3; x+1 comes
+  // from the ring each step): the biharmonic's x-neighbours
+  float2 lw[3] = {f2(0.0f, 0.0f), f2(0.0f, 0.0f), f2(0.0f, 0.0f)};
+  if (lapf) {
+    lw[0] = f2(smx[2 * SLOT + 3 * FS + pc], smx[2 * SLOT + 4 * FS + pc]);
+    lw[1] = f2(smx[3 * SLOT + 3 * FS + pc], smx[3 * SLOT + 4 * FS + pc]);
+  }
+  // per-level constants of the production components (one cell per thread)
+  const float spa = spg ? (float)s.sp_a[kb] : 0.0f, spah = spg ? (float)s.sp_ah[kb] : 0.0f;
+  const float spal = spg ? (float)s.sp_ah[NZ] : 0.0f;  // the lid's
+  const float dragk = drg ? (float)(s.drag_cd / s.drag_dz * s.drag_w[kb]) : 0.0f;
+  const float dnu = (float)s.diff_nu, rdx2 = (float)(1.0 / s.diff_dx2),
+              rdy2 = (float)(1.0 / s.diff_dy2);
   // planes 0..2 are read only here; 7 and 8 refill the slots of 0 and 1
 #pragma unroll
   for (int q = 0; q < 3; ++q) release(q);
@@ -332,13 +362,13 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
         const float* Pu = P;
         const float* Pv = P + FS;
         const float* Pt = P + 2 * FS;
-        const float* Pw = P + 3 * FS;
+        const float* Pw = P + NF * FS;
         const float hr = heat ? (float)s.heat_r[col] : 0.0f;
 #pragma unroll
         for (int c = 0; c < KC; ++c) {
           const int cp = pc + c * NZC, cw = pwx + c * NZC;
           quv[c][(uu + 6) % 7] = f2(N[cp], N[FS + cp]);
-          qtw[c][(uu + 6) % 7] = f2(N[2 * FS + cp], N[3 * FS + pwn + c * NZC]);
+          qtw[c][(uu + 6) % 7] = f2(N[2 * FS + cp], N[NF * FS + pwn + c * NZC]);
           // the windows in x order: x-3 .. x+3
           float2 wuv[7], wtw[7];
 #pragma unroll
@@ -368,24 +398,71 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
               __ffma2_rn(f2(um, vm), m1, f2(Pu[cp + zp[c]], Pv[cp + zp[c]])), f2(fz[c], fz[c]));
           const float2 ctwz = __ffma2_rn(__ffma2_rn(f2(tm, wm1), m1, f2(Pt[cp + zp[c]], wp1)),
                                          f2(fz[c], inv2dz), f2(dth0k[c], 0.0f));
-          const float2 Xuv = ws5_pair(wuv, f2(nsgn(uc), nsgn(uc)));
-          const float2 Yuv = ws5_pair(cuv, f2(nsgn(vc), nsgn(vc)));
-          const float2 Xtw = ws5_pair(wtw, f2(nsgn(uc), nsgn(uh)));
-          const float2 Ytw = ws5_pair(ctw, f2(nsgn(vc), nsgn(vh)));
+          // x and y differences: WS5 (times 60 d) or, in the production form
+          // with centred advection, C2 (times 2 d)
+          float2 Xuv, Yuv, Xtw, Ytw;
+          if (ws5) {
+            Xuv = ws5_pair(wuv, f2(nsgn(uc), nsgn(uc)));
+            Yuv = ws5_pair(cuv, f2(nsgn(vc), nsgn(vc)));
+            Xtw = ws5_pair(wtw, f2(nsgn(uc), nsgn(uh)));
+            Ytw = ws5_pair(ctw, f2(nsgn(vc), nsgn(vh)));
+          } else {
+            Xuv = __ffma2_rn(wuv[2], m1, wuv[4]);
+            Yuv = __ffma2_rn(cuv[2], m1, cuv[4]);
+            Xtw = __ffma2_rn(wtw[2], m1, wtw[4]);
+            Ytw = __ffma2_rn(ctw[2], m1, ctw[4]);
+          }
+          const float sx = ws5 ? inv60dx : (float)s.inv2dx;
+          const float sy = ws5 ? inv60dy : (float)s.inv2dy;
           // tendencies -(u d/dx + v d/dy + w d/dz): (u, v) advected by
           // (uc, vc, wc), (theta', w) by (uc, vc, wc) and (uh, vh, wk)
-          const float nux = -uc * inv60dx, nvy = -vc * inv60dy;
+          const float nux = -uc * sx, nvy = -vc * sy;
           float2 tuv = __fmul2_rn(f2(nux, nux), Xuv);
           tuv = __ffma2_rn(f2(nvy, nvy), Yuv, tuv);
           tuv = __ffma2_rn(f2(-wc, -wc), cuvz, tuv);
-          float2 ttw = __fmul2_rn(f2(nux, -uh * inv60dx), Xtw);
-          ttw = __ffma2_rn(f2(nvy, -vh * inv60dy), Ytw, ttw);
+          float2 ttw = __fmul2_rn(f2(nux, -uh * sx), Xtw);
+          ttw = __ffma2_rn(f2(nvy, -vh * sy), Ytw, ttw);
           ttw = __ffma2_rn(f2(-wc, -wk), ctwz, ttw);
           const size_t oc = o + c * NZC, owc = ow + c * NZC;
           if (cor) tuv = __ffma2_rn(f2(f, -f), f2(vc - v_env, uc - u_env), tuv);
+          if constexpr (PROD) {
+            if (drg) {  // the surface wind of the column drives the drag
+              const float up0 = Pu[pc - kb] - (float)s.drag_u_env;
+              const float vp0 = Pv[pc - kb] - (float)s.drag_v_env;
+              const float al = dragk * sqrtf(up0 * up0 + vp0 * vp0);
+              tuv = __ffma2_rn(f2(-al, -al),
+                               f2(uc - (float)s.drag_u_env, vc - (float)s.drag_v_env), tuv);
+            }
+            if (spg) {
+              tuv = __ffma2_rn(f2(-spa, -spa),
+                               f2(uc - (float)s.sp_u_env, vc - (float)s.sp_v_env), tuv);
+              ttw.x = ttw.x + (-spa) * wtw[3].x;
+            }
+            if (dif == 1) {  // 5-point Laplacian of u, v
+              const float2 lx = __ffma2_rn(f2(-2.0f, -2.0f), wuv[3], __fadd2_rn(wuv[2], wuv[4]));
+              const float2 ly = __ffma2_rn(f2(-2.0f, -2.0f), wuv[3], __fadd2_rn(cuv[2], cuv[4]));
+              tuv = __ffma2_rn(f2(dnu, dnu),
+                               __ffma2_rn(lx, f2(rdx2, rdx2), __fmul2_rn(ly, f2(rdy2, rdy2))),
+                               tuv);
+            } else if (dif == 2) {  // 5-point Laplacian of the inner Laplacians
+              lw[2] = f2(smx[((uu + 4) % 7) * SLOT + 3 * FS + pc],
+                         smx[((uu + 4) % 7) * SLOT + 4 * FS + pc]);
+              const float2 yl = f2(P[3 * FS + pc - NZ], P[4 * FS + pc - NZ]);
+              const float2 yu = f2(P[3 * FS + pc + NZ], P[4 * FS + pc + NZ]);
+              const float2 lx = __ffma2_rn(f2(-2.0f, -2.0f), lw[1], __fadd2_rn(lw[0], lw[2]));
+              const float2 ly = __ffma2_rn(f2(-2.0f, -2.0f), lw[1], __fadd2_rn(yl, yu));
+              tuv = __ffma2_rn(f2(-dnu, -dnu),
+                               __ffma2_rn(lx, f2(rdx2, rdx2), __fmul2_rn(ly, f2(rdy2, rdy2))),
+                               tuv);
+              lw[0] = lw[1];
+              lw[1] = lw[2];
+            }
+            if (cool) ttw.x = ttw.x + (-(float)s.cool_alpha) * wtw[3].x;
+          }
           if (dmp) tuv = __fadd2_rn(tuv, f2(dmp_u[oc], dmp_v[oc]));
           if (heat) ttw.x = ttw.x + hr * heatz[c];
-          if (kb + c * NZC == 0) ttw.y = 0.0f;  // w: no tendency at the surface
+          if (kb + c * NZC == 0) ttw.y = 0.0f;  // w: no advection at the surface
+          if (PROD && spg) ttw.y = ttw.y + (-spah) * wk;  // w's sponge, every half level
           if (OUTMODE == 0) {
             tuv = __ffma2_rn(f2(dts, dts), tuv, wuv[3]);
             ttw = __ffma2_rn(f2(dts, dts), ttw, wtw[3]);
@@ -394,8 +471,10 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC>::per_sm) k_slow
           vo[oc] = tuv.y;
           tho[oc] = ttw.x;
           wo[owc] = ttw.y;
-          if (kb + c * NZC == NZ - 1)  // the lid, level nz: no tendency
-            wo[owc + 1] = OUTMODE == 0 ? wp1 : 0.0f;
+          if (kb + c * NZC == NZ - 1) {  // the lid, level nz: the sponge only
+            const float tl = (PROD && spg) ? (-spal) * wp1 : 0.0f;
+            wo[owc + 1] = OUTMODE == 0 ? wp1 + dts * tl : tl;
+          }
         }
         release(st + 3);  // plane x: read for the last time
         o += plane_cells;

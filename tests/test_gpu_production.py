@@ -174,6 +174,62 @@ def test_production_fp32_slow_forms_at_marching_size():
         assert e <= 2e-5, (name, e)
 
 
+@pytest.mark.parametrize("shape, adv, diff", [
+    ((64, 40, 32), "upwind5h", "biharmonic"), ((48, 24, 80), "centered2", "biharmonic"),
+    ((96, 16, 64), "centered2", "laplacian"), ((40, 12, 48), "upwind5h", "laplacian")])
+def test_production_slow_forms_against_fp64(shape, adv, diff):
+    """The production slow tendency (advection, f-plane Coriolis, surface
+    drag, sponge, Laplacian or biharmonic diffusion, Newtonian cooling) of a
+    random state in every FP32 slow form the grid allows -- the gather
+    (variant 0) and the plane-staged x-march's production form (4, 8; its
+    planes carry the inner Laplacians) -- against the FP64 tendency of the
+    same input: within 2e-5 of each field's max |tendency|.  The shapes cover
+    y-halos that wrap at both ends, several x-segments and a short last one,
+    and the lid (w's sponge on every half level)."""
+    from oraclev8_b200 import _lib as L
+    from oraclev8_b200._plan import Plan, PlanSpec
+    from oraclev8_b200.solver.tendency import drag_fields, sponge_fields
+    from oraclev8_b200.solver import SpongeDampingComponent, SurfaceDragComponent
+    nx, ny, nz = shape
+    Lx, Ly, Lz = nx * 20e3, ny * 20e3, 16e3
+    base = Base(nz, Lz)
+    z = np.asarray(base.z)
+    extra = dict(advection=L.OB_ADV_UPWIND5H if adv == "upwind5h" else L.OB_ADV_CENTERED2,
+                 coriolis=L.OB_COR_FPLANE, f0=5e-5,
+                 diffusion=L.OB_DIFF_BIHARMONIC if diff == "biharmonic" else L.OB_DIFF_LAPLACIAN,
+                 diff_nu=1e13 if diff == "biharmonic" else 2e4,
+                 diff_dx2=(Lx / nx) ** 2, diff_dy2=(Ly / ny) ** 2, cooling=True,
+                 cool_alpha=1.0 / 3600.0,
+                 **drag_fields(SurfaceDragComponent(2e-3, 2000.0, -3.0, 1.0), z),
+                 **sponge_fields(SpongeDampingComponent(Lz, 0.02, 0.3, -3.0, 1.0), z))
+    rng = np.random.default_rng(nx + nz)
+    fields = [np.asarray(a, np.float32).astype(np.float64) for a in (
+        10.0 * rng.standard_normal((nx, ny, nz)), 10.0 * rng.standard_normal((nx, ny, nz)),
+        0.3 * rng.standard_normal((nx, ny, nz + 1)), rng.standard_normal((nx, ny, nz)))]
+    mask = (L.OB_TEND_ADVECTION | L.OB_TEND_CORIOLIS | L.OB_TEND_DRAG | L.OB_TEND_SPONGE
+            | L.OB_TEND_DIFFUSION | L.OB_TEND_COOLING)
+
+    def plan(prec):
+        return Plan(PlanSpec(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, Lz=Lz, rho0=base.rho0,
+                             theta0=base.theta0, precision=prec, autotune=False, **extra))
+    ref = [host(t) for t in plan("fp64").tendency(mask, *(dev(a, torch.float64) for a in fields),
+                                                  30.0)]
+    forms = []
+    for xw in (0, 4, 8):
+        p = plan("fp32")
+        try:
+            p.set_variants(slow_xw=xw)
+        except ValueError:
+            continue
+        forms.append(xw)
+        out = [host(t) for t in p.tendency(mask, *(dev(a, torch.float32) for a in fields), 30.0)]
+        errs = [rel(a, r) for a, r in zip(out, ref)]
+        print(shape, adv, diff, "form", xw, " ".join(f"{e:.2e}" for e in errs))
+        for name, e in zip(("du", "dv", "dw", "dth"), errs):
+            assert e <= 2e-5, (xw, name, e)
+    assert forms[0] == 0 and 4 in forms, forms
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32r"])
 def test_production_run_loop_matches_reference(golden_dir, precision):
     """The production run loop of the reference (run_storm.py:120-172) through
