@@ -1,17 +1,21 @@
-// Slow tendency + forward-Euler half step for FP32 state with WS5 advection,
-// marching along x over planes staged in shared memory by the bulk-copy
-// (TMA) engine: k_slow_xt.  Same terms per cell as k_slow_xw / k_slow_f32
-// (advection tendency.py:965-1062, Coriolis :1220-1234, divergence damping,
-// heating :1731-1732; the half step integrator.py:346-370), in single
-// precision held to its rounding rather than to the reference's operation
-// order: the WS5 derivative is formed as its centred sixth-order part less
-// sgn(a) times its dissipative part, two fields at a time with the paired
-// FP32 instructions (u with v, theta' with w).
+// Slow tendency + forward-Euler half step for FP32 state, marching along x
+// over planes staged in shared memory by the bulk-copy (TMA) engine:
+// k_slow_xt.  Same terms per cell as k_slow_xw / k_slow_f32 (WS5 advection
+// tendency.py:965-1062, Coriolis :1220-1234, divergence damping, heating
+// :1731-1732; in the production form also C2 advection, surface drag,
+// sponge, Laplacian / biharmonic diffusion and Newtonian cooling,
+// tendency.py:1318-1338, 1488-1514, 1548-1627, 1661-1668; the half step
+// integrator.py:346-370), in single precision held to its rounding rather
+// than to the reference's operation order: the WS5 derivative is formed as
+// its centred sixth-order part less sgn(a) times its dissipative part, two
+// fields at a time with the paired FP32 instructions (u with v, theta' with
+// w).
 //
 // A CTA owns R rows (y) by all NZ levels of one x-segment.  Thread t is cell
-// (row t / NZ, level t % NZ): the CTA's rows j0..j0+R-1 are consecutive in
-// memory for a fixed x, so one x-plane of the CTA with its y-halo (rows
-// j0-3..j0+R+2, periodic) is one or two contiguous runs per field.
+// (row t / (NZ / KC), level t % (NZ / KC)), and with KC = 2 also that level
+// + NZ / 2: the CTA's rows j0..j0+R-1 are consecutive in memory for a fixed
+// x, so one x-plane of the CTA with its y-halo (rows j0-3..j0+R+2, periodic)
+// is one or two contiguous runs per field.
 //
 // * The planes arrive by cp.async.bulk, one instruction per run, issued by
 //   one thread, completion counted on an mbarrier per ring slot.  w's rows of
@@ -24,7 +28,8 @@
 // * A ring of 7 plane slots: at step x = i the CTA reads plane i (y- and
 //   z-neighbours) and plane i + 3 (the x-window's new column), while planes
 //   up to i + 6 are in flight: the copies are issued three steps ahead.
-// * Each thread keeps 7-point x-windows of the four fields in registers.
+// * Each thread keeps 7-point x-windows of the four fields in registers (and,
+//   for the biharmonic, 3-point windows of the inner Laplacians).
 //   Steps run in groups of 7 with the group unrolled, so the window's
 //   rotation and the ring's slot indices are compile-time: every shared-
 //   memory read is a register base plus an immediate (NZ is a template
