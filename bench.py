@@ -328,8 +328,14 @@ def kernel_bytes(w, S, fast_stages=3, slow_projections=2):
     P = slow_projections + fast_stages
     fx = (slow_projections * (2 * n * S + nw * S) + fast_stages * (3 * n * S + nw * S)) / P \
         + 2 * ns * c
-    ix = 2 * ns * c + (slow_projections * (2 * (2 * n + nw) * S + n * S)
-                       + fast_stages * ((3 * n + nw) * S + (3 * n + nw) * S)) / P
+    # inverse x: the two spectra in; a slow projection reads and writes
+    # (u, v, w), a fast stage reads (u, v, w, b_half) and writes (u, v, w);
+    # the potential is stored only where the step keeps it (the last fast
+    # stage and the last slow projection)
+    phi_writes = (1 if fast_stages else 0) + (1 if slow_projections else 0)
+    ix = 2 * ns * c + (slow_projections * 2 * (2 * n + nw) * S
+                       + fast_stages * ((2 * n + 2 * nw) * S + (2 * n + nw) * S)
+                       + phi_writes * n * S) / P
     heat = (nx * ny + nz) * 8 if w["heating"] else 0
     return {
         "fx": fx, "fy": 3 * ns * c, "thomas": 2 * ns * c, "iy": 3 * ns * c, "ix": ix,

@@ -319,7 +319,10 @@ long oracle_b200_launch_count(const OraclePlan *plan);
 #define OB_PROF_DIAG 6    /* step diagnostics reductions */
 #define OB_PROF_OTHER 7
 #define OB_PROF_REFINE 8  /* defect-correction passes of single-precision plans */
-#define OB_PROF_CLASSES 9
+#define OB_PROF_THOMAS_LW 9  /* long-wave FP64 columns of a single-precision solve: a few
+                              * CTAs on the plan's side stream, concurrent with the
+                              * OB_PROF_THOMAS sweep of every other column */
+#define OB_PROF_CLASSES 10
 int oracle_b200_profile(OraclePlan *plan, int enable);
 int oracle_b200_profile_read(OraclePlan *plan, double *ms, long *counts, int nclasses);
 

@@ -47,7 +47,8 @@ VARIANTS = ("zc2_fx", "zc2_fxs", "zc2_ix", "zc2_fy", "zc2_iy", "zc3_fx", "zc3_fx
             "zc3_fxd", "zc3_fy", "zc3_fyd", "zc4_fx", "zc4_fxs", "zc4_ix", "zc4_fxd", "zc4_fy",
             "zc4_iy", "slow_xw", "thomas_fast", "rzc2_fx", "rzc2_fy", "zc4_fyd")
 OB_TUNE_FORCE = 1
-PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine")
+PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine",
+                "thomas_lw")
 
 
 class GridDesc(ctypes.Structure):

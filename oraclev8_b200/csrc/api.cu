@@ -995,7 +995,10 @@ int thomas_solve(OraclePlan* p, int cls, cplx<T>* S3, double* diag, int slot_c, 
     // stream, beside the single-precision one
     OB_CUDA(cudaEventRecord(p->ev_fork, st));
     OB_CUDA(cudaStreamWaitEvent(p->aux, p->ev_fork, 0));
-    { Launch L_(p, cls, p->aux); k_thomas<T, kThomasCols, double><<<(unsigned)p->n_lw, kThomasCols, smem_thomas(p, 8), p->aux>>>(
+    // timed as a class of its own: it overlaps the single-precision sweep,
+    // so its events span that sweep too, and it moves few bytes
+    const int cls_lw = (cls == OB_PROF_THOMAS) ? OB_PROF_THOMAS_LW : cls;
+    { Launch L_(p, cls_lw, p->aux); k_thomas<T, kThomasCols, double><<<(unsigned)p->n_lw, kThomasCols, smem_thomas(p, 8), p->aux>>>(
           p->g, thomas_args(p), S3, S3, diag, slot_c, slot_d, p->lw_blocks, nullptr); }
     OB_LAUNCHED();
     // A solve that logs its residuals (every diag_every-th solve, counted
@@ -1581,9 +1584,11 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
     RC((slow_impl<T, 0>(p, all, dts, (const T*)in->u, (const T*)in->v, (const T*)in->w,
                         (const T*)in->theta_prime, (T*)p->Au, (T*)p->Av, (T*)p->Aw,
                         (T*)p->Ath, st)));
+    // its potential is never read: the fast stages (or, without buoyancy,
+    // the projection of y^n below) write the potential the step reports
     if (mom && p->projection)
       RC(project_impl<T>(p, (T*)p->Au, (T*)p->Av, (T*)p->Aw, nullptr, -1.0, (T*)p->Au,
-                         (T*)p->Av, (T*)p->Aw, (T*)p->Aphi, OB_DIAG_LAST_COMPAT,
+                         (T*)p->Av, (T*)p->Aw, (T*)nullptr, OB_DIAG_LAST_COMPAT,
                          OB_DIAG_LAST_DISC, st));
     else
       RC(copy_field<T>(p->Aphi, in->phi, n, st));
@@ -1609,10 +1614,13 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
       OB_LAUNCHED();
       bh = (const T*)p->Bh;
     }
+    // every stage starts from the anchor state, so only the last stage's
+    // potential is read (by the diagnostics and as the reported potential)
     for (int s = 0; s < 3; ++s) {
       const double sdt = alphas[s] * dt;
       RC(project_impl<T>(p, au, av, aw, ath, sdt, (T*)p->Su, (T*)p->Sv, (T*)p->Sw,
-                         (T*)p->Sphi, OB_DIAG_COMPAT0 + s, OB_DIAG_DISC0 + s, st, bh));
+                         s == 2 ? (T*)p->Sphi : (T*)nullptr, OB_DIAG_COMPAT0 + s,
+                         OB_DIAG_DISC0 + s, st, bh));
     }
     su = (const T*)p->Su;
     sv = (const T*)p->Sv;

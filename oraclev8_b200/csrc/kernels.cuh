@@ -691,6 +691,7 @@ enum IxMode { IX_CORRECT = 0, IX_STAGE = 1, IX_GRAD = 2, IX_FIELDS = 3, IX_REFIN
 //   IX_GRAD:    gx, gy (full levels), gz (nz+1 half levels, zero ends)
 //               (tendency.py:487-500).
 //   IX_FIELDS:  real outputs of nf spectra.
+// In IX_CORRECT and IX_STAGE a null phi_out stores no potential.
 template <class T, int MODE, class TS = T>
 __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int nf,
                                             const cplx<T>* __restrict__ phs,
@@ -854,7 +855,7 @@ __global__ void __launch_bounds__(256, 2) k_ix(GridK g, FftPlan px, int zc, int 
     if (z == nz - 1 && (MODE == IX_STAGE || w_out != w_in)) w_out[wi + 1] = wt;
     if (MODE == IX_REFINE)
       phi_out[idx] = (TS)((T)phi_out[idx] + phi);
-    else
+    else if (phi_out)  // null: the caller discards this projection's potential
       phi_out[idx] = (TS)phi;
   }
 }

@@ -218,7 +218,8 @@ __host__ __device__ inline Ix2Layout ix2_layout(int nx) {
 //   IX_STAGE:   out = (u_n - gx, v_n - gy, w_n + sdt b_half - gz, phi)
 //               (integrator.py:483-500), b_half given as the field bh.
 //   IX_REFINE:  as IX_CORRECT but phi_out += phi (a correction potential).
-// grid = (ceil(nz/ZC), ny).
+// In IX_CORRECT and IX_STAGE a null phi_out stores no potential (a projection
+// whose potential the step overwrites unread).  grid = (ceil(nz/ZC), ny).
 template <class T, int MODE, class TS, int ZC>
 __global__ void __launch_bounds__(kPencilThreads, x2_min_blocks<T, ZC>()) k_ix2(
     GridK g, FftPlan px, const cplx<T>* __restrict__ phs, const cplx<T>* __restrict__ psi,
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kPencilThreads, x2_min_blocks<T, ZC>()) k_ix2(
     if (z == nz - 1 && (STAGE || w_out != w_in)) w_out[wi + 1] = wt;
     if (MODE == IX_REFINE)
       phi_out[idx] = (TS)((T)phi_out[idx] + phi);
-    else
+    else if (phi_out)  // null: the caller discards this projection's potential
       phi_out[idx] = (TS)phi;
   }
 }

@@ -265,7 +265,8 @@ template <int ZC>
 constexpr int ix3_min_blocks() { return ZC >= 8 ? 2 : 3; }
 
 // Inverse x-pencil kernel with the velocity correction (k_ix2 semantics and
-// modes, FP32, nx = 512).  grid = (ceil(nz/ZC), ny), 16 (3 ZC + 2) threads.
+// modes, FP32, nx = 512; in IX_CORRECT and IX_STAGE phi_out may be
+// null).  grid = (ceil(nz/ZC), ny), 16 (3 ZC + 2) threads.
 // IX_FIELDS: the real C2R outputs of two spectra, u_out = C2R(phs) and
 // v_out = C2R(psi) (what k_ix IX_FIELDS writes: the Helmholtz damper's inverse
 // x transform); no state is read and nothing else is written.
@@ -488,15 +489,15 @@ __global__ void __launch_bounds__(16 * (3 * ZC + 2), ix3_min_blocks<ZC>()) k_ix3
     if (two && st2) {
       *reinterpret_cast<float2*>(&u_out[idx]) = make_float2(su.x - gx0, su.y - gx1);
       *reinterpret_cast<float2*>(&v_out[idx]) = make_float2(sv.x - gy0, sv.y - gy1);
-      *reinterpret_cast<float2*>(&phi_out[idx]) = make_float2(p0, p1);
+      if (phi_out) *reinterpret_cast<float2*>(&phi_out[idx]) = make_float2(p0, p1);
     } else {
       u_out[idx] = su.x - gx0;
       v_out[idx] = sv.x - gy0;
-      phi_out[idx] = p0;
+      if (phi_out) phi_out[idx] = p0;
       if (two) {
         u_out[idx + 1] = su.y - gx1;
         v_out[idx + 1] = sv.y - gy1;
-        phi_out[idx + 1] = p1;
+        if (phi_out) phi_out[idx + 1] = p1;
       }
     }
     w_out[wi] = w0 - gz0;

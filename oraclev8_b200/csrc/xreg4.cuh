@@ -264,8 +264,8 @@ template <int ZC>
 constexpr int ix4_min_blocks() { return ZC >= 8 ? 1 : 2; }
 
 // Inverse x-pencil kernel with the velocity correction (k_ix3 semantics at
-// nx = 1024; modes IX_CORRECT, IX_STAGE, IX_REFINE).  grid = (ceil(nz/ZC), ny),
-// 32 (3 ZC + 1) threads.
+// nx = 1024; modes IX_CORRECT, IX_STAGE, IX_REFINE; phi_out may be null outside
+// IX_REFINE).  grid = (ceil(nz/ZC), ny), 32 (3 ZC + 1) threads.
 template <int MODE, int ZC>
 __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4(
     GridK g, const cplx<float>* __restrict__ phs, const cplx<float>* __restrict__ psi,
@@ -523,15 +523,15 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
     if (two && st2) {
       *reinterpret_cast<float2*>(&u_out[idx]) = make_float2(su[i][0] - gx0, su[i][1] - gx1);
       *reinterpret_cast<float2*>(&v_out[idx]) = make_float2(sv[i][0] - gy0, sv[i][1] - gy1);
-      *reinterpret_cast<float2*>(&phi_out[idx]) = make_float2(p0, p1);
+      if (phi_out) *reinterpret_cast<float2*>(&phi_out[idx]) = make_float2(p0, p1);
     } else {
       u_out[idx] = su[i][0] - gx0;
       v_out[idx] = sv[i][0] - gy0;
-      phi_out[idx] = p0;
+      if (phi_out) phi_out[idx] = p0;
       if (two) {
         u_out[idx + 1] = su[i][1] - gx1;
         v_out[idx + 1] = sv[i][1] - gy1;
-        phi_out[idx + 1] = p1;
+        if (phi_out) phi_out[idx + 1] = p1;
       }
     }
     w_out[wi] = w0 - gz0;
