@@ -1414,7 +1414,8 @@ bool slow_xt_grid(const OraclePlan* p, int v) {
   const bool adv = p->advection == OB_ADV_UPWIND5H || p->advection == OB_ADV_CENTERED2;
   return p->prec == OB_PREC_F32 && adv && (nz == 32 || nz == 48 || nz == 64 || nz == 80) &&
          (v == 4 || v == 8 || ((v == 24 || v == 28) && !slow_xt_prod(p))) &&
-         p->g.ny % r == 0 && p->g.ny >= r + 6 && p->g.nx >= 7;
+         p->g.ny % r == 0 && p->g.ny >= r + 6 && p->g.nx >= 7 &&
+         (long long)p->g.nx * p->g.ny * (p->g.nz + 1) < (1ll << 31);  // 32-bit offsets
 }
 template <int NZ, int R, int KC, bool PROD = false>
 int slow_xt_attr() {

@@ -218,9 +218,10 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
     return px;
   };
   // where w's run starts in its slot: its first float's offset mod 4 (the
-  // 16-byte aligned copy starts that many floats before it; exact mod 4 in
-  // 32-bit arithmetic)
-  auto lead_of = [&](int px) { return ((px * ny + ga) * NW) & 3; };
+  // 16-byte aligned copy starts that many floats before it).  The run of
+  // plane px starts at float (px ny + ga) NW, and ny % 4 == 0, so the lead is
+  // (ga NW) mod 4 for every plane of the CTA.
+  const int lead = (ga * NW) & 3;
   unsigned long long* full = bar;
   unsigned long long* empty = bar + C::NSLOT;
   // w's run of plane px: floats [wa, we) and, wrapped, [w2, w2e); piece 1
@@ -290,11 +291,10 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     const float* P = smx + q * SLOT;
-    const int ld = lead_of(plane_x(q));
 #pragma unroll
     for (int c = 0; c < KC; ++c) {
       quv[c][q] = f2(P[pc + c * NZC], P[FS + pc + c * NZC]);
-      qtw[c][q] = f2(P[2 * FS + pc + c * NZC], P[NF * FS + ld + pw + c * NZC]);
+      qtw[c][q] = f2(P[2 * FS + pc + c * NZC], P[NF * FS + lead + pw + c * NZC]);
     }
   }
   // the inner Laplacians of u, v at x-1 and x (planes 2 and 3; x+1 comes
@@ -332,25 +332,31 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
     zp[c] = (k < NZ - 1) ? 1 : 0;
     fz[c] = (k == 0 || k == NZ - 1) ? invdz : inv2dz;
   }
-  const size_t plane_cells = (size_t)ny * NZ, plane_w = (size_t)ny * NW;
-  size_t o = ((size_t)i0 * ny + j) * NZ + kb;
-  size_t ow = ((size_t)i0 * ny + j) * NW + kb;
-  size_t col = (size_t)i0 * ny + j;
+  // 32-bit element offsets (the host admits grids of fewer than 2^31 w
+  // values)
+  const unsigned plane_cells = (unsigned)ny * NZ, plane_w = (unsigned)ny * NW;
+  unsigned o = ((unsigned)i0 * ny + j) * NZ + kb;
+  unsigned ow = ((unsigned)i0 * ny + j) * NW + kb;
+  unsigned col = (unsigned)i0 * ny + j;
+  const int pwx = pw + lead;  // this cell's w level in every plane
 
   int iw = 0;  // the warp that issues this step's copies (lane 0)
-  for (int s0 = 0; ok && s0 < len; s0 += 7) {
+  // group gi = s0 / 7 of steps; gp = gi mod 2.  Plane q is the (q / 7)-th
+  // fill of slot q % 7, so the wait for plane st + 6 (st = s0 + uu) is on
+  // phase parity (gi + (uu >= 1)) mod 2 and the release of plane st + 2 on
+  // (gi + (uu >= 5)) mod 2: compile-time offsets, no division per step.
+  for (int s0 = 0, gp = 0; ok && s0 < len; s0 += 7, gp ^= 1) {
 #pragma unroll
     for (int uu = 0; uu < 7; ++uu) {
       const int st = s0 + uu;  // step: x = i0 + st
       if (ok && st < len) {
         // plane st + 6 (the window's new column) must have landed
-        const int qn = st + 6;
-        ok = mbar_wait(&full[(uu + 6) % 7], (unsigned)((qn / 7) & 1));
+        ok = mbar_wait(&full[(uu + 6) % 7], (unsigned)((gp + (uu >= 1 ? 1 : 0)) & 1));
         // refill the slot of plane st + 2 (last read in the previous step)
         // with plane st + 9, once every warp has released it
         if (st + 9 <= qmax) {
           if (warp == iw && lane == 0 && ok) {
-            ok = mbar_wait(&empty[(uu + 2) % 7], (unsigned)(((st + 2) / 7) & 1));
+            ok = mbar_wait(&empty[(uu + 2) % 7], (unsigned)((gp + (uu >= 5 ? 1 : 0)) & 1));
             if (ok) issue(st + 9, (uu + 2) % 7);
           }
           qlast = st + 9;
@@ -360,10 +366,6 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
 
         const float* P = smx + ((uu + 3) % 7) * SLOT;  // plane x
         const float* N = smx + ((uu + 6) % 7) * SLOT;  // plane x + 3
-        const int x = i0 + st;
-        const int pwx = pw + lead_of(x);
-        const int xn = x + 3 - ((x + 3 >= nx) ? nx : 0);
-        const int pwn = pw + lead_of(xn);
         const float* Pu = P;
         const float* Pv = P + FS;
         const float* Pt = P + 2 * FS;
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
         for (int c = 0; c < KC; ++c) {
           const int cp = pc + c * NZC, cw = pwx + c * NZC;
           quv[c][(uu + 6) % 7] = f2(N[cp], N[FS + cp]);
-          qtw[c][(uu + 6) % 7] = f2(N[2 * FS + cp], N[NF * FS + pwn + c * NZC]);
+          qtw[c][(uu + 6) % 7] = f2(N[2 * FS + cp], N[NF * FS + pwx + c * NZC]);
           // the windows in x order: x-3 .. x+3
           float2 wuv[7], wtw[7];
 #pragma unroll
@@ -428,7 +430,7 @@ __global__ void __launch_bounds__(R * NZ / KC, SlowXt<NZ, R, KC, PROD>::per_sm) 
           float2 ttw = __fmul2_rn(f2(nux, -uh * sx), Xtw);
           ttw = __ffma2_rn(f2(nvy, -vh * sy), Ytw, ttw);
           ttw = __ffma2_rn(f2(-wc, -wk), ctwz, ttw);
-          const size_t oc = o + c * NZC, owc = ow + c * NZC;
+          const unsigned oc = o + c * NZC, owc = ow + c * NZC;
           if (cor) tuv = __ffma2_rn(f2(f, -f), f2(vc - v_env, uc - u_env), tuv);
           if constexpr (PROD) {
             if (drg) {  // the surface wind of the column drives the drag

@@ -60,6 +60,7 @@ def w_runs(px, ny, nz, ga, nb, r):
 
 def check_grid(nx, ny, nz, r):
     assert nz in (32, 48, 64, 80) and ny % r == 0 and ny >= r + 6 and nx >= 7
+    assert nx * ny * (nz + 1) < 2 ** 31  # the kernel's 32-bit element offsets
     nw, rh = nz + 1, r + 6
     ws = (rh * nw + 8 + 3) // 4 * 4  # the slot's w region (floats)
     total_w = nx * ny * nw
@@ -70,6 +71,7 @@ def check_grid(nx, ny, nz, r):
         for px in range(nx):
             w0, wa, we, w2, w2e = w_runs(px, ny, nz, ga, nb, r)
             lead = w0 & 3
+            assert lead == (ga * nw) & 3  # the kernel takes one lead for every plane
             assert wa % 4 == 0 and wa >= 0 and we <= total_w and (we - wa) % 4 == 0
             if nb:
                 assert we == w0 + na * nw and we % 4 == 0 and w2 % 4 == 0
@@ -110,6 +112,10 @@ def check_ring(ln):
             issue(q, q - 7)
     for st in range(ln):
         uu = st % 7
+        gp = (st // 7) % 2  # the kernel's group parity
+        # phase parities of the waits: plane q is the (q // 7)-th fill of its slot
+        assert (gp + (uu >= 1)) % 2 == ((st + 6) // 7) % 2
+        assert (gp + (uu >= 5)) % 2 == ((st + 2) // 7) % 2
         assert slot[(uu + 6) % 7] == st + 6
         waited.add(st + 6)
         if st + 9 <= qmax:
