@@ -319,15 +319,25 @@ def reference_procs():
 # per-kernel algorithmic bytes (the kernel's own I/O contract)
 # ---------------------------------------------------------------------------
 
-def kernel_bytes(w, S, fast_stages=3, slow_projections=2):
+def kernel_bytes(w, S, fast_stages=3, slow_projections=2, shared_stages=False):
+    """Algorithmic bytes per launch of each class (the mean over the step's
+    launches of the class).  shared_stages: the fast stages' forward x
+    transforms come from one launch over the anchor state (three spectra
+    written), and each stage's y launch reads three spectra."""
     nx, ny, nz = w["nx"], w["ny"], w["nz"]
     n = nx * ny * nz
     nw = nx * ny * (nz + 1)
     ns = (nx // 2 + 1) * ny * nz  # complex half-spectrum elements
     c = 2 * S
     P = slow_projections + fast_stages
-    fx = (slow_projections * (2 * n * S + nw * S) + fast_stages * (3 * n * S + nw * S)) / P \
-        + 2 * ns * c
+    # forward x: a slow projection reads (u, v, w), a stage (u, v, w, b_half)
+    fx_slow, fx_stage = (2 * n + nw) * S + 2 * ns * c, (2 * n + 2 * nw) * S + 2 * ns * c
+    if shared_stages and fast_stages:
+        fx = (slow_projections * fx_slow + fx_stage + ns * c) / (slow_projections + 1)
+        fy = (slow_projections * 3 * ns * c + fast_stages * 4 * ns * c) / P
+    else:
+        fx = (slow_projections * fx_slow + fast_stages * fx_stage) / P
+        fy = 3 * ns * c
     # inverse x: the two spectra in; a slow projection reads and writes
     # (u, v, w), a fast stage reads (u, v, w, b_half) and writes (u, v, w);
     # the potential is stored only where the step keeps it (the last fast
@@ -338,7 +348,7 @@ def kernel_bytes(w, S, fast_stages=3, slow_projections=2):
                        + phi_writes * n * S) / P
     heat = (nx * ny + nz) * 8 if w["heating"] else 0
     return {
-        "fx": fx, "fy": 3 * ns * c, "thomas": 2 * ns * c, "iy": 3 * ns * c, "ix": ix,
+        "fx": fx, "fy": fy, "thomas": 2 * ns * c, "iy": 3 * ns * c, "ix": ix,
         "slow": 2 * (3 * n + nw) * S + heat, "diag": (4 * n + nw) * S,
     }
 
@@ -564,7 +574,7 @@ def run_b200(args):
 
     # ---- roofline of the dominant kernel ------------------------------------
     peak, peak_kind = load_peaks()
-    kb = kernel_bytes(w, S)
+    kb = kernel_bytes(w, S, shared_stages=bool(integ.plan.variants().get("zc4_fxsh")))
     dom = max((c for c in prof if prof[c][1] > 0 and c in kb), key=lambda c: prof[c][0])
     dms, dn = prof[dom]
     ach = kb[dom] / (dms / dn / 1e3) / 1e9

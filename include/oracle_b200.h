@@ -122,7 +122,12 @@ extern "C" {
 #define OB_VAR_RZC2_FX 19
 #define OB_VAR_RZC2_FY 20
 #define OB_VAR_ZC4_FYD 21   /* FP64 residual y at ny = 1024 (register form, 0 or 2) */
-#define OB_VAR_COUNT 22
+#define OB_VAR_ZC4_FXSH 22  /* FP32 1024 x 1024 plans with fast stages: the three stages'
+                             * forward x transforms in one launch of the anchor state
+                             * (their divergence is linear in the stage's sdt), each
+                             * stage's y pencils forming its spectrum; z-chunk, 0 = off;
+                             * takes effect with the 1024-point y pencils (zc4_fy) */
+#define OB_VAR_COUNT 23
 
 #define OB_TUNE_FORCE 1  /* time the candidates even when a choice is cached */
 

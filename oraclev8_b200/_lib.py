@@ -45,7 +45,7 @@ EXPORTS = (
 # kernel-variant choices of a plan, in OB_VAR_* order (include/oracle_b200.h)
 VARIANTS = ("zc2_fx", "zc2_fxs", "zc2_ix", "zc2_fy", "zc2_iy", "zc3_fx", "zc3_fxs", "zc3_ix",
             "zc3_fxd", "zc3_fy", "zc3_fyd", "zc4_fx", "zc4_fxs", "zc4_ix", "zc4_fxd", "zc4_fy",
-            "zc4_iy", "slow_xw", "thomas_fast", "rzc2_fx", "rzc2_fy", "zc4_fyd")
+            "zc4_iy", "slow_xw", "thomas_fast", "rzc2_fx", "rzc2_fy", "zc4_fyd", "zc4_fxsh")
 OB_TUNE_FORCE = 1
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine",
                 "thomas_lw")

@@ -228,6 +228,10 @@ struct OraclePlan {
   // forward x (stage / correction), inverse x, the FP64 residual x transform,
   // and the y pencils (ny = 1024); z-chunk, 0 = off
   int zc4_fxs = 0, zc4_fx = 0, zc4_ix = 0, zc4_fxd = 0, zc4_fy = 0, zc4_iy = 0, zc4_fyd = 0;
+  // the three fast stages from one forward x transform of the anchor state
+  // (k_fx4 with four column groups into S4..S6, then k_fy4 forming each
+  // stage's divergence spectrum): its z-chunk, 0 = off; needs zc4_fy
+  int zc4_fxsh = 0;
   // FP32 slow tendency: 0 the gather form, 1 marching along x (k_slow_xw),
   // 4 / 8 marching along x over bulk-copied planes of 4 / 8 rows (k_slow_xt)
   int slow_xw = 1;
@@ -246,6 +250,9 @@ struct OraclePlan {
   void *twx = nullptr, *twy = nullptr;
   // scratch
   void *S1 = nullptr, *S2 = nullptr, *S3 = nullptr;           // spectral
+  // the shared stage transforms (allocated where zc4_fxsh can be on):
+  // S4 = i kx' FFTx(rho u) + FFTx(D w), S5 = FFTx(rho v), S6 = FFTx(D b_half)
+  void *S4 = nullptr, *S5 = nullptr, *S6 = nullptr;
   void *Au = nullptr, *Av = nullptr, *Aw = nullptr, *Ath = nullptr, *Aphi = nullptr;
   void *Su = nullptr, *Sv = nullptr, *Sw = nullptr, *Sphi = nullptr;
   void *Du = nullptr, *Dv = nullptr;                         // damper / temp
@@ -452,6 +459,11 @@ int xr4_attrs_zc() {
   int rc;
   if ((rc = xr4_attr_fx<float, false, ZC>()) || (rc = xr4_attr_fx<float, true, ZC>()))
     return rc;
+  OB_CUDA(cudaFuncSetAttribute(k_fx4<float, true, ZC, 4>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fx4_smem<float, true, ZC, 4>()));
+  OB_CUDA(cudaFuncSetAttribute(k_fy4<ZC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Yr4Size<ZC, 3>::total));
   if constexpr (ZC <= 4)
     if ((rc = xr4_attr_fx<double, false, ZC>())) return rc;
   for (auto k : {k_ix4<IX_CORRECT, ZC>, k_ix4<IX_STAGE, ZC>, k_ix4<IX_REFINE, ZC>})
@@ -868,7 +880,24 @@ void fx4_launch(const OraclePlan* q, const float* u, const float* v, const float
                 const float* bh, double sdt, cplx<T>* X0, cplx<T>* X1, cudaStream_t st) {
   const dim3 grid((q->g.nz + ZC - 1) / ZC, q->g.ny);
   k_fx4<T, STAGE, ZC><<<grid, 96 * ZC, fx4_smem<T, STAGE, ZC>(), st>>>(
-      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<T>*)q->twx, X0, X1);
+      q->g, u, v, w, bh, sdt, q->rho, q->rhoh, q->kx, (const cplx<T>*)q->twx, X0, X1, nullptr);
+}
+// the three fast stages' shared forward x transforms: S4, S5, S6
+template <int ZC>
+void fx4sh_launch(const OraclePlan* p, const float* u, const float* v, const float* w,
+                  const float* bh, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.ny);
+  k_fx4<float, true, ZC, 4><<<grid, 128 * ZC, fx4_smem<float, true, ZC, 4>(), st>>>(
+      p->g, u, v, w, bh, 0.0, p->rho, p->rhoh, p->kx, (const cplx<float>*)p->twx,
+      (cplx<float>*)p->S4, (cplx<float>*)p->S5, (cplx<float>*)p->S6);
+}
+void fx4sh(const OraclePlan* p, const float* u, const float* v, const float* w,
+           const float* bh, cudaStream_t st) {
+  switch (p->zc4_fxsh) {
+    case 2: fx4sh_launch<2>(p, u, v, w, bh, st); break;
+    case 4: fx4sh_launch<4>(p, u, v, w, bh, st); break;
+    default: fx4sh_launch<8>(p, u, v, w, bh, st); break;
+  }
 }
 // q's twiddles are of type T (the FP64 refiner plan for T = double)
 template <class T, bool STAGE>
@@ -940,7 +969,24 @@ void yr4_launch(const OraclePlan* p, bool inverse, const cplx<float>* in0,
   if (inverse)
     k_iy4<ZC><<<grid, 64 * ZC, Yr4Size<ZC>::total, st>>>(p->g, in0, p->ky, tw, out0, out1);
   else
-    k_fy4<ZC><<<grid, 64 * ZC, Yr4Size<ZC>::total, st>>>(p->g, in0, in1, p->ky, tw, out0);
+    k_fy4<ZC><<<grid, 64 * ZC, Yr4Size<ZC>::total, st>>>(p->g, in0, in1, p->ky, tw, out0,
+                                                         nullptr, 0.0f);
+}
+// a fast stage's forward y transform from the shared x transforms:
+// d^ = FFTy(S4 + sdt S6) + i ky' FFTy(S5) into S3
+template <int ZC>
+void fy4sh_launch(const OraclePlan* p, float sdt, cudaStream_t st) {
+  const dim3 grid((p->g.nz + ZC - 1) / ZC, p->g.nxh);
+  k_fy4<ZC, true><<<grid, 64 * ZC, Yr4Size<ZC, 3>::total, st>>>(
+      p->g, (const cplx<float>*)p->S4, (const cplx<float>*)p->S5, p->ky,
+      (const cplx<float>*)p->twy, (cplx<float>*)p->S3, (const cplx<float>*)p->S6, sdt);
+}
+void fy4sh(const OraclePlan* p, float sdt, cudaStream_t st) {
+  switch (p->zc4_fy) {
+    case 2: fy4sh_launch<2>(p, sdt, st); break;
+    case 4: fy4sh_launch<4>(p, sdt, st); break;
+    default: fy4sh_launch<8>(p, sdt, st); break;
+  }
 }
 // register-resident FP32 y pencils (ny = 1024): FY_DIV forward or the IY_GRAD inverse
 void yr4(const OraclePlan* p, bool inverse, const cplx<float>* in0, const cplx<float>* in1,
@@ -1164,10 +1210,12 @@ int proj_ix(OraclePlan* p, bool stage, const T* u, const T* v, const T* w, const
 // stage_sdt >= 0: inputs are the anchor state (u, v, w, th); the provisional
 // stage state w + sdt * b_half is formed on the fly and the projected result
 // goes to (uo, vo, wo, phio).
+// shared: a fast stage whose forward x transforms are in S4..S6 (fx4sh ran
+// on the anchor state): the y pencils form the stage's spectrum from them.
 template <class T>
 int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
                  double stage_sdt, T* uo, T* vo, T* wo, T* phio, int slot_c, int slot_d,
-                 cudaStream_t st, const T* bh = nullptr) {
+                 cudaStream_t st, const T* bh = nullptr, bool shared = false) {
   // a stage projection reads the half-level buoyancy in every form but the
   // generic one; without it a selected form would silently fall back
   if (stage_sdt >= 0.0 && !bh && (p->zc2_fxs || p->zc2_ix || p->zc3_fxs || p->zc3_ix || p->zc4_fxs ||
@@ -1186,8 +1234,13 @@ int project_impl(OraclePlan* p, const T* u, const T* v, const T* w, const T* th,
     OB_CUDA(cudaMemsetAsync(p->diag + slot_d, 0, sizeof(double), st));
   }
   const bool stage = stage_sdt >= 0.0;
-  RC(proj_fx<T>(p, stage, u, v, w, th, bh, stage_sdt, st));
-  RC(proj_fy<T>(p, st));
+  if (shared && sizeof(T) == 4 && stage) {
+    { Launch L_(p, 1, st); fy4sh(p, (float)stage_sdt, st); }
+    OB_LAUNCHED();
+  } else {
+    RC(proj_fx<T>(p, stage, u, v, w, th, bh, stage_sdt, st));
+    RC(proj_fy<T>(p, st));
+  }
   RC(thomas_solve<T>(p, 2, (cplx<T>*)p->S3, diag, slot_c, slot_d, st));
   RC(proj_iy<T>(p, 3, st));
   RC(proj_ix<T>(p, stage, u, v, w, th, bh, stage_sdt, uo, vo, wo, phio, st));
@@ -1615,13 +1668,22 @@ int step_impl(OraclePlan* p, const OracleStatePtrs* in, const OracleStatePtrs* o
       OB_LAUNCHED();
       bh = (const T*)p->Bh;
     }
+    // the stages' divergence is linear in their sdt: with the shared form
+    // one forward x launch serves all three (each stage still projects in
+    // full: its own y transforms, solve, inverse transforms and correction)
+    const bool shared = sizeof(T) == 4 && bh && p->zc4_fxsh && p->zc4_fy && p->S4;
+    if (shared) {
+      { Launch L_(p, 0, st); fx4sh(p, (const float*)au, (const float*)av, (const float*)aw,
+                                   (const float*)bh, st); }
+      OB_LAUNCHED();
+    }
     // every stage starts from the anchor state, so only the last stage's
     // potential is read (by the diagnostics and as the reported potential)
     for (int s = 0; s < 3; ++s) {
       const double sdt = alphas[s] * dt;
       RC(project_impl<T>(p, au, av, aw, ath, sdt, (T*)p->Su, (T*)p->Sv, (T*)p->Sw,
                          s == 2 ? (T*)p->Sphi : (T*)nullptr, OB_DIAG_COMPAT0 + s,
-                         OB_DIAG_DISC0 + s, st, bh));
+                         OB_DIAG_DISC0 + s, st, bh, shared));
     }
     su = (const T*)p->Su;
     sv = (const T*)p->Sv;
@@ -1837,6 +1899,7 @@ int* var_field(OraclePlan* p, int i) {
     case OB_VAR_RZC2_FX: return q ? &q->zc2_fx : nullptr;
     case OB_VAR_RZC2_FY: return q ? &q->zc2_fy : nullptr;
     case OB_VAR_ZC4_FYD: return &p->zc4_fyd;
+    case OB_VAR_ZC4_FXSH: return &p->zc4_fxsh;
   }
   return nullptr;
 }
@@ -1900,6 +1963,7 @@ std::vector<int> var_values(const OraclePlan* p, int i) {
       if (f32 && p->dbl) y2(true);
       break;
     case OB_VAR_ZC4_FYD: list(f32 && ny == kY4N && p->dbl, {2}); break;
+    case OB_VAR_ZC4_FXSH: list(f32 && p->S4 != nullptr, {2, 4, 8}); break;
   }
   return v;
 }
@@ -2048,6 +2112,22 @@ int tune_impl(OraclePlan* p, cudaStream_t st) {
     if (slow && var_values(p, OB_VAR_SLOW_XW).size() > 1)
       RC(tune_group<T>(p, {OB_VAR_SLOW_XW}, st, [&] {
         return slow_impl<T, 0>(p, all, 1.0, u, v, w, th, uo, vo, wo, (T*)p->Sphi, st);
+      }));
+    // the fast stages' forward transforms, shared or one x launch per stage:
+    // timed as the three stages' x and y launches together
+    if (stage && p->zc4_fy && var_values(p, OB_VAR_ZC4_FXSH).size() > 1)
+      RC(tune_group<T>(p, {OB_VAR_ZC4_FXSH}, st, [&] {
+        if (p->zc4_fxsh) {
+          fx4sh(p, (const float*)u, (const float*)v, (const float*)w, (const float*)bh, st);
+          for (int s = 0; s < 3; ++s) fy4sh(p, (float)(sdt * (s + 1) / 3.0), st);
+          OB_LAUNCHED();
+          return OB_OK;
+        }
+        for (int s = 0; s < 3; ++s) {
+          RC(proj_fx<T>(p, true, u, v, w, th, bh, sdt * (s + 1) / 3.0, st));
+          RC(proj_fy<T>(p, st));
+        }
+        return OB_OK;
       }));
   }
   OB_CUDA(cudaStreamSynchronize(st));
@@ -2748,6 +2828,12 @@ int oracle_b200_plan_create(const OracleGridDesc* grid, const OracleComponentDes
       ((rc = dalloc(p, &p->Lu, n * e)) || (rc = dalloc(p, &p->Lv, n * e))))
     return bail(rc);
   if (p->buoyancy && p->projection && (rc = dalloc(p, &p->Bh, nw * e))) return bail(rc);
+  // the shared stage transforms: FP32 1024 x 1024 grids with fast stages
+  if (p->buoyancy && p->projection && p->prec == OB_PREC_F32 && nx == kX4N && ny == kY4N &&
+      p->px8_ok &&
+      ((rc = dalloc(p, &p->S4, ns * 2 * e)) || (rc = dalloc(p, &p->S5, ns * 2 * e)) ||
+       (rc = dalloc(p, &p->S6, ns * 2 * e))))
+    return bail(rc);
   if (p->prec == OB_PREC_F32) {
     const long ncols = (long)p->g.nxh * ny;
     const long nblk = (ncols + kThomasCols - 1) / kThomasCols;

@@ -56,10 +56,11 @@ __device__ __forceinline__ void x4_tables(cplx<T>* ytw, cplx<T>* twN, cplx<T>* w
 // ---- forward x: k_fx4 ------------------------------------------------------------
 // Shared memory (bytes): tables, then one region that holds in turn the
 // level-major state tiles (FP32), the columns' exchange blocks and the
-// spectra (arithmetic type T).
-template <class T, bool STAGE, int ZC>
+// spectra (arithmetic type T).  NG: column groups (3: u, v, d; 4: u, v, the
+// flux divergence of w and that of b_half, kept apart).
+template <class T, bool STAGE, int ZC, int NG = 3>
 __host__ __device__ constexpr size_t fx4_smem() {
-  constexpr int B = 3 * ZC, S = x4_stride<ZC>();
+  constexpr int B = NG * ZC, S = x4_stride<ZC>();
   constexpr size_t raw = (size_t)(2 * ZC + (STAGE ? 2 : 1) * (ZC + 1)) * S * 4;
   constexpr size_t ex = (size_t)B * kWEx * sizeof(cplx<T>);
   constexpr size_t xs = (size_t)(kX4M + 1) * (B + 1) * sizeof(cplx<T>);
@@ -76,16 +77,21 @@ constexpr int fx4_min_blocks() { return (sizeof(T) == 8 || ZC >= 8) ? 1 : 2; }
 // defect correction, with k_fx2's operation order in the pack.  3 ZC columns
 // (u, v, d at ZC levels), one warp each.  grid = (ceil(nz/ZC), ny), 96 ZC
 // threads.
-template <class T, bool STAGE, int ZC>
-__global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
+// NG = 4 (FP32, STAGE): the three fast stages' transforms at once.  The
+// stage divergence is linear in sdt, so X0 = i kx' FFTx(rho u) + FFTx(D w),
+// X1 = FFTx(rho v) and X2 = FFTx(D b_half), and stage s's X0 is
+// X0 + sdt_s X2 (formed by the y pencils); 4 ZC columns, 128 ZC threads.
+template <class T, bool STAGE, int ZC, int NG = 3>
+__global__ void __launch_bounds__(32 * NG * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
     GridK g, const float* __restrict__ u, const float* __restrict__ v,
     const float* __restrict__ w, const float* __restrict__ bh, double sdt,
     const double* __restrict__ rho, const double* __restrict__ rhoh,
     const double* __restrict__ kxd, const cplx<T>* __restrict__ twx,
-    cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1) {
+    cplx<T>* __restrict__ X0, cplx<T>* __restrict__ X1, cplx<T>* __restrict__ X2) {
   static_assert(ZC == 2 || ZC == 4 || ZC == 8, "supported z-chunks");
   static_assert(sizeof(T) == 4 || !STAGE, "the FP64 form is the residual transform");
-  constexpr int B = 3 * ZC, NT = 32 * B, M = kX4M, N = kX4N, S = x4_stride<ZC>(), BP = B + 1;
+  static_assert(NG == 3 || (NG == 4 && STAGE && sizeof(T) == 4), "column groups");
+  constexpr int B = NG * ZC, NT = 32 * B, M = kX4M, N = kX4N, S = x4_stride<ZC>(), BP = B + 1;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   cplx<T>* ytw = reinterpret_cast<cplx<T>*>(smem_dyn);
   cplx<T>* twN = ytw + 512;
@@ -157,13 +163,14 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
     const float rl = ok ? (float)rhoh[zj] : 0.0f, ru = ok ? (float)rhoh[zj + 1] : 0.0f;
     const float idz = (float)(1.0 / g.dz);
     const float sd = (float)sdt;
-    const float* Wl = W + j * S + 2 * t;
+    // NG = 4: group 2 differences w, group 3 b_half, each on its own
+    const float* Wl = ((NG == 4 && f == 3) ? BH : W) + j * S + 2 * t;
     const float* Bl = BH + j * S + 2 * t;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       float2 wl = *reinterpret_cast<const float2*>(Wl + 64 * q);
       float2 wu = *reinterpret_cast<const float2*>(Wl + S + 64 * q);
-      if (STAGE) {  // provisional stage w (integrator.py:483-490)
+      if (STAGE && NG == 3) {  // provisional stage w (integrator.py:483-490)
         const float2 bl = *reinterpret_cast<const float2*>(Bl + 64 * q);
         const float2 bu = *reinterpret_cast<const float2*>(Bl + S + 64 * q);
         wl.x += sd * bl.x;
@@ -210,7 +217,8 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
   //    a half-warp reads 16 k of one pair (distinct banks, BP odd), a warp
   //    stores whole 32-byte runs of two pairs per k.
   const bool st2 = sizeof(T) == 4 && (nz & 1) == 0 &&
-                   ((reinterpret_cast<size_t>(X0) | reinterpret_cast<size_t>(X1)) & 15) == 0;
+                   ((reinterpret_cast<size_t>(X0) | reinterpret_cast<size_t>(X1) |
+                     reinterpret_cast<size_t>(X2)) & 15) == 0;
   constexpr int G = 16 * (ZC / 2);  // threads of one 16-k group
   for (int e = tid; e < ((M + 1 + 15) / 16) * G; e += NT) {
     const int grp16 = e / G, r = e - grp16 * G;
@@ -227,14 +235,20 @@ __global__ void __launch_bounds__(96 * ZC, fx4_min_blocks<T, ZC>()) k_fx4(
       if (two && st2) {
         *reinterpret_cast<float4*>(&X0[o]) = make_float4(x00.x, x00.y, x01.x, x01.y);
         *reinterpret_cast<float4*>(&X1[o]) = make_float4(x10.x, x10.y, x11.x, x11.y);
+        if constexpr (NG == 4) {
+          const cplx<T> x20 = XS[k * BP + 3 * ZC + jj], x21 = XS[k * BP + 3 * ZC + jj + 1];
+          *reinterpret_cast<float4*>(&X2[o]) = make_float4(x20.x, x20.y, x21.x, x21.y);
+        }
         continue;
       }
     }
     X0[o] = x00;
     X1[o] = x10;
+    if constexpr (NG == 4) X2[o] = XS[k * BP + 3 * ZC + jj];
     if (two) {
       X0[o + 1] = x01;
       X1[o + 1] = x11;
+      if constexpr (NG == 4) X2[o + 1] = XS[k * BP + 3 * ZC + jj + 1];
     }
   }
 }
@@ -553,10 +567,11 @@ __global__ void __launch_bounds__(32 * (3 * ZC + 1), ix4_min_blocks<ZC>()) k_ix4
 // ---- y pencils: ny = 1024, one warp per column ----------------------------------
 // The two 512-point halves (even / odd samples) share one exchange block;
 // tables from the W_1024 table twy: ytw, tw1k[k] = W_1024^k (k < 512), w32.
-template <int ZC>
+// NI: spectra loaded per level (2; 3 for the shared-stage form of k_fy4)
+template <int ZC, int NI = 2>
 struct Yr4Size {
-  static constexpr int B = 2 * ZC;  // columns (warps)
-  static constexpr int BP = B + 1;  // row stride of the row tiles (odd)
+  static constexpr int B = 2 * ZC;        // columns (warps)
+  static constexpr int BP = NI * ZC + 1;  // row stride of the row tiles (odd)
   static constexpr size_t tables = (size_t)kX4Tw * sizeof(cplx<float>);
   static constexpr size_t rows = (size_t)kY4N * BP * sizeof(cplx<float>);
   static constexpr size_t ex = (size_t)B * kWEx * sizeof(cplx<float>);
@@ -592,13 +607,16 @@ __device__ __forceinline__ void y4_fft(cplx<T> (&e)[16], cplx<T> (&o)[16], int l
 // k_fy3 (FY_DIV) at ny = 1024: d^ = FFTy(X0) + i ky' FFTy(X1), single
 // precision.  Columns: X0 at ZC levels, X1 at ZC levels.
 // grid = (ceil(nz/ZC), nx/2 + 1), 64 ZC threads.
-template <int ZC>
+// AX: a fast stage from the shared x transforms (k_fx4 with NG = 4): the X0
+// column is in0 + sdt in2, formed in the gather (in2 staged as a third
+// group of ZC columns).
+template <int ZC, bool AX = false>
 __global__ void __launch_bounds__(64 * ZC, yr4_min_blocks<ZC>()) k_fy4(
     GridK g, const cplx<float>* __restrict__ in0, const cplx<float>* __restrict__ in1,
     const double* __restrict__ kyd, const cplx<float>* __restrict__ twy,
-    cplx<float>* __restrict__ out0) {
-  using SZ = Yr4Size<ZC>;
-  constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kY4N;
+    cplx<float>* __restrict__ out0, const cplx<float>* __restrict__ in2, float sdt) {
+  using SZ = Yr4Size<ZC, AX ? 3 : 2>;
+  constexpr int B = SZ::B, BP = SZ::BP, NT = 32 * B, N = kY4N, NL = (AX ? 3 : 2) * ZC;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   cplx<float>* ytw = reinterpret_cast<cplx<float>*>(smem_dyn);
   cplx<float>* tw1k = ytw + 512;
@@ -609,12 +627,13 @@ __global__ void __launch_bounds__(64 * ZC, yr4_min_blocks<ZC>()) k_fy4(
   const int kx = blockIdx.y;
   const int z0 = blockIdx.x * ZC;
   const int tid = threadIdx.x;
-  for (int e = tid; e < N * B; e += NT) {
-    const int y = e / B, b = e - y * B;
+  for (int e = tid; e < N * NL; e += NT) {
+    const int y = e / NL, b = e - y * NL;
     const int f = b / ZC, j = b - f * ZC;
     const int z = z0 + j;
     const bool ok = z < nz;
-    copy_or_zero(&R[y * BP + b], (f == 0 ? in0 : in1) + (kx * ny + y) * nz + (ok ? z : 0), ok);
+    const cplx<float>* src = f == 0 ? in0 : (f == 1 ? in1 : in2);
+    copy_or_zero(&R[y * BP + b], src + (kx * ny + y) * nz + (ok ? z : 0), ok);
   }
   cp_commit();
   x4_tables<float>(ytw, tw1k, w32, twy, tid, NT);
@@ -627,6 +646,11 @@ __global__ void __launch_bounds__(64 * ZC, yr4_min_blocks<ZC>()) k_fy4(
     const int n = 2 * (lane + 32 * q);
     e[q] = R[n * BP + c];
     o[q] = R[(n + 1) * BP + c];
+    if (AX && c < ZC) {  // the stage's X0 = X0 + sdt X2
+      const cplx<float> e2 = R[n * BP + 2 * ZC + c], o2 = R[(n + 1) * BP + 2 * ZC + c];
+      e[q] = mk<float>(fmaf(sdt, e2.x, e[q].x), fmaf(sdt, e2.y, e[q].y));
+      o[q] = mk<float>(fmaf(sdt, o2.x, o[q].x), fmaf(sdt, o2.y, o[q].y));
+    }
   }
   __syncthreads();  // every gather done: the exchange blocks reuse the rows' space
   y4_fft<false>(e, o, lane, ytw, w32, tw1k, ex + c * kWEx);

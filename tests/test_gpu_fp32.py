@@ -153,6 +153,57 @@ def test_fp32_steps_track_fp64(shape):
     assert div["fp32r"] <= div["fp32"]
 
 
+@pytest.mark.parametrize("zc", [2, 4, 8])
+def test_shared_stage_transforms_match_per_stage_transforms(zc):
+    """On 1024 x 1024 grids the FP32 plans can take the three fast stages'
+    forward x transforms from one launch over the anchor state (variant
+    zc4_fxsh): a stage's divergence is linear in its sdt, so its X0 spectrum
+    is X0 + sdt X2 with X2 the transform of the buoyancy's flux divergence,
+    and the stage's y pencils form it.  Every stage is still projected in full.
+    Three FP32-refined steps with the form on and off (every other form the
+    same) agree to FP32 rounding, and both track the FP64 step within the
+    bounds of the FP32 forms."""
+    from oraclev8_b200.solver import RK3Integrator, State
+    from tests.test_oracle_golden import oracle_initial_state
+    c = _vortex_case(1024, 1024, 8)
+    s0, _ = oracle_initial_state(c)
+    base = Base(c["nz"], c["Lz"])
+    cfg = b200_config(c)
+    runs = {}
+    for mode in ("fp64", "per_stage", "shared"):
+        prec = "fp64" if mode == "fp64" else "fp32r"
+        dt = torch.float64 if mode == "fp64" else torch.float32
+        integ = RK3Integrator(cfg, base, precision=prec, autotune=False)
+        if mode != "fp64":
+            # the 1024-point forms on (the defaults of this grid), the shared
+            # transforms on or off
+            integ.plan.set_variants(zc4_fx=4, zc4_fxs=4, zc4_ix=4, zc4_fy=4, zc4_iy=4,
+                                    zc4_fxsh=zc if mode == "shared" else 0)
+            assert integ.plan.variants()["zc4_fxsh"] == (zc if mode == "shared" else 0)
+        s = State(dev(s0.u, dt), dev(s0.v, dt), dev(s0.w, dt), dev(s0.theta_prime, dt),
+                  dev(s0.projection_potential, dt), 0.0)
+        for n in range(3):
+            s, _ = integ.step(s, c["dt"], n)
+        runs[mode] = s
+    fields = ("u", "v", "w", "theta_prime", "projection_potential")
+    ref = runs["fp64"]
+    wind = max(float(ref.u.abs().max()), float(ref.v.abs().max()))
+    for f in ("u", "v"):
+        d = float((getattr(runs["shared"], f).double() - getattr(runs["per_stage"], f).double())
+                  .abs().max())
+        assert d <= 1e-6 * wind, (f, d)
+    bound = dict(u=2e-5, v=2e-5, w=1e-3, theta_prime=2e-5, projection_potential=1e-3)
+    for mode in ("per_stage", "shared"):
+        for f in fields:
+            err = rel(getattr(runs[mode], f), host(getattr(ref, f)))
+            print(mode, f, f"{err:.3e}")
+            assert err <= bound[f], (mode, f, err)
+    for f in ("w", "theta_prime", "projection_potential"):
+        e_sh = rel(getattr(runs["shared"], f), host(getattr(ref, f)))
+        e_ps = rel(getattr(runs["per_stage"], f), host(getattr(ref, f)))
+        assert e_sh <= 2.0 * e_ps + 1e-6, (f, e_sh, e_ps)
+
+
 def test_refinement_controls():
     from oraclev8_b200._plan import Plan, PlanSpec
     p64, p32 = _plans(16, 12, 8, 16e4, 12e4, 16e3)
