@@ -71,3 +71,33 @@ def test_new_entry_points_validate_before_cuda():
     assert rc == _lib.OB_ERR_ARG and b"workspace" in lib.oracle_b200_last_error()
     assert lib.oracle_b200_vdiag_centroid(None, 0, 1, 0, 1, None, None) == _lib.OB_ERR_ARG
     assert lib.oracle_b200_vdiag_destroy(None) == _lib.OB_OK
+
+
+def header_defines():
+    """Integer #defines of the public header, by name."""
+    out = {}
+    for h in (ROOT / "include").glob("*.h"):
+        for name, val in re.findall(r"^#define\s+(OB_\w+)\s+(-?\d+)", h.read_text(), flags=re.M):
+            out[name] = int(val)
+    return out
+
+
+def test_bindings_agree_with_the_header_constants():
+    """The Python tables that index the library's arrays (kernel variants,
+    profile classes) and the constants it passes follow the header's
+    numbering, so a variant or class added on one side only fails here."""
+    from oraclev8_b200 import _lib
+    d = header_defines()
+    var = sorted((v, k[len("OB_VAR_"):].lower()) for k, v in d.items()
+                 if k.startswith("OB_VAR_") and k != "OB_VAR_COUNT")
+    assert [v for v, _ in var] == list(range(d["OB_VAR_COUNT"]))
+    assert tuple(n for _, n in var) == _lib.VARIANTS
+    prof = sorted((v, k[len("OB_PROF_"):].lower()) for k, v in d.items()
+                  if k.startswith("OB_PROF_") and k != "OB_PROF_CLASSES")
+    assert [v for v, _ in prof] == list(range(d["OB_PROF_CLASSES"]))
+    assert tuple(n for _, n in prof) == _lib.PROF_CLASSES
+    for name in ("OB_OK", "OB_ERR_ARG", "OB_ERR_CUDA", "OB_ERR_NONFINITE", "OB_ERR_UNSUPPORTED",
+                 "OB_PREC_F64", "OB_PREC_F32", "OB_ADV_CENTERED2", "OB_ADV_UPWIND5H",
+                 "OB_TEND_ADVECTION", "OB_TEND_CORIOLIS", "OB_TEND_DAMPING", "OB_TEND_HEATING",
+                 "OB_TEND_DRAG", "OB_TEND_SPONGE", "OB_TEND_DIFFUSION", "OB_TEND_COOLING"):
+        assert getattr(_lib, name) == d[name], name

@@ -269,3 +269,27 @@ def test_backend_xp_takes_the_harness_spellings():
     assert float(xp.sqrt(xp.mean(t ** 2))) == pytest.approx(float(np.sqrt(np.mean(a ** 2))),
                                                             rel=1e-14)
     assert xp.zeros_like(t).shape == t.shape and isinstance(t, xp.Tensor)
+
+
+def test_bench_byte_model_of_the_shared_stage_transforms():
+    """bench.py's per-launch algorithmic bytes: with the fast stages' forward x
+    transforms shared, a step's forward x and y launches move the bytes of two
+    stage x launches less, plus one more spectrum written by the shared launch
+    and one more read by each stage's y launch; every other class is as it
+    was.  The inverse x class counts the potential only where the step keeps
+    it (two of five launches)."""
+    import bench
+    w = bench.WORKLOADS["config2"]
+    S = 4
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    n, nw, ns = nx * ny * nz, nx * ny * (nz + 1), (nx // 2 + 1) * ny * nz
+    per = bench.kernel_bytes(w, S)
+    sh = bench.kernel_bytes(w, S, shared_stages=True)
+    step = lambda kb, nfx: kb["fx"] * nfx + kb["fy"] * 5
+    stage_fx = (2 * n + 2 * nw) * S + 2 * ns * 2 * S
+    spectrum = ns * 2 * S
+    assert math.isclose(step(per, 5) - step(sh, 3), 2 * stage_fx - 4 * spectrum, rel_tol=1e-12)
+    for c in ("thomas", "iy", "ix", "slow", "diag"):
+        assert sh[c] == per[c]
+    ix_all = 2 * spectrum * 5 + 2 * 2 * (2 * n + nw) * S + 3 * ((2 * n + 2 * nw) + (2 * n + nw)) * S
+    assert math.isclose(per["ix"] * 5, ix_all + 2 * n * S, rel_tol=1e-12)
