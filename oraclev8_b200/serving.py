@@ -169,7 +169,9 @@ def footprint_bytes(req: RunRequest) -> int:
     half-spectrum buffers, 5 anchor and 4 stage fields, 2 temporaries and the
     half-level buoyancy; plus two FP64 spectra for the FP32-refined
     correction; the production physics adds the damper's two tendency fields
-    and the biharmonic's two inner Laplacians), in the state dtype."""
+    and the biharmonic's two inner Laplacians; single-precision 1024 x 1024
+    runs with fast stages add the three spectra of the shared stage
+    transforms), in the state dtype."""
     S = 8 if req.precision == "fp64" else 4
     n = req.cells
     ns = (req.n // 2 + 1) * req.n * req.nz
@@ -178,6 +180,8 @@ def footprint_bytes(req: RunRequest) -> int:
         b += 4 * n * S
     if req.precision != "fp64":
         b += 2 * ns * 16
+        if req.n == 1024 and req.physics == "lh82":  # buoyancy: the fast stages
+            b += 3 * ns * 2 * S
     return int(b * 1.05) + (8 << 20)
 
 

@@ -293,3 +293,38 @@ def test_bench_byte_model_of_the_shared_stage_transforms():
         assert sh[c] == per[c]
     ix_all = 2 * spectrum * 5 + 2 * 2 * (2 * n + nw) * S + 3 * ((2 * n + 2 * nw) + (2 * n + nw)) * S
     assert math.isclose(per["ix"] * 5, ix_all + 2 * n * S, rel_tol=1e-12)
+
+
+def test_serving_footprint_counts_every_plan_buffer():
+    """The serving loop admits a run by footprint_bytes: its state plus the
+    buffers its plan allocates.  A single-precision 1024 x 1024 run with the
+    fast stages also holds the three spectra of the shared stage transforms;
+    other sizes, FP64 runs and the production physics (no fast stages) do
+    not."""
+    from oraclev8_b200.serving import RunRequest, footprint_bytes
+
+    def req(n, nz, precision, physics):
+        return RunRequest(rid=0, n=n, nz=nz, vmax=50.0, rmax=40e3, b=1.6, lat_deg=20.0,
+                          hours=1.0, precision=precision, physics=physics)
+
+    def base(n, nz, precision, physics):
+        S = 8 if precision == "fp64" else 4
+        cells, ns = n * n * nz, (n // 2 + 1) * n * nz
+        b = S * 17 * cells + 3 * ns * 2 * S
+        if physics == "production":
+            b += 4 * cells * S
+        if precision != "fp64":
+            b += 2 * ns * 16
+        return b
+
+    for n, nz in ((96, 32), (384, 64), (1024, 80)):
+        for precision in ("fp64", "fp32r"):
+            for physics in ("lh82", "production"):
+                b = base(n, nz, precision, physics)
+                if n == 1024 and precision == "fp32r" and physics == "lh82":
+                    b += 3 * (n // 2 + 1) * n * nz * 8
+                assert footprint_bytes(req(n, nz, precision, physics)) == int(b * 1.05) + (8 << 20)
+    # the shared transforms are 1.0 GB of the 1024 x 1024 x 80 FP32 run's footprint
+    extra = (footprint_bytes(req(1024, 80, "fp32r", "lh82"))
+             - int(base(1024, 80, "fp32r", "lh82") * 1.05) - (8 << 20))
+    assert 1.05e9 < extra < 1.07e9
