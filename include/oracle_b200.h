@@ -477,6 +477,12 @@ int oracle_b200_poisson_solve_noalloc(const OracleGridDesc *grid, const double *
                                       const void *d, void *phi, void *stream);
 
 const char *oracle_b200_last_error(void);
+/* The ABI version of the library (no counterpart in the reference): raised
+ * whenever a constant, an array length or a struct of this header changes, so
+ * that bindings can refuse a library built from another header.  2: the
+ * shared stage transforms (OB_VAR_ZC4_FXSH, OB_VAR_COUNT 23) and the
+ * long-wave Thomas profile class (OB_PROF_THOMAS_LW, OB_PROF_CLASSES 10). */
+#define OB_ABI_VERSION 2
 int oracle_b200_version(void);
 
 #ifdef __cplusplus

@@ -47,6 +47,7 @@ VARIANTS = ("zc2_fx", "zc2_fxs", "zc2_ix", "zc2_fy", "zc2_iy", "zc3_fx", "zc3_fx
             "zc3_fxd", "zc3_fy", "zc3_fyd", "zc4_fx", "zc4_fxs", "zc4_ix", "zc4_fxd", "zc4_fy",
             "zc4_iy", "slow_xw", "thomas_fast", "rzc2_fx", "rzc2_fy", "zc4_fyd", "zc4_fxsh")
 OB_TUNE_FORCE = 1
+ABI_VERSION = 2  # OB_ABI_VERSION of the header these tables follow
 PROF_CLASSES = ("fx", "fy", "thomas", "iy", "ix", "slow", "diag", "other", "refine",
                 "thomas_lw")
 
@@ -164,6 +165,10 @@ def load(path: Path | None = None):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
+    v = lib.oracle_b200_version()
+    if v != ABI_VERSION:
+        raise RuntimeError(f"{p.name} has ABI version {v}, these bindings need {ABI_VERSION}: "
+                           "rebuild it with `python -m oraclev8_b200.build`")
     _lib = lib
     return lib
 

@@ -2601,7 +2601,7 @@ int oracle_b200_vdiag_centroid(OracleVortexDiag* d, int i0, int i1, int j0, int 
 
 const char* oracle_b200_last_error(void) { return g_err.c_str(); }
 
-int oracle_b200_version(void) { return 1; }
+int oracle_b200_version(void) { return OB_ABI_VERSION; }
 
 size_t oracle_b200_plan_scratch_bytes(const OraclePlan* p) { return p ? p->scratch_bytes : 0; }
 

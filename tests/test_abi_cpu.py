@@ -31,7 +31,7 @@ def test_library_exports_header_symbols():
 def test_version_and_error_string_without_gpu():
     from oraclev8_b200 import _lib
     lib = _lib.load()
-    assert lib.oracle_b200_version() >= 1
+    assert lib.oracle_b200_version() == _lib.ABI_VERSION
     # argument validation happens before any CUDA call
     g = _lib.GridDesc(7, 8, 4, 1.0, 1.0, 1.0, 0)
     c = _lib.ComponentDesc()
@@ -96,6 +96,7 @@ def test_bindings_agree_with_the_header_constants():
                   if k.startswith("OB_PROF_") and k != "OB_PROF_CLASSES")
     assert [v for v, _ in prof] == list(range(d["OB_PROF_CLASSES"]))
     assert tuple(n for _, n in prof) == _lib.PROF_CLASSES
+    assert d["OB_ABI_VERSION"] == _lib.ABI_VERSION
     for name in ("OB_OK", "OB_ERR_ARG", "OB_ERR_CUDA", "OB_ERR_NONFINITE", "OB_ERR_UNSUPPORTED",
                  "OB_PREC_F64", "OB_PREC_F32", "OB_ADV_CENTERED2", "OB_ADV_UPWIND5H",
                  "OB_TEND_ADVECTION", "OB_TEND_CORIOLIS", "OB_TEND_DAMPING", "OB_TEND_HEATING",
