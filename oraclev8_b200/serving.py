@@ -393,16 +393,12 @@ class ServingEngine:
                 now = time.perf_counter() - t0
                 while pending and (not self.realtime or pending[0].arrival_s <= now):
                     queue.append(pending.pop(0))
-                i = 0
-                while (i < len(queue) and len(active) + preparing < self.max_active
-                       and preparing < self.prepare_ahead):
-                    fb = footprint_bytes(queue[i])
-                    if used + fb <= self.budget or not (active or preparing):
-                        todo.put((queue.pop(i), time.perf_counter() - t0))
-                        used += fb
-                        preparing += 1
-                    else:
-                        i += 1
+                admitted, used = admit_from_queue(queue, used, self.budget, len(active),
+                                                  preparing, self.max_active,
+                                                  self.prepare_ahead)
+                for req in admitted:
+                    todo.put((req, time.perf_counter() - t0))
+                    preparing += 1
                 progressed = False
                 while True:
                     try:
@@ -430,14 +426,10 @@ class ServingEngine:
                     if not a.blown and a.left > 0 and float(a.flag[14]) > 0.0:
                         a.blown = True
                         a.left = 0
-                busy = sum(a.req.cells for a in active if a.events)
-                for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
-                    if a.left > 0 and (a.events or busy < self.inflight_cells):
-                        if not a.events:
-                            busy += a.req.cells
-                        while a.left > 0 and len(a.events) < self.depth:
-                            self._launch(a)
-                            progressed = True
+                for a in runs_to_feed(active, self.inflight_cells):
+                    while a.left > 0 and len(a.events) < self.depth:
+                        self._launch(a)
+                        progressed = True
                 for a in list(active):
                     if a.left == 0 and not a.events:
                         done.append(self._retire(a, time.perf_counter() - t0))
@@ -457,6 +449,46 @@ class ServingEngine:
             th.join()
             torch.cuda.synchronize()
         return done
+
+
+def admit_from_queue(queue: list, used: int, budget: float, n_active: int, preparing: int,
+                     max_active: int, prepare_ahead: int, size=footprint_bytes):
+    """Admission of queued requests (FIFO with backfill): in queue order, each
+    request that fits the HBM budget beside the admitted runs is taken; one
+    that does not fit is skipped, so a later, smaller one can take the room.
+    A request larger than the whole budget is admitted alone, when nothing
+    else is resident or being set up.  At most `max_active` runs resident or
+    in set-up, at most `prepare_ahead` in set-up.  Removes the admitted
+    requests from `queue`; returns them in admission order and the new
+    number of bytes in use."""
+    admitted = []
+    i = 0
+    while i < len(queue) and n_active + preparing < max_active and preparing < prepare_ahead:
+        fb = size(queue[i])
+        if used + fb <= budget or not (n_active or preparing):
+            admitted.append(queue.pop(i))
+            used += fb
+            preparing += 1
+        else:
+            i += 1
+    return admitted, used
+
+
+def runs_to_feed(active: list, inflight_cells: float) -> list:
+    """The resident runs that get work this pass: the least remaining work
+    (steps left x cells) first, ties by request id.  A run with work in flight
+    keeps being fed; an idle one starts only while the cells of the runs with
+    work in flight stay under `inflight_cells` (enough concurrent runs to fill
+    the GPU without sharing it among every resident run).  Finished runs get
+    nothing."""
+    busy = sum(a.req.cells for a in active if a.events)
+    out = []
+    for a in sorted(active, key=lambda x: (x.left * x.req.cells, x.req.rid)):
+        if a.left > 0 and (a.events or busy < inflight_cells):
+            if not a.events:
+                busy += a.req.cells
+            out.append(a)
+    return out
 
 
 def shard_requests(requests: "list[RunRequest]", rank: int, world: int

@@ -328,3 +328,54 @@ def test_serving_footprint_counts_every_plan_buffer():
     extra = (footprint_bytes(req(1024, 80, "fp32r", "lh82"))
              - int(base(1024, 80, "fp32r", "lh82") * 1.05) - (8 << 20))
     assert 1.05e9 < extra < 1.07e9
+
+
+def test_serving_admission_is_fifo_with_backfill_under_the_budget():
+    """admit_from_queue (the serving loop's admission): queue order, a request
+    that does not fit is skipped and a later smaller one takes the room, an
+    oversized request runs alone, and the resident / set-up caps hold."""
+    from types import SimpleNamespace as R
+    from oraclev8_b200.serving import admit_from_queue
+    size = lambda r: r.b
+    q = [R(rid=0, b=60), R(rid=1, b=50), R(rid=2, b=30), R(rid=3, b=10)]
+    adm, used = admit_from_queue(q, 0, 100, 0, 0, 8, 8, size)
+    assert [r.rid for r in adm] == [0, 2, 3] and used == 100 and [r.rid for r in q] == [1]
+    # the skipped request is admitted once its room is free
+    adm, used = admit_from_queue(q, used - 60, 100, 2, 0, 8, 8, size)
+    assert [r.rid for r in adm] == [1] and used == 90 and not q
+    # a request larger than the budget: alone, and only when nothing is resident
+    q = [R(rid=4, b=500), R(rid=5, b=10)]
+    adm, used = admit_from_queue(q, 10, 100, 1, 0, 8, 8, size)
+    assert [r.rid for r in adm] == [5] and used == 20
+    adm, used = admit_from_queue(q, 0, 100, 0, 0, 8, 8, size)
+    assert [r.rid for r in adm] == [4] and used == 500 and not q
+    # caps: runs resident or in set-up, runs in set-up
+    q = [R(rid=i, b=1) for i in range(10)]
+    adm, _ = admit_from_queue(q, 0, 100, 3, 1, 6, 8, size)
+    assert [r.rid for r in adm] == [0, 1]
+    adm, _ = admit_from_queue(q, 0, 100, 0, 2, 100, 4, size)
+    assert [r.rid for r in adm] == [2, 3]
+
+
+def test_serving_feeds_least_remaining_work_first_under_the_inflight_cap():
+    """runs_to_feed: shortest remaining work first; runs already in flight keep
+    their work; idle runs start only while the in-flight cells stay under the
+    cap; finished runs get nothing."""
+    from types import SimpleNamespace as R
+    from oraclev8_b200.serving import runs_to_feed
+    run = lambda rid, left, cells, busy=False: R(req=R(rid=rid, cells=cells), left=left,
+                                                  events=[object()] if busy else [])
+    a = run(0, 10, 100)            # 1000 cell-steps left
+    b = run(1, 2, 100)             # 200
+    c = run(2, 5, 100, busy=True)  # 500, in flight
+    d = run(3, 0, 100)             # finished
+    e = run(4, 2, 100)             # 200, ties with b: rid order
+    assert [x.req.rid for x in runs_to_feed([a, b, c, d, e], 1e9)] == [1, 4, 2, 0]
+    # cap of 250 cells, c's 100 in flight: b starts (100 < 250, then 200 in
+    # flight), e starts (200 < 250, then 300), a does not (300 >= 250)
+    fed = [x.req.rid for x in runs_to_feed([a, b, c, d, e], 250)]
+    assert fed == [1, 4, 2]
+    fed = [x.req.rid for x in runs_to_feed([a, b, c, d, e], 150)]
+    assert fed == [1, 2]
+    # nothing idle starts once the runs in flight fill the cap
+    assert [x.req.rid for x in runs_to_feed([a, c], 100)] == [2]
