@@ -379,3 +379,71 @@ def test_serving_feeds_least_remaining_work_first_under_the_inflight_cap():
     assert fed == [1, 2]
     # nothing idle starts once the runs in flight fill the cap
     assert [x.req.rid for x in runs_to_feed([a, c], 100)] == [2]
+
+
+def test_serving_loop_on_a_fake_device(monkeypatch):
+    """The serving loop itself (ServingEngine.run) with the device replaced:
+    runs are set up, fed in chunks, retired and backfilled; the resident bytes
+    never exceed the budget; a run whose blow-up flag is raised gets no
+    further chunks and retires with an error record; every request ends with a
+    record."""
+    import threading
+    import torch
+    from oraclev8_b200 import serving as S
+
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 0)
+    monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a: None)
+
+    class Event:
+        def __init__(self):
+            self.polls = 0
+
+        def query(self):  # completes on its second poll
+            self.polls += 1
+            return self.polls > 1
+
+    class Fake(S.ServingEngine):
+        def __init__(self, blow, **kw):
+            super().__init__(**kw)
+            self.blow, self.lock = set(blow), threading.Lock()
+            self.resident = self.peak = 0
+
+        def _prepare(self, req):
+            with self.lock:
+                self.resident += S.footprint_bytes(req)
+                self.peak = max(self.peak, self.resident)
+            rec = S.RunRecord(req.rid, req.n, req.nz, req.precision, req.nsteps, req.cells,
+                              req.arrival_s)
+            return S._Active(req, rec, None, None, None, {}, req.nsteps,
+                             bytes=S.footprint_bytes(req), flag=[0.0] * 16)
+
+        def _launch(self, a):
+            k = min(self.chunk, a.left)
+            a.events.append(Event())
+            a.left -= k
+            a.launched += k
+            if a.req.rid in self.blow:
+                a.flag[14] = 1.0  # the diagnostics block's blow-up slot
+
+        def _retire(self, a, now):
+            with self.lock:
+                self.resident -= a.bytes
+            a.rec.done_s = now
+            if a.blown:
+                a.rec.error = "blown up"
+            return a.rec
+
+    reqs = [S.RunRequest(rid=i, n=n, nz=nz, vmax=40.0, rmax=40e3, b=1.5, lat_deg=20.0,
+                         hours=1.0, precision="fp32r")
+            for i, (n, nz) in enumerate([(96, 32), (384, 64), (128, 48), (256, 32),
+                                         (192, 64), (96, 48), (384, 32), (128, 32)])]
+    budget = 2.2 * max(S.footprint_bytes(r) for r in reqs)
+    eng = Fake(blow={3}, hbm_budget=budget, chunk=8, depth=2, realtime=False,
+               max_active=4, prepare_ahead=2, inflight_cells=2e6)
+    recs = eng.run(reqs)
+    assert sorted(r.rid for r in recs) == list(range(len(reqs)))
+    assert all(r.done_s == r.done_s for r in recs)  # every run retired (not NaN)
+    assert 0 < eng.peak <= budget and eng.resident == 0
+    by = {r.rid: r for r in recs}
+    assert by[3].error == "blown up" and all(by[i].error is None for i in by if i != 3)
